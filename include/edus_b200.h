@@ -1,0 +1,244 @@
+/*
+ * edus_b200.h — C ABI of the B200-native k-space density-matrix propagator.
+ *
+ * Plain C types only (pointers, sizes, doubles). Complex numbers are passed
+ * as interleaved (re, im) double pairs. Every function returns 0 on success
+ * or a negative EDUS_E* code; edus_strerror() turns a code into text and
+ * edus_last_error() gives the message of the last failure on this thread.
+ *
+ * Reference seams replaced (anpicon/EDUS, paths relative to its root):
+ *   input.txt reader ............ headers/ReadInput.h:332-815 (Read_Input)
+ *   k grid / b shells ........... headers/InitParameters.h:1-40, headers/CalculateWeigths.h:1-226
+ *   k partition ................. headers/Organize_kspaceMPI.h:242-301 (one device-resident grid here)
+ *   H, U, D tabulation .......... Source_Main/save_HUD.cpp:19-53, headers/HUD.h:5-20
+ *   RHS ......................... headers/RungeKutta.h:7-297 (get_derivative_Df)
+ *   stage updates ............... headers/RungeKutta.h:301-355 (Runge_Kutta_Ad / Runge_Kutta_Ac)
+ *   RK4 / AB / Taylor drivers ... Source_Main/RungeKutta.cpp, Source_Main/Linear_Multistep_ODE_solvers.cpp,
+ *                                 Source_Main/Taylor_DE_solver_deriv_Polynom.cpp, headers/ODE_solver.h
+ *   time loops .................. Source_Main/const_dt_evolution.cpp, Source_Main/dyn_dt_evolution.cpp
+ *   Coulomb mean field .......... headers/Coulomb.h:273-541, Source_Main/Fourier_Coulomb.cpp:505-622
+ *   observables ................. headers/Observables_MPI.h:134-140,217-484,559-598,668-775
+ */
+#ifndef EDUS_B200_H
+#define EDUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EDUS_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- errors */
+enum {
+  EDUS_OK = 0,
+  EDUS_EINVAL = -1,       /* bad argument / inconsistent problem */
+  EDUS_ENOMEM = -2,       /* host or HBM allocation failed, or HBM budget exceeded */
+  EDUS_ECUDA = -3,        /* CUDA runtime error */
+  EDUS_ENONFINITE = -4,   /* health check: non-finite rho */
+  EDUS_ETRACE = -5,       /* health check: trace drift above tolerance */
+  EDUS_ETIMEOUT = -6,     /* bounded device wait ran out */
+  EDUS_ECANCELLED = -7,   /* request cancelled */
+  EDUS_EIO = -8,          /* file could not be read or written */
+  EDUS_EPARSE = -9,       /* input.txt grammar error (the reference exits(1) there) */
+  EDUS_EUNSUPPORTED = -10,/* option the reference has that is not built here */
+  EDUS_ENOTREADY = -11    /* result not available yet (serving poll) */
+};
+
+/* ---------------------------------------------------------------- enums */
+enum { EDUS_MODE_TB = 1, EDUS_MODE_WANNIER = 2 };
+enum { EDUS_SOLVER_RK4 = 0, EDUS_SOLVER_AB = 1, EDUS_SOLVER_TAYLOR = 2 };
+enum { EDUS_ENV_NONE = 0, EDUS_ENV_SIN2 = 1, EDUS_ENV_GAUSS = 2, EDUS_ENV_PW = 3 };
+enum { EDUS_PREC_FP64 = 0, EDUS_PREC_MIXED = 1 };
+
+#define EDUS_MAX_PUMPS 8
+#define EDUS_MAX_HOPPING 8
+#define EDUS_MAX_BANDS 16
+#define EDUS_STRLEN 256
+
+/* One laser pulse with every derived quantity resolved (headers/Laser.h:1-51).
+ * Polarisation vectors are Cartesian and already Gram–Schmidt-orthogonalised
+ * as Laser::set_pol does (headers/Laser.h:82-106). */
+typedef struct {
+  int32_t envelope_kind;  /* EDUS_ENV_* (Laser::gaussian / sin2 / PW) */
+  int32_t envelope_only;  /* Laser::envelope: no carrier oscillation (probe) */
+  double wl;              /* angular frequency, a.u. */
+  double period;          /* 2 pi / wl */
+  double lambdanm;
+  double intensity;       /* W/cm^2 */
+  double A0, E0;          /* a.u.; A0 = sqrt(I / 3.51e16) / wl, E0 = A0 wl */
+  double t0, tf;          /* a.u. */
+  double ncycle, sigma;   /* sin2 cycles / gaussian sigma (a.u.) */
+  double w1, w2;          /* pseudo plane wave window */
+  double phase;           /* carrier envelope phase */
+  double pol1[3], pol2[3];
+} edus_laser;
+
+/* Everything input.txt says, resolved to atomic units (the reference's
+ * globals after Read_Input + BZ_parameters). */
+typedef struct {
+  char ref_coord[EDUS_STRLEN];   /* first token; Wannier file stem <ref_coord>_tb.dat */
+  int32_t mode;                  /* EDUS_MODE_* */
+  char tb_type[64];              /* TightBinding::_name */
+  double hopping[EDUS_MAX_HOPPING];
+  int32_t n_hopping;
+  double a[3][3];                /* direct lattice rows, a.u. */
+  double b[3][3];                /* reciprocal lattice rows, a.u. */
+  int32_t nk[3];                 /* Monkhorst–Pack grid */
+  int32_t nb[3];                 /* core, valence, conduction band counts */
+  double conduction_shift;       /* scissor, a.u. (bands{conduction_shift}) */
+  double fermi_energy;
+  /* tdse */
+  double dt, t_fin;              /* a.u. */
+  int32_t solver;                /* EDUS_SOLVER_* */
+  int32_t order;                 /* Adams–Bashforth / Taylor order (SolverOrder) */
+  int32_t dynamical_dt;
+  double eps_step_abs;
+  int32_t ab_rk4_startup;        /* extension: RK4 start-up for AB (reference: 0, zero history) */
+  double gap_correction;
+  /* lasers */
+  int32_t n_pumps;
+  edus_laser pump[EDUS_MAX_PUMPS];
+  edus_laser probe;
+  double delay;
+  /* decoherence (headers/InitParameters.h:203-224) */
+  double T1, T2, Tch;
+  /* observables */
+  int32_t current, tabs, it_resolution;
+  int32_t print_population;
+  double print_start, print_end, print_step;
+  /* Coulomb */
+  int32_t coulomb;
+  int32_t ncut;
+  double qTF, r0, epsilon_static, G_distance;
+  int32_t rytova_keldysh, diag_basis, read_from_files, print_band_dispersion;
+  char coulomb_label[EDUS_STRLEN];
+  int32_t sample_110;            /* sample in xy ("110") instead of yz ("011") */
+  int32_t vectorization;
+  /* execution options (not in the reference) */
+  int32_t precision;             /* EDUS_PREC_* */
+} edus_params;
+
+/* Observables at one output instant (headers/Observables_MPI.h). */
+typedef struct {
+  double t;                      /* a.u. */
+  double EF_pump[3];             /* field printed to EF.txt */
+  double EF_probe[3];            /* field printed to TransientAbs.txt */
+  double J1[6];                  /* complex J1 x,y,z (re, im), Current1 */
+  double J2[3];                  /* -2 Im(...), Current2 */
+  double pop[EDUS_MAX_BANDS];    /* Losses.txt columns */
+  double tabs[6];                /* complex TAbs / nktot */
+  double trace_dev;              /* sum of populations - (Nch + Nv) */
+  double p_cond_max;             /* P_cond_max_loc */
+  double p_min;                  /* Coulomb_set.P_min */
+  double n_cond;
+  double dt;                     /* step used after this instant (adaptive dt) */
+} edus_obs;
+
+/* ------------------------------------------------------- input.txt layer */
+/* Parse input.txt (headers/ReadInput.h:332-815 grammar, BZ_parameters laser
+ * resolution headers/InitParameters.h:1-11). */
+int edus_parse_input(const char* path, edus_params* out);
+int edus_params_default(edus_params* out);   /* Source_Main/variables.cpp defaults */
+
+/* ------------------------------------------------------- problem (host) */
+typedef struct edus_problem edus_problem;
+
+typedef struct {
+  int32_t ncv, nch, nv, nc;
+  int32_t nk;                /* k points */
+  int32_t n1, n2;            /* in-plane grid (rows, columns) */
+  int32_t nshell, nnb;       /* b-vector shells, total neighbours per k */
+  int32_t nrpts;             /* Wannier R vectors (0 for TB) */
+  int32_t n_diss;            /* non-zero dissipation entries */
+  int32_t nsteps;            /* itfi + 1 for constant dt */
+  int32_t nprint;            /* output instants for constant dt */
+  double t_start;            /* -0.21 fs in a.u. */
+  double det_a, jacobian;
+  double dk[3];
+} edus_problem_info;
+
+/* Build the problem on the host: grid, shells, neighbour table, model tables
+ * (H, U, D on the grid, GradientEnergy), dissipation tensor, initial state,
+ * Coulomb coefficient files. workdir holds <ref>_tb.dat and Output/Coulomb/. */
+int edus_problem_create(const edus_params* p, const char* workdir, edus_problem** out);
+int edus_problem_info_get(const edus_problem* pb, edus_problem_info* out);
+/* Copy a named host array out (names: "kpt","H","U","D","GE","P0","nbr",
+ * "weights","bvec","T","wq_A","wq_B","wq_C","wq_D","screen","vhartree",
+ * "HR","rR","Rvec"); nbytes must match exactly. */
+int edus_problem_get(const edus_problem* pb, const char* name, void* dst, size_t nbytes);
+void edus_problem_free(edus_problem* pb);
+
+/* ------------------------------------------------------- device context */
+typedef struct edus_ctx edus_ctx;
+
+typedef struct {
+  int32_t device;            /* CUDA device ordinal */
+  int32_t precision;         /* EDUS_PREC_*; overrides params.precision if >= 0 */
+  int32_t use_graphs;        /* capture step chunks in CUDA graphs */
+  int32_t health_checks;     /* device-side non-finite / trace checks */
+  double trace_tol;
+  int64_t hbm_budget_bytes;  /* 0 = unlimited */
+} edus_options;
+
+int edus_options_default(edus_options* o);
+/* Upload the problem and allocate all device state. */
+int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out);
+void edus_destroy(edus_ctx* ctx);
+
+/* State in the reference layout P[k][i][j], interleaved complex128. */
+int edus_set_state(edus_ctx* ctx, const double* rho);
+int edus_get_state(edus_ctx* ctx, double* rho);
+
+/* Advance nsteps of the configured integrator from the current (it, t, dt).
+ * Reproduces one iteration of the reference time loop per step
+ * (Source_Main/const_dt_evolution.cpp:10-55, dyn_dt_evolution.cpp:28-183),
+ * including the output instants every it_resolution steps, which are
+ * appended to the context's observable log. */
+int edus_step(edus_ctx* ctx, int32_t nsteps);
+/* Run the whole time loop (itfi+1 steps for constant dt). */
+int edus_run(edus_ctx* ctx);
+/* Clock of the loop: iteration index, time (a.u.), current dt. */
+int edus_clock(edus_ctx* ctx, int32_t* it, double* t, double* dt);
+/* Number of logged output instants and a copy of them. */
+int edus_obs_count(edus_ctx* ctx, int32_t* n);
+int edus_obs_get(edus_ctx* ctx, int32_t first, int32_t count, edus_obs* out);
+/* Observables of the current state (does not append to the log). */
+int edus_observables(edus_ctx* ctx, edus_obs* out);
+/* Write Output/{EF,J1,J2,Losses,TransientAbs}.txt in the reference's format. */
+int edus_write_outputs(edus_ctx* ctx, const char* outdir);
+/* Device time (ms, CUDA events) of the last edus_step/edus_run call and the
+ * number of kernel launches it issued. */
+int edus_last_timing(edus_ctx* ctx, double* ms, int64_t* launches);
+
+/* --------------------------------------------- ODE_solver-level mirror
+ * Slots name device arrays of the state shape: 0 = P0, 1 = P1, 2 = P2,
+ * 3 = Pv. These replace the reference's per-thread calls one for one. */
+enum { EDUS_SLOT_P0 = 0, EDUS_SLOT_P1 = 1, EDUS_SLOT_P2 = 2, EDUS_SLOT_PV = 3 };
+/* get_derivative_Df (headers/RungeKutta.h:7-297): Pv = RHS(P_slot).
+ * EF = {pump x,y,z, probe x,y,z} as the reference's EF[0], EF[1]. */
+int edus_get_derivative(edus_ctx* ctx, int32_t p_slot, const double EF[6], double wx2, int32_t e_non0);
+/* Runge_Kutta_Ad (headers/RungeKutta.h:301-328): P_dst = P_src + dt * Pv. */
+int edus_runge_kutta_ad(edus_ctx* ctx, int32_t src, int32_t dst, double dt);
+/* Runge_Kutta_Ac (headers/RungeKutta.h:331-355): P_dst += dt * Pv. */
+int edus_runge_kutta_ac(edus_ctx* ctx, int32_t dst, double dt);
+/* Copy one slot to another (host-side bookkeeping the reference does by assignment). */
+int edus_slot_copy(edus_ctx* ctx, int32_t src, int32_t dst);
+int edus_slot_set(edus_ctx* ctx, int32_t slot, const double* rho);
+int edus_slot_get(edus_ctx* ctx, int32_t slot, double* rho);
+/* Coulomb mean field of slot P: X(k) as the reference adds it to H
+ * (headers/Coulomb.h:273-541 + headers/RungeKutta.h:69-138): writes
+ * Hk_renorm[k][n][n] (interleaved) to hk_out. */
+int edus_coulomb_hk(edus_ctx* ctx, int32_t p_slot, double* hk_out);
+
+/* ------------------------------------------------------- strings */
+const char* edus_strerror(int code);
+const char* edus_last_error(void);
+int edus_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDUS_B200_H */
