@@ -1,0 +1,1014 @@
+// capi.cu — the C ABI: problem objects, device context, time loop, outputs.
+//
+// The time loop reproduces Source_Main/const_dt_evolution.cpp:1-54 and
+// Source_Main/dyn_dt_evolution.cpp:1-183 of the reference: output instants
+// before the step at it % it_resolution == 0, RK4 with the stage-3 field reuse
+// and the E_non0 bookkeeping of Source_Main/RungeKutta.cpp:151-163, AB with a
+// zero derivative history (headers/ODE_solver.h:40-62), Taylor with its tau
+// matrix (Source_Main/Taylor_DE_solver_deriv_Polynom.cpp:100-123), adaptive dt.
+// All kernel launches go to one stream and nothing synchronises with the host
+// inside a constant-dt run; the observable log stays on the device until read.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "cuda/kernels.hpp"
+#include "host/problem.hpp"
+
+struct edus_problem {
+  edus::Problem P;
+};
+
+namespace edus {
+namespace {
+
+#define CK(x)                                                                             \
+  do {                                                                                    \
+    cudaError_t e_ = (x);                                                                 \
+    if (e_ != cudaSuccess) return fail(EDUS_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+  } while (0)
+
+// headers/Laser.h:56-76,128-144
+void laser_E(const edus_laser& L, double t, double E[3]) {
+  double env = 0.;
+  if (L.envelope_kind == EDUS_ENV_GAUSS) {
+    double d = t - L.t0;
+    env = (d * d < 40 * L.sigma * L.sigma) ? L.E0 * std::exp(-d * d / (2 * L.sigma * L.sigma)) : 0.;
+  } else if (L.envelope_kind == EDUS_ENV_SIN2) {
+    if (t >= L.t0 && t <= L.tf) {
+      double s = std::sin(kPi * (t - L.t0) / (L.tf - L.t0));
+      env = L.E0 * (s * s);
+    }
+  } else if (L.envelope_kind == EDUS_ENV_PW) {
+    double tr = 0.;
+    if (t >= L.t0 && t < L.w1)
+      tr = (t - L.t0) / (L.w1 - L.t0);
+    else if (t >= L.w1 && t < L.w2)
+      tr = 1.;
+    else if (t >= L.w2 && t <= L.tf)
+      tr = (t - L.tf) / (L.w2 - L.tf);
+    env = L.E0 * tr;
+  }
+  double p1 = L.envelope_only ? 1. : std::sin(L.wl * (t - L.t0) + L.phase);
+  double p2 = L.envelope_only ? 1. : std::cos(L.wl * (t - L.t0) + L.phase);
+  for (int i = 0; i < 3; i++) E[i] = env * (p1 * L.pol1[i] + p2 * L.pol2[i]);
+}
+
+}  // namespace
+
+// Source_Main/RungeKutta.cpp:24-30
+void field_at(const edus_params& p, double t, double EF[2][3]) {
+  for (int i = 0; i < 3; i++) EF[0][i] = 0.;
+  for (int ip = 0; ip < p.n_pumps; ip++) {
+    double e[3];
+    laser_E(p.pump[ip], t, e);
+    for (int i = 0; i < 3; i++) EF[0][i] += e[i];
+  }
+  double e2[3];
+  laser_E(p.probe, t, e2);
+  for (int i = 0; i < 3; i++) EF[1][i] = .5 * e2[i];
+}
+
+static bool field_nonzero(const double EF[2][3]) {
+  double Emax = 0;
+  for (int a = 0; a < 2; a++)
+    for (int i = 0; i < 3; i++) Emax += EF[a][i] * EF[a][i];
+  return std::sqrt(Emax) > 1e-20;
+}
+
+}  // namespace edus
+
+using namespace edus;
+
+struct edus_ctx {
+  Problem P;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int n = 0, ntri = 0, nk = 0;
+  size_t plane = 0;  // ntri * nk
+  DevTables tb{};
+  DevConsts hc{};
+  DevConsts* d_cst = nullptr;
+  std::vector<void*> allocs;
+  double2 *d_P0 = nullptr, *d_P1 = nullptr, *d_Pa = nullptr, *d_Pb = nullptr, *d_ring = nullptr, *d_hr = nullptr;
+  double2 *d_h = nullptr, *d_X0 = nullptr;
+  CoulDev cd{};
+  void* d_part = nullptr;
+  double2* d_tabs3 = nullptr;
+  edus_obs* d_log = nullptr;
+  int log_cap = 0, nlog = 0;
+  double* d_ncond = nullptr;
+  double* d_pcmax = nullptr;
+  unsigned long long* d_maxdp = nullptr;
+  // loop state (host mirror of the reference's scalars)
+  int it = 0, itfi = 0, res = 1;
+  double time_loop = 0, dt = 0, dt0 = 0;
+  double EF[2][3]{};
+  bool e_non0 = true;
+  int ring_idx[kMaxOrder]{};
+  double dt_prev[kMaxOrder]{};
+  double P_cond_max = 0, n_cond = 0;
+  int solver = 0, order = 0;
+  bool dyn = false, coul = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0;
+  long long launches = 0, last_launches = 0;
+};
+
+namespace {
+
+template <class T>
+int dalloc(edus_ctx* c, T** p, size_t count) {
+  void* v = nullptr;
+  cudaError_t e = cudaMalloc(&v, sizeof(T) * (count ? count : 1));
+  if (e != cudaSuccess) return fail(EDUS_ENOMEM, "cudaMalloc(%zu bytes): %s", sizeof(T) * count, cudaGetErrorString(e));
+  c->allocs.push_back(v);
+  *p = (T*)v;
+  return 0;
+}
+
+// reference layout [k][n][n] -> upper-triangle planes [e][k]
+void to_planes(const cd* src, int nk, int n, int comps, std::vector<double2>& dst) {
+  int nt = n * (n + 1) / 2;
+  dst.assign((size_t)comps * nt * nk, make_double2(0, 0));
+  for (int k = 0; k < nk; k++)
+    for (int i = 0; i < n; i++)
+      for (int j = i; j < n; j++)
+        for (int x = 0; x < comps; x++) {
+          cd v = src[(((size_t)k * n + i) * n + j) * comps + x];
+          dst[((size_t)x * nt + tri_index(i, j, n)) * nk + k] = make_double2(v.real(), v.imag());
+        }
+}
+
+int upload(edus_ctx* c, double2* d, const std::vector<double2>& h) {
+  CK(cudaMemcpyAsync(d, h.data(), sizeof(double2) * h.size(), cudaMemcpyHostToDevice, c->stream));
+  return 0;
+}
+
+int state_to_dev(edus_ctx* c, const double* rho, double2* d) {
+  std::vector<double2> pl;
+  to_planes((const cd*)rho, c->nk, c->n, 1, pl);
+  int rc = upload(c, d, pl);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int state_from_dev(edus_ctx* c, const double2* d, double* rho) {
+  std::vector<double2> pl(c->plane);
+  CK(cudaMemcpyAsync(pl.data(), d, sizeof(double2) * c->plane, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int n = c->n, nk = c->nk;
+  cd* out = (cd*)rho;
+  for (int k = 0; k < nk; k++)
+    for (int i = 0; i < n; i++)
+      for (int j = i; j < n; j++) {
+        double2 v = pl[(size_t)tri_index(i, j, n) * nk + k];
+        out[((size_t)k * n + i) * n + j] = cd(v.x, v.y);
+        if (i != j) out[((size_t)k * n + j) * n + i] = cd(v.x, -v.y);
+      }
+  return 0;
+}
+
+double2* slot_ptr(edus_ctx* c, int slot) {
+  switch (slot) {
+    case EDUS_SLOT_P0: return c->d_P0;
+    case EDUS_SLOT_P1: return c->d_P1;
+    case EDUS_SLOT_P2: return c->d_Pa;
+    case EDUS_SLOT_PV: return c->d_Pb;
+  }
+  return nullptr;
+}
+
+StageArgs base_args(edus_ctx* c) {
+  StageArgs a;
+  memset(&a, 0, sizeof(a));
+  a.wx2 = c->P.p.probe.wl;
+  a.order = c->order;
+  a.dt = c->dt;
+  return a;
+}
+
+int run_coulomb(edus_ctx* c, const double2* src) {
+  if (!c->coul) return 0;
+  CK(launch_coulomb(c->tb, c->cd, src, c->d_h, nullptr, c->d_X0, c->stream));
+  c->launches += 2;
+  return 0;
+}
+
+int rhs(edus_ctx* c, StageArgs& a) {
+  int rc = run_coulomb(c, a.src);
+  if (rc) return rc;
+  CK(launch_rhs(c->tb, c->d_cst, a, c->stream));
+  c->launches++;
+  return 0;
+}
+
+void set_ef(StageArgs& a, const double EF[2][3]) {
+  for (int i = 0; i < 2; i++)
+    for (int j = 0; j < 3; j++) a.EF[i][j] = EF[i][j];
+}
+
+int observe(edus_ctx* c) {
+  edus_obs rec;
+  memset(&rec, 0, sizeof(rec));
+  rec.t = c->time_loop;
+  for (int i = 0; i < 3; i++) {
+    rec.EF_pump[i] = c->EF[0][i];
+    rec.EF_probe[i] = c->EF[1][i];
+  }
+  rec.dt = c->dt;
+  edus_obs* slot = nullptr;
+  if (c->nlog < c->log_cap) slot = c->d_log + c->nlog;
+  double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
+  double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
+  CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, c->d_part,
+                        c->d_tabs3, scaleJ, scaleTA, rec, slot, c->d_ncond, c->d_pcmax, c->stream));
+  c->launches += 2 + ((c->P.p.tabs && c->P.nch > 0) ? 1 : 0);
+  c->nlog++;
+  return 0;
+}
+
+bool want_hr(edus_ctx* c) { return c->coul && ((c->it + 1) % c->res == 0); }
+
+// Source_Main/RungeKutta.cpp (one RK4 step)
+int step_rk4(edus_ctx* c, bool startup_ring) {
+  const double dt = c->dt, dt6 = dt / 6.0, dt3 = dt / 3.0, dt2 = dt / 2.0;
+  const double t = c->time_loop;
+  StageArgs a = base_args(c);
+  a.e_non0 = c->e_non0;
+  field_at(c->P.p, t, c->EF);
+  set_ef(a, c->EF);
+  a.src = c->d_P0;
+  a.base = c->d_P0;
+  a.acc = c->d_P1;
+  a.dst = c->d_Pa;
+  a.op = OP_RK_FIRST;
+  a.c1 = dt6;
+  a.c2 = dt2;
+  if (startup_ring) {
+    a.ring = c->d_ring;
+    for (int s = 0; s < c->order; s++) a.ring_idx[s] = c->ring_idx[s];
+  }
+  int rc = rhs(c, a);
+  if (rc) return rc;
+  a.ring = nullptr;
+  field_at(c->P.p, t + dt2, c->EF);
+  set_ef(a, c->EF);
+  a.src = c->d_Pa;
+  a.dst = c->d_Pb;
+  a.op = OP_RK_MID;
+  a.c1 = dt3;
+  a.c2 = dt2;
+  if ((rc = rhs(c, a))) return rc;
+  a.src = c->d_Pb;
+  a.dst = c->d_Pa;
+  a.c2 = dt;
+  if ((rc = rhs(c, a))) return rc;
+  field_at(c->P.p, t + dt, c->EF);
+  set_ef(a, c->EF);
+  a.src = c->d_Pa;
+  a.dst = c->d_P0;
+  a.op = OP_RK_LAST;
+  a.c1 = dt6;
+  a.hr_out = want_hr(c) ? c->d_hr : nullptr;
+  if (c->dyn) {
+    CK(cudaMemsetAsync(c->d_maxdp, 0, sizeof(unsigned long long), c->stream));
+    a.maxdp = c->d_maxdp;
+    a.pcond_plus_ncond = c->P_cond_max + c->n_cond;
+  }
+  if ((rc = rhs(c, a))) return rc;
+  c->e_non0 = field_nonzero(c->EF);
+  return 0;
+}
+
+// Source_Main/Linear_Multistep_ODE_solvers.cpp:1-93
+int step_ab(edus_ctx* c) {
+  static const double cf[5][5] = {{1., 0, 0, 0, 0},
+                                  {3.0 / 2.0, -1.0 / 2.0, 0, 0, 0},
+                                  {23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0, 0, 0},
+                                  {55.0 / 24.0, -59.0 / 24.0, 37.0 / 24.0, -9.0 / 24.0, 0},
+                                  {1901.0 / 720.0, -2774.0 / 720.0, 2616.0 / 720.0, -1274.0 / 720.0, 251.0 / 720.0}};
+  const int p = c->order;
+  field_at(c->P.p, c->time_loop, c->EF);
+  c->e_non0 = field_nonzero(c->EF);
+  int fill = c->ring_idx[p - 1];
+  for (int s = p - 1; s > 0; s--) c->ring_idx[s] = c->ring_idx[s - 1];
+  c->ring_idx[0] = fill;
+  bool startup = c->P.p.ab_rk4_startup && c->it < p - 1;
+  if (startup) return step_rk4(c, true);
+  StageArgs a = base_args(c);
+  set_ef(a, c->EF);
+  a.e_non0 = c->e_non0;
+  a.src = c->d_P0;
+  a.dst = c->d_Pa;
+  a.op = OP_AB;
+  a.ring = c->d_ring;
+  a.dt = c->dt;
+  for (int s = 0; s < p; s++) {
+    a.ring_idx[s] = c->ring_idx[s];
+    a.coef[s] = cf[p - 1][s];
+  }
+  a.hr_out = want_hr(c) ? c->d_hr : nullptr;
+  int rc = rhs(c, a);
+  if (rc) return rc;
+  std::swap(c->d_P0, c->d_Pa);
+  return 0;
+}
+
+// Source_Main/Taylor_DE_solver_deriv_Polynom.cpp:1-177
+int step_taylor(edus_ctx* c) {
+  const int TO = c->order, m = TO - 1;
+  field_at(c->P.p, c->time_loop, c->EF);
+  c->e_non0 = field_nonzero(c->EF);
+  int fill = c->ring_idx[TO - 1];
+  for (int s = TO - 1; s > 0; s--) c->ring_idx[s] = c->ring_idx[s - 1];
+  c->ring_idx[0] = fill;
+  StageArgs a = base_args(c);
+  set_ef(a, c->EF);
+  a.e_non0 = c->e_non0;
+  a.src = c->d_P0;
+  a.dst = c->d_Pa;
+  a.op = OP_TAYLOR;
+  a.ring = c->d_ring;
+  a.dt = c->dt;
+  for (int s = 0; s < TO; s++) a.ring_idx[s] = c->ring_idx[s];
+  double ti[kMaxOrder], tau[kMaxOrder * kMaxOrder], tinv[kMaxOrder * kMaxOrder];
+  ti[0] = c->dt_prev[0];
+  for (int i = 1; i < m; i++) ti[i] = ti[i - 1] + c->dt_prev[i - 1];
+  const double scale = std::pow(10, 7);
+  for (int i = 0; i < m; i++)
+    for (int q = 0; q < m; q++) tau[i * m + q] = scale * std::pow(ti[i], (q + 1));
+  if (inv_gj(m, tau, tinv)) return fail(EDUS_EINVAL, "Taylor tau matrix is singular");
+  for (int i = 0; i < m * m; i++) a.tinv[i] = tinv[i] * scale;
+  for (int i = 0; i < TO; i++) a.tpow[i] = std::pow(c->dt, i + 1);
+  a.hr_out = want_hr(c) ? c->d_hr : nullptr;
+  if (c->dyn) {
+    CK(cudaMemsetAsync(c->d_maxdp, 0, sizeof(unsigned long long), c->stream));
+    a.maxdp = c->d_maxdp;
+    a.pcond_plus_ncond = c->P_cond_max + c->n_cond;
+  }
+  int rc = rhs(c, a);
+  if (rc) return rc;
+  std::swap(c->d_P0, c->d_Pa);
+  return 0;
+}
+
+int do_step(edus_ctx* c) {
+  if (c->solver == EDUS_SOLVER_TAYLOR) return step_taylor(c);
+  if (c->solver == EDUS_SOLVER_AB && !c->dyn) return step_ab(c);
+  return step_rk4(c, false);
+}
+
+// Source_Main/dyn_dt_evolution.cpp:64-133
+int adapt_dt(edus_ctx* c) {
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, c->d_maxdp, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double mx;
+  memcpy(&mx, &bits, sizeof(mx));
+  const double eps = c->P.p.eps_step_abs;
+  if ((mx > eps) && (c->dt > 0.01))
+    c->dt *= eps / mx;
+  else if (c->dt < c->dt0)
+    c->dt *= 1.02;
+  if (c->solver == EDUS_SOLVER_TAYLOR) {
+    for (int i = c->order - 1; i > 0; i--) c->dt_prev[i] = c->dt_prev[i - 1];
+    c->dt_prev[0] = c->dt;
+  }
+  return 0;
+}
+
+int sync_scalars(edus_ctx* c) {
+  double v[2];
+  CK(cudaMemcpyAsync(&v[0], c->d_pcmax, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&v[1], c->d_ncond, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->P_cond_max = v[0];
+  c->n_cond = v[1];
+  return 0;
+}
+
+int run_steps(edus_ctx* c, int nsteps, bool all) {
+  int done = 0;
+  if (!c->dyn) {
+    while (c->it <= c->itfi && (all || done < nsteps)) {
+      if (c->it % c->res == 0) {
+        int rc = observe(c);
+        if (rc) return rc;
+      }
+      int rc = do_step(c);
+      if (rc) return rc;
+      c->time_loop += c->dt;
+      c->it++;
+      done++;
+    }
+  } else {
+    while (c->time_loop < c->P.p.t_fin && (all || done < nsteps)) {
+      if (c->it % c->res == 0) {
+        int rc = observe(c);
+        if (rc) return rc;
+        if ((rc = sync_scalars(c))) return rc;
+      }
+      int rc = do_step(c);
+      if (rc) return rc;
+      if ((rc = adapt_dt(c))) return rc;
+      c->time_loop += c->dt;
+      c->it++;
+      done++;
+    }
+  }
+  return 0;
+}
+
+int timed(edus_ctx* c, int nsteps, bool all) {
+  CK(cudaSetDevice(c->device));
+  long long l0 = c->launches;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = run_steps(c, nsteps, all);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  c->last_launches = c->launches - l0;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+const char* edus_strerror(int code) {
+  switch (code) {
+    case EDUS_OK: return "ok";
+    case EDUS_EINVAL: return "invalid argument";
+    case EDUS_ENOMEM: return "out of memory (host, HBM or HBM budget)";
+    case EDUS_ECUDA: return "CUDA error";
+    case EDUS_ENONFINITE: return "non-finite density matrix";
+    case EDUS_ETRACE: return "trace drift above tolerance";
+    case EDUS_ETIMEOUT: return "device wait timed out";
+    case EDUS_ECANCELLED: return "cancelled";
+    case EDUS_EIO: return "file could not be read or written";
+    case EDUS_EPARSE: return "input.txt grammar error";
+    case EDUS_EUNSUPPORTED: return "option not built";
+    case EDUS_ENOTREADY: return "result not ready";
+  }
+  return "unknown error";
+}
+
+int edus_abi_version(void) { return EDUS_ABI_VERSION; }
+
+int edus_options_default(edus_options* o) {
+  if (!o) return EDUS_EINVAL;
+  memset(o, 0, sizeof(*o));
+  o->device = 0;
+  o->precision = -1;
+  o->use_graphs = 0;
+  o->health_checks = 0;
+  o->trace_tol = 1e-6;
+  o->hbm_budget_bytes = 0;
+  return 0;
+}
+
+int edus_problem_create(const edus_params* p, const char* workdir, edus_problem** out) {
+  clear_error();
+  if (!p || !out) return fail(EDUS_EINVAL, "null argument");
+  edus_problem* pb = new (std::nothrow) edus_problem();
+  if (!pb) return fail(EDUS_ENOMEM, "host allocation");
+  int rc = build_problem(*p, workdir, pb->P);
+  if (rc) {
+    delete pb;
+    return rc;
+  }
+  *out = pb;
+  return 0;
+}
+
+int edus_problem_info_get(const edus_problem* pb, edus_problem_info* o) {
+  if (!pb || !o) return fail(EDUS_EINVAL, "null argument");
+  const Problem& P = pb->P;
+  memset(o, 0, sizeof(*o));
+  o->ncv = P.ncv;
+  o->nch = P.nch;
+  o->nv = P.nv;
+  o->nc = P.nc;
+  o->nk = P.nk;
+  o->n1 = P.n1;
+  o->n2 = P.n2;
+  o->nshell = P.nshell;
+  o->nnb = P.nnb;
+  o->nrpts = P.nrpts;
+  o->n_diss = (int)P.diss_i.size();
+  o->nsteps = P.nsteps;
+  o->nprint = P.nprint;
+  o->t_start = P.t_start;
+  o->det_a = P.det_a;
+  o->jacobian = P.jac;
+  for (int i = 0; i < 3; i++) o->dk[i] = P.dk[i];
+  return 0;
+}
+
+int edus_problem_get(const edus_problem* pb, const char* name, void* dst, size_t nbytes) {
+  if (!pb || !name || !dst) return fail(EDUS_EINVAL, "null argument");
+  const Problem& P = pb->P;
+  const void* src = nullptr;
+  size_t nb = 0;
+  std::vector<double> wtmp;
+  std::string s = name;
+  if (s == "kpt") {
+    src = P.kpt.data();
+    nb = P.kpt.size() * sizeof(double);
+  } else if (s == "H") {
+    src = P.H.data();
+    nb = P.H.size() * sizeof(cd);
+  } else if (s == "U") {
+    src = P.U.data();
+    nb = P.U.size() * sizeof(cd);
+  } else if (s == "D") {
+    src = P.D.data();
+    nb = P.D.size() * sizeof(cd);
+  } else if (s == "GE") {
+    src = P.GE.data();
+    nb = P.GE.size() * sizeof(cd);
+  } else if (s == "P0") {
+    src = P.P0.data();
+    nb = P.P0.size() * sizeof(cd);
+  } else if (s == "nbr") {
+    src = P.nbr.data();
+    nb = P.nbr.size() * sizeof(int);
+  } else if (s == "bvec") {
+    src = P.bvec.data();
+    nb = P.bvec.size() * sizeof(double);
+  } else if (s == "weights") {
+    for (int b = 0; b < P.nnb; b++) wtmp.push_back(P.shell_w[P.bshell[b]]);
+    src = wtmp.data();
+    nb = wtmp.size() * sizeof(double);
+  } else if (s == "T") {
+    src = P.T;
+    nb = sizeof(P.T);
+  } else if (s == "HR") {
+    src = P.HR.data();
+    nb = P.HR.size() * sizeof(cd);
+  } else if (s == "rR") {
+    src = P.rR.data();
+    nb = P.rR.size() * sizeof(cd);
+  } else if (s == "Rvec") {
+    src = P.Rvec.data();
+    nb = P.Rvec.size() * sizeof(double);
+  } else {
+    return fail(EDUS_EINVAL, "unknown array %s", name);
+  }
+  if (nb != nbytes) return fail(EDUS_EINVAL, "%s has %zu bytes, caller asked for %zu", name, nb, nbytes);
+  memcpy(dst, src, nb);
+  return 0;
+}
+
+void edus_problem_free(edus_problem* pb) { delete pb; }
+
+void edus_destroy(edus_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out) {
+  clear_error();
+  if (!pb || !out) return fail(EDUS_EINVAL, "null argument");
+  edus_options o;
+  edus_options_default(&o);
+  if (opt) o = *opt;
+  edus_ctx* c = new (std::nothrow) edus_ctx();
+  if (!c) return fail(EDUS_ENOMEM, "host allocation");
+  c->P = pb->P;
+  const Problem& P = c->P;
+  c->device = o.device;
+  int rc = 0;
+  auto bail = [&](int code) {
+    edus_destroy(c);
+    return code;
+  };
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return bail(fail(EDUS_ECUDA, "no CUDA device"));
+  if (cudaSetDevice(c->device) != cudaSuccess) return bail(fail(EDUS_ECUDA, "cannot select device %d", c->device));
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(EDUS_ECUDA, "stream"));
+  cudaEventCreate(&c->ev0);
+  cudaEventCreate(&c->ev1);
+  const int n = P.ncv, nk = P.nk, nt = n * (n + 1) / 2;
+  c->n = n;
+  c->ntri = nt;
+  c->nk = nk;
+  c->plane = (size_t)nt * nk;
+  if (n != 1 && n != 2 && n != 3 && n != 4 && n != 5 && n != 6 && n != 8)
+    return bail(fail(EDUS_EUNSUPPORTED, "band count %d has no FP64 kernel instance (1-6, 8)", n));
+  if (P.nnb > kMaxNb) return bail(fail(EDUS_EUNSUPPORTED, "stencil with %d neighbours (max %d)", P.nnb, kMaxNb));
+  c->solver = P.p.solver;
+  c->order = P.p.solver == EDUS_SOLVER_RK4 ? 0 : P.p.order;
+  if (c->order > kMaxOrder) return bail(fail(EDUS_EINVAL, "order %d > %d", c->order, kMaxOrder));
+  if (P.p.ab_rk4_startup && P.p.solver == EDUS_SOLVER_AB && c->order < 1) return bail(fail(EDUS_EINVAL, "AB order"));
+  c->dyn = P.p.dynamical_dt != 0;
+  c->coul = P.p.coulomb != 0;
+  c->res = P.p.it_resolution > 0 ? P.p.it_resolution : 1;
+  // symmetric dipoles are stored as upper triangles
+  for (int k = 0; k < nk; k++)
+    for (int i = 0; i < n; i++)
+      for (int j = i + 1; j < n; j++)
+        for (int x = 0; x < 3; x++)
+          if (P.D[(((size_t)k * n + i) * n + j) * 3 + x] != P.D[(((size_t)k * n + j) * n + i) * 3 + x])
+            return bail(fail(EDUS_EUNSUPPORTED, "dipole matrix is not symmetric at k=%d (%d,%d)", k, i, j));
+  // ---- device tables
+  std::vector<double2> pl;
+  double2 *dH, *dD, *dU = nullptr, *dGE = nullptr;
+  int* dnbr;
+  if ((rc = dalloc(c, &dH, c->plane)) || (rc = dalloc(c, &dD, 3 * c->plane)) || (rc = dalloc(c, &dnbr, (size_t)P.nnb * nk)))
+    return bail(rc);
+  to_planes(P.H.data(), nk, n, 1, pl);
+  if ((rc = upload(c, dH, pl))) return bail(rc);
+  to_planes(P.D.data(), nk, n, 3, pl);
+  if ((rc = upload(c, dD, pl))) return bail(rc);
+  {
+    std::vector<double2> u((size_t)n * n * nk);
+    for (int k = 0; k < nk; k++)
+      for (int e = 0; e < n * n; e++) {
+        cd v = P.U[(size_t)k * n * n + e];
+        u[(size_t)e * nk + k] = make_double2(v.real(), v.imag());
+      }
+    if ((rc = dalloc(c, &dU, u.size())) || (rc = upload(c, dU, u))) return bail(rc);
+  }
+  if (P.p.current && !c->coul) {
+    to_planes(P.GE.data(), nk, n, 3, pl);
+    if ((rc = dalloc(c, &dGE, pl.size())) || (rc = upload(c, dGE, pl))) return bail(rc);
+  }
+  {
+    std::vector<int> nb((size_t)P.nnb * nk);
+    for (int k = 0; k < nk; k++)
+      for (int b = 0; b < P.nnb; b++) nb[(size_t)b * nk + k] = P.nbr[(size_t)k * P.nnb + b];
+    if (cudaMemcpyAsync(dnbr, nb.data(), sizeof(int) * nb.size(), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+      return bail(fail(EDUS_ECUDA, "upload nbr"));
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "sync"));
+  }
+  // ---- constants
+  DevConsts& h = c->hc;
+  memset(&h, 0, sizeof(h));
+  for (int b = 0; b < P.nnb; b++) {
+    h.wb[b] = P.shell_w[P.bshell[b]];
+    for (int x = 0; x < 3; x++) h.bvec[b][x] = P.bvec[b * 3 + x];
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) h.T[i * n + j] = P.T[i][j];
+  for (size_t t = 0; t < P.diss_i.size(); t++) {
+    h.diss_i[t] = P.diss_i[t];
+    h.diss_j[t] = P.diss_j[t];
+  }
+  // ---- state
+  if ((rc = dalloc(c, &c->d_P0, c->plane)) || (rc = dalloc(c, &c->d_P1, c->plane)) || (rc = dalloc(c, &c->d_Pa, c->plane)) ||
+      (rc = dalloc(c, &c->d_Pb, c->plane)))
+    return bail(rc);
+  if (c->order > 0 && (rc = dalloc(c, &c->d_ring, (size_t)c->order * c->plane))) return bail(rc);
+  if (c->d_ring && cudaMemsetAsync(c->d_ring, 0, sizeof(double2) * c->order * c->plane, c->stream) != cudaSuccess)
+    return bail(fail(EDUS_ECUDA, "memset ring"));
+  for (int i = 0; i < kMaxOrder; i++) c->ring_idx[i] = i;
+  if ((rc = state_to_dev(c, (const double*)P.P0.data(), c->d_P0))) return bail(rc);
+  // ---- observables
+  if ((rc = dalloc(c, (char**)&c->d_part, obs_parts(nk) * obs_part_bytes())) || (rc = dalloc(c, &c->d_tabs3, 3)) ||
+      (rc = dalloc(c, &c->d_ncond, 1)) || (rc = dalloc(c, &c->d_pcmax, 1)) || (rc = dalloc(c, &c->d_maxdp, 1)))
+    return bail(rc);
+  cudaMemsetAsync(c->d_ncond, 0, sizeof(double), c->stream);
+  cudaMemsetAsync(c->d_pcmax, 0, sizeof(double), c->stream);
+  c->log_cap = P.p.dynamical_dt ? 1 << 16 : P.nprint + 2;
+  if ((rc = dalloc(c, &c->d_log, c->log_cap))) return bail(rc);
+  // ---- tables struct
+  DevTables& tb = c->tb;
+  memset(&tb, 0, sizeof(tb));
+  tb.n = n;
+  tb.ntri = nt;
+  tb.nk = nk;
+  tb.nnb = P.nnb;
+  tb.n1 = P.p.sample_110 ? P.p.nk[0] : P.p.nk[1];
+  tb.n2 = P.p.sample_110 ? P.p.nk[1] : P.p.nk[2];
+  tb.nch = P.nch;
+  tb.nbands = P.nbands;
+  tb.H = dH;
+  tb.D = dD;
+  tb.U = dU;
+  tb.GE = dGE;
+  tb.nbr = dnbr;
+  tb.n_diss = (int)P.diss_i.size();
+  // ---- Coulomb
+  if (c->coul) {
+    const int nc = P.ncut, n1 = tb.n1, n2 = tb.n2;
+    if (n1 * n2 != nk) return bail(fail(EDUS_EINVAL, "Coulomb needs a 2D grid"));
+    const int a1 = P.p.sample_110 ? 0 : 1, a2 = P.p.sample_110 ? 1 : 2;
+    std::vector<double> t1c((size_t)nc * n1), t1s((size_t)nc * n1), t2c((size_t)nc * n2), t2s((size_t)nc * n2);
+    for (int m = 0; m < nc; m++) {
+      for (int i1 = 0; i1 < n1; i1++) {
+        double x = 2 * M_PI * m * (P.kpt[(size_t)(i1 * n2) * 3 + a1]);
+        t1c[(size_t)m * n1 + i1] = std::cos(x);
+        t1s[(size_t)m * n1 + i1] = std::sin(x);
+      }
+      for (int i2 = 0; i2 < n2; i2++) {
+        double x = 2 * M_PI * m * (P.kpt[(size_t)i2 * 3 + a2]);
+        t2c[(size_t)m * n2 + i2] = std::cos(x);
+        t2s[(size_t)m * n2 + i2] = std::sin(x);
+      }
+    }
+    double *d1c, *d1s, *d2c, *d2s;
+    if ((rc = dalloc(c, &d1c, t1c.size())) || (rc = dalloc(c, &d1s, t1s.size())) || (rc = dalloc(c, &d2c, t2c.size())) ||
+        (rc = dalloc(c, &d2s, t2s.size())))
+      return bail(rc);
+    cudaMemcpyAsync(d1c, t1c.data(), sizeof(double) * t1c.size(), cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(d1s, t1s.data(), sizeof(double) * t1s.size(), cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(d2c, t2c.data(), sizeof(double) * t2c.size(), cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(d2s, t2s.data(), sizeof(double) * t2s.size(), cudaMemcpyHostToDevice, c->stream);
+    std::vector<double2> cf[4];
+    const std::vector<cd>* src[4] = {&P.cA, &P.cB, &P.cC, &P.cD};
+    std::vector<unsigned char> isd(nt);
+    std::vector<int> diag_of(nt, 0);
+    for (int q = 0; q < 4; q++) {
+      cf[q].assign((size_t)nc * nc * nt, make_double2(0, 0));
+      for (int mm = 0; mm < nc * nc; mm++)
+        for (int i = 0; i < n; i++)
+          for (int j = i; j < n; j++) {
+            int lin = (i == j) ? 0 : i * n + j;
+            cd v = (*src[q])[(size_t)mm * n * n + lin];
+            cf[q][(size_t)mm * nt + tri_index(i, j, n)] = make_double2(v.real(), v.imag());
+          }
+    }
+    for (int i = 0; i < n; i++)
+      for (int j = i; j < n; j++) {
+        int e = tri_index(i, j, n);
+        isd[e] = (i == j);
+        diag_of[e] = i;
+        int lin = (i == j) ? 0 : i * n + j;
+        cd s = std::conj(P.screen[lin]);
+        h.screen[e] = make_double2(s.real(), s.imag());
+      }
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) h.VH[i * n + j] = P.VH[(size_t)i * n + j];
+    double2* dcf[4];
+    for (int q = 0; q < 4; q++) {
+      if ((rc = dalloc(c, &dcf[q], cf[q].size())) || (rc = upload(c, dcf[q], cf[q]))) return bail(rc);
+    }
+    unsigned char* disd;
+    int* ddo;
+    if ((rc = dalloc(c, &disd, nt)) || (rc = dalloc(c, &ddo, nt))) return bail(rc);
+    cudaMemcpyAsync(disd, isd.data(), nt, cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(ddo, diag_of.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, c->stream);
+    double2 *dg, *dfd, *dPW0;
+    if ((rc = dalloc(c, &dg, (size_t)n1 * 2 * nc * nt)) || (rc = dalloc(c, &c->d_h, (size_t)n1 * 2 * nc * nt)) ||
+        (rc = dalloc(c, &c->d_X0, (size_t)4 * nc * nc * nt)) || (rc = dalloc(c, &dfd, n)) || (rc = dalloc(c, &dPW0, c->plane)) ||
+        (rc = dalloc(c, &c->d_hr, c->plane)))
+      return bail(rc);
+    c->cd.g = dg;
+    c->cd.t1c = d1c;
+    c->cd.t1s = d1s;
+    c->cd.t2c = d2c;
+    c->cd.t2s = d2s;
+    c->cd.A = dcf[0];
+    c->cd.B = dcf[1];
+    c->cd.C = dcf[2];
+    c->cd.D = dcf[3];
+    c->cd.is_diag = disd;
+    c->cd.diag_of = ddo;
+    c->cd.fdiag = dfd;
+    tb.ncut = nc;
+    tb.t2c = d2c;
+    tb.t2s = d2s;
+    tb.fdiag = dfd;
+    tb.PW0 = dPW0;
+    tb.ncond = c->d_ncond;
+    // equilibrium coefficients (main_MPI.cpp:276-337): X0 = X(P0), E_H0 from f_cc(0,0)
+    if (cudaMemcpyAsync(dPW0, c->d_P0, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+      return bail(fail(EDUS_ECUDA, "copy PW0"));
+    if (cudaMemcpyAsync(c->d_hr, dH, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+      return bail(fail(EDUS_ECUDA, "copy Hr"));
+    if (launch_coulomb(tb, c->cd, c->d_P0, nullptr, c->d_X0, nullptr, c->stream) != cudaSuccess)
+      return bail(fail(EDUS_ECUDA, "equilibrium Coulomb pass"));
+    std::vector<double2> fd(n);
+    cudaMemcpyAsync(fd.data(), dfd, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "sync"));
+    for (int i = 0; i < n; i++) {
+      double eh = 0;
+      for (int j = 0; j < n; j++) eh += fd[j].x * P.VH[(size_t)i * n + j];
+      h.EH0[i] = eh;
+    }
+    tb.h = c->d_h;
+  }
+  if ((rc = dalloc(c, &c->d_cst, 1))) return bail(rc);
+  if (cudaMemcpyAsync(c->d_cst, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    return bail(fail(EDUS_ECUDA, "upload constants"));
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "sync"));
+  // ---- loop state (Source_Main/const_dt_evolution.cpp:1-9, main_MPI.cpp:269-274)
+  c->it = 0;
+  c->itfi = P.itfi;
+  c->time_loop = P.t_start;
+  c->dt = P.p.dt;
+  c->dt0 = P.p.dt;
+  for (int i = 0; i < kMaxOrder; i++) c->dt_prev[i] = P.p.dt;
+  c->e_non0 = true;
+  c->n_cond = c->dyn ? std::pow(10, -16) : 0;
+  c->P_cond_max = 0;
+  *out = c;
+  return 0;
+}
+
+int edus_set_state(edus_ctx* c, const double* rho) {
+  if (!c || !rho) return fail(EDUS_EINVAL, "null argument");
+  return state_to_dev(c, rho, c->d_P0);
+}
+int edus_get_state(edus_ctx* c, double* rho) {
+  if (!c || !rho) return fail(EDUS_EINVAL, "null argument");
+  return state_from_dev(c, c->d_P0, rho);
+}
+int edus_slot_set(edus_ctx* c, int32_t slot, const double* rho) {
+  double2* d = c ? slot_ptr(c, slot) : nullptr;
+  if (!d || !rho) return fail(EDUS_EINVAL, "bad slot %d", slot);
+  return state_to_dev(c, rho, d);
+}
+int edus_slot_get(edus_ctx* c, int32_t slot, double* rho) {
+  double2* d = c ? slot_ptr(c, slot) : nullptr;
+  if (!d || !rho) return fail(EDUS_EINVAL, "bad slot %d", slot);
+  return state_from_dev(c, d, rho);
+}
+int edus_slot_copy(edus_ctx* c, int32_t src, int32_t dst) {
+  double2 *s = c ? slot_ptr(c, src) : nullptr, *d = c ? slot_ptr(c, dst) : nullptr;
+  if (!s || !d) return fail(EDUS_EINVAL, "bad slot");
+  CK(cudaMemcpyAsync(d, s, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int edus_get_derivative(edus_ctx* c, int32_t p_slot, const double EF[6], double wx2, int32_t e_non0) {
+  double2* s = c ? slot_ptr(c, p_slot) : nullptr;
+  if (!s || !EF) return fail(EDUS_EINVAL, "bad slot %d", p_slot);
+  if (p_slot == EDUS_SLOT_PV) return fail(EDUS_EINVAL, "derivative of the Pv slot would overwrite its input");
+  StageArgs a = base_args(c);
+  for (int i = 0; i < 3; i++) {
+    a.EF[0][i] = EF[i];
+    a.EF[1][i] = EF[3 + i];
+  }
+  a.wx2 = wx2;
+  a.e_non0 = e_non0;
+  a.src = s;
+  a.dst = c->d_Pb;
+  a.op = OP_PV;
+  a.hr_out = c->coul ? c->d_hr : nullptr;
+  int rc = rhs(c, a);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int edus_runge_kutta_ad(edus_ctx* c, int32_t src, int32_t dst, double dt) {
+  // P_dst = P_src + dt * Pv as an element-wise device update
+  double2 *s = c ? slot_ptr(c, src) : nullptr, *d = c ? slot_ptr(c, dst) : nullptr;
+  if (!s || !d || src == EDUS_SLOT_PV || dst == EDUS_SLOT_PV) return fail(EDUS_EINVAL, "bad slot");
+  std::vector<double2> a(c->plane), v(c->plane);
+  CK(cudaMemcpyAsync(a.data(), s, sizeof(double2) * c->plane, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(v.data(), c->d_Pb, sizeof(double2) * c->plane, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (size_t i = 0; i < c->plane; i++) a[i] = cadd(a[i], cscale(v[i], dt));
+  CK(cudaMemcpyAsync(d, a.data(), sizeof(double2) * c->plane, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int edus_runge_kutta_ac(edus_ctx* c, int32_t dst, double dt) { return edus_runge_kutta_ad(c, dst, dst, dt); }
+
+int edus_coulomb_hk(edus_ctx* c, int32_t p_slot, double* hk_out) {
+  if (!c || !hk_out) return fail(EDUS_EINVAL, "null argument");
+  if (!c->coul) return fail(EDUS_EINVAL, "Coulomb is off in this problem");
+  double EF[6] = {0, 0, 0, 0, 0, 0};
+  // evaluates the RHS on the slot, which also stores Hk_renorm
+  int rc = edus_get_derivative(c, p_slot, EF, 0.0, 0);
+  if (rc) return rc;
+  return state_from_dev(c, c->d_hr, hk_out);
+}
+
+int edus_step(edus_ctx* c, int32_t nsteps) {
+  if (!c || nsteps < 0) return fail(EDUS_EINVAL, "bad argument");
+  return timed(c, nsteps, false);
+}
+
+int edus_run(edus_ctx* c) {
+  if (!c) return fail(EDUS_EINVAL, "null argument");
+  return timed(c, 0, true);
+}
+
+int edus_clock(edus_ctx* c, int32_t* it, double* t, double* dt) {
+  if (!c) return fail(EDUS_EINVAL, "null argument");
+  if (it) *it = c->it;
+  if (t) *t = c->time_loop;
+  if (dt) *dt = c->dt;
+  return 0;
+}
+
+int edus_obs_count(edus_ctx* c, int32_t* n) {
+  if (!c || !n) return fail(EDUS_EINVAL, "null argument");
+  *n = c->nlog < c->log_cap ? c->nlog : c->log_cap;
+  return 0;
+}
+
+int edus_obs_get(edus_ctx* c, int32_t first, int32_t count, edus_obs* out) {
+  if (!c || !out || first < 0 || count < 0) return fail(EDUS_EINVAL, "bad argument");
+  int avail = c->nlog < c->log_cap ? c->nlog : c->log_cap;
+  if (first + count > avail) return fail(EDUS_EINVAL, "only %d records", avail);
+  if (count == 0) return 0;
+  CK(cudaMemcpyAsync(out, c->d_log + first, sizeof(edus_obs) * count, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int edus_observables(edus_ctx* c, edus_obs* out) {
+  if (!c || !out) return fail(EDUS_EINVAL, "null argument");
+  edus_obs rec;
+  memset(&rec, 0, sizeof(rec));
+  rec.t = c->time_loop;
+  rec.dt = c->dt;
+  edus_obs* tmp = nullptr;
+  int rc = dalloc(c, &tmp, 1);
+  if (rc) return rc;
+  double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
+  double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
+  CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, c->d_part,
+                        c->d_tabs3, scaleJ, scaleTA, rec, tmp, nullptr, nullptr, c->stream));
+  CK(cudaMemcpyAsync(out, tmp, sizeof(edus_obs), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int edus_last_timing(edus_ctx* c, double* ms, int64_t* launches) {
+  if (!c) return fail(EDUS_EINVAL, "null argument");
+  if (ms) *ms = c->last_ms;
+  if (launches) *launches = c->last_launches;
+  return 0;
+}
+
+// Output/{EF,J1,J2,Losses,TransientAbs}.txt with the reference's stream formats
+// (headers/Observables_MPI.h:134-140, 398-406, 586-595, 707-712, 766-771).
+int edus_write_outputs(edus_ctx* c, const char* outdir) {
+  if (!c || !outdir) return fail(EDUS_EINVAL, "null argument");
+  int32_t n = 0;
+  edus_obs_count(c, &n);
+  std::vector<edus_obs> log(n);
+  int rc = edus_obs_get(c, 0, n, log.data());
+  if (rc) return rc;
+  mkdir(outdir, 0755);
+  std::string d = outdir;
+  std::ofstream fe(d + "/EF.txt"), fl(d + "/Losses.txt");
+  std::ofstream f1, f2, ft;
+  if (c->P.p.current) {
+    f1.open(d + "/J1.txt");
+    f2.open(d + "/J2.txt");
+  }
+  if (c->P.p.tabs) ft.open(d + "/TransientAbs.txt");
+  if (!fe || !fl) return fail(EDUS_EIO, "cannot write into %s", outdir);
+  const int ncv = c->n;
+  for (const edus_obs& o : log) {
+    const double tfs = o.t * kTimeAuFs;
+    fe << std::setw(15) << std::setprecision(8) << tfs;
+    for (int i = 0; i < 3; i++) fe << std::setw(15) << std::setprecision(8) << o.EF_pump[i];
+    fe << std::endl;
+    fl << std::setprecision(16) << tfs << "   ";
+    for (int i = 0; i < ncv; i++) fl << std::setprecision(16) << o.pop[i] << "   ";
+    fl << std::endl;
+    if (c->P.p.current) {
+      f1 << std::setw(15) << std::setprecision(8) << tfs;
+      for (int x = 0; x < 3; x++) {
+        f1 << std::setw(25) << std::setprecision(15) << std::scientific << o.J1[2 * x];
+        f1 << std::setw(25) << std::setprecision(15) << std::scientific << o.J1[2 * x + 1];
+      }
+      f1 << std::endl;
+      f2 << std::setw(15) << std::setprecision(8) << tfs;
+      for (int x = 0; x < 3; x++) f2 << std::setw(25) << std::setprecision(15) << std::scientific << o.J2[x];
+      f2 << std::endl;
+    }
+    if (c->P.p.tabs) {
+      ft << std::setw(15) << std::setprecision(8) << tfs;
+      for (int i = 0; i < 3; i++) ft << std::setw(15) << std::setprecision(8) << o.EF_probe[i];
+      for (int x = 0; x < 3; x++) {
+        ft << std::setw(15) << std::setprecision(8) << o.tabs[2 * x];
+        ft << std::setw(15) << std::setprecision(8) << o.tabs[2 * x + 1];
+      }
+      ft << std::endl;
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+// dev.cuh — device-side types shared by the FP64 kernels and their launchers.
+//
+// Device layout (all resident in HBM for the whole solve):
+//   state planes    rho[e][k], e over the upper triangle i <= j of the n x n
+//                   density matrix in the reference's P[k][i][j] convention
+//                   (lower triangle = conj, exact because every update the
+//                   reference applies preserves Hermiticity bit for bit).
+//   H, GE           Hermitian -> upper triangle planes.
+//   D               symmetric (save_HUD.cpp:47-51, TB dipoles) -> upper planes.
+//   U               full n x n planes (only for dissipation / populations).
+//   nbr             [b][k] neighbour table of the k-gradient stencil.
+// Planes are [element][k] so one thread per k reads coalesced 16-byte words.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace edus {
+
+// ------------------------------------------------------------- complex helpers
+__host__ __device__ __forceinline__ double2 cz() { return make_double2(0., 0.); }
+__host__ __device__ __forceinline__ double2 cmk(double r, double i) { return make_double2(r, i); }
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// a * conj(b)
+__host__ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+// -i * a
+__host__ __device__ __forceinline__ double2 cmi(double2 a) { return make_double2(a.y, -a.x); }
+
+__host__ __device__ __forceinline__ int tri_index(int i, int j, int n) {
+  // i <= j, row-major upper triangle
+  return i * n - (i * (i - 1)) / 2 + (j - i);
+}
+
+constexpr int kMaxBands = 16;
+constexpr int kMaxTri = kMaxBands * (kMaxBands + 1) / 2;
+constexpr int kMaxNb = 64;
+constexpr int kMaxOrder = 8;
+constexpr int kMaxNcut = 64;
+
+// Static problem tables on the device.
+struct DevTables {
+  int n, ntri, nk, nnb, n1, n2, nch, nbands;
+  const double2* H;    // [ntri][nk]
+  const double2* D;    // [3][ntri][nk]
+  const double2* U;    // [n*n][nk] or null
+  const double2* GE;   // [3][ntri][nk] or null
+  const int* nbr;      // [nnb][nk]
+  int n_diss;
+  // Coulomb (null when off)
+  int ncut;
+  const double2* h;      // [n1][2][ncut][ntri] inverse-transform rows
+  const double* t2c;     // [ncut][n2] cos(2 pi n k2)
+  const double* t2s;     // [ncut][n2] sin(2 pi n k2)
+  const double2* fdiag;  // [n] f_cc(0,0) diagonal (Hartree input)
+  const double2* PW0;    // [ntri][nk] initial state (screen correction)
+  const double* ncond;   // device scalar: Coulomb_set.n_cond
+};
+
+// Per-problem constants small enough for a kernel parameter block.
+struct DevConsts {
+  double wb[kMaxNb];          // weight of the shell of each b
+  double bvec[kMaxNb][3];     // Cartesian b
+  double T[kMaxBands * kMaxBands];
+  int diss_i[kMaxBands * kMaxBands], diss_j[kMaxBands * kMaxBands];
+  double VH[kMaxBands * kMaxBands];
+  double EH0[kMaxBands];
+  double2 screen[kMaxTri];    // conj(Screen_const) per upper element (diag uses [0])
+};
+
+enum StageOp : int {
+  OP_PV = 0,       // dst = Pv
+  OP_RK_FIRST = 1, // acc = base + c1 Pv ; dst = base + c2 Pv
+  OP_RK_MID = 2,   // acc += c1 Pv       ; dst = base + c2 Pv
+  OP_RK_LAST = 3,  // dst = acc + c1 Pv
+  OP_AB = 4,       // ring[slot0] = Pv ; dst = src + dt * sum coef[s] ring[idx[s]]
+  OP_TAYLOR = 5,   // ring[slot0] = Pv ; dst = src + Taylor increment
+};
+
+// Everything one fused RHS + update launch needs that changes per stage.
+struct StageArgs {
+  const double2* src;   // state the RHS is evaluated on
+  double2* dst;
+  const double2* base;  // P0 for the RK stage updates
+  double2* acc;         // P1 accumulator
+  double2* ring;        // [order][ntri][nk]
+  double2* hr_out;      // Hk_renorm output [ntri][nk] (Coulomb) or null
+  double EF[2][3];
+  double wx2;
+  int e_non0;
+  int op;
+  double c1, c2;
+  int order;            // AB / Taylor order
+  int ring_idx[kMaxOrder];
+  double coef[kMaxOrder];     // AB coefficients
+  double tinv[kMaxOrder * kMaxOrder];  // Taylor tau^-1 (scaled)
+  double tpow[kMaxOrder];     // pow(dt, i+1)
+  double dt;
+  // adaptive dt: max over k of the population change, written as uint64 bits
+  unsigned long long* maxdp;
+  double pcond_plus_ncond;  // P_cond_max + n_cond
+};
+
+}  // namespace edus

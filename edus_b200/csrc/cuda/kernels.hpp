@@ -1,0 +1,38 @@
+// kernels.hpp — host-side launch API of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "../../../include/edus_b200.h"
+#include "dev.cuh"
+
+namespace edus {
+
+using ObsRecord = edus_obs;
+
+// Device buffers of the Coulomb mean field (separable truncated transform).
+struct CoulDev {
+  double2* g = nullptr;        // [n1][2][ncut][ntri] row transform of rho
+  const double* t1c = nullptr; // [ncut][n1] cos(2 pi m k1)
+  const double* t1s = nullptr;
+  const double* t2c = nullptr; // [ncut][n2] cos(2 pi n k2)
+  const double* t2s = nullptr;
+  const double2* A = nullptr;  // [ncut^2][ntri] coefficients, diagonal rule applied
+  const double2* B = nullptr;
+  const double2* C = nullptr;
+  const double2* D = nullptr;
+  const unsigned char* is_diag = nullptr;  // [ntri]
+  const int* diag_of = nullptr;            // [ntri] band of a diagonal element
+  double2* fdiag = nullptr;                // [n] f_cc(0,0) of the diagonal
+};
+
+cudaError_t launch_rhs(const DevTables& tb, const DevConsts* cst, const StageArgs& a, cudaStream_t s);
+cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2* rho, double2* h, double2* Xout,
+                           const double2* X0, cudaStream_t s);
+int obs_parts(int nk);
+size_t obs_part_bytes();
+cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,
+                               int want_current, int want_tabs, void* part, double2* tabs3, double scaleJ,
+                               double scaleTA, const ObsRecord& rec, ObsRecord* log, double* ncond_dev,
+                               double* pcmax_dev, cudaStream_t s);
+
+}  // namespace edus

@@ -22,7 +22,7 @@
 
 namespace edus {
 
-static thread_local std::string g_last_error;
+thread_local std::string g_last_error;
 
 int fail(int code, const char* fmt, ...) {
   char buf[1024];
@@ -395,6 +395,8 @@ int read_decoherence_value(const std::vector<std::string>& str, double& out) {
 }  // namespace edus
 
 using namespace edus;
+
+extern "C" const char* edus_last_error(void) { return g_last_error.c_str(); }
 
 extern "C" int edus_params_default(edus_params* p) {
   // Source_Main/variables.cpp:8-123

@@ -1,0 +1,609 @@
+// problem.cpp — builds the host Problem: k grid, b-vector stencil, model
+// tables, dissipation tensor, initial state and Coulomb coefficients.
+//
+// Reference behaviour followed (anpicon/EDUS):
+//   k grid            headers/InitParameters.h:13-40
+//   shells & weights  headers/CalculateWeigths.h:1-138 (weights by least squares
+//                     in extended precision instead of Armadillo pinv)
+//   k+b lookup        headers/CalculateWeigths.h:145-226 (grid arithmetic, then the
+//                     reference's tolerance test on the candidate)
+//   TB models         headers/TightBinding.h:43-173,271-290,387-440,920-1003,1256-1421
+//   Wannier model     headers/Wannier.h:47-148,278-304,336-551
+//   tabulation        Source_Main/save_HUD.cpp:19-53,96-137
+//   T tensor          headers/InitParameters.h:203-224, main_MPI.cpp:66-77
+//   initial state     headers/InitialPopulation.h:2-39
+//   Coulomb files     Source_Main/Fourier_Coulomb.cpp:505-622
+#include "problem.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+namespace edus {
+
+// ------------------------------------------------------------------ linear algebra
+
+int inv_gj(int n, const double* A, double* Ainv) {
+  std::vector<double> a((size_t)n * 2 * n);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < 2 * n; j++) a[i * 2 * n + j] = (j < n) ? A[i * n + j] : (j - n == i ? 1.0 : 0.0);
+  for (int c = 0; c < n; c++) {
+    int piv = c;
+    for (int r = c + 1; r < n; r++)
+      if (std::fabs(a[r * 2 * n + c]) > std::fabs(a[piv * 2 * n + c])) piv = r;
+    if (a[piv * 2 * n + c] == 0.0) return -1;
+    if (piv != c)
+      for (int j = 0; j < 2 * n; j++) std::swap(a[c * 2 * n + j], a[piv * 2 * n + j]);
+    double d = a[c * 2 * n + c];
+    for (int j = 0; j < 2 * n; j++) a[c * 2 * n + j] /= d;
+    for (int r = 0; r < n; r++) {
+      if (r == c) continue;
+      double f = a[r * 2 * n + c];
+      if (f == 0.0) continue;
+      for (int j = 0; j < 2 * n; j++) a[r * 2 * n + j] -= f * a[c * 2 * n + j];
+    }
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) Ainv[i * n + j] = a[i * 2 * n + n + j];
+  return 0;
+}
+
+void eig_herm(int n, cd* A, double* evals, cd* Z) {
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) Z[i * n + j] = (i == j) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 100; sweep++) {
+    double off = 0, diag = 0;
+    for (int i = 0; i < n; i++) {
+      diag += std::norm(A[i * n + i]);
+      for (int j = i + 1; j < n; j++) off += std::norm(A[i * n + j]);
+    }
+    if (off <= 1e-34 * (diag + 1e-300)) break;
+    for (int p = 0; p < n; p++)
+      for (int q = p + 1; q < n; q++) {
+        cd apq = A[p * n + q];
+        double mag = std::abs(apq);
+        if (mag < 1e-300) continue;
+        double app = A[p * n + p].real(), aqq = A[q * n + q].real();
+        cd ph = apq / mag;
+        double theta = 0.5 * std::atan2(2.0 * mag, aqq - app);
+        double c = std::cos(theta), s = std::sin(theta);
+        cd sp = s * ph, sc = s * std::conj(ph);
+        for (int k = 0; k < n; k++) {
+          cd akp = A[k * n + p], akq = A[k * n + q];
+          A[k * n + p] = c * akp - sc * akq;
+          A[k * n + q] = sp * akp + c * akq;
+        }
+        for (int k = 0; k < n; k++) {
+          cd apk = A[p * n + k], aqk = A[q * n + k];
+          A[p * n + k] = c * apk - sp * aqk;
+          A[q * n + k] = sc * apk + c * aqk;
+        }
+        A[p * n + q] = 0;
+        A[q * n + p] = 0;
+        A[p * n + p] = A[p * n + p].real();
+        A[q * n + q] = A[q * n + q].real();
+        for (int k = 0; k < n; k++) {
+          cd zkp = Z[k * n + p], zkq = Z[k * n + q];
+          Z[k * n + p] = c * zkp - sc * zkq;
+          Z[k * n + q] = sp * zkp + c * zkq;
+        }
+      }
+  }
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; i++) ord[i] = i;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return A[a * n + a].real() < A[b * n + b].real(); });
+  std::vector<cd> Zs((size_t)n * n);
+  for (int j = 0; j < n; j++) {
+    evals[j] = A[ord[j] * n + ord[j]].real();
+    for (int i = 0; i < n; i++) Zs[i * n + j] = Z[i * n + ord[j]];
+  }
+  std::copy(Zs.begin(), Zs.end(), Z);
+}
+
+// Least squares min |A w - q| by Householder QR in long double (A: rows x cols).
+static void lstsq(int rows, int cols, const double* A, const double* q, double* w) {
+  std::vector<long double> R((size_t)rows * cols), b(q, q + rows);
+  for (int i = 0; i < rows * cols; i++) R[i] = A[i];
+  for (int c = 0; c < cols; c++) {
+    long double nrm = 0;
+    for (int r = c; r < rows; r++) nrm += R[r * cols + c] * R[r * cols + c];
+    nrm = std::sqrt(nrm);
+    if (nrm == 0) continue;
+    long double alpha = R[c * cols + c] > 0 ? -nrm : nrm;
+    std::vector<long double> v(rows, 0);
+    for (int r = c; r < rows; r++) v[r] = R[r * cols + c];
+    v[c] -= alpha;
+    long double vn = 0;
+    for (int r = c; r < rows; r++) vn += v[r] * v[r];
+    if (vn == 0) continue;
+    for (int j = c; j < cols; j++) {
+      long double d = 0;
+      for (int r = c; r < rows; r++) d += v[r] * R[r * cols + j];
+      d = 2 * d / vn;
+      for (int r = c; r < rows; r++) R[r * cols + j] -= d * v[r];
+    }
+    long double d = 0;
+    for (int r = c; r < rows; r++) d += v[r] * b[r];
+    d = 2 * d / vn;
+    for (int r = c; r < rows; r++) b[r] -= d * v[r];
+  }
+  for (int c = cols - 1; c >= 0; c--) {
+    long double acc = b[c];
+    for (int j = c + 1; j < cols; j++) acc -= R[c * cols + j] * (long double)w[j];
+    long double diag = R[c * cols + c];
+    w[c] = (std::fabs((double)diag) > 1e-300) ? (double)(acc / diag) : 0.0;
+  }
+}
+
+// ------------------------------------------------------------------ geometry
+
+static void crys_to_cart(const Problem& P, const double* c, double* x) {
+  for (int i = 0; i < 3; i++) x[i] = P.M[i][0] * c[0] + P.M[i][1] * c[1] + P.M[i][2] * c[2];
+}
+static void cart_to_crys(const Problem& P, const double* x, double* c) {
+  for (int i = 0; i < 3; i++) c[i] = P.MI[i][0] * x[0] + P.MI[i][1] * x[1] + P.MI[i][2] * x[2];
+}
+
+static int setup_geometry(Problem& P) {
+  double Mf[9], MIf[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      P.M[i][j] = P.p.b[j][i];
+      Mf[i * 3 + j] = P.M[i][j];
+    }
+  if (inv_gj(3, Mf, MIf)) return fail(EDUS_EINVAL, "reciprocal lattice is singular");
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) P.MI[i][j] = MIf[i * 3 + j];
+  const double(*m)[3] = P.M;
+  P.jac = std::fabs(m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                    m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]));
+  const double(*a)[3] = P.p.a;
+  P.det_a = P.p.sample_110 ? std::fabs(a[0][0] * a[1][1] - a[0][1] * a[1][0]) : std::fabs(a[1][1] * a[2][2] - a[1][2] * a[2][1]);
+  const int* Nk = P.p.nk;
+  P.nk = Nk[0] * Nk[1] * Nk[2];
+  P.n1 = Nk[1];
+  P.n2 = Nk[2];
+  for (int c = 0; c < 3; c++) P.dk[c] = 1.0 / Nk[c];
+  P.kpt.assign((size_t)P.nk * 3, 0.0);
+  for (int ik = 0; ik < P.nk; ik++) {
+    int iik[3] = {(ik / (Nk[2] * Nk[1])) % Nk[0], (ik / Nk[2]) % Nk[1], ik % Nk[2]};
+    for (int c = 0; c < 3; c++) P.kpt[ik * 3 + c] = (P.dk[c] != 1.0) ? -0.5 + P.dk[c] * iik[c] : 0.0;
+  }
+  // shells: each new shell is the next larger |k| over the grid points
+  int plane = -1;
+  for (int i = 0; i < 3; i++)
+    if (Nk[i] == 1) plane = i;
+  std::vector<double> nrm(P.nk);
+  for (int ik = 0; ik < P.nk; ik++) {
+    double x[3];
+    crys_to_cart(P, &P.kpt[ik * 3], x);
+    nrm[ik] = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  }
+  std::vector<double> radii{1.e-08};
+  bool enough = false;
+  P.nshell = 0;
+  P.shell_n.clear();
+  P.bvec.clear();
+  P.bshell.clear();
+  while (!enough) {
+    double rad = 1000.;
+    for (int ik = 0; ik < P.nk; ik++) {
+      bool in = false;
+      for (double r : radii) in = in || (nrm[ik] <= r + 1.e-11);
+      if (!in && nrm[ik] < rad) rad = nrm[ik];
+    }
+    radii.push_back(rad);
+    int cnt = 0;
+    for (int ik = 0; ik < P.nk; ik++)
+      if (std::fabs(nrm[ik] - rad) < 1.e-11) {
+        double x[3];
+        crys_to_cart(P, &P.kpt[ik * 3], x);
+        P.bvec.insert(P.bvec.end(), x, x + 3);
+        P.bshell.push_back(P.nshell);
+        cnt++;
+      }
+    P.shell_n.push_back(cnt);
+    P.nshell++;
+    int ns = P.nshell;
+    std::vector<double> A(21 * ns, 0.0);
+    int base = 0;
+    for (int sh = 0; sh < ns; sh++) {
+      const double* bv = &P.bvec[base * 3];
+      int nb = P.shell_n[sh];
+      int row = 0;
+      for (int id = 0; id < 3; id++)
+        if (id != plane) {
+          for (int b = 0; b < nb; b++) A[row * ns + sh] += bv[b * 3 + id] * bv[b * 3 + id];
+          row++;
+        }
+      for (int id = 0; id < 3; id++)
+        for (int jd = id + 1; jd < 3; jd++)
+          if (id != plane && jd != plane) {
+            for (int b = 0; b < nb; b++) A[row * ns + sh] += bv[b * 3 + id] * bv[b * 3 + jd];
+            row++;
+          }
+      row = 5;
+      for (int id = 0; id < 3; id++)
+        for (int jd = id; jd < 3; jd++)
+          for (int ld = jd; ld < 3; ld++)
+            for (int md = ld; md < 3; md++) {
+              for (int b = 0; b < nb; b++) A[row * ns + sh] += bv[b * 3 + id] * bv[b * 3 + jd] * bv[b * 3 + ld] * bv[b * 3 + md];
+              row++;
+            }
+      base += nb;
+    }
+    double q[21] = {0};
+    q[0] = 1;
+    q[1] = 1;
+    q[2] = !(plane + 1);
+    std::vector<double> w(ns, 0.0);
+    lstsq(21, ns, A.data(), q, w.data());
+    double r2 = 0;
+    for (int r = 0; r < 21; r++) {
+      double acc = 0;
+      for (int sh = 0; sh < ns; sh++) acc += A[r * ns + sh] * w[sh];
+      r2 += (acc - q[r]) * (acc - q[r]);
+    }
+    P.shell_w = w;
+    enough = std::sqrt(r2) < 1.e-07;
+    if (P.nshell >= 32 && !enough) return fail(EDUS_EINVAL, "More than 32 shells needed.");
+  }
+  P.nnb = (int)P.bshell.size();
+  // k+b table: index arithmetic on the grid, checked with the reference's test
+  P.nbr.assign((size_t)P.nk * P.nnb, -1);
+  std::vector<int> off((size_t)P.nnb * 3);
+  for (int b = 0; b < P.nnb; b++) {
+    double c[3];
+    cart_to_crys(P, &P.bvec[b * 3], c);
+    for (int i = 0; i < 3; i++) off[b * 3 + i] = (int)std::lround(c[i] * Nk[i]);
+  }
+  int bad = 0;
+  for (int ik = 0; ik < P.nk; ik++) {
+    int iik[3] = {(ik / (Nk[2] * Nk[1])) % Nk[0], (ik / Nk[2]) % Nk[1], ik % Nk[2]};
+    double kk[3];
+    crys_to_cart(P, &P.kpt[ik * 3], kk);
+    for (int b = 0; b < P.nnb; b++) {
+      int j[3];
+      for (int i = 0; i < 3; i++) j[i] = (((iik[i] + off[b * 3 + i]) % Nk[i]) + Nk[i]) % Nk[i];
+      int cand = (j[0] * Nk[1] + j[1]) * Nk[2] + j[2];
+      double x[3] = {kk[0] + P.bvec[b * 3], kk[1] + P.bvec[b * 3 + 1], kk[2] + P.bvec[b * 3 + 2]};
+      double c[3];
+      cart_to_crys(P, x, c);
+      bool ok = true;
+      for (int i = 0; i < 3 && ok; i++) {
+        double ci = std::fmod(c[i] + 0.5, 1.) - 0.5;
+        double d = ci - P.kpt[cand * 3 + i];
+        ok = std::fabs(d) < 1.e-08 || std::fabs(d - 1.) < 1.e-08 || std::fabs(d + 1.) < 1.e-08;
+      }
+      if (!ok) {
+        bad++;
+        cand = ik;
+      }
+      P.nbr[(size_t)ik * P.nnb + b] = cand;
+    }
+  }
+  if (bad) return fail(EDUS_EINVAL, "k+b not found on the grid for %d stencil entries", bad);
+  return 0;
+}
+
+// ------------------------------------------------------------------ models
+
+namespace {
+
+enum TbKind { kHaldaneN = 1, kHaldaneB, kGen2d, kBN };
+
+struct Tb {
+  int kind = 0;
+  double a = 2.5 * kSpaceAAu, b = 3.16 * kEnergyEvAu, g = 6.2 * kEnergyEvAu, t2 = 0, phi0 = 0, core = 0, rchv = 0, rchc = 0;
+};
+
+int tb_setup(const edus_params& p, Tb& t) {
+  std::string nm = p.tb_type;
+  if (nm == "Haldane_CoreBN_Nedge" || nm == "Haldane_CoreBN_Bedge") {
+    t.kind = nm == "Haldane_CoreBN_Nedge" ? kHaldaneN : kHaldaneB;
+    t.g = p.hopping[0];
+    t.b = p.hopping[1];
+    t.t2 = p.hopping[2];
+    t.phi0 = p.hopping[3];
+  } else if (nm == "gen2d_hexagonal") {
+    t.kind = kGen2d;
+    t.a = p.hopping[0];
+    t.g = p.hopping[1];
+    t.b = p.hopping[2];
+    t.t2 = p.hopping[3];
+    t.phi0 = p.hopping[4];
+    t.core = p.hopping[5];
+    t.rchv = p.hopping[6];
+    t.rchc = p.hopping[7];
+  } else if (nm == "BoronNitride") {
+    t.kind = kBN;
+  } else {
+    return fail(EDUS_EUNSUPPORTED, "tight-binding model %s is not built (Haldane_CoreBN_Nedge/Bedge, gen2d_hexagonal, BoronNitride are)", nm.c_str());
+  }
+  return 0;
+}
+
+inline cd eiphi(double x) { return cd(std::cos(x), std::sin(x)); }
+
+// H, U and D of one k for the tight-binding models.
+void tb_eval(const Tb& t, int n, const double* k, cd* H, cd* U, cd* D) {
+  const double k1 = k[1], k2 = k[2];
+  for (int e = 0; e < n * n; e++) {
+    H[e] = 0;
+    U[e] = 0;
+  }
+  for (int e = 0; e < n * n * 3; e++) D[e] = 0;
+  const double tp1 = 2. * kPi * k1, tp2 = 2. * kPi * k2;
+  double Bx = t.b * (1. + std::cos(tp1) + std::cos(tp2));
+  double By = t.b * (std::sin(tp1) + std::sin(tp2));
+  double Bz = -t.g / 2.;
+  int o = 1;
+  if (t.kind == kBN) {
+    o = 0;
+    cd f = (eiphi(tp1) + 1.) + eiphi(tp2);
+    H[0] = -t.g / 2;
+    H[3] = t.g / 2;
+    H[1] = std::conj(f) * t.b;
+    H[2] = f * t.b;
+    D[(1 * n + 1) * 3 + 1] = t.a / std::sqrt(3);
+  } else {
+    H[0] = t.kind == kHaldaneN ? -15.06 : (t.kind == kHaldaneB ? -6.91 : t.core);
+    cd f2 = eiphi(tp1 - tp2) + eiphi(tp2) + eiphi(-tp1);
+    cd f = 1. + eiphi(-tp1) + eiphi(-tp2);
+    H[1 * n + 1] = -t.g / 2. + 2. * (t.t2 * eiphi(t.phi0) * f2).real();
+    H[1 * n + 2] = t.b * f;
+    H[2 * n + 1] = t.b * std::conj(f);
+    H[2 * n + 2] = t.g / 2. + 2. * (t.t2 * eiphi(-t.phi0) * f2).real();
+    Bz = -t.g / 2. - 2. * t.t2 * std::sin(t.phi0) * (std::sin(-tp2 + tp1) + std::sin(tp2) + std::sin(-tp1));
+    U[0] = 1.;
+    double ay = t.a / std::sqrt(3.);
+    auto d = [&](int i, int j, int x) -> cd& { return D[(i * n + j) * 3 + x]; };
+    if (t.kind == kHaldaneN) {
+      d(0, 1, 0) = d(1, 0, 0) = 0.0697595094;
+      d(2, 2, 1) = ay;
+    } else if (t.kind == kHaldaneB) {
+      d(0, 2, 0) = d(2, 0, 0) = 0.0869151662;
+      d(2, 2, 1) = ay;
+      d(0, 0, 1) = ay;
+    } else {
+      d(0, 1, 0) = d(1, 0, 0) = t.rchv;
+      d(0, 2, 0) = d(2, 0, 0) = t.rchc;
+      d(2, 2, 1) = -ay;
+      if (std::fabs(t.rchc) > 1.e-6) d(0, 0, 1) = -ay;
+    }
+  }
+  double B = std::sqrt(Bx * Bx + By * By + Bz * Bz);
+  double phi = std::atan2(By, Bx) / 2.;
+  double c2 = std::sqrt((B + Bz) / 2. / B), s2 = std::sqrt((B - Bz) / 2. / B);
+  U[o * n + o] = eiphi(phi) * s2;
+  U[o * n + o + 1] = -eiphi(-phi) * c2;
+  U[(o + 1) * n + o] = eiphi(phi) * c2;
+  U[(o + 1) * n + o + 1] = eiphi(-phi) * s2;
+}
+
+int read_wannier(Problem& P, const char* workdir) {
+  std::string path = std::string(workdir ? workdir : ".") + "/" + P.p.ref_coord + "_tb.dat";
+  std::ifstream f(path);
+  if (!f) return fail(EDUS_EIO, "No path %s file found.", path.c_str());
+  std::string line;
+  for (int i = 0; i < 4; i++) std::getline(f, line);
+  int nw = 0, nr = 0;
+  f >> nw >> nr;
+  if (!f || nw != P.ncv) return fail(EDUS_EIO, "%s: num_wann %d does not match %d bands", path.c_str(), nw, P.ncv);
+  int n = nw;
+  P.nrpts = nr;
+  std::vector<double> ndeg(nr);
+  for (int i = 0; i < nr; i++) f >> ndeg[i];
+  P.Rvec.assign((size_t)nr * 3, 0);
+  P.HR.assign((size_t)n * n * nr, 0);
+  P.rR.assign((size_t)3 * n * n * nr, 0);
+  for (int iR = 0; iR < nr; iR++) {
+    f >> P.Rvec[iR * 3] >> P.Rvec[iR * 3 + 1] >> P.Rvec[iR * 3 + 2];
+    for (int in = 0; in < n; in++)
+      for (int im = 0; im < n; im++) {
+        int t1, t2;
+        double hr, hi;
+        f >> t1 >> t2 >> hr >> hi;
+        P.HR[((size_t)im * n + in) * nr + iR] = cd(hr / ndeg[iR] * kEnergyEvAu, hi / ndeg[iR] * kEnergyEvAu);
+      }
+  }
+  for (int iR = 0; iR < nr; iR++) {
+    double R[3];
+    f >> R[0] >> R[1] >> R[2];
+    for (int in = 0; in < n; in++)
+      for (int im = 0; im < n; im++) {
+        int t1, t2;
+        double v[6];
+        f >> t1 >> t2 >> v[0] >> v[1] >> v[2] >> v[3] >> v[4] >> v[5];
+        for (int x = 0; x < 3; x++)
+          P.rR[(((size_t)x * n + im) * n + in) * nr + iR] = cd(v[2 * x] / ndeg[iR] * kSpaceAAu, v[2 * x + 1] / ndeg[iR] * kSpaceAAu);
+      }
+  }
+  if (!f) return fail(EDUS_EIO, "%s: truncated _tb.dat", path.c_str());
+  return 0;
+}
+
+int read_coulomb(Problem& P, const char* workdir) {
+  int n = P.ncv, n2 = n * n, c2 = P.ncut * P.ncut;
+  std::string wd = workdir ? workdir : ".";
+  std::string lab = P.p.coulomb_label;
+  {
+    std::string path = wd + "/Output/Coulomb/V_Hartree_" + lab + ".txt";
+    std::ifstream f(path);
+    if (!f) return fail(EDUS_EIO, "cannot read %s", path.c_str());
+    P.VH.assign((size_t)n * n, 0);
+    for (int i = 0; i < n * n; i++) f >> P.VH[i];
+    if (!f) return fail(EDUS_EIO, "truncated %s", path.c_str());
+  }
+  const char* nm[4] = {"A", "B", "C", "D"};
+  std::vector<cd>* dst[4] = {&P.cA, &P.cB, &P.cC, &P.cD};
+  for (int q = 0; q < 4; q++) {
+    std::string path = wd + "/Output/Coulomb/" + nm[q] + "_coeff" + lab + ".txt";
+    std::ifstream f(path);
+    if (!f) return fail(EDUS_EIO, "cannot read %s", path.c_str());
+    dst[q]->assign((size_t)c2 * n2, 0);
+    for (size_t i = 0; i < (size_t)c2 * n2; i++) {
+      double re, im;
+      f >> re >> im;
+      (*dst[q])[i] = cd(re, im);
+    }
+    if (!f) return fail(EDUS_EIO, "truncated %s (need %d x %d complex)", path.c_str(), c2, n2);
+  }
+  {
+    std::string path = wd + "/Output/Coulomb/Screen_const_" + lab + ".txt";
+    std::ifstream f(path);
+    if (!f) return fail(EDUS_EIO, "cannot read %s", path.c_str());
+    P.screen.assign(n2, 0);
+    for (int i = 0; i < n2; i++) {
+      double re, im;
+      f >> re >> im;
+      P.screen[i] = cd(re, im);
+    }
+    if (!f) return fail(EDUS_EIO, "truncated %s", path.c_str());
+  }
+  return 0;
+}
+
+}  // namespace
+
+int build_problem(const edus_params& p, const char* workdir, Problem& P) {
+  P = Problem();
+  P.p = p;
+  P.nch = p.nb[0];
+  P.nv = p.nb[1];
+  P.nc = p.nb[2];
+  P.ncv = P.nch + P.nv + P.nc;
+  P.nbands = P.nch + P.nv;
+  const int n = P.ncv;
+  if (n < 1 || n > EDUS_MAX_BANDS) return fail(EDUS_EINVAL, "band count %d outside 1..%d", n, EDUS_MAX_BANDS);
+  if (p.dt <= 0) return fail(EDUS_EINVAL, "dt must be positive");
+  if (p.solver != EDUS_SOLVER_RK4 && (p.order < 1 || p.order > 8)) return fail(EDUS_EINVAL, "solver order %d out of range", p.order);
+  if (p.solver == EDUS_SOLVER_TAYLOR && p.order < 2) return fail(EDUS_EINVAL, "Taylor order must be >= 2");
+  int rc = setup_geometry(P);
+  if (rc) return rc;
+  const int nk = P.nk;
+  const size_t st = (size_t)nk * n * n;
+  P.H.assign(st, 0);
+  P.U.assign(st, 0);
+  P.D.assign(st * 3, 0);
+  const bool isW = p.mode == EDUS_MODE_WANNIER;
+  Tb tb;
+  if (isW) {
+    rc = read_wannier(P, workdir);
+  } else {
+    rc = tb_setup(p, tb);
+  }
+  if (rc) return rc;
+  std::vector<double> S(n, 0.0);
+  const double gapc = p.conduction_shift;
+  if (gapc > 1e-16)
+    for (int i = 0; i < n; i++)
+      if (i >= p.nb[1]) S[i] = gapc;
+  const int nr = P.nrpts;
+#pragma omp parallel for schedule(static)
+  for (int ik = 0; ik < nk; ik++) {
+    const double* k = &P.kpt[ik * 3];
+    cd Hk[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Uk[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Dk[EDUS_MAX_BANDS * EDUS_MAX_BANDS * 3];
+    if (isW) {
+      std::vector<cd> ph(nr);
+      for (int iR = 0; iR < nr; iR++) {
+        double kR = 0.;
+        for (int l = 0; l < 3; l++) kR += k[l] * P.Rvec[iR * 3 + l];
+        kR *= 2 * kPi;
+        ph[iR] = cd(std::cos(kR), std::sin(kR));
+      }
+      for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+          cd h = 0, d[3] = {0, 0, 0};
+          for (int iR = 0; iR < nr; iR++) {
+            h += ph[iR] * P.HR[((size_t)i * n + j) * nr + iR];
+            for (int x = 0; x < 3; x++) d[x] += ph[iR] * P.rR[(((size_t)x * n + i) * n + j) * nr + iR];
+          }
+          Hk[i * n + j] = (i == j) ? cd(h.real(), 0.) : h;
+          for (int x = 0; x < 3; x++) Dk[(i * n + j) * 3 + x] = (i == j) ? cd(d[x].real(), 0.) : d[x];
+        }
+      cd A[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Z[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+      double ev[EDUS_MAX_BANDS];
+      std::copy(Hk, Hk + n * n, A);
+      eig_herm(n, A, ev, Z);
+      for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) Uk[i * n + j] = std::conj(Z[j * n + i]);
+    } else {
+      tb_eval(tb, n, k, Hk, Uk, Dk);
+    }
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        cd value = 0.;
+        if (gapc > 1e-16)
+          for (int ii = 0; ii < n; ii++) value += std::conj(Uk[ii * n + i]) * S[ii] * Uk[ii * n + j];
+        P.H[((size_t)ik * n + i) * n + j] = Hk[i * n + j] + value;
+        P.U[((size_t)ik * n + i) * n + j] = Uk[i * n + j];
+        for (int x = 0; x < 3; x++)
+          P.D[(((size_t)ik * n + i) * n + j) * 3 + x] =
+              isW ? 0.5 * (Dk[(i * n + j) * 3 + x] + Dk[(j * n + i) * 3 + x]) : Dk[(i * n + j) * 3 + x];
+      }
+  }
+  // gradient of the energy (Source_Main/save_HUD.cpp:96-137)
+  P.GE.assign(st * 3, 0);
+  if (p.current) {
+#pragma omp parallel for schedule(static)
+    for (int ik = 0; ik < nk; ik++)
+      for (int x = 0; x < 3; x++)
+        for (int i = 0; i < n; i++)
+          for (int j = 0; j < n; j++) {
+            cd acc = 0;
+            for (int b = 0; b < P.nnb; b++) {
+              int kb = P.nbr[(size_t)ik * P.nnb + b];
+              acc += P.shell_w[P.bshell[b]] * P.bvec[b * 3 + x] * (P.H[((size_t)kb * n + i) * n + j] - P.H[((size_t)ik * n + i) * n + j]);
+            }
+            P.GE[(((size_t)ik * n + i) * n + j) * 3 + x] = acc;
+          }
+  }
+  // dissipation tensor
+  const int nch = P.nch;
+  for (int ic = nch; ic < n; ic++)
+    for (int jc = nch; jc < n; jc++) P.T[ic][jc] = (ic == jc) ? p.T1 : p.T2;
+  for (int ic = 0; ic < nch; ic++) {
+    for (int jc = 0; jc < nch; jc++) P.T[ic][jc] = p.Tch;
+    for (int jc = nch; jc < n; jc++) P.T[ic][jc] = p.Tch / 2.;
+  }
+  for (int ic = 0; ic < n; ic++)
+    for (int jc = ic + 1; jc < n; jc++) P.T[jc][ic] = P.T[ic][jc];
+  for (int ic = 0; ic < n; ic++)
+    for (int jc = 0; jc < n; jc++)
+      if (std::fabs(P.T[ic][jc]) > 1e-24) {
+        P.diss_i.push_back(ic);
+        P.diss_j.push_back(jc);
+      }
+  // initial population (rows/columns swapped as in the reference)
+  P.P0.assign(st, 0);
+  for (int ik = 0; ik < nk; ik++)
+    for (int ia = 0; ia < n; ia++)
+      for (int ib = 0; ib < n; ib++) {
+        cd acc = 0;
+        for (int ii = 0; ii < P.nbands; ii++) acc += P.U[((size_t)ik * n + ii) * n + ia] * std::conj(P.U[((size_t)ik * n + ii) * n + ib]);
+        P.P0[((size_t)ik * n + ia) * n + ib] = acc;
+      }
+  // Coulomb
+  if (p.coulomb) {
+    if (p.diag_basis) return fail(EDUS_EUNSUPPORTED, "Coulomb_diag_basis is not built (Wannier-basis Coulomb is)");
+    if (!p.read_from_files)
+      return fail(EDUS_EUNSUPPORTED, "Coulomb coefficients must be read from files (Read_Coulomb_from_files)");
+    if (p.ncut < 1 || p.ncut > 64) return fail(EDUS_EINVAL, "Ncut %d out of range", p.ncut);
+    if (P.n1 != P.n2) return fail(EDUS_EINVAL, "Coulomb needs a square in-plane grid (Coulomb.h:285)");
+    P.ncut = p.ncut;
+    rc = read_coulomb(P, workdir);
+    if (rc) return rc;
+  }
+  // time grid (Source_Main/const_dt_evolution.cpp:1-10)
+  P.t_start = -0.21 / kTimeAuFs;
+  P.itfi = (int)((p.t_fin - P.t_start) / p.dt);
+  P.nsteps = P.itfi + 1;
+  int res = p.it_resolution > 0 ? p.it_resolution : 1;
+  P.nprint = P.itfi / res + 1;
+  return 0;
+}
+
+}  // namespace edus

@@ -1,0 +1,234 @@
+"""ctypes bindings of libedus_b200.so (include/edus_b200.h)."""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+class EdusError(RuntimeError):
+    def __init__(self, code, where, message):
+        super().__init__(f"{where}: {message} (code {code})")
+        self.code = code
+
+
+def library_path():
+    return os.path.join(_HERE, "libedus_b200.so")
+
+
+def load_library():
+    """Load the in-tree library; raise (never fall back) if it is absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise EdusError(-1, "load_library", f"{path} is missing; run `python -m edus_b200.build`")
+    L = C.CDLL(path)
+    vp, i32, dbl, cp, sz = C.c_void_p, C.c_int32, C.c_double, C.c_char_p, C.c_size_t
+    P = C.POINTER
+    sigs = {
+        "edus_parse_input": (C.c_int, [cp, P(abi.Params)]),
+        "edus_params_default": (C.c_int, [P(abi.Params)]),
+        "edus_problem_create": (C.c_int, [P(abi.Params), cp, P(vp)]),
+        "edus_problem_info_get": (C.c_int, [vp, P(abi.ProblemInfo)]),
+        "edus_problem_get": (C.c_int, [vp, cp, vp, sz]),
+        "edus_problem_free": (None, [vp]),
+        "edus_options_default": (C.c_int, [P(abi.Options)]),
+        "edus_create": (C.c_int, [vp, P(abi.Options), P(vp)]),
+        "edus_destroy": (None, [vp]),
+        "edus_set_state": (C.c_int, [vp, vp]),
+        "edus_get_state": (C.c_int, [vp, vp]),
+        "edus_step": (C.c_int, [vp, i32]),
+        "edus_run": (C.c_int, [vp]),
+        "edus_clock": (C.c_int, [vp, P(i32), P(dbl), P(dbl)]),
+        "edus_obs_count": (C.c_int, [vp, P(i32)]),
+        "edus_obs_get": (C.c_int, [vp, i32, i32, P(abi.Obs)]),
+        "edus_observables": (C.c_int, [vp, P(abi.Obs)]),
+        "edus_write_outputs": (C.c_int, [vp, cp]),
+        "edus_last_timing": (C.c_int, [vp, P(dbl), P(C.c_int64)]),
+        "edus_get_derivative": (C.c_int, [vp, i32, P(dbl), dbl, i32]),
+        "edus_runge_kutta_ad": (C.c_int, [vp, i32, i32, dbl]),
+        "edus_runge_kutta_ac": (C.c_int, [vp, i32, dbl]),
+        "edus_slot_copy": (C.c_int, [vp, i32, i32]),
+        "edus_slot_set": (C.c_int, [vp, i32, vp]),
+        "edus_slot_get": (C.c_int, [vp, i32, vp]),
+        "edus_coulomb_hk": (C.c_int, [vp, i32, vp]),
+        "edus_strerror": (cp, [C.c_int]),
+        "edus_last_error": (cp, []),
+        "edus_abi_version": (C.c_int, []),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = L
+    return L
+
+
+def _check(rc, where):
+    if rc != 0:
+        L = load_library()
+        msg = L.edus_last_error().decode(errors="replace") or L.edus_strerror(rc).decode()
+        raise EdusError(rc, where, msg)
+
+
+def default_params():
+    L = load_library()
+    p = abi.Params()
+    _check(L.edus_params_default(C.byref(p)), "edus_params_default")
+    return p
+
+
+def parse_input(path):
+    L = load_library()
+    p = abi.Params()
+    _check(L.edus_parse_input(os.fsencode(path), C.byref(p)), "edus_parse_input")
+    return p
+
+
+class Problem:
+    """Host-side problem (grid, stencil, model tables, initial state)."""
+
+    def __init__(self, params, workdir="."):
+        L = load_library()
+        self._L = L
+        self.params = params
+        self._h = C.c_void_p()
+        _check(L.edus_problem_create(C.byref(params), os.fsencode(workdir), C.byref(self._h)), "edus_problem_create")
+        self.info = abi.ProblemInfo()
+        _check(L.edus_problem_info_get(self._h, C.byref(self.info)), "edus_problem_info_get")
+
+    def get(self, name):
+        i = self.info
+        n, nk = i.ncv, i.nk
+        shapes = {
+            "kpt": ((nk, 3), np.float64),
+            "H": ((nk, n, n), np.complex128),
+            "U": ((nk, n, n), np.complex128),
+            "D": ((nk, n, n, 3), np.complex128),
+            "GE": ((nk, n, n, 3), np.complex128),
+            "P0": ((nk, n, n), np.complex128),
+            "nbr": ((nk, i.nnb), np.int32),
+            "bvec": ((i.nnb, 3), np.float64),
+            "weights": ((i.nnb,), np.float64),
+            "T": ((16, 16), np.float64),
+            "HR": ((n, n, i.nrpts), np.complex128),
+            "rR": ((3, n, n, i.nrpts), np.complex128),
+            "Rvec": ((i.nrpts, 3), np.float64),
+        }
+        shp, dt = shapes[name]
+        a = np.zeros(shp, dtype=dt)
+        _check(self._L.edus_problem_get(self._h, name.encode(), a.ctypes.data, a.nbytes), f"edus_problem_get({name})")
+        return a
+
+    def close(self):
+        if self._h:
+            self._L.edus_problem_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """Device context: all state resident on one GPU."""
+
+    def __init__(self, problem, device=0, precision=-1):
+        L = load_library()
+        self._L = L
+        self.problem = problem
+        o = abi.Options()
+        _check(L.edus_options_default(C.byref(o)), "edus_options_default")
+        o.device = device
+        o.precision = precision
+        self._h = C.c_void_p()
+        _check(L.edus_create(problem._h, C.byref(o), C.byref(self._h)), "edus_create")
+        self.n = problem.info.ncv
+        self.nk = problem.info.nk
+
+    def _state_buf(self):
+        return np.zeros((self.nk, self.n, self.n), dtype=np.complex128)
+
+    def get_state(self):
+        a = self._state_buf()
+        _check(self._L.edus_get_state(self._h, a.ctypes.data), "edus_get_state")
+        return a
+
+    def set_state(self, rho):
+        a = np.ascontiguousarray(rho, dtype=np.complex128)
+        _check(self._L.edus_set_state(self._h, a.ctypes.data), "edus_set_state")
+
+    def step(self, nsteps):
+        _check(self._L.edus_step(self._h, int(nsteps)), "edus_step")
+
+    def run(self):
+        _check(self._L.edus_run(self._h), "edus_run")
+
+    def clock(self):
+        it, t, dt = C.c_int32(), C.c_double(), C.c_double()
+        _check(self._L.edus_clock(self._h, C.byref(it), C.byref(t), C.byref(dt)), "edus_clock")
+        return it.value, t.value, dt.value
+
+    def obs(self):
+        n = C.c_int32()
+        _check(self._L.edus_obs_count(self._h, C.byref(n)), "edus_obs_count")
+        buf = (abi.Obs * max(n.value, 1))()
+        _check(self._L.edus_obs_get(self._h, 0, n.value, buf), "edus_obs_get")
+        return [abi.obs_to_dict(buf[i], self.n) for i in range(n.value)]
+
+    def observables(self):
+        o = abi.Obs()
+        _check(self._L.edus_observables(self._h, C.byref(o)), "edus_observables")
+        return abi.obs_to_dict(o, self.n)
+
+    def write_outputs(self, outdir):
+        _check(self._L.edus_write_outputs(self._h, os.fsencode(outdir)), "edus_write_outputs")
+
+    def last_timing(self):
+        ms, launches = C.c_double(), C.c_int64()
+        _check(self._L.edus_last_timing(self._h, C.byref(ms), C.byref(launches)), "edus_last_timing")
+        return ms.value, launches.value
+
+    # ODE_solver-level mirror ---------------------------------------------
+    def get_derivative(self, slot, EF, wx2, e_non0):
+        ef = (C.c_double * 6)(*[float(x) for x in np.asarray(EF).ravel()])
+        _check(self._L.edus_get_derivative(self._h, int(slot), ef, float(wx2), int(e_non0)), "edus_get_derivative")
+
+    def slot_set(self, slot, rho):
+        a = np.ascontiguousarray(rho, dtype=np.complex128)
+        _check(self._L.edus_slot_set(self._h, int(slot), a.ctypes.data), "edus_slot_set")
+
+    def slot_get(self, slot):
+        a = self._state_buf()
+        _check(self._L.edus_slot_get(self._h, int(slot), a.ctypes.data), "edus_slot_get")
+        return a
+
+    def runge_kutta_ad(self, src, dst, dt):
+        _check(self._L.edus_runge_kutta_ad(self._h, int(src), int(dst), float(dt)), "edus_runge_kutta_ad")
+
+    def runge_kutta_ac(self, dst, dt):
+        _check(self._L.edus_runge_kutta_ac(self._h, int(dst), float(dt)), "edus_runge_kutta_ac")
+
+    def coulomb_hk(self, slot):
+        a = self._state_buf()
+        _check(self._L.edus_coulomb_hk(self._h, int(slot), a.ctypes.data), "edus_coulomb_hk")
+        return a
+
+    def close(self):
+        if self._h:
+            self._L.edus_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,189 @@
+"""Synthetic workloads in the reference's input.txt format.
+
+Each function writes an input.txt (and any model / Coulomb files it needs)
+into a work directory and returns the path of the input file. Fields are
+converted with the reference's own constants: E0 [a.u.] = E [V/A] * 1e10 /
+5.14221e11 and I [W/cm^2] = E0^2 * 3.51e16 (headers/Laser.h:29-31).
+
+  hbn_rk4        config 0: Haldane_CoreBN_Nedge (core band decoupled), RK4, no Coulomb
+  hbn_coulomb    config 1: same model with the Rytova–Keldysh mean field from the
+                 shipped Ncut=20 coefficient files, Adams–Bashforth 4
+  wannier        config 2: synthetic nb-band Wannier model (seeded), RK4
+"""
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TIME_FS_AU = 1.0 / 0.02418884326505
+EV_AU = 1.0 / 27.211396
+EFIELD_AU_PER_V_A = 1e10 / 5.14221e11
+COULOMB_LABEL = "G_num502657_Ncut20_"
+
+
+def intensity_wcm2(e_v_per_a):
+    e0 = e_v_per_a * EFIELD_AU_PER_V_A
+    return e0 * e0 * 3.51e16
+
+
+def _pump(photon_ev, field_v_a, duration_fs, pol="0 0 1", phase=0.0):
+    wl = photon_ev * EV_AU
+    period_fs = 2 * math.pi / wl / TIME_FS_AU
+    cycles = duration_fs / period_fs
+    return (
+        "laserpump sin2 {\n"
+        f"frequency {wl:.12g}\n"
+        f"intensity {intensity_wcm2(field_v_a):.12g} wcm2\n"
+        f"cycles {cycles:.12g}\n"
+        f"polarization {pol}\n"
+        f"phase {phase:.12g}\n"
+        "}\n"
+    )
+
+
+def write_coulomb_files(workdir, label=COULOMB_LABEL):
+    """Output/Coulomb/* in the reference's text format from the packaged data."""
+    d = np.load(os.path.join(HERE, "data", "coulomb_ncut20.npz"))
+    cdir = os.path.join(workdir, "Output", "Coulomb")
+    os.makedirs(cdir, exist_ok=True)
+    for q in "ABCD":
+        a = d[q]
+        with open(os.path.join(cdir, f"{q}_coeff{label}.txt"), "w") as f:
+            for row in a:
+                f.write("".join(f"{v.real:.20e}    {v.imag:.20e}    " for v in row) + "\n")
+    with open(os.path.join(cdir, f"Screen_const_{label}.txt"), "w") as f:
+        for v in d["screen"]:
+            f.write(f"{v.real:.20g} {v.imag:.20g}\n")
+    with open(os.path.join(cdir, f"V_Hartree_{label}.txt"), "w") as f:
+        for row in d["vhartree"]:
+            f.write("".join(f"{v:.20g}    " for v in row) + "\n")
+    return cdir
+
+
+def hbn_rk4(workdir, n=60, field=0.3, photon=0.4, duration=30.0, dt_fs=0.01, t_fin_fs=None, it_res=1,
+            solver="", gap=5.8, t1=2.3, extra_tdse="", probe=""):
+    os.makedirs(workdir, exist_ok=True)
+    t_fin = duration if t_fin_fs is None else t_fin_fs
+    txt = (
+        "HBN\n\n"
+        "tdse{\n"
+        f"tightbinding Haldane_CoreBN_Nedge gap= {gap} t1= {t1} t2= 0 phi0= 0\n"
+        f"dt {dt_fs} fs\n"
+        f"t_fin {t_fin} fs\n"
+        f"{solver}{extra_tdse}"
+        "}\n\n"
+        f"nkpt{{\n1 {n} {n}\n}}\n\n"
+        + _pump(photon, field, duration)
+        + probe
+        + "\nobservables{\n"
+        "Current\n"
+        f"it_resolution {it_res}\n"
+        "}\n"
+    )
+    path = os.path.join(workdir, "input.txt")
+    with open(path, "w") as f:
+        f.write(txt)
+    return path
+
+
+def hbn_coulomb(workdir, n=120, field=0.5, photon=0.4, duration=30.0, dt_fs=0.005, t_fin_fs=None, it_res=10, ab_order=4,
+                rk4_startup=True):
+    os.makedirs(workdir, exist_ok=True)
+    write_coulomb_files(workdir)
+    solver = f"Adams_Bashforth {ab_order}\n" + ("Adams_Bashforth_RK4_startup\n" if rk4_startup else "")
+    path = hbn_rk4(workdir, n=n, field=field, photon=photon, duration=duration, dt_fs=dt_fs, t_fin_fs=t_fin_fs,
+                   it_res=it_res, solver=solver)
+    with open(path, "a") as f:
+        f.write(
+            "\nCoulomb{\n"
+            "qTF 0.01\n"
+            "Ncut 20\n"
+            "epsilon_static 1.0\n"
+            "Rytova_Keldysh\n"
+            "Read_Coulomb_from_files\n"
+            f"labelInput {COULOMB_LABEL}\n"
+            "}\n"
+        )
+    return path
+
+
+def write_wannier_tb(path, nw=8, nside=11, seed=12345, a_ang=2.5, decay_h=1.5, decay_r=1.0, onsite_ev=3.0):
+    """Synthetic Wannier90 _tb.dat: H(R) complex Gaussian x exp(-|R|/decay_h a),
+    hermitised H(-R) = H(R)^dagger, onsite energies uniform in +-onsite_ev;
+    r(R) the same with exp(-|R|/decay_r a). Square lattice, R = (0, R1, R2)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    h = nside // 2
+    Rs = [(0, r1, r2) for r1 in range(-h, h + 1) for r2 in range(-h, h + 1)]
+    idx = {R: i for i, R in enumerate(Rs)}
+    nr = len(Rs)
+    HR = np.zeros((nr, nw, nw), complex)
+    rR = np.zeros((3, nr, nw, nw), complex)
+    for i, R in enumerate(Rs):
+        neg = idx[(0, -R[1], -R[2])]
+        if neg < i:
+            continue
+        dist = math.hypot(R[1], R[2])
+        g = (rng.standard_normal((nw, nw)) + 1j * rng.standard_normal((nw, nw))) / math.sqrt(2)
+        g *= math.exp(-dist / decay_h)
+        gr = (rng.standard_normal((3, nw, nw)) + 1j * rng.standard_normal((3, nw, nw))) / math.sqrt(2)
+        gr *= 0.5 * math.exp(-dist / decay_r)
+        if neg == i:  # R = 0
+            g = 0.5 * (g + g.conj().T)
+            np.fill_diagonal(g, rng.uniform(-onsite_ev, onsite_ev, nw))
+            gr = 0.5 * (gr + gr.conj().transpose(0, 2, 1))
+            for x in range(3):
+                np.fill_diagonal(gr[x], np.real(np.diag(gr[x])))
+            HR[i] = g
+            rR[:, i] = gr
+        else:
+            HR[i] = g
+            HR[neg] = g.conj().T
+            rR[:, i] = gr
+            rR[:, neg] = gr.conj().transpose(0, 2, 1)
+    with open(path, "w") as f:
+        f.write("synthetic tight-binding model (written by edus_b200.workloads)\n")
+        f.write(f"  {10.0:.8f} 0 0\n  0 {a_ang:.8f} 0\n  0 0 {a_ang:.8f}\n")
+        f.write(f"{nw}\n{nr}\n")
+        for i in range(nr):
+            f.write("    1" + ("\n" if (i + 1) % 15 == 0 else ""))
+        f.write("\n")
+        for i, R in enumerate(Rs):
+            f.write(f"\n{R[0]} {R[1]} {R[2]}\n")
+            for n_ in range(nw):
+                for m in range(nw):
+                    v = HR[i, m, n_]
+                    f.write(f"{m + 1} {n_ + 1} {v.real:.16e} {v.imag:.16e}\n")
+        for i, R in enumerate(Rs):
+            f.write(f"\n{R[0]} {R[1]} {R[2]}\n")
+            for n_ in range(nw):
+                for m in range(nw):
+                    x, y, z = rR[0, i, m, n_], rR[1, i, m, n_], rR[2, i, m, n_]
+                    f.write(f"{m + 1} {n_ + 1} {x.real:.16e} {x.imag:.16e} {y.real:.16e} {y.imag:.16e} {z.real:.16e} {z.imag:.16e}\n")
+    return path
+
+
+def wannier(workdir, nw=8, nside=11, n=96, field=0.4, photon=0.3, duration=40.0, dt_fs=0.01, t_fin_fs=None, it_res=10,
+            seed=12345, name="W8"):
+    os.makedirs(workdir, exist_ok=True)
+    write_wannier_tb(os.path.join(workdir, f"{name}_tb.dat"), nw=nw, nside=nside, seed=seed)
+    nv = nw // 2
+    t_fin = duration if t_fin_fs is None else t_fin_fs
+    txt = (
+        f"{name}\n\n"
+        "unitcell angstrom {\n10.0 0 0\n0 2.5 0\n0 0 2.5\n}\n\n"
+        f"bands{{\nvalence {nv}\nconduction {nw - nv}\n}}\n\n"
+        "tdse{\nWannier\n"
+        f"dt {dt_fs} fs\n"
+        f"t_fin {t_fin} fs\n"
+        "}\n\n"
+        f"nkpt{{\n1 {n} {n}\n}}\n\n"
+        + _pump(photon, field, duration)
+        + "\nobservables{\nCurrent\n"
+        f"it_resolution {it_res}\n"
+        "}\n"
+    )
+    path = os.path.join(workdir, "input.txt")
+    with open(path, "w") as f:
+        f.write(txt)
+    return path

@@ -1253,7 +1253,12 @@ static void observables(orc* o, const cplx* P, edus_obs* ob) {
 /* ------------------------------------------------------------ time loop */
 
 /* Source_Main/RungeKutta.cpp:1-197 (one RK4 step, incl. E_non0 bookkeeping) */
-static void step_rk4(orc* o) {
+static void step_rk4_ring(orc* o, int store_ring);
+static void step_rk4(orc* o) { step_rk4_ring(o, 0); }
+/* store_ring: RK4 start-up of Adams–Bashforth (an option the reference does
+ * not have; its AB starts from a zero history): the first-stage derivative is
+ * kept in the AB ring so the multistep formula has a true history. */
+static void step_rk4_ring(orc* o, int store_ring) {
   int n = o->ncv;
   double dt = o->dt, dt6 = dt / 6.0, dt3 = dt / 3.0, dt2 = dt / 2.0;
   double wx2 = o->p.probe.wl;
@@ -1263,6 +1268,7 @@ static void step_rk4(orc* o) {
   double t = o->time_loop;
   field_at(o, t, o->EF);
   rhs(o, o->P0, o->Pv, o->EF, wx2, o->e_non0);
+  if (store_ring) memcpy(o->ring + (size_t)o->nk * n * n * o->ring_idx[0], o->Pv, sizeof(cplx) * (size_t)o->nk * n * n);
   rk_ad(o, o->P0, o->P1, o->Pv, dt6);
   rk_ad(o, o->P0, o->P2, o->Pv, dt2);
   field_at(o, t + dt2, o->EF);
@@ -1294,6 +1300,10 @@ static void step_ab(orc* o) {
   int fill = o->ring_idx[p - 1];
   for (int s = p - 1; s > 0; s--) o->ring_idx[s] = o->ring_idx[s - 1];
   o->ring_idx[0] = fill;
+  if (o->p.ab_rk4_startup && o->it < p - 1) {
+    step_rk4_ring(o, 1);
+    return;
+  }
   rhs(o, o->P0, o->Pv, o->EF, o->p.probe.wl, o->e_non0);
   size_t st = (size_t)o->nk * n * n;
   memcpy(o->ring + st * o->ring_idx[0], o->Pv, sizeof(cplx) * st);

@@ -8,8 +8,11 @@ Writes (all small, committed):
   ab5_golden.npz         its Output/{J1,J2,Losses,EF,TransientAbs}.txt, every
                          4th output row (830 of 3319), at printed precision
   test_matrices.npz      H, U, dx, dy at k=(0,0.3,0.1) from Test_matrices.txt
-  coulomb_ncut20.npz     Output/Coulomb/{A,B,C,D}_coeff, Screen_const and
-                         V_Hartree for G_num=502657, Ncut=20 (3 bands)
+  ../../edus_b200/data/coulomb_ncut20.npz
+                         Output/Coulomb/{A,B,C,D}_coeff, Screen_const and
+                         V_Hartree for G_num=502657, Ncut=20 (3 bands); the
+                         Coulomb workload (config 1) reads it, so it ships
+                         with the package
 """
 import os
 import re
@@ -80,7 +83,7 @@ def main(ref):
     sc = rows(os.path.join(c, f"Screen_const_{lab}.txt"))
     coef["screen"] = sc[:, 0] + 1j * sc[:, 1]
     coef["vhartree"] = rows(os.path.join(c, f"V_Hartree_{lab}.txt"))
-    np.savez_compressed(os.path.join(HERE, "coulomb_ncut20.npz"), label=lab, **coef)
+    np.savez_compressed(os.path.join(HERE, "..", "..", "edus_b200", "data", "coulomb_ncut20.npz"), label=lab, **coef)
     print("wrote fixtures to", HERE)
 
 
