@@ -100,7 +100,8 @@ struct edus_ctx {
   double2 *d_h = nullptr, *d_X0 = nullptr;
   CoulDev cd{};
   void* d_part = nullptr;
-  double2* d_tabs3 = nullptr;
+  unsigned int* d_done = nullptr;
+  int* d_err = nullptr;  // device error word set by bounded waits
   edus_obs* d_log = nullptr;
   int log_cap = 0, nlog = 0;
   double* d_ncond = nullptr;
@@ -119,6 +120,29 @@ struct edus_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
   long long launches = 0, last_launches = 0;
+  // per-kernel event timing
+  bool profiling = false;
+  cudaEvent_t prof_open[2]{};
+  struct ProfPair {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfPair> prof_pairs;
+  // CUDA graph of the whole constant-dt loop from it = 0 (captured once, replayed after edus_reset)
+  bool use_graphs = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  long long graph_launches = 0;
+  double2* d_Pinit = nullptr;
+  double2 *P0_start = nullptr, *Pa_start = nullptr;
+  struct HostClock {
+    int it, nlog;
+    double time_loop, dt;
+    double EF[2][3];
+    bool e_non0;
+    int ring_idx[kMaxOrder];
+    double2 *P0, *Pa;
+  } after_graph{};
 };
 
 namespace {
@@ -195,19 +219,35 @@ StageArgs base_args(edus_ctx* c) {
   return a;
 }
 
+// Per-kernel event timing (edus_profile): kind 0 = RHS + stage update, 1 = Coulomb transform pair.
+int prof_mark(edus_ctx* c, int kind, bool begin) {
+  if (!c->profiling) return 0;
+  cudaEvent_t ev;
+  CK(cudaEventCreate(&ev));
+  CK(cudaEventRecord(ev, c->stream));
+  if (begin)
+    c->prof_open[kind] = ev;
+  else
+    c->prof_pairs.push_back({kind, c->prof_open[kind], ev});
+  return 0;
+}
+
 int run_coulomb(edus_ctx* c, const double2* src) {
   if (!c->coul) return 0;
+  int rc = prof_mark(c, 1, true);
+  if (rc) return rc;
   CK(launch_coulomb(c->tb, c->cd, src, c->d_h, nullptr, c->d_X0, c->stream));
   c->launches += 2;
-  return 0;
+  return prof_mark(c, 1, false);
 }
 
 int rhs(edus_ctx* c, StageArgs& a) {
   int rc = run_coulomb(c, a.src);
   if (rc) return rc;
+  if ((rc = prof_mark(c, 0, true))) return rc;
   CK(launch_rhs(c->tb, c->d_cst, a, c->stream));
   c->launches++;
-  return 0;
+  return prof_mark(c, 0, false);
 }
 
 void set_ef(StageArgs& a, const double EF[2][3]) {
@@ -229,8 +269,8 @@ int observe(edus_ctx* c) {
   double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
   double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
   CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, c->d_part,
-                        c->d_tabs3, scaleJ, scaleTA, rec, slot, c->d_ncond, c->d_pcmax, c->stream));
-  c->launches += 2 + ((c->P.p.tabs && c->P.nch > 0) ? 1 : 0);
+                        c->d_done, scaleJ, scaleTA, rec, slot, c->d_ncond, c->d_pcmax, c->stream));
+  c->launches += 1;
   c->nlog++;
   return 0;
 }
@@ -430,15 +470,66 @@ int run_steps(edus_ctx* c, int nsteps, bool all) {
 int timed(edus_ctx* c, int nsteps, bool all) {
   CK(cudaSetDevice(c->device));
   long long l0 = c->launches;
-  CK(cudaEventRecord(c->ev0, c->stream));
-  int rc = run_steps(c, nsteps, all);
-  if (rc) return rc;
+  const bool graph = all && !c->dyn && c->use_graphs && c->it == 0;
+  if (graph && !c->gexec) {
+    // capture the whole loop once; the captured kernels run at cudaGraphLaunch below
+    c->P0_start = c->d_P0;
+    c->Pa_start = c->d_Pa;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = run_steps(c, nsteps, all);
+    cudaGraph_t g = nullptr;
+    cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ec != cudaSuccess) return fail(EDUS_ECUDA, "stream capture: %s", cudaGetErrorString(ec));
+    c->graph = g;
+    CK(cudaGraphInstantiate(&c->gexec, g, 0));
+    c->graph_launches = c->launches - l0;
+    auto& h = c->after_graph;
+    h.it = c->it;
+    h.nlog = c->nlog;
+    h.time_loop = c->time_loop;
+    h.dt = c->dt;
+    memcpy(h.EF, c->EF, sizeof(h.EF));
+    h.e_non0 = c->e_non0;
+    memcpy(h.ring_idx, c->ring_idx, sizeof(h.ring_idx));
+    h.P0 = c->d_P0;
+    h.Pa = c->d_Pa;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    CK(cudaGraphLaunch(c->gexec, c->stream));
+  } else if (graph) {
+    // replay from the state edus_reset restored; advance the host clock as the capture did
+    CK(cudaEventRecord(c->ev0, c->stream));
+    CK(cudaGraphLaunch(c->gexec, c->stream));
+    c->launches += c->graph_launches;
+    const auto& h = c->after_graph;
+    c->it = h.it;
+    c->nlog = h.nlog;
+    c->time_loop = h.time_loop;
+    c->dt = h.dt;
+    memcpy(c->EF, h.EF, sizeof(h.EF));
+    c->e_non0 = h.e_non0;
+    memcpy(c->ring_idx, h.ring_idx, sizeof(h.ring_idx));
+    c->d_P0 = h.P0;
+    c->d_Pa = h.Pa;
+  } else {
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = run_steps(c, nsteps, all);
+    if (rc) return rc;
+  }
+  {
+  }
   CK(cudaEventRecord(c->ev1, c->stream));
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last_ms = ms;
   c->last_launches = c->launches - l0;
+  int derr = 0;
+  CK(cudaMemcpy(&derr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (derr) return fail(EDUS_ETIMEOUT, "a bounded device wait ran out (error word %d)", derr);
   CK(cudaGetLastError());
   return 0;
 }
@@ -474,7 +565,7 @@ int edus_options_default(edus_options* o) {
   memset(o, 0, sizeof(*o));
   o->device = 0;
   o->precision = -1;
-  o->use_graphs = 0;
+  o->use_graphs = 1;
   o->health_checks = 0;
   o->trace_tol = 1e-6;
   o->hbm_budget_bytes = 0;
@@ -576,11 +667,27 @@ int edus_problem_get(const edus_problem* pb, const char* name, void* dst, size_t
 
 void edus_problem_free(edus_problem* pb) { delete pb; }
 
+int edus_model_hud(const edus_problem* pb, const double kcrys[3], double* H, double* U, double* D) {
+  if (!pb || !kcrys || !H || !U || !D) return fail(EDUS_EINVAL, "null argument");
+  return model_hud(pb->P, kcrys, (cd*)H, (cd*)U, (cd*)D);
+}
+
+int edus_struct_sizes(int64_t out[4]) {
+  if (!out) return fail(EDUS_EINVAL, "null argument");
+  out[0] = sizeof(edus_params);
+  out[1] = sizeof(edus_obs);
+  out[2] = sizeof(edus_problem_info);
+  out[3] = sizeof(edus_options);
+  return 0;
+}
+
 void edus_destroy(edus_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (void* p : c->allocs) cudaFree(p);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->graph) cudaGraphDestroy(c->graph);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -614,8 +721,8 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   c->ntri = nt;
   c->nk = nk;
   c->plane = (size_t)nt * nk;
-  if (n != 1 && n != 2 && n != 3 && n != 4 && n != 5 && n != 6 && n != 8)
-    return bail(fail(EDUS_EUNSUPPORTED, "band count %d has no FP64 kernel instance (1-6, 8)", n));
+  if (n != 1 && n != 2 && n != 3 && n != 4 && n != 5 && n != 8)
+    return bail(fail(EDUS_EUNSUPPORTED, "band count %d has no FP64 kernel instance (1-5, 8)", n));
   if (P.nnb > kMaxNb) return bail(fail(EDUS_EUNSUPPORTED, "stencil with %d neighbours (max %d)", P.nnb, kMaxNb));
   c->solver = P.p.solver;
   c->order = P.p.solver == EDUS_SOLVER_RK4 ? 0 : P.p.order;
@@ -684,11 +791,18 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
     return bail(fail(EDUS_ECUDA, "memset ring"));
   for (int i = 0; i < kMaxOrder; i++) c->ring_idx[i] = i;
   if ((rc = state_to_dev(c, (const double*)P.P0.data(), c->d_P0))) return bail(rc);
+  if ((rc = dalloc(c, &c->d_Pinit, c->plane))) return bail(rc);
+  if (cudaMemcpyAsync(c->d_Pinit, c->d_P0, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+    return bail(fail(EDUS_ECUDA, "copy initial state"));
+  c->use_graphs = o.use_graphs != 0;
   // ---- observables
-  if ((rc = dalloc(c, (char**)&c->d_part, obs_parts(nk) * obs_part_bytes())) || (rc = dalloc(c, &c->d_tabs3, 3)) ||
-      (rc = dalloc(c, &c->d_ncond, 1)) || (rc = dalloc(c, &c->d_pcmax, 1)) || (rc = dalloc(c, &c->d_maxdp, 1)))
+  if ((rc = dalloc(c, (char**)&c->d_part, obs_parts(nk) * obs_part_bytes())) || (rc = dalloc(c, &c->d_done, 1)) ||
+      (rc = dalloc(c, &c->d_ncond, 1)) || (rc = dalloc(c, &c->d_pcmax, 1)) || (rc = dalloc(c, &c->d_maxdp, 1)) ||
+      (rc = dalloc(c, &c->d_err, 1)))
     return bail(rc);
   cudaMemsetAsync(c->d_ncond, 0, sizeof(double), c->stream);
+  cudaMemsetAsync(c->d_done, 0, sizeof(unsigned int), c->stream);
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
   cudaMemsetAsync(c->d_pcmax, 0, sizeof(double), c->stream);
   c->log_cap = P.p.dynamical_dt ? 1 << 16 : P.nprint + 2;
   if ((rc = dalloc(c, &c->d_log, c->log_cap))) return bail(rc);
@@ -708,6 +822,7 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   tb.U = dU;
   tb.GE = dGE;
   tb.nbr = dnbr;
+  tb.err = c->d_err;
   tb.n_diss = (int)P.diss_i.size();
   // ---- Coulomb
   if (c->coul) {
@@ -735,6 +850,26 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
     cudaMemcpyAsync(d1s, t1s.data(), sizeof(double) * t1s.size(), cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(d2c, t2c.data(), sizeof(double) * t2c.size(), cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(d2s, t2s.data(), sizeof(double) * t2s.size(), cudaMemcpyHostToDevice, c->stream);
+    // bulk-copy layouts: t2T [n2][2 ncut] and t1P [2][ncut][n1|1], both padded to 16 bytes
+    std::vector<double> t2T(coulomb_t2T_count(n2, nc), 0.0), t1P(coulomb_t1P_count(n1, nc), 0.0);
+    for (int i2 = 0; i2 < n2; i2++)
+      for (int m = 0; m < nc; m++) {
+        t2T[(size_t)i2 * 2 * nc + m] = t2c[(size_t)m * n2 + i2];
+        t2T[(size_t)i2 * 2 * nc + nc + m] = t2s[(size_t)m * n2 + i2];
+      }
+    const int ld = n1 | 1;
+    for (int m = 0; m < nc; m++)
+      for (int i1 = 0; i1 < n1; i1++) {
+        t1P[(size_t)m * ld + i1] = t1c[(size_t)m * n1 + i1];
+        t1P[(size_t)(nc + m) * ld + i1] = t1s[(size_t)m * n1 + i1];
+      }
+    double *d2T, *d1P;
+    if ((rc = dalloc(c, &d2T, t2T.size())) || (rc = dalloc(c, &d1P, t1P.size()))) return bail(rc);
+    cudaMemcpyAsync(d2T, t2T.data(), sizeof(double) * t2T.size(), cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(d1P, t1P.data(), sizeof(double) * t1P.size(), cudaMemcpyHostToDevice, c->stream);
+    c->cd.t2T = d2T;
+    c->cd.t1P = d1P;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "upload trig tables"));
     std::vector<double2> cf[4];
     const std::vector<cd>* src[4] = {&P.cA, &P.cB, &P.cC, &P.cD};
     std::vector<unsigned char> isd(nt);
@@ -797,6 +932,7 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
       return bail(fail(EDUS_ECUDA, "copy PW0"));
     if (cudaMemcpyAsync(c->d_hr, dH, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
       return bail(fail(EDUS_ECUDA, "copy Hr"));
+    if (coulomb_prepare(tb) != cudaSuccess) return bail(fail(EDUS_EUNSUPPORTED, "Coulomb tables exceed shared memory"));
     if (launch_coulomb(tb, c->cd, c->d_P0, nullptr, c->d_X0, nullptr, c->stream) != cudaSuccess)
       return bail(fail(EDUS_ECUDA, "equilibrium Coulomb pass"));
     std::vector<double2> fd(n);
@@ -824,6 +960,34 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   c->n_cond = c->dyn ? std::pow(10, -16) : 0;
   c->P_cond_max = 0;
   *out = c;
+  return 0;
+}
+
+int edus_reset(edus_ctx* c) {
+  if (!c) return fail(EDUS_EINVAL, "null argument");
+  CK(cudaSetDevice(c->device));
+  if (c->P0_start) {
+    c->d_P0 = c->P0_start;
+    c->d_Pa = c->Pa_start;
+  }
+  CK(cudaMemcpyAsync(c->d_P0, c->d_Pinit, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
+  if (c->d_ring) CK(cudaMemsetAsync(c->d_ring, 0, sizeof(double2) * c->order * c->plane, c->stream));
+  CK(cudaMemsetAsync(c->d_ncond, 0, sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_pcmax, 0, sizeof(double), c->stream));
+  if (c->coul) CK(cudaMemcpyAsync(c->d_hr, c->tb.H, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->it = 0;
+  c->time_loop = c->P.t_start;
+  c->dt = c->P.p.dt;
+  for (int i = 0; i < kMaxOrder; i++) {
+    c->ring_idx[i] = i;
+    c->dt_prev[i] = c->P.p.dt;
+  }
+  memset(c->EF, 0, sizeof(c->EF));
+  c->e_non0 = true;
+  c->n_cond = c->dyn ? std::pow(10, -16) : 0;
+  c->P_cond_max = 0;
+  c->nlog = 0;
   return 0;
 }
 
@@ -946,9 +1110,37 @@ int edus_observables(edus_ctx* c, edus_obs* out) {
   double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
   double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
   CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, c->d_part,
-                        c->d_tabs3, scaleJ, scaleTA, rec, tmp, nullptr, nullptr, c->stream));
+                        c->d_done, scaleJ, scaleTA, rec, tmp, nullptr, nullptr, c->stream));
   CK(cudaMemcpyAsync(out, tmp, sizeof(edus_obs), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int edus_profile(edus_ctx* c, int32_t nsteps, double* rhs_ms, int64_t* rhs_launches, double* coul_ms,
+                 int64_t* coul_launches) {
+  if (!c || nsteps < 0) return fail(EDUS_EINVAL, "bad argument");
+  CK(cudaSetDevice(c->device));
+  c->profiling = true;
+  c->prof_pairs.clear();
+  int rc = run_steps(c, nsteps, false);
+  c->profiling = false;
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  double t[2] = {0, 0};
+  int64_t n[2] = {0, 0};
+  for (auto& p : c->prof_pairs) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, p.a, p.b));
+    t[p.kind] += ms;
+    n[p.kind]++;
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+  }
+  c->prof_pairs.clear();
+  if (rhs_ms) *rhs_ms = t[0];
+  if (rhs_launches) *rhs_launches = n[0];
+  if (coul_ms) *coul_ms = t[1];
+  if (coul_launches) *coul_launches = n[1];
   return 0;
 }
 

@@ -38,6 +38,45 @@ __host__ __device__ __forceinline__ int tri_index(int i, int j, int n) {
   return i * n - (i * (i - 1)) / 2 + (j - i);
 }
 
+// ------------------------------------------------------------- async bulk copies
+// 1-D TMA bulk copies global -> shared completing on an mbarrier. Addresses
+// and sizes must be multiples of 16 bytes. Waits are bounded: a wait that runs
+// out records kErrTimeout in *err and returns false instead of spinning on.
+constexpr int kErrTimeout = 1;
+constexpr int kBulkWaitIters = 1 << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t phase, int* err) {
+  for (int it = 0; it < kBulkWaitIters; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  if (err) atomicExch(err, kErrTimeout);
+  return false;
+}
+
 constexpr int kMaxBands = 16;
 constexpr int kMaxTri = kMaxBands * (kMaxBands + 1) / 2;
 constexpr int kMaxNb = 64;
@@ -61,6 +100,7 @@ struct DevTables {
   const double2* fdiag;  // [n] f_cc(0,0) diagonal (Hartree input)
   const double2* PW0;    // [ntri][nk] initial state (screen correction)
   const double* ncond;   // device scalar: Coulomb_set.n_cond
+  int* err;              // device error word (kErrTimeout from bounded waits)
 };
 
 // Per-problem constants small enough for a kernel parameter block.
@@ -105,6 +145,7 @@ struct StageArgs {
   // adaptive dt: max over k of the population change, written as uint64 bits
   unsigned long long* maxdp;
   double pcond_plus_ncond;  // P_cond_max + n_cond
+  int stage_rows;           // set by the launcher: k-grid rows of Coulomb tables staged per block
 };
 
 }  // namespace edus

@@ -1,20 +1,16 @@
-// fp64.cu — FP64 kernels of the k-space density-matrix propagation (sm_100a).
+// fp64.cu — Coulomb transform and observable kernels (FP64, sm_100a).
 //
-// k_rhs<N>       one thread per k point: builds H~ = H + E.D (+ Coulomb X + Hartree),
-//                evaluates -i[H~, rho] (headers/RungeKutta.h:158-212), the RWA term
-//                (:209), dissipation (:219-254), the k-gradient stencil (:258-276),
-//                hermitizes (:283-294) and applies the stage update of the integrator
-//                in the same pass (RK4 headers/RungeKutta.h:301-355 +
-//                Source_Main/RungeKutta.cpp; Adams–Bashforth
-//                Source_Main/Linear_Multistep_ODE_solvers.cpp:57-94; Taylor
-//                Source_Main/Taylor_DE_solver_deriv_Polynom.cpp:100-177). Pv never
-//                touches HBM.
-// k_coul_rows    first half of the separable truncated Fourier transform of rho over
-//                the k grid (headers/Coulomb.h:300-350 restated as two 1-D passes).
-// k_coul_modes   second pass + combination with A,B,C,D (Coulomb.h:424-466) + first
-//                pass of the inverse transform (Coulomb.h:510-541).
-// k_obs / k_obs_final  populations (Observables_MPI.h:217-484), J1/J2 (:668-775),
-//                transient absorption (:559-598), reduced in a fixed block order.
+// k_coul_rows    first pass of the separable truncated Fourier transform of rho
+//                over the k grid (headers/Coulomb.h:300-350 restated as two 1-D
+//                passes): g[i1][cs][n][e] = sum_i2 rho_e(i1,i2) {cos,sin}(2 pi n k2).
+//                One block per k-grid row; the row and the trig table sit in
+//                shared memory and every thread owns whole dot products.
+// k_coul_modes   second pass + combination with A,B,C,D (Coulomb.h:424-466) and
+//                the first pass of the inverse transform (Coulomb.h:510-541).
+// k_obs          populations (Observables_MPI.h:217-484), J1/J2 (:668-775) and the
+//                transient absorption (:559-598) per k; the last block to finish
+//                reduces the per-block partials in a fixed order and writes the
+//                output record (no second launch, no host round trip).
 #include <cstdio>
 
 #include "dev.cuh"
@@ -22,21 +18,14 @@
 
 namespace edus {
 
-// ----------------------------------------------------------------------- helpers
-
 template <int N>
 struct Tri {
   static constexpr int NT = N * (N + 1) / 2;
   static __device__ __forceinline__ int idx(int i, int j) { return i * N - (i * (i - 1)) / 2 + (j - i); }
 };
 
-__device__ __forceinline__ void atomic_max_pos(unsigned long long* p, double v) {
-  // non-negative doubles order like their bit patterns
-  atomicMax(p, (unsigned long long)__double_as_longlong(v));
-}
-
-// Hermitian eigenvectors by cyclic Jacobi (device copy of the host routine);
-// Z columns are eigenvectors, eigenvalues ascending.
+// Hermitian eigenvectors by cyclic Jacobi; Z columns are eigenvectors,
+// eigenvalues ascending (Armadillo eig_sym in Observables_MPI.h:294).
 template <int N>
 __device__ void eig_herm_dev(double2* A, double2* Z) {
   for (int i = 0; i < N; i++)
@@ -80,7 +69,6 @@ __device__ void eig_herm_dev(double2* A, double2* Z) {
         }
       }
   }
-  // insertion sort of columns by eigenvalue
   for (int i = 1; i < N; i++) {
     int j = i;
     while (j > 0 && A[(j - 1) * N + (j - 1)].x > A[j * N + j].x) {
@@ -97,322 +85,112 @@ __device__ void eig_herm_dev(double2* A, double2* Z) {
   }
 }
 
-// ----------------------------------------------------------------------- RHS + update
-
-template <int N>
-__global__ void __launch_bounds__(128) k_rhs(DevTables tb, const DevConsts* __restrict__ cst, StageArgs a) {
-  constexpr int NT = Tri<N>::NT;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nk = tb.nk;
-  if (k >= nk) return;
-  const int nch = tb.nch;
-
-  double2 P[NT];
-#pragma unroll
-  for (int e = 0; e < NT; e++) P[e] = a.src[(size_t)e * nk + k];
-
-  // H~ (Hermitian, upper) = H + Coulomb X + Hartree
-  double2 Hu[NT];
-#pragma unroll
-  for (int e = 0; e < NT; e++) Hu[e] = tb.H[(size_t)e * nk + k];
-  if (tb.h) {
-    const int i1 = k / tb.n2, i2 = k - (k / tb.n2) * tb.n2;
-    const int nc = tb.ncut;
-    const double2* hrow = tb.h + (size_t)i1 * 2 * nc * NT;
-    double2 Y[NT];
-#pragma unroll
-    for (int e = 0; e < NT; e++) Y[e] = cz();
-    for (int m = 0; m < nc; m++) {
-      const double cn = tb.t2c[m * tb.n2 + i2], sn = tb.t2s[m * tb.n2 + i2];
-      const double2* hc = hrow + (size_t)m * NT;
-      const double2* hs = hrow + (size_t)(nc + m) * NT;
-#pragma unroll
-      for (int e = 0; e < NT; e++) {
-        double2 c = hc[e], s = hs[e];
-        Y[e].x += c.x * cn + s.x * sn;
-        Y[e].y += c.y * cn + s.y * sn;
-      }
-    }
-    const bool screen = *tb.ncond > 1e-20;
-    // Hartree shift E_H[a] = sum_j Re f_cc(0,0)_jj VH[a][j] - E_H0[a]
-#pragma unroll
-    for (int i = 0; i < N; i++)
-#pragma unroll
-      for (int j = i; j < N; j++) {
-        const int e = Tri<N>::idx(i, j);
-        double2 X = cmk(-Y[e].x, Y[e].y);  // conj(-Y)
-        if (screen) {
-          double2 dP = csub(P[e], tb.PW0[(size_t)e * nk + k]);
-          X = csub(X, cmul(cst->screen[e], cconj(dP)));
-        }
-        if (i == j) {
-          X.y = 0.;
-          double eh = 0.;
-#pragma unroll
-          for (int jj = 0; jj < N; jj++) eh += tb.fdiag[jj].x * cst->VH[i * N + jj];
-          eh -= cst->EH0[i];
-          Hu[e] = cadd(Hu[e], X);
-          Hu[e].x += eh;
-        } else {
-          Hu[e] = cadd(Hu[e], X);
-        }
-      }
-    if (a.hr_out) {
-#pragma unroll
-      for (int e = 0; e < NT; e++) a.hr_out[(size_t)e * nk + k] = Hu[e];
-    }
-  }
-
-  // field-dressed H~F[i][j] = H~[i][j] + EF[w] . D[i][j], w = probe iff exactly one index is core
-  double2 HF[N * N];
-#pragma unroll
-  for (int i = 0; i < N; i++)
-#pragma unroll
-    for (int j = 0; j < N; j++) {
-      const int lo = i < j ? i : j, hi = i < j ? j : i;
-      const int e = Tri<N>::idx(lo, hi);
-      double2 h = (i <= j) ? Hu[e] : cconj(Hu[e]);
-      const int w = (i >= nch && j < nch) || (i < nch && j >= nch);
-      const double2 d0 = tb.D[(size_t)(0 * NT + e) * nk + k];
-      const double2 d1 = tb.D[(size_t)(1 * NT + e) * nk + k];
-      const double2 d2 = tb.D[(size_t)(2 * NT + e) * nk + k];
-      h = cadd(h, cscale(d0, a.EF[w][0]));
-      h = cadd(h, cscale(d1, a.EF[w][1]));
-      h = cadd(h, cscale(d2, a.EF[w][2]));
-      HF[i * N + j] = h;
-    }
-  auto Pf = [&](int i, int j) -> double2 { return (i <= j) ? P[Tri<N>::idx(i, j)] : cconj(P[Tri<N>::idx(j, i)]); };
-
-  double2 Pv[NT];
-  // populations: Pv_ii = 2 Im sum_j H~F[i][j] P[i][j]
-#pragma unroll
-  for (int i = 0; i < N; i++) {
-    double2 beta = cz();
-#pragma unroll
-    for (int j = 0; j < N; j++) beta = cadd(beta, cmul(HF[i * N + j], Pf(i, j)));
-    Pv[Tri<N>::idx(i, i)] = cmk(2. * beta.y, 0.);
-  }
-  // coherences: Pv_ij = -i sum_l (H~F[j][l] P[i][l] - conj(H~F[i][l] P[j][l]))
-#pragma unroll
-  for (int i = 0; i < N; i++)
-#pragma unroll
-    for (int j = i + 1; j < N; j++) {
-      double2 beta = cz();
-#pragma unroll
-      for (int l = 0; l < N; l++) {
-        double2 x = cmul(HF[j * N + l], Pf(i, l));
-        double2 y = cmul(HF[i * N + l], Pf(j, l));
-        beta = cadd(beta, csub(x, cconj(y)));
-      }
-      double2 v = cmi(beta);
-      if (i < nch && j >= nch) v = cadd(v, cmi(cscale(P[Tri<N>::idx(i, j)], -a.wx2)));
-      Pv[Tri<N>::idx(i, j)] = v;
-    }
-  // dissipation (Wannier gauge)
-  if (tb.n_diss > 0) {
-    double2 Uk[N * N];
-#pragma unroll
-    for (int e = 0; e < N * N; e++) Uk[e] = tb.U[(size_t)e * nk + k];
-    double2 Mk[N * N];
-#pragma unroll
-    for (int e = 0; e < N * N; e++) Mk[e] = cz();
-    for (int t = 0; t < tb.n_diss; t++) {
-      const int ii = cst->diss_i[t], jj = cst->diss_j[t];
-      double2 m = cz();
-#pragma unroll
-      for (int i = 0; i < N; i++)
-#pragma unroll
-        for (int j = 0; j < N; j++) m = cadd(m, cmul(cmulc(Uk[jj * N + j], Uk[ii * N + i]), Pf(i, j)));
-      Mk[ii * N + jj] = m;
-    }
-#pragma unroll
-    for (int i = 0; i < N; i++)
-#pragma unroll
-      for (int j = i; j < N; j++) {
-        double2 v = Pv[Tri<N>::idx(i, j)];
-        for (int t = 0; t < tb.n_diss; t++) {
-          const int ii = cst->diss_i[t], jj = cst->diss_j[t];
-          // hU[j][jj] = conj(U[jj][j])
-          double2 hu = cconj(Uk[jj * N + j]);
-          double2 f = cscale(cmulc(hu, Uk[i * N + ii]), cst->T[ii * N + jj]);
-          v = csub(v, cmul(f, Mk[ii * N + jj]));
-        }
-        double2 tii = cz();
-        for (int q = 0; q < tb.nbands; q++) {
-          // hU[j][q] * conj(hU[i][q]) = conj(U[q][j]) * U[q][i]
-          double2 f = cmulc(Uk[q * N + i], Uk[q * N + j]);
-          tii = cadd(tii, cscale(f, cst->T[q * N + q]));
-        }
-        Pv[Tri<N>::idx(i, j)] = cadd(v, tii);
-      }
-  }
-  // k-gradient: sum_b (w_b E_pump . b) rho(k+b)
-  if (a.e_non0) {
-    double2 G[NT];
-#pragma unroll
-    for (int e = 0; e < NT; e++) G[e] = cz();
-    for (int b = 0; b < tb.nnb; b++) {
-      const int kb = tb.nbr[(size_t)b * nk + k];
-      const double c0 = cst->wb[b] * a.EF[0][0] * cst->bvec[b][0];
-      const double c1 = cst->wb[b] * a.EF[0][1] * cst->bvec[b][1];
-      const double c2 = cst->wb[b] * a.EF[0][2] * cst->bvec[b][2];
-#pragma unroll
-      for (int e = 0; e < NT; e++) {
-        const double2 pn = a.src[(size_t)e * nk + kb];
-        G[e] = cadd(G[e], cscale(pn, c0));
-        G[e] = cadd(G[e], cscale(pn, c1));
-        G[e] = cadd(G[e], cscale(pn, c2));
-      }
-    }
-#pragma unroll
-    for (int e = 0; e < NT; e++) Pv[e] = cadd(Pv[e], G[e]);
-  }
-  // hermitize: diagonal real
-#pragma unroll
-  for (int i = 0; i < N; i++) Pv[Tri<N>::idx(i, i)].y = 0.;
-
-  // ---- stage update
-  double dpmax = 0.;
-  switch (a.op) {
-    case OP_PV:
-#pragma unroll
-      for (int e = 0; e < NT; e++) a.dst[(size_t)e * nk + k] = Pv[e];
-      break;
-    case OP_RK_FIRST:
-#pragma unroll
-      for (int e = 0; e < NT; e++) {
-        if (a.ring) a.ring[((size_t)a.ring_idx[0] * NT + e) * nk + k] = Pv[e];  // RK4 start-up of AB
-        const double2 b0 = a.base[(size_t)e * nk + k];
-        a.acc[(size_t)e * nk + k] = cadd(b0, cscale(Pv[e], a.c1));
-        a.dst[(size_t)e * nk + k] = cadd(b0, cscale(Pv[e], a.c2));
-      }
-      break;
-    case OP_RK_MID:
-#pragma unroll
-      for (int e = 0; e < NT; e++) {
-        const double2 b0 = a.base[(size_t)e * nk + k];
-        a.acc[(size_t)e * nk + k] = cadd(a.acc[(size_t)e * nk + k], cscale(Pv[e], a.c1));
-        a.dst[(size_t)e * nk + k] = cadd(b0, cscale(Pv[e], a.c2));
-      }
-      break;
-    case OP_RK_LAST:
-#pragma unroll
-      for (int e = 0; e < NT; e++) {
-        const double2 nv = cadd(a.acc[(size_t)e * nk + k], cscale(Pv[e], a.c1));
-        if (a.maxdp) {
-#pragma unroll
-          for (int i = 0; i < N; i++)
-            if (e == Tri<N>::idx(i, i)) {
-              const double2 old = a.dst[(size_t)e * nk + k];
-              double v = 2 * hypot(old.x - nv.x, old.y - nv.y) / (a.pcond_plus_ncond + hypot(nv.x, nv.y) + 1.0e-7);
-              dpmax = fmax(dpmax, v);
-            }
-        }
-        a.dst[(size_t)e * nk + k] = nv;
-      }
-      break;
-    case OP_AB:
-#pragma unroll
-      for (int e = 0; e < NT; e++) {
-        a.ring[((size_t)a.ring_idx[0] * NT + e) * nk + k] = Pv[e];
-        double2 d = cz();
-        for (int s = 0; s < a.order; s++) {
-          const double2 f = (s == 0) ? Pv[e] : a.ring[((size_t)a.ring_idx[s] * NT + e) * nk + k];
-          d = cadd(d, cscale(f, a.coef[s]));
-        }
-        a.dst[(size_t)e * nk + k] = cadd(a.src[(size_t)e * nk + k], cscale(d, a.dt));
-      }
-      break;
-    case OP_TAYLOR: {
-      const int TO = a.order, m = TO - 1;
-#pragma unroll
-      for (int e = 0; e < NT; e++) {
-        a.ring[((size_t)a.ring_idx[0] * NT + e) * nk + k] = Pv[e];
-        const double2 f0 = Pv[e];
-        double2 dP[kMaxOrder];
-        for (int i = 0; i < m; i++) dP[i] = csub(f0, a.ring[((size_t)a.ring_idx[i + 1] * NT + e) * nk + k]);
-        double2 d = cscale(f0, a.dt);
-        for (int i = 1; i < TO; i++) {
-          double2 al = cz();
-          for (int q = 0; q < m; q++) al = cadd(al, cscale(dP[q], a.tinv[(i - 1) * m + q]));
-          const double2 inc = cscale(cscale(al, a.tpow[i]), 1.0 / (double)(i + 1));
-          d = cadd(d, inc);
-        }
-        const double2 old = a.src[(size_t)e * nk + k];
-        const double2 nv = cadd(old, d);
-        if (a.maxdp) {
-#pragma unroll
-          for (int i = 0; i < N; i++)
-            if (e == Tri<N>::idx(i, i)) {
-              double v = 2 * hypot(old.x - nv.x, old.y - nv.y) / (a.pcond_plus_ncond + hypot(nv.x, nv.y) + 1.0e-7);
-              dpmax = fmax(dpmax, v);
-            }
-        }
-        a.dst[(size_t)e * nk + k] = nv;
-      }
-    } break;
-  }
-  if (a.maxdp) {
-    for (int o = 16; o > 0; o >>= 1) dpmax = fmax(dpmax, __shfl_xor_sync(0xffffffffu, dpmax, o));
-    if ((threadIdx.x & 31) == 0) atomic_max_pos(a.maxdp, dpmax);
-  }
-}
-
 // ----------------------------------------------------------------------- Coulomb
 
-// g[i1][cs][n][e] = sum_i2 rho_e(i1,i2) {cos,sin}(2 pi n k2(i2))
-__global__ void k_coul_rows(const double2* __restrict__ rho, int nk, int n1, int n2, int ntri, int ncut,
-                            const double* __restrict__ t2c, const double* __restrict__ t2s, double2* __restrict__ g) {
+constexpr int kRowThreads = 256;
+
+// grid (n1), block kRowThreads: g[i1][cs][n][e] = sum_i2 rho_e(i1,i2) t_n(i2).
+// The row of rho (all elements) and the k2 trig table (transposed to [i2][cs*ncut+n])
+// are staged in shared memory; each thread owns whole dot products.
+__global__ void __launch_bounds__(kRowThreads) k_coul_rows(const double2* __restrict__ rho, int nk, int n1, int n2, int ntri,
+                                                           int ncut, const double* __restrict__ t2T, double2* __restrict__ g,
+                                                           int* __restrict__ err) {
+  extern __shared__ double2 srow[];  // [ntri][n2] then trig [n2][2 ncut] doubles
+  __shared__ unsigned long long bar;
   const int i1 = blockIdx.x;
-  const int nout = 2 * ncut * ntri;
-  for (int o = threadIdx.x; o < nout; o += blockDim.x) {
-    const int e = o % ntri;
-    const int cn = o / ntri;  // cs * ncut + n
-    const int cs = cn / ncut, n = cn - cs * ncut;
-    const double* t = (cs == 0 ? t2c : t2s) + (size_t)n * n2;
-    const double2* r = rho + (size_t)e * nk + (size_t)i1 * n2;
-    double sx = 0, sy = 0;
-    for (int i2 = 0; i2 < n2; i2++) {
-      const double2 v = r[i2];
-      const double tv = t[i2];
-      sx += v.x * tv;
-      sy += v.y * tv;
+  const int nq = 2 * ncut;
+  double* st = reinterpret_cast<double*>(srow + (size_t)ntri * n2);
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t row_bytes = (uint32_t)n2 * sizeof(double2);
+    const uint32_t trig_bytes = ((uint32_t)(n2 * nq * sizeof(double)) + 15u) & ~15u;
+    mbar_expect_tx(&bar, (uint32_t)ntri * row_bytes + trig_bytes);
+    for (int e = 0; e < ntri; e++) bulk_g2s(srow + (size_t)e * n2, rho + (size_t)e * nk + (size_t)i1 * n2, row_bytes, &bar);
+    bulk_g2s(st, t2T, trig_bytes, &bar);
+  }
+  mbar_wait(&bar, 0, err);
+  for (int o = threadIdx.x; o < ntri * nq; o += kRowThreads) {
+    const int e = o / nq, q = o - e * nq;
+    const double2* r = srow + (size_t)e * n2;
+    double ax = 0, ay = 0, bx = 0, by = 0;
+    int i2 = 0;
+    for (; i2 + 1 < n2; i2 += 2) {
+      const double2 v0 = r[i2], v1 = r[i2 + 1];
+      const double t0 = st[i2 * nq + q], t1 = st[(i2 + 1) * nq + q];
+      ax += v0.x * t0;
+      ay += v0.y * t0;
+      bx += v1.x * t1;
+      by += v1.y * t1;
     }
-    g[((size_t)i1 * 2 * ncut + cn) * ntri + e] = cmk(sx, sy);
+    if (i2 < n2) {
+      const double2 v0 = r[i2];
+      const double t0 = st[i2 * nq + q];
+      ax += v0.x * t0;
+      ay += v0.y * t0;
+    }
+    g[((size_t)q * ntri + e) * n1 + i1] = cmk(ax + bx, ay + by);  // column-contiguous for k_coul_modes
   }
 }
 
+constexpr int kModeThreads = 128;
+
 // One block per (n, e): f_xy(m,n,e) over m, X_xy = combine(A,B,C,D) - X0,
-// h(i1, {c,s}, n, e) = sum_m X t_m(i1).
-__global__ void k_coul_modes(const double2* __restrict__ g, int n1, int ntri, int ncut, double invN,
-                             const double* __restrict__ t1c, const double* __restrict__ t1s,
-                             const double2* __restrict__ cA, const double2* __restrict__ cB,
-                             const double2* __restrict__ cC, const double2* __restrict__ cD,
-                             const double2* __restrict__ X0, const unsigned char* __restrict__ is_diag,
-                             double2* __restrict__ h, double2* __restrict__ Xout, double2* __restrict__ fdiag,
-                             const int* __restrict__ diag_of) {
+// h(i1, {c,s}, n, e) = sum_m X t_m(i1). The k1 trig tables and the g column
+// are staged in shared memory.
+__global__ void __launch_bounds__(kModeThreads) k_coul_modes(const double2* __restrict__ g, int n1, int ntri, int ncut,
+                                                             double invN, const double* __restrict__ t1P, int* __restrict__ err,
+                                                             const double2* __restrict__ cA,
+                                                             const double2* __restrict__ cB, const double2* __restrict__ cC,
+                                                             const double2* __restrict__ cD, const double2* __restrict__ X0,
+                                                             const unsigned char* __restrict__ is_diag, double2* __restrict__ h,
+                                                             double2* __restrict__ Xout, double2* __restrict__ fdiag,
+                                                             const int* __restrict__ diag_of) {
   const int n = blockIdx.x, e = blockIdx.y;
   extern __shared__ double2 sm[];
-  double2* f = sm;               // [4][ncut]: cc, cs, sc, ss
-  double2* X = sm + 4 * ncut;    // [4][ncut]
+  double2* gc = sm;           // [2][n1] column of g for this (n, e)
+  double2* f = gc + 2 * n1;   // [4][ncut]: cc, cs, sc, ss
+  double2* X = f + 4 * ncut;  // [4][ncut]
+  const int ld = n1 | 1;  // odd row stride: per-m reads across threads hit distinct banks
+  double* tc = reinterpret_cast<double*>(X + 4 * ncut);  // [ncut][ld] (host-padded copy of cos)
+  double* ts = tc + (size_t)ncut * ld;                     // [ncut][ld] (sin)
   const double PI = 3.14159265358979323846;
-  for (int o = threadIdx.x; o < 4 * ncut; o += blockDim.x) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t col_bytes = (uint32_t)n1 * sizeof(double2);
+    const uint32_t trig_bytes = ((uint32_t)(2 * ncut * ld * sizeof(double)) + 15u) & ~15u;
+    mbar_expect_tx(&bar, 2 * col_bytes + trig_bytes);
+    bulk_g2s(gc, g + ((size_t)n * ntri + e) * n1, col_bytes, &bar);
+    bulk_g2s(gc + n1, g + ((size_t)(ncut + n) * ntri + e) * n1, col_bytes, &bar);
+    bulk_g2s(tc, t1P, trig_bytes, &bar);
+  }
+  mbar_wait(&bar, 0, err);
+  for (int o = threadIdx.x; o < 4 * ncut; o += kModeThreads) {
     const int xy = o / ncut, m = o - xy * ncut;
-    const double* t = (xy < 2 ? t1c : t1s) + (size_t)m * n1;
-    const int ycs = xy & 1;  // second letter: 0 = c (g cos), 1 = s (g sin)
-    double sx = 0, sy = 0;
-    for (int i1 = 0; i1 < n1; i1++) {
-      const double2 v = g[((size_t)i1 * 2 * ncut + ycs * ncut + n) * ntri + e];
-      sx += v.x * t[i1];
-      sy += v.y * t[i1];
+    const double* t = (xy < 2 ? tc : ts) + (size_t)m * ld;
+    const double2* gv = gc + (xy & 1) * n1;
+    double ax = 0, ay = 0, bx = 0, by = 0;
+    int i1 = 0;
+    for (; i1 + 1 < n1; i1 += 2) {
+      const double2 v0 = gv[i1], v1 = gv[i1 + 1];
+      ax += v0.x * t[i1];
+      ay += v0.y * t[i1];
+      bx += v1.x * t[i1 + 1];
+      by += v1.y * t[i1 + 1];
+    }
+    if (i1 < n1) {
+      ax += gv[i1].x * t[i1];
+      ay += gv[i1].y * t[i1];
     }
     const double corr = -4 * PI * PI * (double)(m * m + n * n) * invN / 27.0;
     const double sc = invN * (1. + corr);
-    f[o] = cmk(sx * sc, sy * sc);
+    f[o] = cmk((ax + bx) * sc, (ay + by) * sc);
   }
   __syncthreads();
   const bool dg = is_diag[e];
-  for (int m = threadIdx.x; m < ncut; m += blockDim.x) {
+  for (int m = threadIdx.x; m < ncut; m += kModeThreads) {
     const size_t mm = (size_t)m * ncut + n;
     const double2 A = cA[mm * ntri + e], D = cD[mm * ntri + e];
     const double2 fcc = f[0 * ncut + m], fcs = f[1 * ncut + m], fsc = f[2 * ncut + m], fss = f[3 * ncut + m];
@@ -447,18 +225,18 @@ __global__ void k_coul_modes(const double2* __restrict__ g, int n1, int ntri, in
   if (n == 0 && dg && threadIdx.x == 0 && fdiag) fdiag[diag_of[e]] = f[0];
   __syncthreads();
   if (!h) return;
-  for (int o = threadIdx.x; o < 2 * n1; o += blockDim.x) {
+  for (int o = threadIdx.x; o < 2 * n1; o += kModeThreads) {
     const int cs = o / n1, i1 = o - cs * n1;
-    double2 acc = cz();
+    double ax = 0, ay = 0;
     // cs = 0: sum_m X_cc c_m + X_sc s_m ; cs = 1: sum_m X_cs c_m + X_ss s_m
     const double2* Xc = X + (cs == 0 ? 0 : 1) * ncut;
     const double2* Xs = X + (cs == 0 ? 2 : 3) * ncut;
     for (int m = 0; m < ncut; m++) {
-      const double c = t1c[(size_t)m * n1 + i1], s = t1s[(size_t)m * n1 + i1];
-      acc.x += Xc[m].x * c + Xs[m].x * s;
-      acc.y += Xc[m].y * c + Xs[m].y * s;
+      const double c = tc[(size_t)m * ld + i1], s = ts[(size_t)m * ld + i1];
+      ax += Xc[m].x * c + Xs[m].x * s;
+      ay += Xc[m].y * c + Xs[m].y * s;
     }
-    h[((size_t)i1 * 2 * ncut + cs * ncut + n) * ntri + e] = acc;
+    h[((size_t)i1 * 2 * ncut + cs * ncut + n) * ntri + e] = cmk(ax, ay);
   }
 }
 
@@ -466,22 +244,53 @@ __global__ void k_coul_modes(const double2* __restrict__ g, int n1, int ntri, in
 
 struct ObsPart {
   double pop[kMaxBands];
-  double2 J1[3], J2[3];
+  double2 J1[3], J2[3], TA[3];
   double pmax, pmin;
 };
 
+__device__ __forceinline__ void obs_zero(ObsPart& p) {
+  for (int i = 0; i < kMaxBands; i++) p.pop[i] = 0;
+  for (int x = 0; x < 3; x++) p.J1[x] = p.J2[x] = p.TA[x] = cz();
+  p.pmax = 0;
+  p.pmin = 1.0;
+}
+__device__ __forceinline__ void obs_add(ObsPart& d, const ObsPart& o, int n) {
+  for (int i = 0; i < n; i++) d.pop[i] += o.pop[i];
+  for (int x = 0; x < 3; x++) {
+    d.J1[x] = cadd(d.J1[x], o.J1[x]);
+    d.J2[x] = cadd(d.J2[x], o.J2[x]);
+    d.TA[x] = cadd(d.TA[x], o.TA[x]);
+  }
+  d.pmax = fmax(d.pmax, o.pmax);
+  d.pmin = fmin(d.pmin, o.pmin);
+}
+
+struct ObsArgs {
+  const double2* rho;
+  const double2* hr;
+  int want_current, want_tabs;
+  ObsPart* part;
+  unsigned int* done;
+  double scaleJ, scaleTA;
+  ObsRecord rec;
+  ObsRecord* log;
+  double* ncond_dev;
+  double* pcmax_dev;
+};
+
+constexpr int kObsThreads = 128;
+
 template <int N>
-__global__ void __launch_bounds__(128) k_obs(DevTables tb, const DevConsts* __restrict__ cst, const double2* __restrict__ rho,
-                                             const double2* __restrict__ hr, int want_current, ObsPart* __restrict__ part) {
+__global__ void __launch_bounds__(kObsThreads) k_obs(DevTables tb, const DevConsts* __restrict__ cst, ObsArgs a) {
   constexpr int NT = Tri<N>::NT;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int nk = tb.nk;
-  __shared__ ObsPart sp[128];
+  __shared__ ObsPart sp[kObsThreads];
+  __shared__ bool last;
   ObsPart my;
-  for (int i = 0; i < kMaxBands; i++) my.pop[i] = 0;
-  for (int x = 0; x < 3; x++) my.J1[x] = my.J2[x] = cz();
-  my.pmax = 0;
-  my.pmin = 1.0;
+  obs_zero(my);
+  const double2* rho = a.rho;
+  const double2* hr = a.hr;
   if (k < nk) {
     double2 P[NT];
 #pragma unroll
@@ -507,7 +316,6 @@ __global__ void __launch_bounds__(128) k_obs(DevTables tb, const DevConsts* __re
 #pragma unroll
       for (int e = 0; e < N * N; e++) Ue[e] = tb.U[(size_t)e * nk + k];
     }
-    // populations in the eigenbasis: Re sum_ii conj(U[c][ii]) sum_jj P[ii][jj] U[c][jj]
 #pragma unroll
     for (int c = 0; c < N; c++) {
       double2 acc = cz();
@@ -528,8 +336,7 @@ __global__ void __launch_bounds__(128) k_obs(DevTables tb, const DevConsts* __re
         my.pmin = fmin(my.pmin, Pik);
       }
     }
-    if (want_current) {
-      // J1 = sum_ij P_ij GE_ij ; GE from the renormalised H when Coulomb is on
+    if (a.want_current) {
 #pragma unroll
       for (int i = 0; i < N; i++)
 #pragma unroll
@@ -555,7 +362,6 @@ __global__ void __launch_bounds__(128) k_obs(DevTables tb, const DevConsts* __re
             if (i != j) my.J1[x] = cadd(my.J1[x], cmul(cconj(P[e]), cconj(ge[x])));
           }
         }
-      // J2 = sum_{i,j,l} P[i][j] Hs[i][l] conj(D[j][l])
       const double2* Hs = hr ? hr : tb.H;
 #pragma unroll
       for (int i = 0; i < N; i++)
@@ -575,165 +381,136 @@ __global__ void __launch_bounds__(128) k_obs(DevTables tb, const DevConsts* __re
           }
         }
     }
+    if (a.want_tabs)
+      for (int i = 0; i < tb.nch; i++)
+        for (int j = tb.nch; j < N; j++) {
+          const int e = Tri<N>::idx(i, j);
+          for (int x = 0; x < 3; x++)
+            my.TA[x] = csub(my.TA[x], cmul(cscale(tb.D[(size_t)(x * NT + e) * nk + k], 2.), P[e]));
+        }
   }
   sp[threadIdx.x] = my;
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s) {
-      ObsPart& d = sp[threadIdx.x];
-      const ObsPart& o = sp[threadIdx.x + s];
-      for (int i = 0; i < N; i++) d.pop[i] += o.pop[i];
-      for (int x = 0; x < 3; x++) {
-        d.J1[x] = cadd(d.J1[x], o.J1[x]);
-        d.J2[x] = cadd(d.J2[x], o.J2[x]);
-      }
-      d.pmax = fmax(d.pmax, o.pmax);
-      d.pmin = fmin(d.pmin, o.pmin);
-    }
+  for (int s = kObsThreads / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) obs_add(sp[threadIdx.x], sp[threadIdx.x + s], N);
     __syncthreads();
   }
-  if (threadIdx.x == 0) part[blockIdx.x] = sp[0];
-}
-
-// transient absorption: -2 sum_{i<nch<=j} D_ij P_ij (one block; tiny for nch=0 or 1)
-__global__ void k_tabs(DevTables tb, const double2* __restrict__ rho, double2* __restrict__ out3) {
-  __shared__ double2 s[3][256];
-  double2 acc[3] = {cz(), cz(), cz()};
-  const int n = tb.n, nk = tb.nk, ntri = tb.ntri;
-  for (int k = threadIdx.x; k < nk; k += blockDim.x)
-    for (int i = 0; i < tb.nch; i++)
-      for (int j = tb.nch; j < n; j++) {
-        const int e = tri_index(i, j, n);
-        const double2 p = rho[(size_t)e * nk + k];
-        for (int x = 0; x < 3; x++) acc[x] = csub(acc[x], cmul(cscale(tb.D[(size_t)(x * ntri + e) * nk + k], 2.), p));
-      }
-  for (int x = 0; x < 3; x++) s[x][threadIdx.x] = acc[x];
+  if (threadIdx.x == 0) {
+    a.part[blockIdx.x] = sp[0];
+    __threadfence();
+    const unsigned int prev = atomicAdd(a.done, 1u);
+    last = (prev == gridDim.x - 1);
+  }
   __syncthreads();
-  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
-    if (threadIdx.x < st)
-      for (int x = 0; x < 3; x++) s[x][threadIdx.x] = cadd(s[x][threadIdx.x], s[x][threadIdx.x + st]);
+  if (!last) return;
+  // last block: fixed-order reduction of all block partials
+  __threadfence();
+  ObsPart t;
+  obs_zero(t);
+  for (int b = threadIdx.x; b < gridDim.x; b += kObsThreads) obs_add(t, a.part[b], N);
+  sp[threadIdx.x] = t;
+  __syncthreads();
+  for (int s = kObsThreads / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) obs_add(sp[threadIdx.x], sp[threadIdx.x + s], N);
     __syncthreads();
   }
-  if (threadIdx.x == 0)
-    for (int x = 0; x < 3; x++) out3[x] = s[x][0];
-}
-
-__global__ void k_obs_final(const ObsPart* __restrict__ part, int nparts, int n, int nbands, int nk, double scaleJ,
-                            double scaleTA, const double2* __restrict__ tabs3, ObsRecord rec, ObsRecord* __restrict__ log,
-                            double* __restrict__ ncond_dev, double* __restrict__ pcmax_dev) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  ObsPart t;
-  for (int i = 0; i < kMaxBands; i++) t.pop[i] = 0;
-  for (int x = 0; x < 3; x++) t.J1[x] = t.J2[x] = cz();
-  t.pmax = 0;
-  t.pmin = 1.0;
-  for (int b = 0; b < nparts; b++) {
-    const ObsPart& p = part[b];
-    for (int i = 0; i < n; i++) t.pop[i] += p.pop[i];
-    for (int x = 0; x < 3; x++) {
-      t.J1[x] = cadd(t.J1[x], p.J1[x]);
-      t.J2[x] = cadd(t.J2[x], p.J2[x]);
-    }
-    t.pmax = fmax(t.pmax, p.pmax);
-    t.pmin = fmin(t.pmin, p.pmin);
-  }
+  if (threadIdx.x != 0) return;
+  const ObsPart& T = sp[0];
+  ObsRecord rec = a.rec;
   const double inv = 1. / nk;
-  double trace = -(double)nbands;
+  double trace = -(double)tb.nbands;
   double nc = 0;
-  for (int i = 0; i < n; i++) {
-    double v = t.pop[i] * inv;
+  for (int i = 0; i < N; i++) {
+    double v = T.pop[i] * inv;
     trace += v;
-    if (i < nbands) v = 1.0 - v;
+    if (i < tb.nbands) v = 1.0 - v;
     rec.pop[i] = v;
     if (v > nc) nc = v;
   }
   for (int x = 0; x < 3; x++) {
-    rec.J1[2 * x] = t.J1[x].x * scaleJ;
-    rec.J1[2 * x + 1] = t.J1[x].y * scaleJ;
-    rec.J2[x] = -2. * (t.J2[x].y * scaleJ);
-    if (tabs3) {
-      rec.tabs[2 * x] = tabs3[x].x * scaleTA * inv;
-      rec.tabs[2 * x + 1] = tabs3[x].y * scaleTA * inv;
-    }
+    rec.J1[2 * x] = T.J1[x].x * a.scaleJ;
+    rec.J1[2 * x + 1] = T.J1[x].y * a.scaleJ;
+    rec.J2[x] = -2. * (T.J2[x].y * a.scaleJ);
+    rec.tabs[2 * x] = T.TA[x].x * a.scaleTA * inv;
+    rec.tabs[2 * x + 1] = T.TA[x].y * a.scaleTA * inv;
   }
   rec.trace_dev = trace;
-  rec.p_cond_max = t.pmax;
-  rec.p_min = t.pmin;
+  rec.p_cond_max = T.pmax;
+  rec.p_min = T.pmin;
   rec.n_cond = nc;
-  if (log) *log = rec;
-  if (ncond_dev) *ncond_dev = nc;
-  if (pcmax_dev) *pcmax_dev = t.pmax;
+  if (a.log) *a.log = rec;
+  if (a.ncond_dev) *a.ncond_dev = nc;
+  if (a.pcmax_dev) *a.pcmax_dev = T.pmax;
+  *a.done = 0u;
 }
 
 // ----------------------------------------------------------------------- launchers
 
-template <int N>
-static cudaError_t launch_rhs_n(const DevTables& tb, const DevConsts* cst, const StageArgs& a, cudaStream_t s) {
-  const int bs = 128;
-  k_rhs<N><<<(tb.nk + bs - 1) / bs, bs, 0, s>>>(tb, cst, a);
-  return cudaGetLastError();
+static size_t pad16(size_t b) { return (b + 15) & ~(size_t)15; }
+size_t coulomb_rows_smem(const DevTables& tb) {
+  return sizeof(double2) * (size_t)tb.ntri * tb.n2 + pad16(sizeof(double) * 2 * (size_t)tb.ncut * tb.n2);
 }
+size_t coulomb_modes_smem(const DevTables& tb) {
+  return sizeof(double2) * (2 * (size_t)tb.n1 + 8 * (size_t)tb.ncut) + pad16(sizeof(double) * 2 * (size_t)tb.ncut * (tb.n1 | 1));
+}
+// element counts (doubles, padded to 16 bytes) of the host-prepared trig layouts
+size_t coulomb_t2T_count(int n2, int ncut) { return pad16(sizeof(double) * 2 * (size_t)ncut * n2) / sizeof(double); }
+size_t coulomb_t1P_count(int n1, int ncut) { return pad16(sizeof(double) * 2 * (size_t)ncut * (n1 | 1)) / sizeof(double); }
 
-cudaError_t launch_rhs(const DevTables& tb, const DevConsts* cst, const StageArgs& a, cudaStream_t s) {
-  switch (tb.n) {
-    case 1: return launch_rhs_n<1>(tb, cst, a, s);
-    case 2: return launch_rhs_n<2>(tb, cst, a, s);
-    case 3: return launch_rhs_n<3>(tb, cst, a, s);
-    case 4: return launch_rhs_n<4>(tb, cst, a, s);
-    case 5: return launch_rhs_n<5>(tb, cst, a, s);
-    case 6: return launch_rhs_n<6>(tb, cst, a, s);
-    case 8: return launch_rhs_n<8>(tb, cst, a, s);
-    default: return cudaErrorInvalidValue;
-  }
+cudaError_t coulomb_prepare(const DevTables& tb) {
+  // opt in to more than 48 KB of dynamic shared memory where needed (227 KB max per block)
+  cudaError_t e = cudaFuncSetAttribute(k_coul_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coulomb_rows_smem(tb));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_coul_modes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)coulomb_modes_smem(tb));
 }
 
 cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2* rho, double2* h, double2* Xout,
                            const double2* X0, cudaStream_t s) {
-  k_coul_rows<<<tb.n1, 256, 0, s>>>(rho, tb.nk, tb.n1, tb.n2, tb.ntri, tb.ncut, c.t2c, c.t2s, c.g);
+  k_coul_rows<<<tb.n1, kRowThreads, coulomb_rows_smem(tb), s>>>(rho, tb.nk, tb.n1, tb.n2, tb.ntri, tb.ncut, c.t2T, c.g, tb.err);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   dim3 grid(tb.ncut, tb.ntri);
-  size_t smem = sizeof(double2) * 8 * tb.ncut;
-  k_coul_modes<<<grid, 128, smem, s>>>(c.g, tb.n1, tb.ntri, tb.ncut, 1.0 / tb.nk, c.t1c, c.t1s, c.A, c.B, c.C, c.D, X0,
-                                       c.is_diag, h, Xout, c.fdiag, c.diag_of);
+  k_coul_modes<<<grid, kModeThreads, coulomb_modes_smem(tb), s>>>(c.g, tb.n1, tb.ntri, tb.ncut, 1.0 / tb.nk, c.t1P, tb.err,
+                                                                   c.A, c.B, c.C, c.D, X0, c.is_diag, h, Xout, c.fdiag,
+                                                                   c.diag_of);
   return cudaGetLastError();
 }
 
-template <int N>
-static cudaError_t launch_obs_n(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,
-                                int want_current, ObsPart* part, cudaStream_t s) {
-  k_obs<N><<<(tb.nk + 127) / 128, 128, 0, s>>>(tb, cst, rho, hr, want_current, part);
-  return cudaGetLastError();
-}
-
-int obs_parts(int nk) { return (nk + 127) / 128; }
+int obs_parts(int nk) { return (nk + kObsThreads - 1) / kObsThreads; }
 size_t obs_part_bytes() { return sizeof(ObsPart); }
 
+template <int N>
+static cudaError_t launch_obs_n(const DevTables& tb, const DevConsts* cst, const ObsArgs& a, cudaStream_t s) {
+  k_obs<N><<<obs_parts(tb.nk), kObsThreads, 0, s>>>(tb, cst, a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,
-                               int want_current, int want_tabs, void* part, double2* tabs3, double scaleJ,
+                               int want_current, int want_tabs, void* part, unsigned int* done, double scaleJ,
                                double scaleTA, const ObsRecord& rec, ObsRecord* log, double* ncond_dev,
                                double* pcmax_dev, cudaStream_t s) {
-  cudaError_t e;
-  ObsPart* pp = (ObsPart*)part;
+  ObsArgs a;
+  a.rho = rho;
+  a.hr = hr;
+  a.want_current = want_current;
+  a.want_tabs = want_tabs && tb.nch > 0;
+  a.part = (ObsPart*)part;
+  a.done = done;
+  a.scaleJ = scaleJ;
+  a.scaleTA = scaleTA;
+  a.rec = rec;
+  a.log = log;
+  a.ncond_dev = ncond_dev;
+  a.pcmax_dev = pcmax_dev;
   switch (tb.n) {
-    case 1: e = launch_obs_n<1>(tb, cst, rho, hr, want_current, pp, s); break;
-    case 2: e = launch_obs_n<2>(tb, cst, rho, hr, want_current, pp, s); break;
-    case 3: e = launch_obs_n<3>(tb, cst, rho, hr, want_current, pp, s); break;
-    case 4: e = launch_obs_n<4>(tb, cst, rho, hr, want_current, pp, s); break;
-    case 5: e = launch_obs_n<5>(tb, cst, rho, hr, want_current, pp, s); break;
-    case 6: e = launch_obs_n<6>(tb, cst, rho, hr, want_current, pp, s); break;
-    case 8: e = launch_obs_n<8>(tb, cst, rho, hr, want_current, pp, s); break;
+    case 1: return launch_obs_n<1>(tb, cst, a, s);
+    case 2: return launch_obs_n<2>(tb, cst, a, s);
+    case 3: return launch_obs_n<3>(tb, cst, a, s);
+    case 4: return launch_obs_n<4>(tb, cst, a, s);
+    case 5: return launch_obs_n<5>(tb, cst, a, s);
+    case 8: return launch_obs_n<8>(tb, cst, a, s);
     default: return cudaErrorInvalidValue;
   }
-  if (e != cudaSuccess) return e;
-  if (want_tabs && tb.nch > 0) {
-    k_tabs<<<1, 256, 0, s>>>(tb, rho, tabs3);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
-  k_obs_final<<<1, 32, 0, s>>>(pp, obs_parts(tb.nk), tb.n, tb.nbands, tb.nk, scaleJ, scaleTA,
-                                (want_tabs && tb.nch > 0) ? tabs3 : nullptr, rec, log, ncond_dev, pcmax_dev);
-  return cudaGetLastError();
 }
 
 }  // namespace edus

@@ -16,6 +16,8 @@ struct CoulDev {
   const double* t1s = nullptr;
   const double* t2c = nullptr; // [ncut][n2] cos(2 pi n k2)
   const double* t2s = nullptr;
+  const double* t2T = nullptr; // [n2][2 ncut] cos then sin, transposed for the row pass
+  const double* t1P = nullptr; // [2][ncut][n1|1] cos / sin rows padded to an odd stride
   const double2* A = nullptr;  // [ncut^2][ntri] coefficients, diagonal rule applied
   const double2* B = nullptr;
   const double2* C = nullptr;
@@ -26,12 +28,15 @@ struct CoulDev {
 };
 
 cudaError_t launch_rhs(const DevTables& tb, const DevConsts* cst, const StageArgs& a, cudaStream_t s);
+cudaError_t coulomb_prepare(const DevTables& tb);
+size_t coulomb_t2T_count(int n2, int ncut);
+size_t coulomb_t1P_count(int n1, int ncut);
 cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2* rho, double2* h, double2* Xout,
                            const double2* X0, cudaStream_t s);
 int obs_parts(int nk);
 size_t obs_part_bytes();
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,
-                               int want_current, int want_tabs, void* part, double2* tabs3, double scaleJ,
+                               int want_current, int want_tabs, void* part, unsigned int* done, double scaleJ,
                                double scaleTA, const ObsRecord& rec, ObsRecord* log, double* ncond_dev,
                                double* pcmax_dev, cudaStream_t s);
 

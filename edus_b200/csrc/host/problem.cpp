@@ -466,7 +466,66 @@ int read_coulomb(Problem& P, const char* workdir) {
   return 0;
 }
 
+// One k point as Source_Main/save_HUD.cpp:19-53 stores it: the model's H, U, D
+// (gHUD, headers/HUD.h:5-20), the scissor shift of the conduction bands added to
+// H, and the Wannier dipole made symmetric, D := (D + D^T)/2.
+void eval_k(const Problem& P, const Tb& tb, const double* k, cd* H, cd* U, cd* D) {
+  const int n = P.ncv, nr = P.nrpts;
+  const bool isW = P.p.mode == EDUS_MODE_WANNIER;
+  cd Hk[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Uk[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Dk[EDUS_MAX_BANDS * EDUS_MAX_BANDS * 3];
+  if (isW) {
+    std::vector<cd> ph(nr);
+    for (int iR = 0; iR < nr; iR++) {
+      double kR = 0.;
+      for (int l = 0; l < 3; l++) kR += k[l] * P.Rvec[iR * 3 + l];
+      kR *= 2 * kPi;
+      ph[iR] = cd(std::cos(kR), std::sin(kR));
+    }
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        cd h = 0, d[3] = {0, 0, 0};
+        for (int iR = 0; iR < nr; iR++) {
+          h += ph[iR] * P.HR[((size_t)i * n + j) * nr + iR];
+          for (int x = 0; x < 3; x++) d[x] += ph[iR] * P.rR[(((size_t)x * n + i) * n + j) * nr + iR];
+        }
+        Hk[i * n + j] = (i == j) ? cd(h.real(), 0.) : h;
+        for (int x = 0; x < 3; x++) Dk[(i * n + j) * 3 + x] = (i == j) ? cd(d[x].real(), 0.) : d[x];
+      }
+    cd A[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Z[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+    double ev[EDUS_MAX_BANDS];
+    std::copy(Hk, Hk + n * n, A);
+    eig_herm(n, A, ev, Z);
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) Uk[i * n + j] = std::conj(Z[j * n + i]);
+  } else {
+    tb_eval(tb, n, k, Hk, Uk, Dk);
+  }
+  double S[EDUS_MAX_BANDS];
+  const double gapc = P.p.conduction_shift;
+  for (int i = 0; i < n; i++) S[i] = (gapc > 1e-16 && i >= P.p.nb[1]) ? gapc : 0.0;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) {
+      cd value = 0.;
+      if (gapc > 1e-16)
+        for (int ii = 0; ii < n; ii++) value += std::conj(Uk[ii * n + i]) * S[ii] * Uk[ii * n + j];
+      H[i * n + j] = Hk[i * n + j] + value;
+      U[i * n + j] = Uk[i * n + j];
+      for (int x = 0; x < 3; x++)
+        D[(i * n + j) * 3 + x] = isW ? 0.5 * (Dk[(i * n + j) * 3 + x] + Dk[(j * n + i) * 3 + x]) : Dk[(i * n + j) * 3 + x];
+    }
+}
+
 }  // namespace
+
+int model_hud(const Problem& P, const double* kcrys, cd* H, cd* U, cd* D) {
+  Tb tb;
+  if (P.p.mode != EDUS_MODE_WANNIER) {
+    int rc = tb_setup(P.p, tb);
+    if (rc) return rc;
+  }
+  eval_k(P, tb, kcrys, H, U, D);
+  return 0;
+}
 
 int build_problem(const edus_params& p, const char* workdir, Problem& P) {
   P = Problem();
@@ -496,55 +555,9 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P) {
     rc = tb_setup(p, tb);
   }
   if (rc) return rc;
-  std::vector<double> S(n, 0.0);
-  const double gapc = p.conduction_shift;
-  if (gapc > 1e-16)
-    for (int i = 0; i < n; i++)
-      if (i >= p.nb[1]) S[i] = gapc;
-  const int nr = P.nrpts;
 #pragma omp parallel for schedule(static)
-  for (int ik = 0; ik < nk; ik++) {
-    const double* k = &P.kpt[ik * 3];
-    cd Hk[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Uk[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Dk[EDUS_MAX_BANDS * EDUS_MAX_BANDS * 3];
-    if (isW) {
-      std::vector<cd> ph(nr);
-      for (int iR = 0; iR < nr; iR++) {
-        double kR = 0.;
-        for (int l = 0; l < 3; l++) kR += k[l] * P.Rvec[iR * 3 + l];
-        kR *= 2 * kPi;
-        ph[iR] = cd(std::cos(kR), std::sin(kR));
-      }
-      for (int i = 0; i < n; i++)
-        for (int j = 0; j < n; j++) {
-          cd h = 0, d[3] = {0, 0, 0};
-          for (int iR = 0; iR < nr; iR++) {
-            h += ph[iR] * P.HR[((size_t)i * n + j) * nr + iR];
-            for (int x = 0; x < 3; x++) d[x] += ph[iR] * P.rR[(((size_t)x * n + i) * n + j) * nr + iR];
-          }
-          Hk[i * n + j] = (i == j) ? cd(h.real(), 0.) : h;
-          for (int x = 0; x < 3; x++) Dk[(i * n + j) * 3 + x] = (i == j) ? cd(d[x].real(), 0.) : d[x];
-        }
-      cd A[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Z[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
-      double ev[EDUS_MAX_BANDS];
-      std::copy(Hk, Hk + n * n, A);
-      eig_herm(n, A, ev, Z);
-      for (int i = 0; i < n; i++)
-        for (int j = 0; j < n; j++) Uk[i * n + j] = std::conj(Z[j * n + i]);
-    } else {
-      tb_eval(tb, n, k, Hk, Uk, Dk);
-    }
-    for (int i = 0; i < n; i++)
-      for (int j = 0; j < n; j++) {
-        cd value = 0.;
-        if (gapc > 1e-16)
-          for (int ii = 0; ii < n; ii++) value += std::conj(Uk[ii * n + i]) * S[ii] * Uk[ii * n + j];
-        P.H[((size_t)ik * n + i) * n + j] = Hk[i * n + j] + value;
-        P.U[((size_t)ik * n + i) * n + j] = Uk[i * n + j];
-        for (int x = 0; x < 3; x++)
-          P.D[(((size_t)ik * n + i) * n + j) * 3 + x] =
-              isW ? 0.5 * (Dk[(i * n + j) * 3 + x] + Dk[(j * n + i) * 3 + x]) : Dk[(i * n + j) * 3 + x];
-      }
-  }
+  for (int ik = 0; ik < nk; ik++)
+    eval_k(P, tb, &P.kpt[ik * 3], &P.H[(size_t)ik * n * n], &P.U[(size_t)ik * n * n], &P.D[(size_t)ik * n * n * 3]);
   // gradient of the energy (Source_Main/save_HUD.cpp:96-137)
   P.GE.assign(st * 3, 0);
   if (p.current) {

@@ -38,6 +38,8 @@ def load_library():
         "edus_problem_info_get": (C.c_int, [vp, P(abi.ProblemInfo)]),
         "edus_problem_get": (C.c_int, [vp, cp, vp, sz]),
         "edus_problem_free": (None, [vp]),
+        "edus_model_hud": (C.c_int, [vp, P(dbl), vp, vp, vp]),
+        "edus_struct_sizes": (C.c_int, [P(C.c_int64)]),
         "edus_options_default": (C.c_int, [P(abi.Options)]),
         "edus_create": (C.c_int, [vp, P(abi.Options), P(vp)]),
         "edus_destroy": (None, [vp]),
@@ -45,12 +47,14 @@ def load_library():
         "edus_get_state": (C.c_int, [vp, vp]),
         "edus_step": (C.c_int, [vp, i32]),
         "edus_run": (C.c_int, [vp]),
+        "edus_reset": (C.c_int, [vp]),
         "edus_clock": (C.c_int, [vp, P(i32), P(dbl), P(dbl)]),
         "edus_obs_count": (C.c_int, [vp, P(i32)]),
         "edus_obs_get": (C.c_int, [vp, i32, i32, P(abi.Obs)]),
         "edus_observables": (C.c_int, [vp, P(abi.Obs)]),
         "edus_write_outputs": (C.c_int, [vp, cp]),
         "edus_last_timing": (C.c_int, [vp, P(dbl), P(C.c_int64)]),
+        "edus_profile": (C.c_int, [vp, i32, P(dbl), P(C.c_int64), P(dbl), P(C.c_int64)]),
         "edus_get_derivative": (C.c_int, [vp, i32, P(dbl), dbl, i32]),
         "edus_runge_kutta_ad": (C.c_int, [vp, i32, i32, dbl]),
         "edus_runge_kutta_ac": (C.c_int, [vp, i32, dbl]),
@@ -126,6 +130,16 @@ class Problem:
         _check(self._L.edus_problem_get(self._h, name.encode(), a.ctypes.data, a.nbytes), f"edus_problem_get({name})")
         return a
 
+    def model_hud(self, kcrys):
+        """H, U, D of the model at one crystal k point (gHUD)."""
+        n = self.info.ncv
+        H = np.zeros((n, n), np.complex128)
+        U = np.zeros((n, n), np.complex128)
+        D = np.zeros((n, n, 3), np.complex128)
+        k = (C.c_double * 3)(*[float(x) for x in kcrys])
+        _check(self._L.edus_model_hud(self._h, k, H.ctypes.data, U.ctypes.data, D.ctypes.data), "edus_model_hud")
+        return H, U, D
+
     def close(self):
         if self._h:
             self._L.edus_problem_free(self._h)
@@ -141,7 +155,7 @@ class Problem:
 class Context:
     """Device context: all state resident on one GPU."""
 
-    def __init__(self, problem, device=0, precision=-1):
+    def __init__(self, problem, device=0, precision=-1, use_graphs=True):
         L = load_library()
         self._L = L
         self.problem = problem
@@ -149,6 +163,7 @@ class Context:
         _check(L.edus_options_default(C.byref(o)), "edus_options_default")
         o.device = device
         o.precision = precision
+        o.use_graphs = 1 if use_graphs else 0
         self._h = C.c_void_p()
         _check(L.edus_create(problem._h, C.byref(o), C.byref(self._h)), "edus_create")
         self.n = problem.info.ncv
@@ -171,6 +186,9 @@ class Context:
 
     def run(self):
         _check(self._L.edus_run(self._h), "edus_run")
+
+    def reset(self):
+        _check(self._L.edus_reset(self._h), "edus_reset")
 
     def clock(self):
         it, t, dt = C.c_int32(), C.c_double(), C.c_double()
@@ -196,6 +214,12 @@ class Context:
         ms, launches = C.c_double(), C.c_int64()
         _check(self._L.edus_last_timing(self._h, C.byref(ms), C.byref(launches)), "edus_last_timing")
         return ms.value, launches.value
+
+    def profile(self, nsteps):
+        """Device time of the fused RHS kernel and of the Coulomb pair over nsteps (eager)."""
+        a, b, c, d = C.c_double(), C.c_int64(), C.c_double(), C.c_int64()
+        _check(self._L.edus_profile(self._h, int(nsteps), C.byref(a), C.byref(b), C.byref(c), C.byref(d)), "edus_profile")
+        return {"rhs_ms": a.value, "rhs_launches": b.value, "coulomb_ms": c.value, "coulomb_launches": d.value}
 
     # ODE_solver-level mirror ---------------------------------------------
     def get_derivative(self, slot, EF, wx2, e_non0):

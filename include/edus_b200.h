@@ -170,6 +170,12 @@ int edus_problem_info_get(const edus_problem* pb, edus_problem_info* out);
  * "HR","rR","Rvec"); nbytes must match exactly. */
 int edus_problem_get(const edus_problem* pb, const char* name, void* dst, size_t nbytes);
 void edus_problem_free(edus_problem* pb);
+/* H(k), U(k) and D(k) of the problem's model at one crystal k point, as
+ * gHUD (headers/HUD.h:5-20) returns them: H, U [n][n], D [n][n][3] interleaved
+ * complex. */
+int edus_model_hud(const edus_problem* pb, const double kcrys[3], double* H, double* U, double* D);
+/* sizeof of the ABI structs: params, obs, problem_info, options (for bindings). */
+int edus_struct_sizes(int64_t out[4]);
 
 /* ------------------------------------------------------- device context */
 typedef struct edus_ctx edus_ctx;
@@ -187,6 +193,11 @@ int edus_options_default(edus_options* o);
 /* Upload the problem and allocate all device state. */
 int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out);
 void edus_destroy(edus_ctx* ctx);
+
+/* Restore the initial state (ground-state projector, zero multistep history)
+ * and the clock (it = 0, t = -0.21 fs); the next edus_run replays the CUDA
+ * graph captured by the first one. */
+int edus_reset(edus_ctx* ctx);
 
 /* State in the reference layout P[k][i][j], interleaved complex128. */
 int edus_set_state(edus_ctx* ctx, const double* rho);
@@ -212,6 +223,11 @@ int edus_write_outputs(edus_ctx* ctx, const char* outdir);
 /* Device time (ms, CUDA events) of the last edus_step/edus_run call and the
  * number of kernel launches it issued. */
 int edus_last_timing(edus_ctx* ctx, double* ms, int64_t* launches);
+/* Run nsteps eagerly with CUDA events around every launch of the fused
+ * RHS + stage-update kernel and of the Coulomb transform pair; returns their
+ * summed device times (ms) and launch counts. */
+int edus_profile(edus_ctx* ctx, int32_t nsteps, double* rhs_ms, int64_t* rhs_launches, double* coul_ms,
+                 int64_t* coul_launches);
 
 /* --------------------------------------------- ODE_solver-level mirror
  * Slots name device arrays of the state shape: 0 = P0, 1 = P1, 2 = P2,

@@ -1,0 +1,186 @@
+"""Parity of the sm_100a path with the CPU oracle (and the reference's golden run).
+
+Tolerances: the FP64 path must match the reference to <= 1e-12 relative in rho_k
+and J(t). rho is compared as max |difference| (entries are O(1)); J1 by relative
+L2 over t; J2 and populations, whose small values come from cancelling sums over
+k, by absolute difference against their noise floor.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import edus_b200 as E
+from edus_b200 import abi
+from edus_b200 import workloads as W
+from conftest import GOLDEN, GOLDEN_INPUT
+from oracle_lib import Oracle
+
+pytestmark = pytest.mark.gpu
+
+RHO_TOL = 1e-13   # max |rho_gpu - rho_oracle|
+J1_TOL = 1e-11    # relative L2 over t
+TIME_AU_FS = 0.02418884326505
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300))
+
+
+def run_pair(path, wd, steps, **ctx_kw):
+    p = E.parse_input(path)
+    pb = E.Problem(p, wd)
+    ctx = E.Context(pb, **ctx_kw)
+    ctx.step(steps)
+    o = Oracle(p, wd)
+    lo = o.run(steps)
+    return ctx, o, ctx.obs(), lo
+
+
+def check_logs(g, o, pop_abs=2e-15):
+    assert len(g) == len(o) and len(g) > 0
+    for a, b in zip(g, o):
+        assert a["t"] == b["t"]
+        np.testing.assert_array_equal(a["EF_pump"], b["EF_pump"])
+    J1g, J1o = np.array([x["J1"] for x in g]), np.array([x["J1"] for x in o])
+    if np.abs(J1o).max() > 1e-14:
+        assert rel(J1g, J1o) < J1_TOL
+    J2g, J2o = np.array([x["J2"] for x in g]), np.array([x["J2"] for x in o])
+    assert np.abs(J2g - J2o).max() <= 1e-9 * max(np.abs(J2o).max(), 1e-20)
+    pg, po = np.array([x["pop"] for x in g]), np.array([x["pop"] for x in o])
+    assert np.abs(pg - po).max() <= pop_abs
+
+
+def test_rhs_matches_oracle():
+    p = E.parse_input(GOLDEN_INPUT)
+    pb = E.Problem(p)
+    ctx = E.Context(pb)
+    o = Oracle(p)
+    rng = np.random.default_rng(1)
+    P0 = pb.get("P0")
+    X = (rng.standard_normal(P0.shape) + 1j * rng.standard_normal(P0.shape)) * 0.01
+    P = P0 + X + np.conj(np.transpose(X, (0, 2, 1)))
+    for i in range(P.shape[1]):
+        P[:, i, i] = P[:, i, i].real
+    for EF, e_non0 in [([0.0, 3e-4, -2e-4, 1e-5, 0.0, 0.0], 1), ([0, 0, 0, 0, 0, 0], 0)]:
+        ctx.slot_set(abi.SLOT_P0, P)
+        ctx.get_derivative(abi.SLOT_P0, EF, p.probe.wl, e_non0)
+        g = ctx.slot_get(abi.SLOT_PV)
+        r = o.rhs(P, EF, p.probe.wl, e_non0)
+        assert np.abs(g - r).max() <= 1e-15 * max(1.0, np.abs(r).max() * 10)
+        # Pv is Hermitian with a real diagonal, exactly
+        assert np.array_equal(g, np.conj(np.transpose(g, (0, 2, 1))))
+
+
+def test_stage_updates_match_reference_formulae():
+    p = E.parse_input(GOLDEN_INPUT)
+    pb = E.Problem(p)
+    ctx = E.Context(pb)
+    P0 = pb.get("P0")
+    ctx.slot_set(abi.SLOT_P0, P0)
+    ctx.get_derivative(abi.SLOT_P0, [0, 1e-3, 0, 0, 0, 0], 0.0, 1)
+    Pv = ctx.slot_get(abi.SLOT_PV)
+    ctx.runge_kutta_ad(abi.SLOT_P0, abi.SLOT_P1, 0.05)  # Runge_Kutta_Ad: P1 = P0 + dt Pv
+    np.testing.assert_allclose(ctx.slot_get(abi.SLOT_P1), P0 + Pv * 0.05, rtol=0, atol=1e-16)
+    ctx.runge_kutta_ac(abi.SLOT_P1, 0.05)  # Runge_Kutta_Ac: P1 += dt Pv
+    np.testing.assert_allclose(ctx.slot_get(abi.SLOT_P1), (P0 + Pv * 0.05) + Pv * 0.05, rtol=0, atol=1e-16)
+
+
+def test_golden_run_on_gpu():
+    """The whole shipped AB5 run (16591 steps) on the GPU against the golden outputs."""
+    p = E.parse_input(GOLDEN_INPUT)
+    ctx = E.Context(E.Problem(p))
+    ctx.run()
+    log = ctx.obs()
+    G = np.load(os.path.join(GOLDEN, "ab5_golden.npz"))
+    rows = G["rows"]
+    assert len(log) == int(G["nrows"])
+    J1 = np.array([log[i]["J1"] for i in rows])
+    J1r = G["J1"][:, 1::2] + 1j * G["J1"][:, 2::2]
+    assert rel(J1, J1r) < 1e-12
+    J2 = np.array([log[i]["J2"] for i in rows])
+    assert np.abs(J2 - G["J2"][:, 1:]).max() < 1e-10 * np.abs(G["J2"][:, 1:]).max()
+    pop = np.array([log[i]["pop"] for i in rows])
+    assert np.abs(pop - G["Losses"][:, 1:4]).max() < 1e-13
+    assert rel(pop[:, 2], G["Losses"][:, 3]) < 1e-11
+
+
+def test_rk4_matches_oracle(workdir):
+    ctx, o, g, lo = run_pair(W.hbn_rk4(workdir, n=24, t_fin_fs=3.0, it_res=5), workdir, 400)
+    assert np.abs(ctx.get_state() - o.get("P0")).max() < RHO_TOL
+    check_logs(g, lo)
+
+
+def test_coulomb_ab4_rk4_startup_matches_oracle(workdir):
+    ctx, o, g, lo = run_pair(W.hbn_coulomb(workdir, n=24, t_fin_fs=2.0, it_res=5), workdir, 300)
+    assert np.abs(ctx.get_state() - o.get("P0")).max() < RHO_TOL
+    check_logs(g, lo)
+    P = ctx.get_state()
+    np.testing.assert_allclose(ctx.coulomb_hk(abi.SLOT_P0), o.coulomb_hk(P), rtol=0, atol=1e-14)
+
+
+def test_coulomb_ab4_zero_history_matches_oracle(workdir):
+    ctx, o, g, lo = run_pair(W.hbn_coulomb(workdir, n=24, t_fin_fs=2.0, it_res=5, rk4_startup=False), workdir, 300)
+    assert np.abs(ctx.get_state() - o.get("P0")).max() < RHO_TOL
+    check_logs(g, lo)
+
+
+def test_taylor_dynamic_dt_matches_oracle(workdir):
+    solver = "Taylor\nTaylorOrder 6\ndynamical_dt_evolution\nepsStepAbs 0.02\n"
+    ctx, o, g, lo = run_pair(W.hbn_rk4(workdir, n=24, t_fin_fs=2.0, it_res=3, solver=solver, dt_fs=0.002), workdir, 300)
+    assert np.abs(ctx.get_state() - o.get("P0")).max() < RHO_TOL
+    # the adaptive step divides by a population change of ~1e-9 (dyn_dt_evolution.cpp:88):
+    # its relative rounding is ~1e-7, so compare times loosely and populations absolutely
+    it_g, t_g, dt_g = ctx.clock()
+    it_o, t_o, dt_o = o.clock()
+    assert it_g == it_o and abs(t_g - t_o) < 1e-6
+    pg, po = np.array([x["pop"] for x in g]), np.array([x["pop"] for x in lo])
+    assert np.abs(pg - po).max() < 1e-14
+
+
+def test_rk4_dynamic_dt_matches_oracle(workdir):
+    ctx, o, g, lo = run_pair(W.hbn_rk4(workdir, n=24, t_fin_fs=2.0, it_res=3, solver="dynamical_dt_evolution\nepsStepAbs 0.001\n"),
+                             workdir, 200)
+    assert np.abs(ctx.get_state() - o.get("P0")).max() < 1e-12
+    assert ctx.clock()[0] == o.clock()[0]
+
+
+def test_wannier_8band_matches_oracle(workdir):
+    ctx, o, g, lo = run_pair(W.wannier(workdir, n=16, t_fin_fs=1.0, it_res=5), workdir, 100)
+    assert np.abs(ctx.get_state() - o.get("P0")).max() < RHO_TOL
+    check_logs(g, lo)
+
+
+def test_graph_replay_equals_eager(workdir):
+    path = W.hbn_coulomb(workdir, n=24, t_fin_fs=1.0, it_res=5)
+    pb = E.Problem(E.parse_input(path), workdir)
+    a = E.Context(pb, use_graphs=True)
+    a.run()
+    sa, la = a.get_state(), a.obs()
+    b = E.Context(pb, use_graphs=False)
+    b.run()
+    assert np.array_equal(sa, b.get_state())
+    a.reset()
+    a.run()
+    assert np.array_equal(sa, a.get_state())
+    assert all(np.array_equal(x["J1"], y["J1"]) for x, y in zip(la, a.obs()))
+
+
+def test_write_outputs_format(workdir, tmp_path):
+    p = E.parse_input(GOLDEN_INPUT)
+    p.t_fin = -8.0  # a few output instants only
+    ctx = E.Context(E.Problem(p))
+    ctx.run()
+    out = str(tmp_path / "Output")
+    ctx.write_outputs(out)
+    log = ctx.obs()
+    lines = open(os.path.join(out, "J1.txt")).read().splitlines()
+    assert len(lines) == len(log)
+    # the reference leaves std::scientific set after the first line (Observables_MPI.h:710)
+    assert lines[0].startswith("          -0.21")
+    assert "e-01" in lines[1].split()[0]
+    vals = np.array([[float(x) for x in l.split()] for l in lines])
+    J1 = np.array([x["J1"] for x in log])
+    np.testing.assert_allclose(vals[:, 1::2], J1.real, rtol=1e-14, atol=1e-300)
+    losses = open(os.path.join(out, "Losses.txt")).read().splitlines()
+    assert losses[0].split()[0] == "-0.21" and len(losses[0].split()) == 4
