@@ -14,6 +14,7 @@
 #include <cstring>
 #include <fstream>
 #include <iomanip>
+#include <mutex>
 #include <string>
 #include <sys/stat.h>
 #include <vector>
@@ -1204,3 +1205,71 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// edus_observables_static — observables of the current state with the
+// reduction scratch (per-block partial sums, the arrival counter of the
+// last-block reduction, the output record) in a file-scope device array
+// instead of device memory the call or the context allocates.
+namespace {
+
+// Up to 4096 per-block partials of the observable reduction, i.e. up to
+// 4096 * 128 = 524 288 k points; 320 bytes per partial (the record is 288).
+constexpr int kStaticObsParts = 4096;
+constexpr size_t kStaticPartBytes = 320;
+constexpr size_t kStaticDoneOff = (size_t)kStaticObsParts * kStaticPartBytes;  // 256-aligned
+constexpr size_t kStaticRecOff = kStaticDoneOff + 256;
+constexpr size_t kStaticScratchBytes = kStaticRecOff + 512;
+static_assert(sizeof(edus_obs) <= 512, "observable record exceeds its static slot");
+static_assert(kStaticDoneOff % 256 == 0, "counter offset must stay aligned");
+
+static __device__ __align__(256) unsigned char g_obs_scratch[kStaticScratchBytes];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+unsigned char* g_static_base[kStaticMaxDevices] = {};
+
+// Once per device, with that device current: the address of the scratch
+// array in this device's memory.
+int static_scratch(int device, unsigned char** base) {
+  if (device < 0 || device >= kStaticMaxDevices) return fail(EDUS_EINVAL, "device %d out of range", device);
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_base[device]) {
+    unsigned char* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_obs_scratch);
+    if (e != cudaSuccess) return fail(EDUS_ECUDA, "cudaGetSymbolAddress(static observable scratch): %s", cudaGetErrorString(e));
+    g_static_base[device] = p;
+  }
+  *base = g_static_base[device];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int edus_observables_static(edus_ctx* c, edus_obs* out) {
+  if (!c || !out) return fail(EDUS_EINVAL, "null argument");
+  const int parts = obs_parts(c->P.nk);
+  if (parts > kStaticObsParts)
+    return fail(EDUS_EINVAL, "%d k points exceed the static observable scratch (at most %d k points)", c->P.nk,
+                kStaticObsParts * 128);
+  if (obs_part_bytes() > kStaticPartBytes) return fail(EDUS_EUNSUPPORTED, "observable partial larger than its static slot");
+  CK(cudaSetDevice(c->device));
+  unsigned char* base = nullptr;
+  int rc = static_scratch(c->device, &base);
+  if (rc) return rc;
+  unsigned int* done = (unsigned int*)(base + kStaticDoneOff);
+  edus_obs* rec_dev = (edus_obs*)(base + kStaticRecOff);
+  // the last-block reduction counts arriving blocks from zero
+  CK(cudaMemsetAsync(done, 0, sizeof(unsigned int), c->stream));
+  edus_obs rec;
+  memset(&rec, 0, sizeof(rec));
+  rec.t = c->time_loop;
+  rec.dt = c->dt;
+  double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
+  double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
+  CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, base, done,
+                        scaleJ, scaleTA, rec, rec_dev, nullptr, nullptr, c->stream));
+  CK(cudaMemcpyAsync(out, rec_dev, sizeof(edus_obs), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}

@@ -218,6 +218,20 @@ int edus_obs_count(edus_ctx* ctx, int32_t* n);
 int edus_obs_get(edus_ctx* ctx, int32_t first, int32_t count, edus_obs* out);
 /* Observables of the current state (does not append to the log). */
 int edus_observables(edus_ctx* ctx, edus_obs* out);
+/* Same result as edus_observables, but the call allocates no memory: the
+ * reduction scratch (per-block partial sums, the arrival counter that starts
+ * at zero, the output record) lives in a fixed device array inside the
+ * library. For callers that cannot take an allocation at this point: a
+ * serving loop whose HBM is fully committed to admitted solves, or a caller
+ * that must not run into the device-wide synchronisation a device
+ * free brings. No counterpart in the reference (its observables reduce into
+ * host arrays over MPI).
+ * Limits: at most 524 288 k points (4096 partials of 128 k points), else
+ * EDUS_EINVAL. The first call on a device looks the array up on that device
+ * (make it outside any stream capture). The array is shared by every context
+ * on a device: calls that overlap in time (two host threads, or two streams)
+ * race on it and must be serialised by the caller. */
+int edus_observables_static(edus_ctx* ctx, edus_obs* out);
 /* Write Output/{EF,J1,J2,Losses,TransientAbs}.txt in the reference's format. */
 int edus_write_outputs(edus_ctx* ctx, const char* outdir);
 /* Device time (ms, CUDA events) of the last edus_step/edus_run call and the
