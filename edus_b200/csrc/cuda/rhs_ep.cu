@@ -35,8 +35,8 @@ template <int N, int KT>
 __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const DevConsts* __restrict__ cst, StageArgs a) {
   constexpr int NT = TriEP<N>::NT;
   __shared__ double2 sP[NT][KT];
-  __shared__ double2 sH[NT][KT];
-  __shared__ double2 sD[3][NT][KT];
+  __shared__ double2 sHu[NT][KT];  // H~_ij, i <= j
+  __shared__ double2 sHl[NT][KT];  // H~_ji, i <= j (D is symmetric, H Hermitian)
   extern __shared__ double2 dyn[];  // Coulomb row tables: h rows [nrows][2][ncut][NT], trig [2][ncut][KT]
   const int kl = threadIdx.x, e = threadIdx.y;
   const int k0 = blockIdx.x * KT;
@@ -71,11 +71,12 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
     }
   }
   double2 Pe = cz(), He = cz(), G = cz();
+  double2 De[3] = {cz(), cz(), cz()};
   if (valid) {
     Pe = a.src[(size_t)e * nk + k];
     He = tb.H[(size_t)e * nk + k];
 #pragma unroll
-    for (int x = 0; x < 3; x++) sD[x][e][kl] = tb.D[(size_t)(x * NT + e) * nk + k];
+    for (int x = 0; x < 3; x++) De[x] = tb.D[(size_t)(x * NT + e) * nk + k];
   }
   if (staged) {
     __syncthreads();  // trig table + barrier init visible to all threads
@@ -141,8 +142,20 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
       }
     }
   }
-  sP[e][kl] = Pe;
-  sH[e][kl] = He;
+  {
+    // H~ = H + E^w . D with w = probe when exactly one of (i, j) is a core band
+    // (headers/RungeKutta.h:158-208); the lower entry uses conj(H) and the same D
+    const int w = (i < nch) != (j < nch);
+    double2 hu = He, hl = cconj(He);
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+      hu = cadd(hu, cscale(De[x], a.EF[w][x]));
+      hl = cadd(hl, cscale(De[x], a.EF[w][x]));
+    }
+    sP[e][kl] = Pe;
+    sHu[e][kl] = hu;
+    sHl[e][kl] = hl;
+  }
   __syncthreads();
 
   double dpmax = 0.;
@@ -151,14 +164,7 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
       return (r <= c) ? sP[TriEP<N>::idx(r, c)][kl] : cconj(sP[TriEP<N>::idx(c, r)][kl]);
     };
     auto HF = [&](int r, int c) -> double2 {
-      const int lo = r < c ? r : c, hi = r < c ? c : r;
-      const int t = TriEP<N>::idx(lo, hi);
-      double2 h = (r <= c) ? sH[t][kl] : cconj(sH[t][kl]);
-      const int w = (r >= nch && c < nch) || (r < nch && c >= nch);
-      h = cadd(h, cscale(sD[0][t][kl], a.EF[w][0]));
-      h = cadd(h, cscale(sD[1][t][kl], a.EF[w][1]));
-      h = cadd(h, cscale(sD[2][t][kl], a.EF[w][2]));
-      return h;
+      return (r <= c) ? sHu[TriEP<N>::idx(r, c)][kl] : sHl[TriEP<N>::idx(c, r)][kl];
     };
     double2 v;
     if (i == j) {
@@ -264,7 +270,7 @@ static cudaError_t launch_ep(const DevTables& tb, const DevConsts* cst, const St
     // rows of the k grid one block of KT consecutive k points can touch
     const int rows = (tb.n2 + KT - 2) / tb.n2 + 1;
     const size_t bytes = sizeof(double2) * ((size_t)rows * 2 * tb.ncut * NT + tb.ncut * KT);
-    const size_t static_bytes = sizeof(double2) * 5 * NT * KT;
+    const size_t static_bytes = sizeof(double2) * 3 * NT * KT;
     if (bytes + static_bytes <= 48 * 1024) {
       b.stage_rows = rows;
       dyn = bytes;
