@@ -9,6 +9,7 @@ from .lib import (  # noqa: F401
     EdusError,
     Problem,
     Context,
+    Batch,
     load_library,
     parse_input,
     default_params,
@@ -16,4 +17,4 @@ from .lib import (  # noqa: F401
 )
 from . import abi  # noqa: F401
 
-__all__ = ["EdusError", "Problem", "Context", "load_library", "parse_input", "default_params", "abi", "library_path"]
+__all__ = ["EdusError", "Problem", "Context", "Batch", "load_library", "parse_input", "default_params", "abi", "library_path"]

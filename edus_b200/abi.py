@@ -179,3 +179,33 @@ def obs_to_dict(o, ncv):
         "n_cond": o.n_cond,
         "dt": o.dt,
     }
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("precision", C.c_int32),
+        ("max_instances", C.c_int32),
+        ("chunk_steps", C.c_int32),
+        ("use_graphs", C.c_int32),
+        ("tile_k", C.c_int32 * (EDUS_MAX_BANDS + 1)),
+        ("hbm_budget_bytes", C.c_int64),
+    ]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("ticks", C.c_int64),
+        ("active", C.c_int32),
+        ("done", C.c_int32),
+        ("free_slots", C.c_int32),
+        ("pad", C.c_int32),
+        ("bytes_used", C.c_int64),
+        ("bytes_budget", C.c_int64),
+        ("device_ms", C.c_double),
+        ("kpoint_steps", C.c_double),
+        ("launches", C.c_int64),
+    ]
+
+
+EDUS_INST_FREE, EDUS_INST_RUNNING, EDUS_INST_DONE = 0, 1, 2

@@ -1,0 +1,619 @@
+// batch.cu — host side of the batched engine: instance admission and release,
+// per-class tile tables, chunked CUDA-graph replay (C ABI edus_batch_*).
+//
+// The time loop of each instance is the reference's constant-dt loop
+// (Source_Main/const_dt_evolution.cpp:1-54) with the RK4 step of
+// Source_Main/RungeKutta.cpp; instances share only the GPU. Device memory of
+// an instance comes from a stream-ordered pool owned by the batch, so admission
+// and release never synchronise the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "cuda/batch.cuh"
+#include "host/problem.hpp"
+
+namespace edus {
+namespace batch {
+namespace {
+
+#define BCK(x)                                                                            \
+  do {                                                                                    \
+    cudaError_t e_ = (x);                                                                 \
+    if (e_ != cudaSuccess) return fail(EDUS_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+  } while (0)
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int default_tile(int n) {
+  switch (n) {
+    case 2: return 32;
+    case 3: return 32;
+    case 4: return 16;
+    case 5: return 16;
+    case 8: return 8;
+    case 16: return 2;
+  }
+  return 0;
+}
+
+struct Slot {
+  int status = EDUS_INST_FREE;
+  int n = 0, kt = 0, nk = 0, ntri = 0, itfi = 0, res = 1, nlog = 0, ntiles = 0;
+  int64_t tag = 0;
+  int64_t bytes = 0;
+  long long tick_admit = 0;
+  std::vector<void*> mem;
+  Inst inst{};
+};
+
+struct ClassTab {
+  int n = 0, kt = 0;
+  std::vector<Tile> tiles;
+  Tile* d_tiles = nullptr;
+  size_t cap = 0;
+  int* d_ntiles = nullptr;
+  int sgrid = 0, ogrid = 0;
+  bool dirty = false;
+};
+
+struct Layout {
+  size_t state, H, D, GE, U, nbr, field, log, part;
+  size_t eq;  // initial state kept for the mixed-precision deviation form
+  size_t total() const { return 4 * state + eq + H + D + GE + U + nbr + field + log + part + 256; }
+};
+
+}  // namespace
+}  // namespace batch
+}  // namespace edus
+
+using namespace edus;
+using namespace edus::batch;
+
+struct edus_batch {
+  edus_batch_options opt{};
+  bool mixed = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;
+  std::vector<Slot> slots;
+  Inst* d_insts = nullptr;
+  int* d_it[2] = {nullptr, nullptr};
+  std::map<int, ClassTab> classes;
+  long long tick = 0;
+  int64_t bytes_used = 0, budget = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::string graph_key;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  double device_ms = 0, kpoint_steps = 0;
+  long long launches = 0;
+};
+
+namespace {
+
+int tile_len(const edus_batch* b, int n) {
+  int kt = (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.tile_k[n] : 0;
+  return kt > 0 ? kt : default_tile(n);
+}
+
+Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
+  const size_t n = P.ncv, nk = P.nk, nt = n * (n + 1) / 2;
+  const size_t s = b->mixed ? sizeof(float2) : sizeof(double2);
+  Layout L;
+  L.state = align256(nt * nk * sizeof(double2));
+  L.eq = b->mixed ? L.state : 0;
+  L.H = align256(nt * nk * s);
+  L.D = align256(3 * nt * nk * s);
+  L.GE = P.p.current ? align256(3 * nt * nk * s) : 0;
+  L.U = align256(n * n * nk * s);
+  L.nbr = align256((size_t)P.nnb * nk * sizeof(int));
+  L.field = align256((size_t)(P.itfi + 2) * sizeof(FieldRow));
+  const int res = std::max(1, P.p.it_resolution);
+  L.log = align256((size_t)(P.itfi / res + 1) * sizeof(edus_obs));
+  L.part = align256(((nk + kt - 1) / kt) * obs_part_bytes());
+  return L;
+}
+
+int check_problem(const edus_batch* b, const Problem& P) {
+  const int n = P.ncv;
+  if (!class_supported(n, tile_len(b, n)))
+    return fail(EDUS_EUNSUPPORTED, "batch: %d bands with %d k points per tile is not built", n, tile_len(b, n));
+  if (P.p.coulomb) return fail(EDUS_EUNSUPPORTED, "batch: the Coulomb mean field runs only in single-solve contexts");
+  if (!P.diss_i.empty()) return fail(EDUS_EUNSUPPORTED, "batch: dissipation runs only in single-solve contexts");
+  if (P.p.solver != EDUS_SOLVER_RK4 || P.p.dynamical_dt)
+    return fail(EDUS_EUNSUPPORTED, "batch: instances integrate with RK4 at constant dt");
+  if (P.nnb > kBatchMaxNb) return fail(EDUS_EUNSUPPORTED, "batch: %d stencil neighbours (max %d)", P.nnb, kBatchMaxNb);
+  return 0;
+}
+
+template <class T>
+T mkc(const cd& v);
+template <>
+double2 mkc<double2>(const cd& v) { return make_double2(v.real(), v.imag()); }
+template <>
+float2 mkc<float2>(const cd& v) { return make_float2((float)v.real(), (float)v.imag()); }
+
+// reference layout [k][n][n](x comps) -> upper-triangle planes [x][e][k]
+template <class T>
+void planes(const cd* src, int nk, int n, int comps, std::vector<T>& dst) {
+  const int nt = n * (n + 1) / 2;
+  dst.resize((size_t)comps * nt * nk);
+  for (int k = 0; k < nk; k++)
+    for (int i = 0; i < n; i++)
+      for (int j = i; j < n; j++)
+        for (int x = 0; x < comps; x++)
+          dst[((size_t)x * nt + tri_index(i, j, n)) * nk + k] = mkc<T>(src[(((size_t)k * n + i) * n + j) * comps + x]);
+}
+
+template <class T>
+int put(edus_batch* b, void* d, const std::vector<T>& h) {
+  BCK(cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, b->stream));
+  return 0;
+}
+
+template <class T>
+int upload_model(edus_batch* b, const Problem& P, const Inst& I) {
+  const int n = P.ncv, nk = P.nk;
+  std::vector<T> pl;
+  int rc;
+  planes<T>(P.H.data(), nk, n, 1, pl);
+  if ((rc = put(b, (void*)I.H, pl))) return rc;
+  planes<T>(P.D.data(), nk, n, 3, pl);
+  if ((rc = put(b, (void*)I.D, pl))) return rc;
+  if (I.GE) {
+    planes<T>(P.GE.data(), nk, n, 3, pl);
+    if ((rc = put(b, (void*)I.GE, pl))) return rc;
+  }
+  pl.resize((size_t)n * n * nk);
+  for (int k = 0; k < nk; k++)
+    for (int e = 0; e < n * n; e++) pl[(size_t)e * nk + k] = mkc<T>(P.U[(size_t)k * n * n + e]);
+  return put(b, (void*)I.U, pl);
+}
+
+void free_slot_mem(edus_batch* b, Slot& s) {
+  for (void* p : s.mem) cudaFreeAsync(p, b->stream);
+  s.mem.clear();
+}
+
+int sync_tiles(edus_batch* b) {
+  for (auto& kv : b->classes) {
+    ClassTab& c = kv.second;
+    if (!c.dirty) continue;
+    if (c.tiles.size() > c.cap) {
+      size_t cap = std::max<size_t>(1024, c.cap);
+      while (cap < c.tiles.size()) cap *= 2;
+      Tile* nt = nullptr;
+      BCK(cudaMallocAsync((void**)&nt, cap * sizeof(Tile), b->pool, b->stream));
+      if (c.d_tiles) cudaFreeAsync(c.d_tiles, b->stream);
+      c.d_tiles = nt;
+      c.cap = cap;
+    }
+    if (!c.tiles.empty()) BCK(cudaMemcpyAsync(c.d_tiles, c.tiles.data(), c.tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, b->stream));
+    const int nt = (int)c.tiles.size();
+    BCK(cudaMemcpyAsync(c.d_ntiles, &nt, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    // pageable source: the copy has left nt before the call returns
+    c.dirty = false;
+  }
+  return 0;
+}
+
+std::string graph_key(const edus_batch* b) {
+  std::string k;
+  for (const auto& kv : b->classes) {
+    char buf[96];
+    snprintf(buf, sizeof(buf), "%d:%d:%p;", kv.second.n, kv.second.kt, (const void*)kv.second.d_tiles);
+    k += buf;
+  }
+  return k;
+}
+
+int record_chunk(edus_batch* b) {
+  const int S = b->opt.chunk_steps;
+  for (int s = 0; s < S; s++) {
+    const int parity = s & 1;
+    for (auto& kv : b->classes) {
+      ClassTab& c = kv.second;
+      View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles};
+      BCK(launch_obs(c.n, c.kt, b->mixed, v, parity, c.ogrid, b->stream));
+    }
+    for (int st = 0; st < 4; st++)
+      for (auto& kv : b->classes) {
+        ClassTab& c = kv.second;
+        View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles};
+        BCK(launch_stage(c.n, c.kt, b->mixed, v, st, parity, c.sgrid, b->stream));
+      }
+  }
+  return 0;
+}
+
+int run_chunk(edus_batch* b) {
+  int rc = sync_tiles(b);
+  if (rc) return rc;
+  bool any = false;
+  for (auto& kv : b->classes) any = any || kv.second.d_tiles;
+  if (!any) return 0;
+  const std::string key = graph_key(b);
+  BCK(cudaEventRecord(b->e0, b->stream));
+  if (b->opt.use_graphs) {
+    if (!b->gexec || key != b->graph_key) {
+      if (b->gexec) cudaGraphExecDestroy(b->gexec);
+      if (b->graph) cudaGraphDestroy(b->graph);
+      b->gexec = nullptr;
+      b->graph = nullptr;
+      BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      rc = record_chunk(b);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+      if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (e != cudaSuccess) return fail(EDUS_ECUDA, "capture of the batch chunk: %s", cudaGetErrorString(e));
+      b->graph = g;
+      BCK(cudaGraphInstantiate(&b->gexec, g, 0));
+      b->graph_key = key;
+    }
+    BCK(cudaGraphLaunch(b->gexec, b->stream));
+  } else {
+    if ((rc = record_chunk(b))) return rc;
+  }
+  BCK(cudaEventRecord(b->e1, b->stream));
+  BCK(cudaEventSynchronize(b->e1));
+  float ms = 0;
+  BCK(cudaEventElapsedTime(&ms, b->e0, b->e1));
+  b->device_ms += ms;
+  const int S = b->opt.chunk_steps;
+  b->launches += (long long)S * 5 * b->classes.size();
+  // progress of every running instance over this chunk
+  for (size_t q = 0; q < b->slots.size(); q++) {
+    Slot& s = b->slots[q];
+    if (s.status != EDUS_INST_RUNNING) continue;
+    const long long it0 = b->tick - s.tick_admit;
+    const long long steps = std::max(0LL, std::min<long long>(S, (long long)s.itfi + 1 - it0));
+    b->kpoint_steps += (double)steps * s.nk;
+  }
+  b->tick += S;
+  // retire instances past the end of their time grid
+  for (size_t q = 0; q < b->slots.size(); q++) {
+    Slot& s = b->slots[q];
+    if (s.status == EDUS_INST_RUNNING && b->tick - s.tick_admit > s.itfi) {
+      s.status = EDUS_INST_DONE;
+      ClassTab& c = b->classes[s.n];
+      c.tiles.erase(std::remove_if(c.tiles.begin(), c.tiles.end(), [&](const Tile& t) { return t.inst == (int)q; }), c.tiles.end());
+      c.dirty = true;
+    }
+  }
+  return 0;
+}
+
+Slot* slot_of(edus_batch* b, int32_t slot) {
+  if (!b || slot < 0 || slot >= (int)b->slots.size()) return nullptr;
+  return &b->slots[slot];
+}
+
+}  // namespace
+
+extern "C" {
+
+int edus_batch_options_default(edus_batch_options* o) {
+  if (!o) return fail(EDUS_EINVAL, "null argument");
+  memset(o, 0, sizeof(*o));
+  o->device = 0;
+  o->precision = EDUS_PREC_FP64;
+  o->max_instances = 1024;
+  o->chunk_steps = 16;
+  o->use_graphs = 1;
+  o->hbm_budget_bytes = 0;
+  return 0;
+}
+
+int edus_batch_create(const edus_batch_options* o, edus_batch** out) {
+  if (!o || !out) return fail(EDUS_EINVAL, "null argument");
+  if (o->max_instances <= 0 || o->chunk_steps <= 0 || (o->chunk_steps & 1))
+    return fail(EDUS_EINVAL, "batch: max_instances > 0 and an even chunk_steps are required");
+  if (o->precision != EDUS_PREC_FP64 && o->precision != EDUS_PREC_MIXED) return fail(EDUS_EINVAL, "batch: unknown precision");
+  edus_batch* b = new edus_batch();
+  b->opt = *o;
+  b->mixed = o->precision == EDUS_PREC_MIXED;
+  b->device = o->device;
+  auto bail = [&](int rc) {
+    edus_batch_destroy(b);
+    return rc;
+  };
+  if (cudaSetDevice(b->device) != cudaSuccess) return bail(fail(EDUS_ECUDA, "cannot select device %d", b->device));
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(EDUS_ECUDA, "stream"));
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = b->device;
+  if (cudaMemPoolCreate(&b->pool, &props) != cudaSuccess) return bail(fail(EDUS_ECUDA, "memory pool"));
+  uint64_t keep = ~0ull;
+  cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  b->budget = o->hbm_budget_bytes > 0 ? o->hbm_budget_bytes : (int64_t)(0.9 * (double)fr);
+  const int cap = o->max_instances;
+  b->slots.resize(cap);
+  if (cudaMalloc(&b->d_insts, sizeof(Inst) * cap) != cudaSuccess || cudaMalloc(&b->d_it[0], sizeof(int) * cap) != cudaSuccess ||
+      cudaMalloc(&b->d_it[1], sizeof(int) * cap) != cudaSuccess)
+    return bail(fail(EDUS_ENOMEM, "batch tables"));
+  cudaMemsetAsync(b->d_insts, 0, sizeof(Inst) * cap, b->stream);
+  cudaMemsetAsync(b->d_it[0], 0xff, sizeof(int) * cap, b->stream);
+  cudaMemsetAsync(b->d_it[1], 0xff, sizeof(int) * cap, b->stream);
+  if (cudaEventCreate(&b->e0) != cudaSuccess || cudaEventCreate(&b->e1) != cudaSuccess) return bail(fail(EDUS_ECUDA, "events"));
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "sync"));
+  *out = b;
+  return 0;
+}
+
+void edus_batch_destroy(edus_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto& s : b->slots) free_slot_mem(b, s);
+  for (auto& kv : b->classes) {
+    if (kv.second.d_tiles) cudaFreeAsync(kv.second.d_tiles, b->stream);
+    if (kv.second.d_ntiles) cudaFree(kv.second.d_ntiles);
+  }
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  cudaFree(b->d_insts);
+  cudaFree(b->d_it[0]);
+  cudaFree(b->d_it[1]);
+  if (b->pool) cudaMemPoolDestroy(b->pool);
+  if (b->e0) cudaEventDestroy(b->e0);
+  if (b->e1) cudaEventDestroy(b->e1);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int edus_batch_footprint(edus_batch* b, const edus_problem* pb, int64_t* bytes) {
+  if (!b || !pb || !bytes) return fail(EDUS_EINVAL, "null argument");
+  int rc = check_problem(b, pb->P);
+  if (rc) return rc;
+  *bytes = (int64_t)layout_of(b, pb->P, tile_len(b, pb->P.ncv)).total();
+  return 0;
+}
+
+int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* slot_out) {
+  if (!b || !pb || !slot_out) return fail(EDUS_EINVAL, "null argument");
+  const Problem& P = pb->P;
+  int rc = check_problem(b, P);
+  if (rc) return rc;
+  const int n = P.ncv, nk = P.nk, nt = n * (n + 1) / 2, kt = tile_len(b, n);
+  const Layout L = layout_of(b, P, kt);
+  const int64_t bytes = (int64_t)L.total();
+  if (b->bytes_used + bytes > b->budget)
+    return fail(EDUS_ENOMEM, "batch: %lld bytes do not fit the HBM budget (%lld of %lld used)", (long long)bytes,
+                (long long)b->bytes_used, (long long)b->budget);
+  int q = -1;
+  for (size_t i = 0; i < b->slots.size(); i++)
+    if (b->slots[i].status == EDUS_INST_FREE) {
+      q = (int)i;
+      break;
+    }
+  if (q < 0) return fail(EDUS_ENOMEM, "batch: all %zu slots are in use", b->slots.size());
+  BCK(cudaSetDevice(b->device));
+  Slot s;
+  s.n = n;
+  s.kt = kt;
+  s.nk = nk;
+  s.ntri = nt;
+  s.itfi = P.itfi;
+  s.res = std::max(1, P.p.it_resolution);
+  s.nlog = s.itfi / s.res + 1;
+  s.ntiles = (nk + kt - 1) / kt;
+  s.tag = tag;
+  s.bytes = bytes;
+  // one allocation, carved in the layout order
+  char* base = nullptr;
+  if (cudaMallocAsync((void**)&base, L.total(), b->pool, b->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(EDUS_ENOMEM, "batch: device allocation of %lld bytes failed", (long long)bytes);
+  }
+  s.mem.push_back(base);
+  char* p = base;
+  auto carve = [&](size_t sz) {
+    char* r = sz ? p : nullptr;
+    p += sz;
+    return r;
+  };
+  Inst& I = s.inst;
+  memset(&I, 0, sizeof(I));
+  I.n = n;
+  I.ntri = nt;
+  I.nk = nk;
+  I.nnb = P.nnb;
+  I.nch = P.nch;
+  I.nbands = P.nbands;
+  I.itfi = P.itfi;
+  I.res = s.res;
+  I.want_current = P.p.current;
+  I.want_tabs = P.p.tabs && P.nch > 0;
+  I.ntiles = s.ntiles;
+  I.dt = P.p.dt;
+  I.wx2 = P.p.probe.wl;
+  I.scaleJ = P.dk[0] * P.dk[1] * P.dk[2] / P.det_a;
+  I.scaleTA = std::fabs(P.jac) * P.dk[0] * P.dk[1] * P.dk[2];
+  I.P0 = (double2*)carve(L.state);
+  I.P1 = (double2*)carve(L.state);
+  I.Pa = (double2*)carve(L.state);
+  I.Pb = (double2*)carve(L.state);
+  I.Peq = (const double2*)carve(L.eq);
+  I.H = carve(L.H);
+  I.D = carve(L.D);
+  I.GE = carve(L.GE);
+  I.U = carve(L.U);
+  I.nbr = (const int*)carve(L.nbr);
+  I.field = (const FieldRow*)carve(L.field);
+  I.log = (edus_obs*)carve(L.log);
+  I.part = carve(L.part);
+  I.done = (unsigned int*)carve(256);
+  for (int bb = 0; bb < P.nnb; bb++) {
+    I.wb[bb] = P.shell_w[P.bshell[bb]];
+    for (int x = 0; x < 3; x++) I.bvec[bb][x] = P.bvec[bb * 3 + x];
+  }
+  auto undo = [&](int code) {
+    free_slot_mem(b, s);
+    return code;
+  };
+  // tables and initial state
+  rc = b->mixed ? upload_model<float2>(b, P, I) : upload_model<double2>(b, P, I);
+  if (rc) return undo(rc);
+  {
+    std::vector<double2> st;
+    planes<double2>(P.P0.data(), nk, n, 1, st);
+    if ((rc = put(b, I.P0, st))) return undo(rc);
+    if (I.Peq && (rc = put(b, (void*)I.Peq, st))) return undo(rc);
+    std::vector<int> nb((size_t)P.nnb * nk);
+    for (int k = 0; k < nk; k++)
+      for (int bb = 0; bb < P.nnb; bb++) nb[(size_t)bb * nk + k] = P.nbr[(size_t)k * P.nnb + bb];
+    if ((rc = put(b, (void*)I.nbr, nb))) return undo(rc);
+    // field table: the single-solve loop's times (t += dt) and fields
+    std::vector<FieldRow> fr((size_t)P.itfi + 2);
+    double t = P.t_start;
+    for (auto& row : fr) {
+      memset(&row, 0, sizeof(row));
+      row.t = t;
+      double E[2][3];
+      field_at(P.p, t, E);
+      for (int x = 0; x < 6; x++) row.Et[x] = E[x / 3][x % 3];
+      field_at(P.p, t + P.p.dt / 2.0, E);
+      for (int x = 0; x < 6; x++) row.Eh[x] = E[x / 3][x % 3];
+      t += P.p.dt;
+    }
+    if ((rc = put(b, (void*)I.field, fr))) return undo(rc);
+  }
+  if (cudaMemsetAsync(I.done, 0, sizeof(unsigned int), b->stream) != cudaSuccess ||
+      cudaMemcpyAsync(b->d_insts + q, &I, sizeof(Inst), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
+    return undo(fail(EDUS_ECUDA, "batch: upload of the instance descriptor"));
+  const int zero = 0;
+  if (cudaMemcpyAsync(b->d_it[b->tick & 1] + q, &zero, sizeof(int), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
+    return undo(fail(EDUS_ECUDA, "batch: clock"));
+  // tiles
+  ClassTab& c = b->classes[n];
+  if (!c.n) {
+    c.n = n;
+    c.kt = kt;
+    c.sgrid = stage_grid(n, kt, b->mixed);
+    c.ogrid = obs_grid(n, kt, b->mixed);
+    if (cudaMalloc(&c.d_ntiles, sizeof(int)) != cudaSuccess) return undo(fail(EDUS_ENOMEM, "tile count"));
+  }
+  for (int t = 0; t < s.ntiles; t++) c.tiles.push_back(Tile{q, t * kt, t, 0});
+  c.dirty = true;
+  s.status = EDUS_INST_RUNNING;
+  s.tick_admit = b->tick;
+  b->bytes_used += bytes;
+  b->slots[q] = std::move(s);
+  *slot_out = q;
+  return 0;
+}
+
+int edus_batch_advance(edus_batch* b, int32_t nsteps) {
+  if (!b || nsteps < 0) return fail(EDUS_EINVAL, "bad argument");
+  BCK(cudaSetDevice(b->device));
+  const int S = b->opt.chunk_steps;
+  for (int done = 0; done < nsteps; done += S) {
+    int rc = run_chunk(b);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int edus_batch_poll(edus_batch* b, int32_t slot, int32_t* status, int32_t* it, int64_t* tag) {
+  Slot* s = slot_of(b, slot);
+  if (!s) return fail(EDUS_EINVAL, "bad slot");
+  if (status) *status = s->status;
+  if (it) *it = s->status == EDUS_INST_FREE ? 0 : (int32_t)std::min<long long>(b->tick - s->tick_admit, s->itfi + 1);
+  if (tag) *tag = s->tag;
+  return 0;
+}
+
+int edus_batch_obs_count(edus_batch* b, int32_t slot, int32_t* n) {
+  Slot* s = slot_of(b, slot);
+  if (!s || !n || s->status == EDUS_INST_FREE) return fail(EDUS_EINVAL, "bad slot");
+  const long long it = std::min<long long>(b->tick - s->tick_admit, s->itfi + 1);
+  *n = (int32_t)std::min<long long>(s->nlog, (it + s->res - 1) / s->res);
+  return 0;
+}
+
+int edus_batch_obs_get(edus_batch* b, int32_t slot, int32_t first, int32_t count, edus_obs* out) {
+  Slot* s = slot_of(b, slot);
+  if (!s || !out || s->status == EDUS_INST_FREE) return fail(EDUS_EINVAL, "bad slot");
+  if (first < 0 || count < 0 || first + count > s->nlog) return fail(EDUS_EINVAL, "range outside the log");
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaMemcpyAsync(out, s->inst.log + first, sizeof(edus_obs) * count, cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  return 0;
+}
+
+int edus_batch_get_state(edus_batch* b, int32_t slot, double* rho) {
+  Slot* s = slot_of(b, slot);
+  if (!s || !rho || s->status == EDUS_INST_FREE) return fail(EDUS_EINVAL, "bad slot");
+  BCK(cudaSetDevice(b->device));
+  const int n = s->n, nk = s->nk;
+  std::vector<double2> pl((size_t)s->ntri * nk);
+  BCK(cudaMemcpyAsync(pl.data(), s->inst.P0, sizeof(double2) * pl.size(), cudaMemcpyDeviceToHost, b->stream));
+  BCK(cudaStreamSynchronize(b->stream));
+  cd* o = (cd*)rho;
+  for (int k = 0; k < nk; k++)
+    for (int i = 0; i < n; i++)
+      for (int j = i; j < n; j++) {
+        const double2 v = pl[(size_t)tri_index(i, j, n) * nk + k];
+        o[((size_t)k * n + i) * n + j] = cd(v.x, v.y);
+        if (i != j) o[((size_t)k * n + j) * n + i] = cd(v.x, -v.y);
+      }
+  return 0;
+}
+
+int edus_batch_release(edus_batch* b, int32_t slot) {
+  Slot* s = slot_of(b, slot);
+  if (!s) return fail(EDUS_EINVAL, "bad slot");
+  if (s->status == EDUS_INST_FREE) return 0;
+  BCK(cudaSetDevice(b->device));
+  if (s->status == EDUS_INST_RUNNING) {
+    ClassTab& c = b->classes[s->n];
+    c.tiles.erase(std::remove_if(c.tiles.begin(), c.tiles.end(), [&](const Tile& t) { return t.inst == slot; }), c.tiles.end());
+    c.dirty = true;
+    // the tile table is rewritten before the next chunk; nothing reads the slot after that
+    int rc = sync_tiles(b);
+    if (rc) return rc;
+  }
+  free_slot_mem(b, *s);
+  b->bytes_used -= s->bytes;
+  *s = Slot();
+  return 0;
+}
+
+int edus_batch_stats_get(edus_batch* b, edus_batch_stats* out) {
+  if (!b || !out) return fail(EDUS_EINVAL, "null argument");
+  memset(out, 0, sizeof(*out));
+  out->ticks = b->tick;
+  for (const auto& s : b->slots) {
+    if (s.status == EDUS_INST_RUNNING) out->active++;
+    if (s.status == EDUS_INST_DONE) out->done++;
+    if (s.status == EDUS_INST_FREE) out->free_slots++;
+  }
+  out->bytes_used = b->bytes_used;
+  out->bytes_budget = b->budget;
+  out->device_ms = b->device_ms;
+  out->kpoint_steps = b->kpoint_steps;
+  out->launches = b->launches;
+  return 0;
+}
+
+int edus_batch_tile_k(edus_batch* b, int32_t nbands, int32_t* kt) {
+  if (!b || !kt) return fail(EDUS_EINVAL, "null argument");
+  *kt = tile_len(b, nbands);
+  return 0;
+}
+
+}  // extern "C"

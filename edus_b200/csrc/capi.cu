@@ -22,10 +22,6 @@
 #include "cuda/kernels.hpp"
 #include "host/problem.hpp"
 
-struct edus_problem {
-  edus::Problem P;
-};
-
 namespace edus {
 namespace {
 

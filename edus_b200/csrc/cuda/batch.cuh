@@ -1,0 +1,86 @@
+// batch.cuh — device-side description of many independent solves advanced
+// together (pulse sweeps, served requests).
+//
+// Every instance keeps its own tables and state in HBM (same plane layout as
+// the single-solve path: upper-triangle planes [e][k]). A class of instances
+// with the same band count N shares one tile table: a tile is KT consecutive
+// k points of one instance. Stage and observable kernels are persistent: a
+// fixed grid walks the tile table, so the table can change between chunks
+// without touching the captured CUDA graph.
+//
+// Time: each instance carries a host-built field table (field at t and
+// t + dt/2 for every step, plus t itself), so the device never evaluates the
+// laser and the values are the ones the single-solve path uses. The step
+// counter of an instance is double buffered by tick parity: kernels of tick
+// T read it[T & 1], the observable kernel of tick T writes it[(T + 1) & 1].
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../../include/edus_b200.h"
+#include "dev.cuh"
+
+namespace edus {
+namespace batch {
+
+// Most k-gradient neighbours of a batch instance (hexagonal and square grids use 12).
+constexpr int kBatchMaxNb = 24;
+
+// Field table row of one step: t, E(t) = {pump x,y,z, 0.5 probe x,y,z}, E(t + dt/2).
+struct FieldRow {
+  double t;
+  double pad;
+  double Et[6];
+  double Eh[6];
+  double pad2[2];
+};
+static_assert(sizeof(FieldRow) == 128, "field rows are 128 bytes");
+
+struct Inst {
+  int n, ntri, nk, nnb;
+  int nch, nbands, itfi, res;
+  int want_current, want_tabs, ntiles, pad0;
+  double dt, wx2, scaleJ, scaleTA;
+  const int* nbr;          // [nnb][nk]
+  const void* H;           // [ntri][nk]   double2 (FP64) or float2 (mixed)
+  const void* D;           // [3][ntri][nk]
+  const void* GE;          // [3][ntri][nk] or null
+  const void* U;           // [n*n][nk]
+  double2 *P0, *P1, *Pa, *Pb;
+  const double2* Peq;      // mixed precision: initial state [ntri][nk]
+  const FieldRow* field;   // [itfi + 2]
+  edus_obs* log;           // [itfi / res + 1]
+  void* part;              // [ntiles] observable partials
+  unsigned int* done;      // arrival counter of the last-tile reduction
+  double wb[kMaxNb];
+  double bvec[kMaxNb][3];
+};
+
+struct Tile {
+  int inst;     // slot
+  int k0;       // first k point
+  int t_in;     // index of the tile within its instance
+  int pad;
+};
+
+struct View {
+  const Inst* insts;
+  int* it[2];            // step counter per slot, by tick parity
+  const Tile* tiles;     // tile table of one class
+  const int* ntiles;     // its length (device scalar)
+};
+
+// One RK4 stage (0..3, Source_Main/RungeKutta.cpp schedule) over every tile of
+// the class; N is the band count, kt the tile length the table was built with.
+cudaError_t launch_stage(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
+// Observables of the instances due at this tick (it % res == 0) and the
+// step-counter advance of every instance of the class.
+cudaError_t launch_obs(int N, int kt, bool mixed, const View& v, int parity, int grid, cudaStream_t s);
+// Persistent grid sizes (SMs x resident blocks) of the two kernels.
+int stage_grid(int N, int kt, bool mixed);
+int obs_grid(int N, int kt, bool mixed);
+bool class_supported(int N, int kt);
+size_t obs_part_bytes();
+
+}  // namespace batch
+}  // namespace edus

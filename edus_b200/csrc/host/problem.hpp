@@ -55,4 +55,13 @@ void eig_herm(int n, cd* A, double* evals, cd* Z);
 // Gauss–Jordan inverse with partial pivoting (row-major).
 int inv_gj(int n, const double* A, double* Ainv);
 
+// Laser field of the run at time t: EF[0] = sum of pumps, EF[1] = probe / 2
+// (Source_Main/RungeKutta.cpp:24-30).
+void field_at(const edus_params& p, double t, double EF[2][3]);
+
 }  // namespace edus
+
+// Opaque handle of the C ABI.
+struct edus_problem {
+  edus::Problem P;
+};

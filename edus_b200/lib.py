@@ -62,6 +62,20 @@ def load_library():
         "edus_slot_set": (C.c_int, [vp, i32, vp]),
         "edus_slot_get": (C.c_int, [vp, i32, vp]),
         "edus_coulomb_hk": (C.c_int, [vp, i32, vp]),
+        "edus_observables_static": (C.c_int, [vp, P(abi.Obs)]),
+        "edus_batch_options_default": (C.c_int, [P(abi.BatchOptions)]),
+        "edus_batch_create": (C.c_int, [P(abi.BatchOptions), P(vp)]),
+        "edus_batch_destroy": (None, [vp]),
+        "edus_batch_footprint": (C.c_int, [vp, vp, P(C.c_int64)]),
+        "edus_batch_add": (C.c_int, [vp, vp, C.c_int64, P(i32)]),
+        "edus_batch_advance": (C.c_int, [vp, i32]),
+        "edus_batch_poll": (C.c_int, [vp, i32, P(i32), P(i32), P(C.c_int64)]),
+        "edus_batch_obs_count": (C.c_int, [vp, i32, P(i32)]),
+        "edus_batch_obs_get": (C.c_int, [vp, i32, i32, i32, P(abi.Obs)]),
+        "edus_batch_get_state": (C.c_int, [vp, i32, vp]),
+        "edus_batch_release": (C.c_int, [vp, i32]),
+        "edus_batch_stats_get": (C.c_int, [vp, P(abi.BatchStats)]),
+        "edus_batch_tile_k": (C.c_int, [vp, i32, P(i32)]),
         "edus_strerror": (cp, [C.c_int]),
         "edus_last_error": (cp, []),
         "edus_abi_version": (C.c_int, []),
@@ -249,6 +263,100 @@ class Context:
     def close(self):
         if self._h:
             self._L.edus_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many solves advanced together on one GPU (edus_batch_* of the C ABI)."""
+
+    def __init__(self, device=0, precision=abi.EDUS_PREC_FP64, max_instances=1024, chunk_steps=16, use_graphs=True,
+                 hbm_budget_bytes=0, tile_k=None):
+        L = load_library()
+        self._L = L
+        o = abi.BatchOptions()
+        _check(L.edus_batch_options_default(C.byref(o)), "edus_batch_options_default")
+        o.device = device
+        o.precision = precision
+        o.max_instances = max_instances
+        o.chunk_steps = chunk_steps
+        o.use_graphs = 1 if use_graphs else 0
+        o.hbm_budget_bytes = int(hbm_budget_bytes)
+        for n, k in (tile_k or {}).items():
+            o.tile_k[n] = k
+        self._h = C.c_void_p()
+        _check(L.edus_batch_create(C.byref(o), C.byref(self._h)), "edus_batch_create")
+        self._n = {}
+        self._nk = {}
+
+    def footprint(self, problem):
+        b = C.c_int64()
+        _check(self._L.edus_batch_footprint(self._h, problem._h, C.byref(b)), "edus_batch_footprint")
+        return b.value
+
+    def add(self, problem, tag=0):
+        s = C.c_int32()
+        _check(self._L.edus_batch_add(self._h, problem._h, int(tag), C.byref(s)), "edus_batch_add")
+        self._n[s.value] = problem.info.ncv
+        self._nk[s.value] = problem.info.nk
+        return s.value
+
+    def try_add(self, problem, tag=0):
+        """Slot, or None when the HBM budget or the slots are used up."""
+        s = C.c_int32()
+        rc = self._L.edus_batch_add(self._h, problem._h, int(tag), C.byref(s))
+        if rc == abi.EDUS_ENOMEM:
+            return None
+        _check(rc, "edus_batch_add")
+        self._n[s.value] = problem.info.ncv
+        self._nk[s.value] = problem.info.nk
+        return s.value
+
+    def advance(self, nsteps):
+        _check(self._L.edus_batch_advance(self._h, int(nsteps)), "edus_batch_advance")
+
+    def poll(self, slot):
+        st, it, tag = C.c_int32(), C.c_int32(), C.c_int64()
+        _check(self._L.edus_batch_poll(self._h, int(slot), C.byref(st), C.byref(it), C.byref(tag)), "edus_batch_poll")
+        return st.value, it.value, tag.value
+
+    def obs(self, slot):
+        n = C.c_int32()
+        _check(self._L.edus_batch_obs_count(self._h, int(slot), C.byref(n)), "edus_batch_obs_count")
+        buf = (abi.Obs * max(n.value, 1))()
+        if n.value:
+            _check(self._L.edus_batch_obs_get(self._h, int(slot), 0, n.value, buf), "edus_batch_obs_get")
+        return [abi.obs_to_dict(buf[i], self._n[slot]) for i in range(n.value)]
+
+    def get_state(self, slot):
+        n, nk = self._n[slot], self._nk[slot]
+        a = np.zeros((nk, n, n), dtype=np.complex128)
+        _check(self._L.edus_batch_get_state(self._h, int(slot), a.ctypes.data), "edus_batch_get_state")
+        return a
+
+    def release(self, slot):
+        _check(self._L.edus_batch_release(self._h, int(slot)), "edus_batch_release")
+        self._n.pop(slot, None)
+        self._nk.pop(slot, None)
+
+    def stats(self):
+        s = abi.BatchStats()
+        _check(self._L.edus_batch_stats_get(self._h, C.byref(s)), "edus_batch_stats_get")
+        return {f: getattr(s, f) for f, _ in abi.BatchStats._fields_ if f != "pad"}
+
+    def tile_k(self, nbands):
+        k = C.c_int32()
+        _check(self._L.edus_batch_tile_k(self._h, int(nbands), C.byref(k)), "edus_batch_tile_k")
+        return k.value
+
+    def close(self):
+        if self._h:
+            self._L.edus_batch_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -9,6 +9,7 @@ converted with the reference's own constants: E0 [a.u.] = E [V/A] * 1e10 /
   hbn_coulomb    config 1: same model with the Rytova–Keldysh mean field from the
                  shipped Ncut=20 coefficient files, Adams–Bashforth 4
   wannier        config 2: synthetic nb-band Wannier model (seeded), RK4
+  sweep          config 3: seeded pulse sweep mixing both models on uneven grids
 """
 import math
 import os
@@ -62,7 +63,7 @@ def write_coulomb_files(workdir, label=COULOMB_LABEL):
 
 
 def hbn_rk4(workdir, n=60, field=0.3, photon=0.4, duration=30.0, dt_fs=0.01, t_fin_fs=None, it_res=1,
-            solver="", gap=5.8, t1=2.3, extra_tdse="", probe=""):
+            solver="", gap=5.8, t1=2.3, extra_tdse="", probe="", phase=0.0):
     os.makedirs(workdir, exist_ok=True)
     t_fin = duration if t_fin_fs is None else t_fin_fs
     txt = (
@@ -74,7 +75,7 @@ def hbn_rk4(workdir, n=60, field=0.3, photon=0.4, duration=30.0, dt_fs=0.01, t_f
         f"{solver}{extra_tdse}"
         "}\n\n"
         f"nkpt{{\n1 {n} {n}\n}}\n\n"
-        + _pump(photon, field, duration)
+        + _pump(photon, field, duration, phase=phase)
         + probe
         + "\nobservables{\n"
         "Current\n"
@@ -164,9 +165,10 @@ def write_wannier_tb(path, nw=8, nside=11, seed=12345, a_ang=2.5, decay_h=1.5, d
 
 
 def wannier(workdir, nw=8, nside=11, n=96, field=0.4, photon=0.3, duration=40.0, dt_fs=0.01, t_fin_fs=None, it_res=10,
-            seed=12345, name="W8"):
+            seed=12345, name="W8", phase=0.0, write_model=True):
     os.makedirs(workdir, exist_ok=True)
-    write_wannier_tb(os.path.join(workdir, f"{name}_tb.dat"), nw=nw, nside=nside, seed=seed)
+    if write_model or not os.path.exists(os.path.join(workdir, f"{name}_tb.dat")):
+        write_wannier_tb(os.path.join(workdir, f"{name}_tb.dat"), nw=nw, nside=nside, seed=seed)
     nv = nw // 2
     t_fin = duration if t_fin_fs is None else t_fin_fs
     txt = (
@@ -178,7 +180,7 @@ def wannier(workdir, nw=8, nside=11, n=96, field=0.4, photon=0.3, duration=40.0,
         f"t_fin {t_fin} fs\n"
         "}\n\n"
         f"nkpt{{\n1 {n} {n}\n}}\n\n"
-        + _pump(photon, field, duration)
+        + _pump(photon, field, duration, phase=phase)
         + "\nobservables{\nCurrent\n"
         f"it_resolution {it_res}\n"
         "}\n"
@@ -187,3 +189,32 @@ def wannier(workdir, nw=8, nside=11, n=96, field=0.4, photon=0.3, duration=40.0,
     with open(path, "w") as f:
         f.write(txt)
     return path
+
+
+def sweep(count=256, seed=20261203, nmin=48, nmax=144, emin=0.05, emax=0.8, dmin=10.0, dmax=60.0, it_res=10,
+          dt_fs=0.01):
+    """Seeded pulse sweep: half hBN (hbn_rk4 model), half the 8-band Wannier
+    model of `wannier`; grid N x N with N even, uniform in [nmin, nmax]; peak
+    field log-uniform in [emin, emax] V/A; CEP uniform in [0, 2 pi); pulse
+    duration uniform in [dmin, dmax] fs (the run ends with the pulse).
+    Returns a list of dicts (kind, n, field, phase, duration, ...)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(count):
+        kind = "hbn" if i % 2 == 0 else "wannier"
+        n = 2 * int(rng.integers(nmin // 2, nmax // 2 + 1))
+        field = float(math.exp(rng.uniform(math.log(emin), math.log(emax))))
+        phase = float(rng.uniform(0.0, 2 * math.pi))
+        duration = float(rng.uniform(dmin, dmax))
+        out.append(dict(kind=kind, n=n, field=field, phase=phase, duration=duration, it_res=it_res, dt_fs=dt_fs))
+    return out
+
+
+def write_instance(workdir, spec):
+    """input.txt (and model file) of one sweep or serving instance."""
+    if spec["kind"] == "hbn":
+        return hbn_rk4(workdir, n=spec["n"], field=spec["field"], duration=spec["duration"], it_res=spec["it_res"],
+                       dt_fs=spec["dt_fs"], phase=spec["phase"])
+    return wannier(workdir, nw=spec.get("nw", 8), nside=spec.get("nside", 11), n=spec["n"], field=spec["field"],
+                   duration=spec["duration"], it_res=spec["it_res"], dt_fs=spec["dt_fs"], phase=spec["phase"],
+                   name=spec.get("name", "W8"), write_model=False)

@@ -263,6 +263,61 @@ int edus_slot_get(edus_ctx* ctx, int32_t slot, double* rho);
  * Hk_renorm[k][n][n] (interleaved) to hk_out. */
 int edus_coulomb_hk(edus_ctx* ctx, int32_t p_slot, double* hk_out);
 
+/* ------------------------------------------------------- batches
+ * Many independent solves (pulse sweeps, served requests) advanced together
+ * on one GPU. No counterpart in the reference, which runs one solve per MPI
+ * job. Every instance keeps its own state and tables in HBM; all active
+ * instances step in lockstep, one RK4 step per tick, and a chunk of ticks is
+ * replayed from one CUDA graph of persistent kernels. Instances join and
+ * leave only between chunks. Supported per instance: RK4 at constant dt,
+ * band counts 2, 3, 4, 5, 8, 16, no Coulomb mean field, no dissipation
+ * (others: EDUS_EUNSUPPORTED). */
+typedef struct edus_batch edus_batch;
+
+typedef struct {
+  int32_t device;
+  int32_t precision;        /* EDUS_PREC_FP64 or EDUS_PREC_MIXED (FP32 H, D, commutator; FP64 rho) */
+  int32_t max_instances;    /* slots */
+  int32_t chunk_steps;      /* time steps per graph replay (even) */
+  int32_t use_graphs;
+  int32_t tile_k[EDUS_MAX_BANDS + 1]; /* k points per tile by band count; 0 = tuned default */
+  int64_t hbm_budget_bytes; /* admission limit; 0 = 90 % of the free device memory at create */
+} edus_batch_options;
+
+enum { EDUS_INST_FREE = 0, EDUS_INST_RUNNING = 1, EDUS_INST_DONE = 2 };
+
+typedef struct {
+  int64_t ticks;            /* time steps advanced by the batch */
+  int32_t active, done, free_slots, pad;
+  int64_t bytes_used, bytes_budget;
+  double device_ms;         /* CUDA-event time of all chunk replays */
+  double kpoint_steps;      /* k-point steps advanced (sum over instances) */
+  int64_t launches;         /* kernel launches replayed */
+} edus_batch_stats;
+
+int edus_batch_options_default(edus_batch_options* o);
+int edus_batch_create(const edus_batch_options* o, edus_batch** out);
+void edus_batch_destroy(edus_batch* b);
+/* HBM bytes an instance of this problem takes in this batch. */
+int edus_batch_footprint(edus_batch* b, const edus_problem* pb, int64_t* bytes);
+/* Admit a solve: uploads its tables and initial state; it starts at the next
+ * tick. EDUS_ENOMEM when the budget or the slots are used up (nothing is
+ * changed then). */
+int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* slot);
+/* Advance every running instance by nsteps time steps (rounded up to whole
+ * chunks); instances that reach the end of their time grid become DONE. */
+int edus_batch_advance(edus_batch* b, int32_t nsteps);
+int edus_batch_poll(edus_batch* b, int32_t slot, int32_t* status, int32_t* it, int64_t* tag);
+int edus_batch_obs_count(edus_batch* b, int32_t slot, int32_t* n);
+int edus_batch_obs_get(edus_batch* b, int32_t slot, int32_t first, int32_t count, edus_obs* out);
+/* State of a slot in the reference layout P[k][i][j] (interleaved complex128). */
+int edus_batch_get_state(edus_batch* b, int32_t slot, double* rho);
+/* Free a slot and its device memory. */
+int edus_batch_release(edus_batch* b, int32_t slot);
+int edus_batch_stats_get(edus_batch* b, edus_batch_stats* out);
+/* Tile length in use for a band count (after the autotuner). */
+int edus_batch_tile_k(edus_batch* b, int32_t nbands, int32_t* kt);
+
 /* ------------------------------------------------------- strings */
 const char* edus_strerror(int code);
 const char* edus_last_error(void);

@@ -1,0 +1,134 @@
+"""Batched engine (edus_batch_*): every instance of a batch against the
+single-solve path on the same input.
+
+FP64 instances reproduce the single-solve FP64 path (same host field table,
+same arithmetic; only the order of the observable reductions differs):
+rho to 1e-13 absolute, J1 to 1e-11 relative L2 (the tolerance of the single-solve
+parity tests: these short runs have currents near the summation noise). Mixed-precision instances
+(FP32 H, D and commutator, FP64 rho) are held to 1e-5 relative L2 in J1 on
+these short runs; the full-size error is reported by bench.py.
+"""
+import numpy as np
+import pytest
+
+import edus_b200 as E
+from edus_b200 import abi
+from edus_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def single(problem):
+    ctx = E.Context(problem, use_graphs=False)
+    ctx.run()
+    return ctx.get_state(), ctx.obs()
+
+
+def drain(batch, slots, chunk=16):
+    for _ in range(100000):
+        if all(batch.poll(s)[0] == abi.EDUS_INST_DONE for s in slots):
+            return
+        batch.advance(chunk)
+    raise AssertionError("batch did not finish")
+
+
+def J1(log):
+    return np.array([x["J1"] for x in log])
+
+
+def problems(workdir):
+    out = []
+    for i, (n, tf) in enumerate([(16, 0.6), (20, 0.4), (12, 0.8)]):
+        d = f"{workdir}/hbn{i}"
+        out.append(E.Problem(E.parse_input(W.hbn_rk4(d, n=n, t_fin_fs=tf, it_res=3, field=0.3 + 0.1 * i)), d))
+    d = f"{workdir}/wan"
+    out.append(E.Problem(E.parse_input(W.wannier(d, n=12, t_fin_fs=0.4, it_res=4)), d))
+    return out
+
+
+def test_fp64_batch_matches_single_solves(workdir):
+    pbs = problems(workdir)
+    ref = [single(p) for p in pbs]
+    b = E.Batch(precision=abi.EDUS_PREC_FP64, chunk_steps=8)
+    slots = [b.add(p, tag=i) for i, p in enumerate(pbs)]
+    drain(b, slots, 8)
+    for s, (rho, log) in zip(slots, ref):
+        assert np.abs(b.get_state(s) - rho).max() < 1e-13
+        lb = b.obs(s)
+        assert len(lb) == len(log)
+        assert all(x["t"] == y["t"] for x, y in zip(lb, log))
+        assert rel(J1(lb), J1(log)) < 1e-11
+        pg, po = np.array([x["pop"] for x in lb]), np.array([x["pop"] for x in log])
+        assert np.abs(pg - po).max() < 1e-14
+    st = b.stats()
+    assert st["done"] == len(slots) and st["kpoint_steps"] > 0 and st["device_ms"] > 0
+
+
+def test_late_admission_gives_the_same_result(workdir):
+    """Continuous batching: an instance admitted while others run equals its solo run."""
+    pbs = problems(workdir)
+    b = E.Batch(chunk_steps=8)
+    first = [b.add(p) for p in pbs[:2]]
+    b.advance(24)
+    late = b.add(pbs[2])
+    b.advance(8)
+    b.release(first[0])            # leaves while the others run
+    again = b.add(pbs[3])          # reuses memory of the released slot
+    drain(b, [first[1], late, again], 8)
+    for s, p in [(first[1], pbs[1]), (late, pbs[2]), (again, pbs[3])]:
+        rho, log = single(p)
+        assert np.abs(b.get_state(s) - rho).max() < 1e-13
+        assert rel(J1(b.obs(s)), J1(log)) < 1e-11
+
+
+def test_graph_and_eager_chunks_agree(workdir):
+    pbs = problems(workdir)[:2]
+    out = []
+    for g in (True, False):
+        b = E.Batch(chunk_steps=4, use_graphs=g)
+        slots = [b.add(p) for p in pbs]
+        drain(b, slots, 4)
+        out.append([b.get_state(s) for s in slots])
+    for x, y in zip(*out):
+        assert np.array_equal(x, y)
+
+
+def test_mixed_precision_error_is_small(workdir):
+    pbs = problems(workdir)
+    ref = [single(p) for p in pbs]
+    b = E.Batch(precision=abi.EDUS_PREC_MIXED)
+    slots = [b.add(p) for p in pbs]
+    drain(b, slots)
+    for s, (rho, log) in zip(slots, ref):
+        assert np.abs(b.get_state(s) - rho).max() < 1e-5
+        assert rel(J1(b.obs(s)), J1(log)) < 1e-5
+
+
+def test_admission_by_hbm_budget(workdir):
+    pbs = problems(workdir)
+    probe = E.Batch()
+    need = probe.footprint(pbs[0])
+    probe.close()
+    b = E.Batch(hbm_budget_bytes=int(need * 2.5))
+    a = b.try_add(pbs[0])
+    c = b.try_add(pbs[0])
+    assert a is not None and c is not None
+    assert b.try_add(pbs[0]) is None          # the third does not fit
+    st = b.stats()
+    assert st["active"] == 2 and st["bytes_used"] == 2 * need
+    b.release(a)
+    assert b.try_add(pbs[0]) is not None      # fits again once a slot is released
+
+
+def test_unsupported_instances_are_refused(workdir):
+    d = f"{workdir}/coul"
+    p = E.Problem(E.parse_input(W.hbn_coulomb(d, n=12, t_fin_fs=0.2)), d)
+    b = E.Batch()
+    with pytest.raises(E.EdusError) as ei:
+        b.add(p)
+    assert ei.value.code == abi.EDUS_EUNSUPPORTED
