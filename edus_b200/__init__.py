@@ -10,6 +10,7 @@ from .lib import (  # noqa: F401
     Problem,
     Context,
     Batch,
+    Server,
     load_library,
     parse_input,
     default_params,
@@ -17,4 +18,4 @@ from .lib import (  # noqa: F401
 )
 from . import abi  # noqa: F401
 
-__all__ = ["EdusError", "Problem", "Context", "Batch", "load_library", "parse_input", "default_params", "abi", "library_path"]
+__all__ = ["EdusError", "Problem", "Context", "Batch", "Server", "load_library", "parse_input", "default_params", "abi", "library_path"]

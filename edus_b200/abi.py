@@ -209,3 +209,51 @@ class BatchStats(C.Structure):
 
 
 EDUS_INST_FREE, EDUS_INST_RUNNING, EDUS_INST_DONE = 0, 1, 2
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [
+        ("batch", BatchOptions),
+        ("setup_threads", C.c_int32),
+        ("drop_decoupled_core", C.c_int32),
+        ("max_bypass_s", C.c_double),
+    ]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("error", C.c_int32),
+        ("nbands", C.c_int32),
+        ("nobs", C.c_int32),
+        ("nk", C.c_int64),
+        ("steps", C.c_int64),
+        ("footprint_bytes", C.c_int64),
+        ("t_submit", C.c_double),
+        ("t_ready", C.c_double),
+        ("t_admit", C.c_double),
+        ("t_done", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("failed", C.c_int64),
+        ("running", C.c_int64),
+        ("waiting", C.c_int64),
+        ("span_s", C.c_double),
+        ("solves_per_s", C.c_double),
+        ("kpoint_steps_per_s", C.c_double),
+        ("p50_latency_s", C.c_double),
+        ("p99_latency_s", C.c_double),
+        ("max_latency_s", C.c_double),
+        ("device_ms", C.c_double),
+        ("peak_bytes", C.c_int64),
+        ("peak_active", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+
+EDUS_REQ_QUEUED, EDUS_REQ_SETUP, EDUS_REQ_READY, EDUS_REQ_RUNNING, EDUS_REQ_DONE, EDUS_REQ_FAILED = range(6)

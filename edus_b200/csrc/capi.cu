@@ -583,6 +583,11 @@ int edus_problem_create(const edus_params* p, const char* workdir, edus_problem*
   return 0;
 }
 
+int edus_problem_drop_decoupled_core(edus_problem* pb) {
+  if (!pb) return fail(EDUS_EINVAL, "null argument");
+  return drop_decoupled_core(pb->P);
+}
+
 int edus_problem_info_get(const edus_problem* pb, edus_problem_info* o) {
   if (!pb || !o) return fail(EDUS_EINVAL, "null argument");
   const Problem& P = pb->P;

@@ -619,4 +619,58 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P) {
   return 0;
 }
 
+// Drop core bands that no term of the run couples to the other bands: H, D and
+// GradientEnergy have no core/non-core entries (or only dipole components the
+// pump field never has), the probe is off and nothing dissipates. The core
+// rows of the equations of motion are then constant (rho_cc = 1), and the
+// remaining block evolves exactly as in the full problem.
+int drop_decoupled_core(Problem& P) {
+  const int nch = P.nch, n = P.ncv, nk = P.nk;
+  if (nch == 0) return fail(EDUS_EINVAL, "no core band to drop");
+  if (!P.diss_i.empty()) return fail(EDUS_EUNSUPPORTED, "core band is coupled: dissipation is on");
+  if (P.p.probe.E0 != 0.0) return fail(EDUS_EUNSUPPORTED, "core band is coupled: the probe field is on");
+  if (P.p.coulomb) return fail(EDUS_EUNSUPPORTED, "core band is coupled: Coulomb mean field is on");
+  bool field_x[3] = {false, false, false};
+  for (int ip = 0; ip < P.p.n_pumps; ip++)
+    for (int x = 0; x < 3; x++)
+      if (P.p.pump[ip].pol1[x] != 0.0 || P.p.pump[ip].pol2[x] != 0.0) field_x[x] = true;
+  for (int k = 0; k < nk; k++)
+    for (int i = 0; i < nch; i++)
+      for (int j = nch; j < n; j++) {
+        const size_t ij = ((size_t)k * n + i) * n + j, ji = ((size_t)k * n + j) * n + i;
+        if (P.H[ij] != 0.0 || P.H[ji] != 0.0) return fail(EDUS_EUNSUPPORTED, "core band is coupled through H");
+        for (int x = 0; x < 3; x++) {
+          if (field_x[x] && (P.D[ij * 3 + x] != 0.0 || P.D[ji * 3 + x] != 0.0))
+            return fail(EDUS_EUNSUPPORTED, "core band is coupled through the dipole along the field");
+          if (P.GE[ij * 3 + x] != 0.0 || P.GE[ji * 3 + x] != 0.0) return fail(EDUS_EUNSUPPORTED, "core band is coupled through dH/dk");
+        }
+      }
+  const int m = n - nch;
+  auto shrink = [&](std::vector<cd>& A, int comps) {
+    if (A.empty()) return;
+    std::vector<cd> B((size_t)nk * m * m * comps);
+    for (int k = 0; k < nk; k++)
+      for (int i = 0; i < m; i++)
+        for (int j = 0; j < m; j++)
+          for (int x = 0; x < comps; x++)
+            B[(((size_t)k * m + i) * m + j) * comps + x] = A[(((size_t)k * n + i + nch) * n + j + nch) * comps + x];
+    A.swap(B);
+  };
+  // U rows are eigenvectors; the model's non-core rows have no core components
+  for (int k = 0; k < nk; k++)
+    for (int i = nch; i < n; i++)
+      for (int c = 0; c < nch; c++)
+        if (P.U[((size_t)k * n + i) * n + c] != 0.0) return fail(EDUS_EUNSUPPORTED, "core band mixes into the band basis");
+  shrink(P.H, 1);
+  shrink(P.U, 1);
+  shrink(P.D, 3);
+  shrink(P.GE, 3);
+  shrink(P.P0, 1);
+  P.ncv = m;
+  P.nch = 0;
+  P.nbands = P.nv;
+  P.p.nb[0] = 0;
+  return 0;
+}
+
 }  // namespace edus

@@ -46,6 +46,8 @@ struct Problem {
 };
 
 int build_problem(const edus_params& p, const char* workdir, Problem& out);
+// Remove core bands the run never couples (see problem.cpp); EDUS_EUNSUPPORTED if coupled.
+int drop_decoupled_core(Problem& P);
 // H, U, D of the problem's model at one crystal k point (save_HUD.cpp conventions).
 int model_hud(const Problem& P, const double* kcrys, cd* H, cd* U, cd* D);
 

@@ -36,6 +36,7 @@ def load_library():
         "edus_params_default": (C.c_int, [P(abi.Params)]),
         "edus_problem_create": (C.c_int, [P(abi.Params), cp, P(vp)]),
         "edus_problem_info_get": (C.c_int, [vp, P(abi.ProblemInfo)]),
+        "edus_problem_drop_decoupled_core": (C.c_int, [vp]),
         "edus_problem_get": (C.c_int, [vp, cp, vp, sz]),
         "edus_problem_free": (None, [vp]),
         "edus_model_hud": (C.c_int, [vp, P(dbl), vp, vp, vp]),
@@ -76,6 +77,16 @@ def load_library():
         "edus_batch_release": (C.c_int, [vp, i32]),
         "edus_batch_stats_get": (C.c_int, [vp, P(abi.BatchStats)]),
         "edus_batch_tile_k": (C.c_int, [vp, i32, P(i32)]),
+        "edus_server_options_default": (C.c_int, [P(abi.ServerOptions)]),
+        "edus_server_create": (C.c_int, [P(abi.ServerOptions), P(vp)]),
+        "edus_server_submit": (C.c_int, [vp, P(abi.Params), cp, P(C.c_int64)]),
+        "edus_server_info": (C.c_int, [vp, C.c_int64, P(abi.RequestInfo)]),
+        "edus_server_obs": (C.c_int, [vp, C.c_int64, i32, i32, P(abi.Obs)]),
+        "edus_server_forget": (C.c_int, [vp, C.c_int64]),
+        "edus_server_drain": (C.c_int, [vp, dbl]),
+        "edus_server_stats_get": (C.c_int, [vp, P(abi.ServerStats)]),
+        "edus_server_clock": (dbl, [vp]),
+        "edus_server_destroy": (None, [vp]),
         "edus_strerror": (cp, [C.c_int]),
         "edus_last_error": (cp, []),
         "edus_abi_version": (C.c_int, []),
@@ -120,6 +131,14 @@ class Problem:
         _check(L.edus_problem_create(C.byref(params), os.fsencode(workdir), C.byref(self._h)), "edus_problem_create")
         self.info = abi.ProblemInfo()
         _check(L.edus_problem_info_get(self._h, C.byref(self.info)), "edus_problem_info_get")
+
+    def drop_decoupled_core(self):
+        """Remove core bands nothing in the run couples (edus_problem_drop_decoupled_core)."""
+        L = load_library()
+        _check(L.edus_problem_drop_decoupled_core(self._h), "edus_problem_drop_decoupled_core")
+        self.info = abi.ProblemInfo()
+        _check(L.edus_problem_info_get(self._h, C.byref(self.info)), "edus_problem_info_get")
+        return self
 
     def get(self, name):
         i = self.info
@@ -357,6 +376,78 @@ class Batch:
     def close(self):
         if self._h:
             self._L.edus_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Request loop over one batch (edus_server_* of the C ABI): submit solves at
+    any time; they are admitted by HBM footprint and run concurrently."""
+
+    def __init__(self, device=0, precision=abi.EDUS_PREC_FP64, max_instances=1024, chunk_steps=16,
+                 hbm_budget_bytes=0, setup_threads=4, drop_decoupled_core=True, max_bypass_s=2.0, tile_k=None):
+        L = load_library()
+        self._L = L
+        o = abi.ServerOptions()
+        _check(L.edus_server_options_default(C.byref(o)), "edus_server_options_default")
+        o.batch.device = device
+        o.batch.precision = precision
+        o.batch.max_instances = max_instances
+        o.batch.chunk_steps = chunk_steps
+        o.batch.hbm_budget_bytes = int(hbm_budget_bytes)
+        for n, k in (tile_k or {}).items():
+            o.batch.tile_k[n] = k
+        o.setup_threads = setup_threads
+        o.drop_decoupled_core = 1 if drop_decoupled_core else 0
+        o.max_bypass_s = max_bypass_s
+        self._h = C.c_void_p()
+        _check(L.edus_server_create(C.byref(o), C.byref(self._h)), "edus_server_create")
+        self._keep = {}
+
+    def submit(self, params, workdir="."):
+        rid = C.c_int64()
+        _check(self._L.edus_server_submit(self._h, C.byref(params), os.fsencode(workdir), C.byref(rid)), "edus_server_submit")
+        self._keep[rid.value] = params
+        return rid.value
+
+    def info(self, rid):
+        o = abi.RequestInfo()
+        _check(self._L.edus_server_info(self._h, int(rid), C.byref(o)), "edus_server_info")
+        return {f: getattr(o, f) for f, _ in abi.RequestInfo._fields_}
+
+    def obs(self, rid):
+        i = self.info(rid)
+        if i["status"] == abi.EDUS_REQ_FAILED:
+            msg = self._L.edus_last_error().decode(errors="replace")
+            raise EdusError(i["error"], "edus_server_obs", msg)
+        buf = (abi.Obs * max(i["nobs"], 1))()
+        if i["nobs"]:
+            _check(self._L.edus_server_obs(self._h, int(rid), 0, i["nobs"], buf), "edus_server_obs")
+        return [abi.obs_to_dict(buf[q], i["nbands"]) for q in range(i["nobs"])]
+
+    def forget(self, rid):
+        _check(self._L.edus_server_forget(self._h, int(rid)), "edus_server_forget")
+        self._keep.pop(rid, None)
+
+    def drain(self, timeout_s=600.0):
+        _check(self._L.edus_server_drain(self._h, float(timeout_s)), "edus_server_drain")
+
+    def stats(self):
+        s = abi.ServerStats()
+        _check(self._L.edus_server_stats_get(self._h, C.byref(s)), "edus_server_stats_get")
+        return {f: getattr(s, f) for f, _ in abi.ServerStats._fields_ if f != "pad"}
+
+    def clock(self):
+        return self._L.edus_server_clock(self._h)
+
+    def close(self):
+        if self._h:
+            self._L.edus_server_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -165,6 +165,14 @@ typedef struct {
  * Coulomb coefficient files. workdir holds <ref>_tb.dat and Output/Coulomb/. */
 int edus_problem_create(const edus_params* p, const char* workdir, edus_problem** out);
 int edus_problem_info_get(const edus_problem* pb, edus_problem_info* out);
+/* Remove the core bands when nothing in the run couples them to the other
+ * bands (no probe, no dissipation, no Coulomb, no H / dH/dk entries and no
+ * dipole component along the pump between core and the rest). The remaining
+ * bands then evolve exactly as in the full problem, with fewer elements per
+ * k point (the Haldane_CoreBN models with an in-plane pump become 2-band).
+ * EDUS_EUNSUPPORTED (problem unchanged) when a coupling exists. No
+ * counterpart in the reference. */
+int edus_problem_drop_decoupled_core(edus_problem* pb);
 /* Copy a named host array out (names: "kpt","H","U","D","GE","P0","nbr",
  * "weights","bvec","T","wq_A","wq_B","wq_C","wq_D","screen","vhartree",
  * "HR","rR","Rvec"); nbytes must match exactly. */
@@ -317,6 +325,61 @@ int edus_batch_release(edus_batch* b, int32_t slot);
 int edus_batch_stats_get(edus_batch* b, edus_batch_stats* out);
 /* Tile length in use for a band count (after the autotuner). */
 int edus_batch_tile_k(edus_batch* b, int32_t nbands, int32_t* kt);
+
+/* ------------------------------------------------------- serving
+ * A request loop over one batch. Submitted solves are set up on host threads
+ * (input -> grid, stencil, model tables), then admitted into the batch when
+ * their HBM footprint fits, oldest first (a younger request may pass one that
+ * does not fit yet, for at most max_bypass_s). Admitted solves keep their
+ * state on the device and advance together with every other running solve;
+ * each is retired when its time grid ends, its observables copied to the host
+ * and its memory returned. The loop runs on its own thread; every function
+ * here may be called from any thread. No counterpart in the reference. */
+typedef struct edus_server edus_server;
+
+typedef struct {
+  edus_batch_options batch;
+  int32_t setup_threads;        /* host threads building problems */
+  int32_t drop_decoupled_core;  /* apply edus_problem_drop_decoupled_core where it holds */
+  double max_bypass_s;          /* how long younger requests may pass one that does not fit */
+} edus_server_options;
+
+enum { EDUS_REQ_QUEUED = 0, EDUS_REQ_SETUP = 1, EDUS_REQ_READY = 2, EDUS_REQ_RUNNING = 3, EDUS_REQ_DONE = 4, EDUS_REQ_FAILED = 5 };
+
+typedef struct {
+  int32_t status, error;        /* EDUS_REQ_*, EDUS_E* when FAILED */
+  int32_t nbands, nobs;
+  int64_t nk, steps;
+  int64_t footprint_bytes;
+  double t_submit, t_ready, t_admit, t_done;  /* seconds on the server clock */
+} edus_request_info;
+
+typedef struct {
+  int64_t submitted, completed, failed, running, waiting;
+  double span_s;                /* first submission to last completion */
+  double solves_per_s;          /* completed / span_s */
+  double kpoint_steps_per_s;    /* k-point steps of the completed solves / span_s */
+  double p50_latency_s, p99_latency_s, max_latency_s;  /* t_done - t_submit */
+  double device_ms;             /* CUDA-event time of the batch chunks */
+  int64_t peak_bytes;           /* largest HBM footprint in use at once */
+  int32_t peak_active, pad;
+} edus_server_stats;
+
+int edus_server_options_default(edus_server_options* o);
+int edus_server_create(const edus_server_options* o, edus_server** out);
+/* Queue a solve; returns at once. workdir holds its model files. */
+int edus_server_submit(edus_server* s, const edus_params* p, const char* workdir, int64_t* id);
+int edus_server_info(edus_server* s, int64_t id, edus_request_info* out);
+/* Observables of a DONE request (EDUS_ENOTREADY before). */
+int edus_server_obs(edus_server* s, int64_t id, int32_t first, int32_t count, edus_obs* out);
+/* Drop a finished request's results. */
+int edus_server_forget(edus_server* s, int64_t id);
+/* Wait until every submitted request is DONE or FAILED (EDUS_ETIMEOUT otherwise). */
+int edus_server_drain(edus_server* s, double timeout_s);
+int edus_server_stats_get(edus_server* s, edus_server_stats* out);
+/* Seconds on the server clock (the time base of edus_request_info). */
+double edus_server_clock(edus_server* s);
+void edus_server_destroy(edus_server* s);
 
 /* ------------------------------------------------------- strings */
 const char* edus_strerror(int code);
