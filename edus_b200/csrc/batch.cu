@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "cuda/batch.cuh"
+#include "cuda/model_build.hpp"
 #include "host/problem.hpp"
 
 namespace edus {
@@ -174,6 +175,91 @@ int upload_model(edus_batch* b, const Problem& P, const Inst& I) {
   for (int k = 0; k < nk; k++)
     for (int e = 0; e < n * n; e++) pl[(size_t)e * nk + k] = mkc<T>(P.U[(size_t)k * n * n + e]);
   return put(b, (void*)I.U, pl);
+}
+
+// Deferred Wannier model: tabulate H, D, U, dH/dk and the initial state on the
+// device (cuda/model_build.cu) straight into the instance's tables; mixed
+// precision goes through FP64 scratch and is rounded once.
+int build_model_on_device(edus_batch* b, const Problem& P, const Inst& I) {
+  const int n = P.ncv, nt = n * (n + 1) / 2, nk = P.nk, nr = P.nrpts;
+  std::vector<double2> coef((size_t)4 * nt * nr);
+  for (int i = 0; i < n; i++)
+    for (int j = i; j < n; j++) {
+      const int e = tri_index(i, j, n);
+      for (int r = 0; r < nr; r++) {
+        coef[(size_t)e * nr + r] = mkc<double2>(P.HR[((size_t)i * n + j) * nr + r]);
+        for (int x = 0; x < 3; x++) {
+          const cd v = 0.5 * (P.rR[(((size_t)x * n + i) * n + j) * nr + r] + P.rR[(((size_t)x * n + j) * n + i) * nr + r]);
+          coef[((size_t)(1 + x) * nt + e) * nr + r] = mkc<double2>(v);
+        }
+      }
+    }
+  std::vector<double> gb((size_t)P.nnb * 3);
+  for (int bb = 0; bb < P.nnb; bb++)
+    for (int x = 0; x < 3; x++) gb[bb * 3 + x] = P.shell_w[P.bshell[bb]] * P.bvec[bb * 3 + x];
+  const size_t plane = (size_t)nt * nk;
+  // scratch: inputs, and FP64 outputs when the instance stores FP32
+  size_t bytes = align256(sizeof(double) * 3 * nk) + align256(sizeof(double) * 3 * nr) + align256(sizeof(double2) * coef.size()) +
+                 align256(sizeof(double) * gb.size());
+  if (b->mixed) bytes += align256(sizeof(double2) * plane) * (4 + (I.GE ? 3 : 0)) + align256(sizeof(double2) * n * n * nk);
+  char* base = nullptr;
+  if (cudaMallocAsync((void**)&base, bytes, b->pool, b->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(EDUS_ENOMEM, "batch: model build scratch of %zu bytes", bytes);
+  }
+  char* p = base;
+  auto carve = [&](size_t sz) {
+    char* r = p;
+    p += align256(sz);
+    return r;
+  };
+  ModelBuildArgs a;
+  memset(&a, 0, sizeof(a));
+  a.n = n;
+  a.ntri = nt;
+  a.nk = nk;
+  a.nr = nr;
+  a.nnb = P.nnb;
+  a.nbands = P.nbands;
+  a.nv = P.p.nb[1];
+  a.scissor = P.p.conduction_shift;
+  double* dk = (double*)carve(sizeof(double) * 3 * nk);
+  double* dR = (double*)carve(sizeof(double) * 3 * nr);
+  double2* dc = (double2*)carve(sizeof(double2) * coef.size());
+  double* dg = (double*)carve(sizeof(double) * gb.size());
+  int rc;
+  if ((rc = put(b, dk, P.kpt)) || (rc = put(b, dR, P.Rvec)) || (rc = put(b, dc, coef)) || (rc = put(b, dg, gb))) {
+    cudaFreeAsync(base, b->stream);
+    return rc;
+  }
+  a.kpt = dk;
+  a.Rvec = dR;
+  a.coef = dc;
+  a.gb = dg;
+  a.nbr = I.nbr;
+  a.P0 = I.P0;
+  if (b->mixed) {
+    a.H = (double2*)carve(sizeof(double2) * plane);
+    a.D = (double2*)carve(sizeof(double2) * 3 * plane);
+    a.U = (double2*)carve(sizeof(double2) * n * n * nk);
+    a.GE = I.GE ? (double2*)carve(sizeof(double2) * 3 * plane) : nullptr;
+  } else {
+    a.H = (double2*)I.H;
+    a.D = (double2*)I.D;
+    a.U = (double2*)I.U;
+    a.GE = (double2*)I.GE;
+  }
+  cudaError_t e = build_wannier_model(a, b->stream);
+  if (e == cudaSuccess && b->mixed) {
+    if (e == cudaSuccess) e = planes_to_float(a.H, (float2*)I.H, plane, b->stream);
+    if (e == cudaSuccess) e = planes_to_float(a.D, (float2*)I.D, 3 * plane, b->stream);
+    if (e == cudaSuccess) e = planes_to_float(a.U, (float2*)I.U, (size_t)n * n * nk, b->stream);
+    if (e == cudaSuccess && I.GE) e = planes_to_float(a.GE, (float2*)I.GE, 3 * plane, b->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((void*)I.Peq, I.P0, sizeof(double2) * plane, cudaMemcpyDeviceToDevice, b->stream);
+  }
+  cudaFreeAsync(base, b->stream);
+  if (e != cudaSuccess) return fail(EDUS_ECUDA, "batch: device model build: %s", cudaGetErrorString(e));
+  return 0;
 }
 
 void free_slot_mem(edus_batch* b, Slot& s) {
@@ -465,18 +551,25 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
     free_slot_mem(b, s);
     return code;
   };
-  // tables and initial state
-  rc = b->mixed ? upload_model<float2>(b, P, I) : upload_model<double2>(b, P, I);
-  if (rc) return undo(rc);
+  // neighbour table, then model tables and initial state (host-built, or
+  // tabulated on the device from H(R), r(R) for a deferred Wannier model)
   {
-    std::vector<double2> st;
-    planes<double2>(P.P0.data(), nk, n, 1, st);
-    if ((rc = put(b, I.P0, st))) return undo(rc);
-    if (I.Peq && (rc = put(b, (void*)I.Peq, st))) return undo(rc);
     std::vector<int> nb((size_t)P.nnb * nk);
     for (int k = 0; k < nk; k++)
       for (int bb = 0; bb < P.nnb; bb++) nb[(size_t)bb * nk + k] = P.nbr[(size_t)k * P.nnb + bb];
     if ((rc = put(b, (void*)I.nbr, nb))) return undo(rc);
+  }
+  if (P.model_deferred) {
+    if ((rc = build_model_on_device(b, P, I))) return undo(rc);
+  } else {
+    rc = b->mixed ? upload_model<float2>(b, P, I) : upload_model<double2>(b, P, I);
+    if (rc) return undo(rc);
+    std::vector<double2> st;
+    planes<double2>(P.P0.data(), nk, n, 1, st);
+    if ((rc = put(b, I.P0, st))) return undo(rc);
+    if (I.Peq && (rc = put(b, (void*)I.Peq, st))) return undo(rc);
+  }
+  {
     // field table: the single-solve loop's times (t += dt) and fields
     std::vector<FieldRow> fr((size_t)P.itfi + 2);
     double t = P.t_start;

@@ -583,6 +583,20 @@ int edus_problem_create(const edus_params* p, const char* workdir, edus_problem*
   return 0;
 }
 
+int edus_problem_create_deferred(const edus_params* p, const char* workdir, edus_problem** out) {
+  clear_error();
+  if (!p || !out) return fail(EDUS_EINVAL, "null argument");
+  edus_problem* pb = new (std::nothrow) edus_problem();
+  if (!pb) return fail(EDUS_ENOMEM, "host allocation");
+  int rc = build_problem(*p, workdir, pb->P, true);
+  if (rc) {
+    delete pb;
+    return rc;
+  }
+  *out = pb;
+  return 0;
+}
+
 int edus_problem_drop_decoupled_core(edus_problem* pb) {
   if (!pb) return fail(EDUS_EINVAL, "null argument");
   return drop_decoupled_core(pb->P);
@@ -699,6 +713,8 @@ void edus_destroy(edus_ctx* c) {
 int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out) {
   clear_error();
   if (!pb || !out) return fail(EDUS_EINVAL, "null argument");
+  if (pb->P.model_deferred)
+    return fail(EDUS_EUNSUPPORTED, "the problem's model is tabulated on the device only in batches (edus_problem_create)");
   edus_options o;
   edus_options_default(&o);
   if (opt) o = *opt;

@@ -527,7 +527,7 @@ int model_hud(const Problem& P, const double* kcrys, cd* H, cd* U, cd* D) {
   return 0;
 }
 
-int build_problem(const edus_params& p, const char* workdir, Problem& P) {
+int build_problem(const edus_params& p, const char* workdir, Problem& P, bool defer_model) {
   P = Problem();
   P.p = p;
   P.nch = p.nb[0];
@@ -544,10 +544,13 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P) {
   if (rc) return rc;
   const int nk = P.nk;
   const size_t st = (size_t)nk * n * n;
-  P.H.assign(st, 0);
-  P.U.assign(st, 0);
-  P.D.assign(st * 3, 0);
   const bool isW = p.mode == EDUS_MODE_WANNIER;
+  // a deferred Wannier model keeps only H(R), r(R); the device tabulates it
+  P.model_deferred = isW && defer_model;
+  const size_t sk = P.model_deferred ? 0 : st;
+  P.H.assign(sk, 0);
+  P.U.assign(sk, 0);
+  P.D.assign(sk * 3, 0);
   Tb tb;
   if (isW) {
     rc = read_wannier(P, workdir);
@@ -555,12 +558,14 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P) {
     rc = tb_setup(p, tb);
   }
   if (rc) return rc;
+  if (!P.model_deferred) {
 #pragma omp parallel for schedule(static)
-  for (int ik = 0; ik < nk; ik++)
-    eval_k(P, tb, &P.kpt[ik * 3], &P.H[(size_t)ik * n * n], &P.U[(size_t)ik * n * n], &P.D[(size_t)ik * n * n * 3]);
+    for (int ik = 0; ik < nk; ik++)
+      eval_k(P, tb, &P.kpt[ik * 3], &P.H[(size_t)ik * n * n], &P.U[(size_t)ik * n * n], &P.D[(size_t)ik * n * n * 3]);
+  }
   // gradient of the energy (Source_Main/save_HUD.cpp:96-137)
-  P.GE.assign(st * 3, 0);
-  if (p.current) {
+  P.GE.assign(sk * 3, 0);
+  if (p.current && !P.model_deferred) {
 #pragma omp parallel for schedule(static)
     for (int ik = 0; ik < nk; ik++)
       for (int x = 0; x < 3; x++)
@@ -591,8 +596,8 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P) {
         P.diss_j.push_back(jc);
       }
   // initial population (rows/columns swapped as in the reference)
-  P.P0.assign(st, 0);
-  for (int ik = 0; ik < nk; ik++)
+  P.P0.assign(sk, 0);
+  for (int ik = 0; ik < (P.model_deferred ? 0 : nk); ik++)
     for (int ia = 0; ia < n; ia++)
       for (int ib = 0; ib < n; ib++) {
         cd acc = 0;
@@ -627,6 +632,7 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P) {
 int drop_decoupled_core(Problem& P) {
   const int nch = P.nch, n = P.ncv, nk = P.nk;
   if (nch == 0) return fail(EDUS_EINVAL, "no core band to drop");
+  if (P.model_deferred) return fail(EDUS_EUNSUPPORTED, "model tables are not tabulated on the host");
   if (!P.diss_i.empty()) return fail(EDUS_EUNSUPPORTED, "core band is coupled: dissipation is on");
   if (P.p.probe.E0 != 0.0) return fail(EDUS_EUNSUPPORTED, "core band is coupled: the probe field is on");
   if (P.p.coulomb) return fail(EDUS_EUNSUPPORTED, "core band is coupled: Coulomb mean field is on");

@@ -43,9 +43,11 @@ struct Problem {
   double t_start = 0;
   int itfi = 0;                   // last iteration index (constant dt)
   int nsteps = 0, nprint = 0;
+  // Wannier model left untabulated (H, U, D, GE, P0 empty): built on the device
+  bool model_deferred = false;
 };
 
-int build_problem(const edus_params& p, const char* workdir, Problem& out);
+int build_problem(const edus_params& p, const char* workdir, Problem& out, bool defer_model = false);
 // Remove core bands the run never couples (see problem.cpp); EDUS_EUNSUPPORTED if coupled.
 int drop_decoupled_core(Problem& P);
 // H, U, D of the problem's model at one crystal k point (save_HUD.cpp conventions).

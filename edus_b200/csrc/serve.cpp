@@ -87,7 +87,8 @@ void setup_worker(edus_server* s) {
       r->status = EDUS_REQ_SETUP;
     }
     std::unique_ptr<edus_problem> pb(new (std::nothrow) edus_problem());
-    int rc = pb ? edus::build_problem(r->p, r->workdir.c_str(), pb->P) : EDUS_ENOMEM;
+    // Wannier models are tabulated on the device at admission
+    int rc = pb ? edus::build_problem(r->p, r->workdir.c_str(), pb->P, true) : EDUS_ENOMEM;
     if (rc == 0 && s->opt.drop_decoupled_core && pb->P.nch > 0) {
       // applies only where it holds; otherwise the problem is left as built
       if (edus::drop_decoupled_core(pb->P) != 0) edus::clear_error();

@@ -37,6 +37,7 @@ def load_library():
         "edus_problem_create": (C.c_int, [P(abi.Params), cp, P(vp)]),
         "edus_problem_info_get": (C.c_int, [vp, P(abi.ProblemInfo)]),
         "edus_problem_drop_decoupled_core": (C.c_int, [vp]),
+        "edus_problem_create_deferred": (C.c_int, [P(abi.Params), cp, P(vp)]),
         "edus_problem_get": (C.c_int, [vp, cp, vp, sz]),
         "edus_problem_free": (None, [vp]),
         "edus_model_hud": (C.c_int, [vp, P(dbl), vp, vp, vp]),
@@ -123,12 +124,16 @@ def parse_input(path):
 class Problem:
     """Host-side problem (grid, stencil, model tables, initial state)."""
 
-    def __init__(self, params, workdir="."):
+    def __init__(self, params, workdir=".", defer_model=False):
         L = load_library()
         self._L = L
         self.params = params
         self._h = C.c_void_p()
-        _check(L.edus_problem_create(C.byref(params), os.fsencode(workdir), C.byref(self._h)), "edus_problem_create")
+        if defer_model:
+            _check(L.edus_problem_create_deferred(C.byref(params), os.fsencode(workdir), C.byref(self._h)),
+                   "edus_problem_create_deferred")
+        else:
+            _check(L.edus_problem_create(C.byref(params), os.fsencode(workdir), C.byref(self._h)), "edus_problem_create")
         self.info = abi.ProblemInfo()
         _check(L.edus_problem_info_get(self._h, C.byref(self.info)), "edus_problem_info_get")
 

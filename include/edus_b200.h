@@ -165,6 +165,12 @@ typedef struct {
  * Coulomb coefficient files. workdir holds <ref>_tb.dat and Output/Coulomb/. */
 int edus_problem_create(const edus_params* p, const char* workdir, edus_problem** out);
 int edus_problem_info_get(const edus_problem* pb, edus_problem_info* out);
+/* As edus_problem_create, but a Wannier model is not tabulated on the host:
+ * H(k), D(k), U(k), dH/dk and the initial state are built on the device when
+ * the problem is admitted to a batch (seconds of host work become
+ * milliseconds of device work). Single-solve contexts need host tables and
+ * refuse such a problem. Tight-binding models are tabulated as usual. */
+int edus_problem_create_deferred(const edus_params* p, const char* workdir, edus_problem** out);
 /* Remove the core bands when nothing in the run couples them to the other
  * bands (no probe, no dissipation, no Coulomb, no H / dH/dk entries and no
  * dipole component along the pump between core and the rest). The remaining

@@ -132,3 +132,23 @@ def test_unsupported_instances_are_refused(workdir):
     with pytest.raises(E.EdusError) as ei:
         b.add(p)
     assert ei.value.code == abi.EDUS_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("nw,nside,name", [(8, 11, "W8"), (16, 13, "W16")])
+def test_device_built_wannier_model_matches_host_build(workdir, nw, nside, name):
+    """A deferred problem (model tabulated on the device at admission) evolves
+    like the host-tabulated one: rho0 is the same projector, J(t) and the
+    populations agree (eigenvector phases differ and cancel)."""
+    d = f"{workdir}/{name}"
+    p = E.parse_input(W.wannier(d, nw=nw, nside=nside, n=12, t_fin_fs=0.3, it_res=4, name=name))
+    host = E.Problem(p, d)
+    dev = E.Problem(p, d, defer_model=True)
+    b = E.Batch(chunk_steps=8)
+    sh, sd = b.add(host), b.add(dev)
+    assert np.abs(b.get_state(sh) - b.get_state(sd)).max() < 1e-13
+    drain(b, [sh, sd], 8)
+    assert np.abs(b.get_state(sh) - b.get_state(sd)).max() < 1e-12
+    lh, ld = b.obs(sh), b.obs(sd)
+    assert rel(J1(ld), J1(lh)) < 1e-10
+    ph, pd = np.array([x["pop"] for x in lh]), np.array([x["pop"] for x in ld])
+    assert np.abs(ph - pd).max() < 1e-12

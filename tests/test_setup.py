@@ -97,3 +97,12 @@ def test_problem_rejects_bad_input(workdir):
     with pytest.raises(E.EdusError) as ei:
         E.Problem(p, workdir)
     assert ei.value.code == E.abi.EDUS_EUNSUPPORTED
+
+
+def test_deferred_problem_is_refused_by_single_solve_contexts(workdir):
+    p = E.parse_input(W.wannier(workdir, n=8, t_fin_fs=0.1))
+    pb = E.Problem(p, workdir, defer_model=True)
+    assert pb.info.nrpts == 121
+    with pytest.raises(E.EdusError) as ei:
+        E.Context(pb)
+    assert ei.value.code == E.abi.EDUS_EUNSUPPORTED
