@@ -9,6 +9,12 @@ one complete solve (6043 time steps of 14400 k points). Inputs are synthetic
 (generated by edus_b200.workloads); nothing is read from the reference.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py --workload wannier|sweep|serve [--requests R]
+
+--workload selects the batched / served measurements of edus_b200.suite
+(8-band Wannier solves, the 256-instance pulse sweep, the request stream),
+each against the plain FP64 single-solve path and with the J(t) error of the
+mixed-precision path.
 
 N > 1 runs one independent solve per GPU (replicas, weak scaling); the time is
 the max over ranks. --impl reference times the CPU restatement of the reference
@@ -42,6 +48,9 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["coulomb", "wannier", "sweep", "serve"], default="coulomb")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the stream")
+    ap.add_argument("--rate", type=float, default=None, help="serve: Poisson arrival rate (1/s); default all at once")
     return ap.parse_args()
 
 
@@ -286,10 +295,31 @@ def run_ours(args):
     return 0
 
 
+def run_suite(args):
+    import torch
+
+    from edus_b200 import suite
+
+    torch.cuda.set_device(0)
+    sampler = ClockSampler(0)
+    sampler.start()
+    if args.workload == "wannier":
+        line = suite.wannier_line()
+    elif args.workload == "sweep":
+        line = suite.sweep_line()
+    else:
+        line = suite.serve_line(count=args.requests, rate=args.rate)
+    line.update({"n_gpus": 1, "clocks": sampler.stop()})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "coulomb":
+        return run_suite(args)
     return run_ours(args)
 
 

@@ -65,8 +65,9 @@ struct ClassTab {
 
 struct Layout {
   size_t state, H, D, GE, U, nbr, field, log, part;
-  size_t eq;  // initial state kept for the mixed-precision deviation form
-  size_t total() const { return 4 * state + eq + H + D + GE + U + nbr + field + log + part + 256; }
+  size_t eq;     // initial state kept for the mixed-precision deviation form
+  size_t hdiag;  // FP64 band energies of the mixed-precision commutator
+  size_t total() const { return 4 * state + eq + hdiag + H + D + GE + U + nbr + field + log + part + 256; }
 };
 
 }  // namespace
@@ -109,6 +110,7 @@ Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
   Layout L;
   L.state = align256(nt * nk * sizeof(double2));
   L.eq = b->mixed ? L.state : 0;
+  L.hdiag = b->mixed ? align256(n * nk * sizeof(double)) : 0;
   L.H = align256(nt * nk * s);
   L.D = align256(3 * nt * nk * s);
   L.GE = P.p.current ? align256(3 * nt * nk * s) : 0;
@@ -174,7 +176,14 @@ int upload_model(edus_batch* b, const Problem& P, const Inst& I) {
   pl.resize((size_t)n * n * nk);
   for (int k = 0; k < nk; k++)
     for (int e = 0; e < n * n; e++) pl[(size_t)e * nk + k] = mkc<T>(P.U[(size_t)k * n * n + e]);
-  return put(b, (void*)I.U, pl);
+  if ((rc = put(b, (void*)I.U, pl))) return rc;
+  if (I.Hdiag) {
+    std::vector<double> hd((size_t)n * nk);
+    for (int k = 0; k < nk; k++)
+      for (int i = 0; i < n; i++) hd[(size_t)i * nk + k] = P.H[((size_t)k * n + i) * n + i].real();
+    if ((rc = put(b, (void*)I.Hdiag, hd))) return rc;
+  }
+  return 0;
 }
 
 // Deferred Wannier model: tabulate H, D, U, dH/dk and the initial state on the
@@ -251,6 +260,7 @@ int build_model_on_device(edus_batch* b, const Problem& P, const Inst& I) {
   }
   cudaError_t e = build_wannier_model(a, b->stream);
   if (e == cudaSuccess && b->mixed) {
+    if (e == cudaSuccess) e = planes_diagonal(a.H, (double*)I.Hdiag, n, nk, b->stream);
     if (e == cudaSuccess) e = planes_to_float(a.H, (float2*)I.H, plane, b->stream);
     if (e == cudaSuccess) e = planes_to_float(a.D, (float2*)I.D, 3 * plane, b->stream);
     if (e == cudaSuccess) e = planes_to_float(a.U, (float2*)I.U, (size_t)n * n * nk, b->stream);
@@ -534,6 +544,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   I.Pa = (double2*)carve(L.state);
   I.Pb = (double2*)carve(L.state);
   I.Peq = (const double2*)carve(L.eq);
+  I.Hdiag = (const double*)carve(L.hdiag);
   I.H = carve(L.H);
   I.D = carve(L.D);
   I.GE = carve(L.GE);

@@ -48,6 +48,7 @@ struct Inst {
   const void* U;           // [n*n][nk]
   double2 *P0, *P1, *Pa, *Pb;
   const double2* Peq;      // mixed precision: initial state [ntri][nk]
+  const double* Hdiag;     // mixed precision: diagonal of H in FP64 [n][nk]
   const FieldRow* field;   // [itfi + 2]
   edus_obs* log;           // [itfi / res + 1]
   void* part;              // [ntiles] observable partials

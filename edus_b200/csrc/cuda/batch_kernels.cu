@@ -97,6 +97,7 @@ struct StageSmem {
   C H[N * N * KT];                  // H~ = H + E^w . D
   C Q[MIX ? N * N * KT : 1];        // mixed: rho_eq
   C X[MIX ? N * N * KT : 1];        // mixed: E^w . D
+  double Ed[MIX ? N * KT : 1];      // mixed: diagonal of H~ in FP64
   double E[2][3];
   double G[kBatchMaxNb][3];
   int nb[kBatchMaxNb][KT];          // neighbour k of the tile's k points
@@ -148,8 +149,10 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
     double2 p1v = cz(), p0v = cz(), Pe = cz();
     S He = xmk<S>(0, 0), De[3] = {xmk<S>(0, 0), xmk<S>(0, 0), xmk<S>(0, 0)};
     double2 Qe = cz();
+    double Hii = 0.;
     if (valid) {
       Pe = src[o];
+      if (MIX && i == j) Hii = I->Hdiag[(size_t)i * nk + k];
       He = reinterpret_cast<const S*>(I->H)[o];
       const S* Dp = reinterpret_cast<const S*>(I->D);
 #pragma unroll
@@ -175,6 +178,15 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
       const C pc = MIX ? cvt<C>(csub(Pe, Qe)) : cvt<C>(Pe);
       s.P[(i * N + j) * KT + kl] = pc;
       s.P[(j * N + i) * KT + kl] = xconj(pc);
+      if (MIX && i == j) {
+        // the band energies enter in FP64: their FP32 rounding would be the same
+        // at every k and turn into a coherent phase drift
+        double ed = Hii;
+#pragma unroll
+        for (int x = 0; x < 3; x++) ed += (double)De[x].x * s.E[0][x];
+        s.Ed[i * KT + kl] = ed;
+        hu = hl = xmk<C>(0, 0);
+      }
       s.H[(i * N + j) * KT + kl] = hu;
       s.H[(j * N + i) * KT + kl] = hl;
       if (MIX) {
@@ -243,8 +255,13 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
       C vv = xmi(beta);
       if (i < nch && j >= nch) vv = xadd(vv, xmi(xscale(cvt<C>(Pe), (R)(-I->wx2))));
       vv = xadd(vv, G);
-      if (i == j) vv.y = 0;
-      const double2 d = cvt<double2>(vv);
+      double2 d = cvt<double2>(vv);
+      if constexpr (MIX) {
+        // diagonal part of [H~, rho - rho_eq]: (H~_jj - H~_ii) (rho - rho_eq)_ij in FP64
+        const double dE = s.Ed[j * KT + kl] - s.Ed[i * KT + kl];
+        d = cadd(d, cmi(cscale(csub(Pe, Qe), dE)));
+      }
+      if (i == j) d.y = 0;
       const double dt = I->dt, dt6 = dt / 6.0, dt3 = dt / 3.0, dt2 = dt / 2.0;
       switch (stage) {
         case 0:

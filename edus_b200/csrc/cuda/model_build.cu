@@ -113,7 +113,18 @@ __global__ void k_to_float(const double2* __restrict__ src, float2* __restrict__
     dst[i] = make_float2((float)src[i].x, (float)src[i].y);
 }
 
+__global__ void k_diag(const double2* __restrict__ H, double* __restrict__ out, int n, int nk) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (k < nk) out[(size_t)i * nk + k] = H[(size_t)(i * n - (i * (i - 1)) / 2) * nk + k].x;
+}
+
 }  // namespace
+
+cudaError_t planes_diagonal(const double2* H, double* out, int n, int nk, cudaStream_t s) {
+  k_diag<<<dim3((nk + 255) / 256, n), 256, 0, s>>>(H, out, n, nk);
+  return cudaGetLastError();
+}
 
 cudaError_t build_wannier_model(const ModelBuildArgs& a, cudaStream_t s) {
   const size_t smem = sizeof(double2) * kContractKT * a.nr;

@@ -24,6 +24,8 @@ struct ModelBuildArgs {
 
 cudaError_t build_wannier_model(const ModelBuildArgs& a, cudaStream_t s);
 cudaError_t planes_to_float(const double2* src, float2* dst, size_t count, cudaStream_t s);
+// out[i][k] = Re H[idx(i,i)][k] for the upper-triangle planes of an n-band model
+cudaError_t planes_diagonal(const double2* H, double* out, int n, int nk, cudaStream_t s);
 
 }  // namespace batch
 }  // namespace edus

@@ -1,0 +1,222 @@
+"""Measurements of the batched and served forms on the configuration workloads.
+
+Each function returns one JSON-ready dict in the bench line format. They run on
+one GPU; inputs are synthetic (edus_b200.workloads).
+
+  wannier_line  8-band Wannier model, 96x96, 40 fs, RK4 (one solve): the plain
+                FP64 single-solve path against M copies of the same solve (CEP
+                varied) run concurrently in the mixed-precision batch.
+  sweep_line    seeded 256-instance pulse sweep (half hBN, half 8-band Wannier,
+                grids 48^2-144^2, 10-60 fs) in one mixed-precision batch, against
+                the plain FP64 single-solve path run request by request on a
+                sample of the same instances.
+  serve_line    Poisson stream of requests (2, 8 or 16 bands, grids 32^2-192^2,
+                10-100 fs) through the served engine (continuous batching),
+                against the FP64 path run request by request on a sample.
+
+The error of the mixed path is the relative L2 norm over t of J1(t) against
+the FP64 single-solve path (which matches the reference's CPU output to 1e-12).
+"""
+import math
+import os
+import tempfile
+import time
+
+import numpy as np
+
+import edus_b200 as E
+from edus_b200 import abi
+from edus_b200 import workloads as W
+
+METRIC = "k-point·steps/s"
+
+
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _J1(log):
+    return np.array([x["J1"] for x in log])
+
+
+class _Dirs:
+    def __init__(self):
+        self.root = tempfile.mkdtemp(prefix="edus_suite_")
+        self.models = {}
+
+    def instance(self, spec, i):
+        d = os.path.join(self.root, f"i{i}")
+        os.makedirs(d, exist_ok=True)
+        if spec["kind"] == "wannier":
+            name = spec.get("name", "W8")
+            key = (name, spec.get("nw", 8), spec.get("nside", 11))
+            if key not in self.models:
+                self.models[key] = W.write_wannier_tb(os.path.join(self.root, f"{name}_{key[1]}_{key[2]}_tb.dat"), nw=key[1],
+                                                      nside=key[2])
+            link = os.path.join(d, f"{name}_tb.dat")
+            if not os.path.exists(link):
+                os.symlink(self.models[key], link)
+        return W.write_instance(d, spec), d
+
+
+def _single_fp64(path, d, graphs=True):
+    """Plain FP64 single-solve path: (k-point steps / s, observable log)."""
+    p = E.parse_input(path)
+    pb = E.Problem(p, d)
+    ctx = E.Context(pb, use_graphs=graphs)
+    ctx.run()
+    ms, _ = ctx.last_timing()
+    log = ctx.obs()
+    units = pb.info.nk * pb.info.nsteps
+    ctx.close()
+    pb.close()
+    return units, ms * 1e-3, log
+
+
+def _batch_run(problems, precision, chunk=16, **kw):
+    b = E.Batch(precision=precision, chunk_steps=chunk, **kw)
+    slots = [b.add(p) for p in problems]
+    while not all(b.poll(s)[0] == abi.EDUS_INST_DONE for s in slots):
+        b.advance(chunk * 8)
+    st = b.stats()
+    logs = [b.obs(s) for s in slots]
+    b.close()
+    return st, logs
+
+
+def wannier_line(copies=16, n=96, duration=40.0):
+    D = _Dirs()
+    spec = dict(kind="wannier", n=n, field=0.4, phase=0.0, duration=duration, it_res=10, dt_fs=0.01)
+    path, d = D.instance(spec, 0)
+    units, secs, ref_log = _single_fp64(path, d)
+    fp64_rate = units / secs
+    problems = []
+    for c in range(copies):
+        pth, dd = D.instance(dict(spec, phase=2 * math.pi * c / copies), c)
+        problems.append(E.Problem(E.parse_input(pth), dd, defer_model=True))
+    st, logs = _batch_run(problems, abi.EDUS_PREC_MIXED)
+    mixed_rate = st["kpoint_steps"] / (st["device_ms"] * 1e-3)
+    err = _rel(_J1(logs[0]), _J1(ref_log))
+    st64, logs64 = _batch_run(problems[:1], abi.EDUS_PREC_FP64)
+    return {
+        "metric": METRIC, "value": mixed_rate, "unit": METRIC, "higher_is_better": True, "dtype": "mixed (fp32 commutator, fp64 rho)",
+        "data": "synthetic",
+        "config": {"workload": f"wannier8_{n}x{n}_rk4_dt0.01fs_{duration:g}fs", "form": f"{copies} concurrent solves, mixed batch"},
+        "fp64_single_solve": fp64_rate, "speedup_vs_fp64_single": mixed_rate / fp64_rate,
+        "fp64_batch_one_solve": st64["kpoint_steps"] / (st64["device_ms"] * 1e-3),
+        "j1_rel_l2_vs_fp64": err,
+    }
+
+
+def sweep_line(count=256, fp64_sample_every=16, err_sample=16):
+    D = _Dirs()
+    specs = W.sweep(count)
+    problems, paths = [], []
+    t0 = time.perf_counter()
+    for i, s in enumerate(specs):
+        pth, d = D.instance(s, i)
+        paths.append((pth, d))
+        pb = E.Problem(E.parse_input(pth), d, defer_model=(s["kind"] == "wannier"))
+        if s["kind"] == "hbn":
+            pb.drop_decoupled_core()
+        problems.append(pb)
+    setup_s = time.perf_counter() - t0
+    st, logs = _batch_run(problems, abi.EDUS_PREC_MIXED)
+    mixed_rate = st["kpoint_steps"] / (st["device_ms"] * 1e-3)
+    for p in problems:
+        p.close()
+    # plain FP64 single-solve path, request by request, on every fp64_sample_every-th instance
+    units = secs = 0.0
+    errs = []
+    sample = [i for i in range(count) if i % fp64_sample_every in (0, 1)]  # both kinds alternate
+    for i in sample:
+        u, s, ref = _single_fp64(*paths[i])
+        units += u
+        secs += s
+        if len(errs) < err_sample:
+            errs.append(_rel(_J1(logs[i]), _J1(ref)))
+    fp64_rate = units / secs
+    return {
+        "metric": METRIC, "value": mixed_rate, "unit": METRIC, "higher_is_better": True, "dtype": "mixed (fp32 commutator, fp64 rho)",
+        "data": "synthetic",
+        "config": {"workload": f"pulse_sweep_{count}_hbn+wannier8_48-144_10-60fs", "form": "one batch, chunked graph replay",
+                   "kpoint_steps": st["kpoint_steps"], "device_s": st["device_ms"] * 1e-3, "host_setup_s": setup_s},
+        "fp64_single_solve_sample": {"value": fp64_rate, "instances": len(sample)},
+        "speedup_vs_fp64_single": mixed_rate / fp64_rate,
+        "j1_rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "instances": len(errs)},
+    }
+
+
+def serve_requests(count, seed=7, nmin=32, nmax=192, dmin=10.0, dmax=100.0):
+    """Request stream of the serving workload: band count 2 (hBN, core band
+    dropped), 8 or 16 (Wannier, 11x11 / 13x13 R); grid N x N, N even in
+    [nmin, nmax]; duration uniform in [dmin, dmax] fs; peak field log-uniform
+    0.05-0.8 V/A; CEP uniform."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(count):
+        nb = int(rng.choice([2, 8, 16]))
+        n = 2 * int(rng.integers(nmin // 2, nmax // 2 + 1))
+        spec = dict(n=n, field=float(math.exp(rng.uniform(math.log(0.05), math.log(0.8)))),
+                    phase=float(rng.uniform(0, 2 * math.pi)), duration=float(rng.uniform(dmin, dmax)), it_res=10, dt_fs=0.01)
+        if nb == 2:
+            spec["kind"] = "hbn"
+        else:
+            spec.update(kind="wannier", nw=nb, nside=11 if nb == 8 else 13, name=f"W{nb}")
+        out.append(spec)
+    return out
+
+
+def serve_line(count=2000, rate=None, fp64_sample=6, seed=7, max_s=None, **kw):
+    D = _Dirs()
+    specs = serve_requests(count, seed=seed, **kw)
+    reqs = [(E.parse_input(p), d) for p, d in (D.instance(s, i) for i, s in enumerate(specs))]
+    arrivals_rng = np.random.Generator(np.random.PCG64(seed + 1))
+    if rate is None:
+        rate = 1e9  # everything arrives at once: the GPU stays saturated from the start
+    gaps = arrivals_rng.exponential(1.0 / rate, size=count)
+    s = E.Server(precision=abi.EDUS_PREC_MIXED)
+    t_start = s.clock()
+    ids = []
+    for (p, d), g in zip(reqs, gaps):
+        target = (s.clock() - t_start) + g
+        while s.clock() - t_start < target - 1e-4:
+            time.sleep(min(0.01, max(0.0, target - (s.clock() - t_start))))
+        ids.append(s.submit(p, d))
+    s.drain(max_s or 7200)
+    st = s.stats()
+    logs = {}
+    for q in range(min(fp64_sample, count)):
+        logs[q] = s.obs(ids[q])
+    s.close()
+    # FP64, request by request (one request on the GPU at a time), on the first requests
+    units = secs = 0.0
+    lat = []
+    errs = []
+    for q in range(min(fp64_sample, count)):
+        f = E.Server(precision=abi.EDUS_PREC_FP64)
+        t0 = f.clock()
+        rid = f.submit(*reqs[q])
+        f.drain(3600)
+        info = f.info(rid)
+        ref = f.obs(rid)
+        f.close()
+        lat.append(info["t_done"] - t0)
+        units += info["nk"] * info["steps"]
+        secs += info["t_done"] - t0
+        errs.append(_rel(_J1(logs[q]), _J1(ref)))
+    fp64_rate = units / secs
+    return {
+        "metric": "solves/s", "value": st["solves_per_s"], "unit": "solves/s", "higher_is_better": True,
+        "dtype": "mixed (fp32 commutator, fp64 rho)", "data": "synthetic",
+        "config": {"workload": f"serving_{count}_requests_nb2-8-16_32-192_10-100fs", "arrival_rate_per_s": rate,
+                   "coulomb": "not in the served mix (batch instances run without the mean field)"},
+        "kpoint_steps_per_s": st["kpoint_steps_per_s"], "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+        "max_latency_s": st["max_latency_s"], "completed": st["completed"], "failed": st["failed"], "span_s": st["span_s"],
+        "peak_active": st["peak_active"], "peak_bytes": st["peak_bytes"],
+        "fp64_request_by_request_sample": {"kpoint_steps_per_s": fp64_rate, "requests": len(lat),
+                                           "mean_latency_s": float(np.mean(lat))},
+        "speedup_vs_fp64_request_by_request": st["kpoint_steps_per_s"] / fp64_rate,
+        "j1_rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "requests": len(errs)},
+    }
