@@ -189,6 +189,7 @@ class BatchOptions(C.Structure):
         ("chunk_steps", C.c_int32),
         ("use_graphs", C.c_int32),
         ("tile_k", C.c_int32 * (EDUS_MAX_BANDS + 1)),
+        ("regs_profile", C.c_int32 * (EDUS_MAX_BANDS + 1)),
         ("hbm_budget_bytes", C.c_int64),
     ]
 

@@ -54,7 +54,7 @@ struct Slot {
 };
 
 struct ClassTab {
-  int n = 0, kt = 0;
+  int n = 0, kt = 0, occ = 0;
   std::vector<Tile> tiles;
   Tile* d_tiles = nullptr;
   size_t cap = 0;
@@ -184,6 +184,43 @@ int upload_model(edus_batch* b, const Problem& P, const Inst& I) {
     if ((rc = put(b, (void*)I.Hdiag, hd))) return rc;
   }
   return 0;
+}
+
+// The k-gradient neighbours of a Monkhorst-Pack grid are fixed lattice steps
+// with periodic wrap. Find the step of every b from k = 0 and keep the table
+// path unless every k agrees.
+void detect_lattice(const Problem& P, Inst& I) {
+  const int* Nk = P.p.nk;
+  int n1 = 0, n2 = 0;
+  if (Nk[0] == 1) {
+    n1 = Nk[1];
+    n2 = Nk[2];
+  } else if (Nk[2] == 1) {
+    n1 = Nk[0];
+    n2 = Nk[1];
+  }
+  I.n1 = n1 > 0 ? n1 : 1;
+  I.n2 = n2 > 0 ? n2 : P.nk;
+  I.lattice = 0;
+  if (n1 <= 0 || n2 <= 0 || (size_t)n1 * n2 != (size_t)P.nk || P.nnb > kBatchMaxNb) return;
+  for (int b = 0; b < P.nnb; b++) {
+    const int kb = P.nbr[b];
+    int d1 = kb / n2, d2 = kb % n2;
+    if (d1 > n1 / 2) d1 -= n1;
+    if (d2 > n2 / 2) d2 -= n2;
+    I.off[b][0] = d1;
+    I.off[b][1] = d2;
+  }
+  for (int k = 0; k < P.nk; k++) {
+    const int i1 = k / n2, i2 = k % n2;
+    for (int b = 0; b < P.nnb; b++) {
+      const int j1 = ((i1 + I.off[b][0]) % n1 + n1) % n1, j2 = ((i2 + I.off[b][1]) % n2 + n2) % n2;
+      if (P.nbr[(size_t)k * P.nnb + b] != j1 * n2 + j2) return;
+    }
+  }
+  for (int b = 0; b < P.nnb; b++)
+    if (I.off[b][0] <= -n1 || I.off[b][0] >= n1 || I.off[b][1] <= -n2 || I.off[b][1] >= n2) return;
+  I.lattice = 1;
 }
 
 // Deferred Wannier model: tabulate H, D, U, dH/dk and the initial state on the
@@ -322,7 +359,7 @@ int record_chunk(edus_batch* b) {
       for (auto& kv : b->classes) {
         ClassTab& c = kv.second;
         View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles};
-        BCK(launch_stage(c.n, c.kt, b->mixed, v, st, parity, c.sgrid, b->stream));
+        BCK(launch_stage(c.n, c.kt, c.occ, b->mixed, v, st, parity, c.sgrid, b->stream));
       }
   }
   return 0;
@@ -558,6 +595,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
     I.wb[bb] = P.shell_w[P.bshell[bb]];
     for (int x = 0; x < 3; x++) I.bvec[bb][x] = P.bvec[bb * 3 + x];
   }
+  detect_lattice(P, I);
   auto undo = [&](int code) {
     free_slot_mem(b, s);
     return code;
@@ -607,7 +645,8 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   if (!c.n) {
     c.n = n;
     c.kt = kt;
-    c.sgrid = stage_grid(n, kt, b->mixed);
+    c.occ = b->opt.regs_profile[n] ? 1 : 0;
+    c.sgrid = stage_grid(n, kt, c.occ, b->mixed);
     c.ogrid = obs_grid(n, kt, b->mixed);
     if (cudaMalloc(&c.d_ntiles, sizeof(int)) != cudaSuccess) return undo(fail(EDUS_ENOMEM, "tile count"));
   }

@@ -38,6 +38,7 @@ static_assert(sizeof(FieldRow) == 128, "field rows are 128 bytes");
 
 struct Inst {
   int n, ntri, nk, nnb;
+  int n1, n2, lattice, pad1;   // grid k = i1 * n2 + i2; lattice: stencil given by off[]
   int nch, nbands, itfi, res;
   int want_current, want_tabs, ntiles, pad0;
   double dt, wx2, scaleJ, scaleTA;
@@ -55,6 +56,7 @@ struct Inst {
   unsigned int* done;      // arrival counter of the last-tile reduction
   double wb[kMaxNb];
   double bvec[kMaxNb][3];
+  int off[kBatchMaxNb][2];   // lattice step (d1, d2) of each b when lattice != 0
 };
 
 struct Tile {
@@ -72,13 +74,14 @@ struct View {
 };
 
 // One RK4 stage (0..3, Source_Main/RungeKutta.cpp schedule) over every tile of
-// the class; N is the band count, kt the tile length the table was built with.
-cudaError_t launch_stage(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
+// the class; N is the band count, kt the tile length the table was built with,
+// occ the register profile (0: 56 registers, more resident warps; 1: more registers).
+cudaError_t launch_stage(int N, int kt, int occ, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
 // Observables of the instances due at this tick (it % res == 0) and the
 // step-counter advance of every instance of the class.
 cudaError_t launch_obs(int N, int kt, bool mixed, const View& v, int parity, int grid, cudaStream_t s);
 // Persistent grid sizes (SMs x resident blocks) of the two kernels.
-int stage_grid(int N, int kt, bool mixed);
+int stage_grid(int N, int kt, int occ, bool mixed);
 int obs_grid(int N, int kt, bool mixed);
 bool class_supported(int N, int kt);
 size_t obs_part_bytes();

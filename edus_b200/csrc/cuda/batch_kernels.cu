@@ -83,122 +83,132 @@ __device__ __forceinline__ bool field_on(const double* E) {
 //   s=1: P1 += dt/3 k2,     Pb = P0 + dt/2 k2     (field at t + dt/2)
 //   s=2: P1 += dt/3 k3,     Pa = P0 + dt k3       (stage-2 field reused)
 //   s=3: P0 = P1 + dt/6 k4                        (field at t + dt)
-// Resident blocks per SM the register budget is sized for (about 36 warps).
-constexpr int min_blocks(int nthr) { return 1152 / nthr > 0 ? 1152 / nthr : 1; }
+// Resident blocks per SM the register budget is sized for: register profile 0
+// aims at about 36 warps per SM (56 registers), profile 1 at 24 warps (up to
+// 80-96 registers, fewer spills). The autotuner picks one per class.
+constexpr int min_blocks(int nthr, int occ) {
+  const int target = occ == 0 ? 1152 : 768;
+  return target / nthr > 0 ? target / nthr : 1;
+}
 
 // Shared-memory exchange of one tile: full n x n matrices (the lower triangle
 // written as the conjugate / mirrored entry), element (r, c) of k point kl at
-// [(r * N + c) * KT + kl], so every operand of the commutator is a constant
-// offset from a per-thread row pointer.
-template <int N, int KT, bool MIX>
-struct StageSmem {
-  using C = typename Types<MIX>::C;
-  C P[N * N * KT];                  // FP64: rho; mixed: rho - rho_eq
-  C H[N * N * KT];                  // H~ = H + E^w . D
-  C Q[MIX ? N * N * KT : 1];        // mixed: rho_eq
-  C X[MIX ? N * N * KT : 1];        // mixed: E^w . D
-  double Ed[MIX ? N * KT : 1];      // mixed: diagonal of H~ in FP64
-  double E[2][3];
-  double G[kBatchMaxNb][3];
-  int nb[kBatchMaxNb][KT];          // neighbour k of the tile's k points
-  int on;
+// [r * RS + c * KT + kl], so every operand of the commutator is a constant
+// offset from a per-thread row pointer. The tile's field, gradient
+// coefficients and neighbour indices are written one tile ahead.
+// Row r of a shared matrix starts at r * RS(N, KT): one entry of padding per
+// row keeps the rows of a warp's elements on different banks.
+template <int N, int KT>
+struct Rows {
+  static constexpr int RS = N * KT + 1;
+  static constexpr int SIZE = N * RS;
 };
 
 template <int N, int KT, bool MIX>
-__global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* TriB<N>::NT)))
+struct StageSmem {
+  using C = typename Types<MIX>::C;
+  static constexpr int SZ = Rows<N, KT>::SIZE;
+  C P[SZ];                          // FP64: rho; mixed: rho - rho_eq
+  C H[SZ];                          // H~ = H + E^w . D (mixed: off-diagonal part)
+  C Q[MIX ? SZ : 1];                // mixed: rho_eq
+  C X[MIX ? SZ : 1];                // mixed: E^w . D
+  double Ed[MIX ? N * KT : 1];      // mixed: diagonal of H~ in FP64
+  double E[2][3];                   // field of the stage: pump, probe / 2
+  double G[kBatchMaxNb][3];         // w_b E_pump,x b_x per neighbour
+  int nb[kBatchMaxNb][KT];          // k + b of the tile's k points
+  int on;                           // k-gradient on (E_non0)
+  int active;                       // the tile's instance is inside its time grid
+};
+
+// k + b of the k-gradient stencil: from the lattice steps of the stencil
+// (every b of a Monkhorst-Pack grid is a fixed step (d1, d2) with periodic
+// wrap, verified against the neighbour table at admission), else the table.
+__device__ __forceinline__ int neighbour(const Inst* I, int k, int b) {
+  if (!I->lattice) return I->nbr[(size_t)b * I->nk + k];
+  const int i1 = k / I->n2, i2 = k - i1 * I->n2;
+  int j1 = i1 + I->off[b][0], j2 = i2 + I->off[b][1];
+  j1 += j1 < 0 ? I->n1 : (j1 >= I->n1 ? -I->n1 : 0);
+  j2 += j2 < 0 ? I->n2 : (j2 >= I->n2 ? -I->n2 : 0);
+  return j1 * I->n2 + j2;
+}
+
+// Per-tile set-up of smem slot s for tile tl at step it (written before the
+// barrier of the preceding tile, read after it).
+template <int N, int KT, bool MIX>
+__device__ __forceinline__ void tile_setup(StageSmem<N, KT, MIX>& s, const View& v, const Tile& tl, int it, int stage) {
+  const Inst* I = v.insts + tl.inst;
+  const bool active = it >= 0 && it <= I->itfi;
+  const int tid = threadIdx.x;
+  if (tid == 0) s.active = active;
+  if (!active) return;
+  const int nk = I->nk, nnb = I->nnb;
+  const FieldRow* fr = I->field + it;
+  const double* Es = stage == 0 ? fr->Et : (stage == 3 ? fr[1].Et : fr->Eh);
+  if (tid < nnb) {
+    const int b = tid;
+    for (int x = 0; x < 3; x++) s.G[b][x] = I->wb[b] * Es[x] * I->bvec[b][x];
+  }
+  if (tid == 0) {
+    for (int q = 0; q < 6; q++) s.E[q / 3][q % 3] = Es[q];
+    s.on = (it == 0) || field_on(fr->Et);
+  }
+  for (int q = tid; q < nnb * KT; q += blockDim.x) {
+    const int b = q / KT, kq = tl.k0 + q % KT;
+    s.nb[b][q % KT] = kq < nk ? neighbour(I, kq, b) : 0;
+  }
+}
+
+template <int N, int KT, bool MIX, int OCC>
+__global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* TriB<N>::NT), OCC))
     k_bstage(View v, int stage, int parity) {
   constexpr int NT = TriB<N>::NT;
   using S = typename Types<MIX>::S;
   using C = typename Types<MIX>::C;
   using R = decltype(C::x);
-  __shared__ StageSmem<N, KT, MIX> sm[2];  // double buffered by tile: one barrier less per tile
+  __shared__ StageSmem<N, KT, MIX> sm[2];  // double buffered by tile: one barrier per tile
   const int tid = threadIdx.x;
   const int kl = tid % KT, e = tid / KT;
   const bool lane_ok = e < NT;
   int i = 0, j = 0;
   if (lane_ok) TriB<N>::ij(e, i, j);
   const int ntiles = *v.ntiles;
+  if ((int)blockIdx.x >= ntiles) return;  // uniform over the block
   int buf = 0;
+  Tile tl = v.tiles[blockIdx.x];
+  int it = v.it[parity][tl.inst];
+  tile_setup(sm[0], v, tl, it, stage);
+  __syncthreads();
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = v.tiles[t];
-    const int it = v.it[parity][tl.inst];
-    const Inst* I = v.insts + tl.inst;
-    if (it < 0 || it > I->itfi) continue;  // uniform over the block
     StageSmem<N, KT, MIX>& s = sm[buf];
+    StageSmem<N, KT, MIX>& sn = sm[buf ^ 1];
     buf ^= 1;
+    const Inst* I = v.insts + tl.inst;
+    const bool active = s.active;
     const int nk = I->nk, nch = I->nch, nnb = I->nnb;
-    const FieldRow* fr = I->field + it;
-    const double* Es = stage == 0 ? fr->Et : (stage == 3 ? fr[1].Et : fr->Eh);
-    if (tid < nnb) {
-      const int b = tid;
-      for (int x = 0; x < 3; x++) s.G[b][x] = I->wb[b] * Es[x] * I->bvec[b][x];
-    }
-    if (tid == 0) {
-      for (int q = 0; q < 6; q++) s.E[q / 3][q % 3] = Es[q];
-      s.on = (it == 0) || field_on(fr->Et);
-    }
-    for (int q = tid; q < nnb * KT; q += blockDim.x) {
-      const int b = q / KT, kq = tl.k0 + q % KT;
-      s.nb[b][q % KT] = kq < nk ? I->nbr[(size_t)b * nk + kq] : 0;
-    }
     const int k = tl.k0 + kl;
-    const bool valid = lane_ok && k < nk;
+    const bool valid = active && lane_ok && k < nk;
     const double2* src = stage == 0 ? I->P0 : (stage == 2 ? I->Pb : I->Pa);
     const size_t o = (size_t)e * nk + k;
-    // operands of the stage update, in flight while the RHS is evaluated
-    double2 p1v = cz(), p0v = cz(), Pe = cz();
-    S He = xmk<S>(0, 0), De[3] = {xmk<S>(0, 0), xmk<S>(0, 0), xmk<S>(0, 0)};
-    double2 Qe = cz();
+    double2 p1v = cz(), p0v = cz(), Pe = cz(), Qe = cz();
     double Hii = 0.;
+    S He = xmk<S>(0, 0), De[3] = {xmk<S>(0, 0), xmk<S>(0, 0), xmk<S>(0, 0)};
+    C G = xmk<C>(0, 0);
     if (valid) {
+      // every global load of the tile is issued here, the stencil gathers included
       Pe = src[o];
-      if (MIX && i == j) Hii = I->Hdiag[(size_t)i * nk + k];
       He = reinterpret_cast<const S*>(I->H)[o];
       const S* Dp = reinterpret_cast<const S*>(I->D);
 #pragma unroll
       for (int x = 0; x < 3; x++) De[x] = Dp[(size_t)x * NT * nk + o];
-      if (MIX) Qe = I->Peq[o];
+      if (MIX) {
+        Qe = I->Peq[o];
+        if (i == j) Hii = I->Hdiag[(size_t)i * nk + k];
+      }
       if (stage > 0) p1v = I->P1[o];
       if (stage == 1 || stage == 2) p0v = I->P0[o];
-    }
-    __syncthreads();
-    C G = xmk<C>(0, 0);
-    if (valid) {
-      // H~ = H + E^w . D, w = probe when exactly one index is a core band; the
-      // lower entry is conj(H) + E^w . D (D symmetric)
-      const int w = (i < nch) != (j < nch);
-      C hu = cvt<C>(He), hl = xconj(cvt<C>(He)), xd = xmk<C>(0, 0);
-#pragma unroll
-      for (int x = 0; x < 3; x++) {
-        const C d = cvt<C>(De[x]);
-        hu = xadd(hu, xscale(d, (R)s.E[w][x]));
-        hl = xadd(hl, xscale(d, (R)s.E[w][x]));
-        if (MIX) xd = xadd(xd, xscale(d, (R)s.E[w][x]));
-      }
-      const C pc = MIX ? cvt<C>(csub(Pe, Qe)) : cvt<C>(Pe);
-      s.P[(i * N + j) * KT + kl] = pc;
-      s.P[(j * N + i) * KT + kl] = xconj(pc);
-      if (MIX && i == j) {
-        // the band energies enter in FP64: their FP32 rounding would be the same
-        // at every k and turn into a coherent phase drift
-        double ed = Hii;
-#pragma unroll
-        for (int x = 0; x < 3; x++) ed += (double)De[x].x * s.E[0][x];
-        s.Ed[i * KT + kl] = ed;
-        hu = hl = xmk<C>(0, 0);
-      }
-      s.H[(i * N + j) * KT + kl] = hu;
-      s.H[(j * N + i) * KT + kl] = hl;
-      if (MIX) {
-        const C qc = cvt<C>(Qe);
-        s.Q[(i * N + j) * KT + kl] = qc;
-        s.Q[(j * N + i) * KT + kl] = xconj(qc);
-        s.X[(i * N + j) * KT + kl] = xd;
-        s.X[(j * N + i) * KT + kl] = xd;
-      }
       if (s.on) {
-        // k-gradient: sum_b (w_b E_pump . b) rho_e(k + b) (headers/RungeKutta.h:258-276);
-        // gathers issued four at a time, summed in b order
+        // k-gradient: sum_b (w_b E_pump . b) rho_e(k + b) (headers/RungeKutta.h:258-276),
+        // gathers four at a time, summed in b order
         const double2* row = src + (size_t)e * nk;
         constexpr int GB = 4;
         for (int b0 = 0; b0 < nnb; b0 += GB) {
@@ -221,6 +231,49 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
         }
       }
     }
+    // set-up of the next tile of this block, published by the barrier below
+    const int tn = t + gridDim.x;
+    if (tn < ntiles) {
+      tl = v.tiles[tn];
+      it = v.it[parity][tl.inst];
+      tile_setup(sn, v, tl, it, stage);
+    }
+    if (valid) {
+      // H~ = H + E^w . D, w = probe when exactly one index is a core band; the
+      // lower entry is conj(H) + E^w . D (D symmetric)
+      const int w = (i < nch) != (j < nch);
+      C hu = cvt<C>(He), hl = xconj(cvt<C>(He)), xd = xmk<C>(0, 0);
+#pragma unroll
+      for (int x = 0; x < 3; x++) {
+        const C d = cvt<C>(De[x]);
+        hu = xadd(hu, xscale(d, (R)s.E[w][x]));
+        hl = xadd(hl, xscale(d, (R)s.E[w][x]));
+        if (MIX) xd = xadd(xd, xscale(d, (R)s.E[w][x]));
+      }
+      constexpr int RS = Rows<N, KT>::RS;
+      const int oij = i * RS + j * KT + kl, oji = j * RS + i * KT + kl;
+      const C pc = MIX ? cvt<C>(csub(Pe, Qe)) : cvt<C>(Pe);
+      s.P[oij] = pc;
+      s.P[oji] = xconj(pc);
+      if (MIX && i == j) {
+        // the band energies enter in FP64: their FP32 rounding would be the same
+        // at every k and turn into a coherent phase drift
+        double ed = Hii;
+#pragma unroll
+        for (int x = 0; x < 3; x++) ed += (double)De[x].x * s.E[0][x];
+        s.Ed[i * KT + kl] = ed;
+        hu = hl = xmk<C>(0, 0);
+      }
+      s.H[oij] = hu;
+      s.H[oji] = hl;
+      if (MIX) {
+        const C qc = cvt<C>(Qe);
+        s.Q[oij] = qc;
+        s.Q[oji] = xconj(qc);
+        s.X[oij] = xd;
+        s.X[oji] = xd;
+      }
+    }
     __syncthreads();
     if (valid) {
       // -i[H~, rho]_ij in the reference's transposed convention
@@ -229,10 +282,11 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
       // Mixed: -i([H~, rho - rho_eq] + [E.D, rho_eq]); the dropped [H, rho_eq]
       // vanishes for the ground-state projector, so every FP32 rounding is
       // relative to the driven part instead of the O(1) background.
-      const C* Hi = s.H + i * N * KT + kl;
-      const C* Hj = s.H + j * N * KT + kl;
-      const C* Pi = s.P + i * N * KT + kl;
-      const C* Pj = s.P + j * N * KT + kl;
+      constexpr int RS = Rows<N, KT>::RS;
+      const C* Hi = s.H + i * RS + kl;
+      const C* Hj = s.H + j * RS + kl;
+      const C* Pi = s.P + i * RS + kl;
+      const C* Pj = s.P + j * RS + kl;
       C beta = xmk<C>(0, 0);
 #pragma unroll
       for (int l = 0; l < N; l++) {
@@ -241,10 +295,10 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
         beta = xadd(beta, xsub(x, xconj(y)));
       }
       if constexpr (MIX) {
-        const C* Xi = s.X + i * N * KT + kl;
-        const C* Xj = s.X + j * N * KT + kl;
-        const C* Qi = s.Q + i * N * KT + kl;
-        const C* Qj = s.Q + j * N * KT + kl;
+        const C* Xi = s.X + i * RS + kl;
+        const C* Xj = s.X + j * RS + kl;
+        const C* Qi = s.Q + i * RS + kl;
+        const C* Qj = s.Q + j * RS + kl;
 #pragma unroll
         for (int l = 0; l < N; l++) {
           const C x = xmul(Xj[l * KT], Qi[l * KT]);
@@ -516,18 +570,18 @@ __global__ void __launch_bounds__(pad32(KO* TriB<N>::NT)) k_bobs(View v, int par
 }
 
 // ------------------------------------------------------------------ dispatch
-template <int N, int KT, bool MIX>
+template <int N, int KT, bool MIX, int OCC>
 cudaError_t stage_n(const View& v, int stage, int parity, int grid, cudaStream_t s) {
-  k_bstage<N, KT, MIX><<<grid, pad32(KT * TriB<N>::NT), 0, s>>>(v, stage, parity);
+  k_bstage<N, KT, MIX, OCC><<<grid, pad32(KT * TriB<N>::NT), 0, s>>>(v, stage, parity);
   return cudaGetLastError();
 }
 
-template <int N, int KT, bool MIX>
+template <int N, int KT, bool MIX, int OCC>
 int stage_grid_n() {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bstage<N, KT, MIX>, pad32(KT * TriB<N>::NT), 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bstage<N, KT, MIX, OCC>, pad32(KT * TriB<N>::NT), 0);
   return sms * (per > 0 ? per : 1);
 }
 
@@ -566,18 +620,24 @@ bool class_supported(int N, int kt) {
   return false;
 }
 
-cudaError_t launch_stage(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s) {
-#define X(n, k)                                                                     \
-  if (N == n && kt == k)                                                            \
-    return mixed ? stage_n<n, k, true>(v, stage, parity, grid, s) : stage_n<n, k, false>(v, stage, parity, grid, s);
+cudaError_t launch_stage(int N, int kt, int occ, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s) {
+#define X(n, k)                                                                                       \
+  if (N == n && kt == k) {                                                                            \
+    if (occ == 0)                                                                                     \
+      return mixed ? stage_n<n, k, true, 0>(v, stage, parity, grid, s) : stage_n<n, k, false, 0>(v, stage, parity, grid, s); \
+    return mixed ? stage_n<n, k, true, 1>(v, stage, parity, grid, s) : stage_n<n, k, false, 1>(v, stage, parity, grid, s);   \
+  }
   EDUS_BATCH_CLASSES(X)
 #undef X
   return cudaErrorInvalidValue;
 }
 
-int stage_grid(int N, int kt, bool mixed) {
-#define X(n, k) \
-  if (N == n && kt == k) return mixed ? stage_grid_n<n, k, true>() : stage_grid_n<n, k, false>();
+int stage_grid(int N, int kt, int occ, bool mixed) {
+#define X(n, k)                                                                                   \
+  if (N == n && kt == k) {                                                                        \
+    if (occ == 0) return mixed ? stage_grid_n<n, k, true, 0>() : stage_grid_n<n, k, false, 0>(); \
+    return mixed ? stage_grid_n<n, k, true, 1>() : stage_grid_n<n, k, false, 1>();               \
+  }
   EDUS_BATCH_CLASSES(X)
 #undef X
   return 0;

@@ -300,7 +300,7 @@ class Batch:
     """Many solves advanced together on one GPU (edus_batch_* of the C ABI)."""
 
     def __init__(self, device=0, precision=abi.EDUS_PREC_FP64, max_instances=1024, chunk_steps=16, use_graphs=True,
-                 hbm_budget_bytes=0, tile_k=None):
+                 hbm_budget_bytes=0, tile_k=None, regs_profile=None):
         L = load_library()
         self._L = L
         o = abi.BatchOptions()
@@ -313,6 +313,8 @@ class Batch:
         o.hbm_budget_bytes = int(hbm_budget_bytes)
         for n, k in (tile_k or {}).items():
             o.tile_k[n] = k
+        for n, r in (regs_profile or {}).items():
+            o.regs_profile[n] = r
         self._h = C.c_void_p()
         _check(L.edus_batch_create(C.byref(o), C.byref(self._h)), "edus_batch_create")
         self._n = {}
@@ -395,7 +397,8 @@ class Server:
     any time; they are admitted by HBM footprint and run concurrently."""
 
     def __init__(self, device=0, precision=abi.EDUS_PREC_FP64, max_instances=1024, chunk_steps=16,
-                 hbm_budget_bytes=0, setup_threads=4, drop_decoupled_core=True, max_bypass_s=2.0, tile_k=None):
+                 hbm_budget_bytes=0, setup_threads=4, drop_decoupled_core=True, max_bypass_s=2.0, tile_k=None,
+                 regs_profile=None):
         L = load_library()
         self._L = L
         o = abi.ServerOptions()
@@ -407,6 +410,8 @@ class Server:
         o.batch.hbm_budget_bytes = int(hbm_budget_bytes)
         for n, k in (tile_k or {}).items():
             o.batch.tile_k[n] = k
+        for n, r in (regs_profile or {}).items():
+            o.batch.regs_profile[n] = r
         o.setup_threads = setup_threads
         o.drop_decoupled_core = 1 if drop_decoupled_core else 0
         o.max_bypass_s = max_bypass_s
