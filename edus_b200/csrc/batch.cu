@@ -123,10 +123,14 @@ Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
   return L;
 }
 
+int profile_of(const edus_batch* b, int n) { return (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.regs_profile[n] : 0; }
+
 int check_problem(const edus_batch* b, const Problem& P) {
   const int n = P.ncv;
-  if (!class_supported(n, tile_len(b, n)))
-    return fail(EDUS_EUNSUPPORTED, "batch: %d bands with %d k points per tile is not built", n, tile_len(b, n));
+  const bool ok = profile_of(b, n) == 2 ? mm_supported(n, tile_len(b, n)) : class_supported(n, tile_len(b, n));
+  if (!ok)
+    return fail(EDUS_EUNSUPPORTED, "batch: %d bands with %d k points per tile (profile %d) is not built", n, tile_len(b, n),
+                profile_of(b, n));
   if (P.p.coulomb) return fail(EDUS_EUNSUPPORTED, "batch: the Coulomb mean field runs only in single-solve contexts");
   if (!P.diss_i.empty()) return fail(EDUS_EUNSUPPORTED, "batch: dissipation runs only in single-solve contexts");
   if (P.p.solver != EDUS_SOLVER_RK4 || P.p.dynamical_dt)
@@ -359,7 +363,10 @@ int record_chunk(edus_batch* b) {
       for (auto& kv : b->classes) {
         ClassTab& c = kv.second;
         View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles};
-        BCK(launch_stage(c.n, c.kt, c.occ, b->mixed, v, st, parity, c.sgrid, b->stream));
+        if (c.occ == 2)
+          BCK(launch_stage_mm(c.n, c.kt, b->mixed, v, st, parity, c.sgrid, b->stream));
+        else
+          BCK(launch_stage(c.n, c.kt, c.occ, b->mixed, v, st, parity, c.sgrid, b->stream));
       }
   }
   return 0;
@@ -645,8 +652,8 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   if (!c.n) {
     c.n = n;
     c.kt = kt;
-    c.occ = b->opt.regs_profile[n] ? 1 : 0;
-    c.sgrid = stage_grid(n, kt, c.occ, b->mixed);
+    c.occ = profile_of(b, n);
+    c.sgrid = c.occ == 2 ? stage_grid_mm(n, kt, b->mixed) : stage_grid(n, kt, c.occ ? 1 : 0, b->mixed);
     c.ogrid = obs_grid(n, kt, b->mixed);
     if (cudaMalloc(&c.d_ntiles, sizeof(int)) != cudaSuccess) return undo(fail(EDUS_ENOMEM, "tile count"));
   }

@@ -84,6 +84,10 @@ cudaError_t launch_obs(int N, int kt, bool mixed, const View& v, int parity, int
 int stage_grid(int N, int kt, int occ, bool mixed);
 int obs_grid(int N, int kt, bool mixed);
 bool class_supported(int N, int kt);
+// Matrix-product form of the stage kernel (batch_mm.cu), register profile 2.
+bool mm_supported(int N, int kt);
+cudaError_t launch_stage_mm(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
+int stage_grid_mm(int N, int kt, bool mixed);
 size_t obs_part_bytes();
 
 }  // namespace batch

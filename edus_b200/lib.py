@@ -296,12 +296,21 @@ class Context:
             pass
 
 
+def _tuned(precision):
+    """Tile lengths and register profiles of the autotuner's cache for this GPU."""
+    from . import autotune
+
+    return autotune.tuned_options(precision)
+
+
 class Batch:
     """Many solves advanced together on one GPU (edus_batch_* of the C ABI)."""
 
     def __init__(self, device=0, precision=abi.EDUS_PREC_FP64, max_instances=1024, chunk_steps=16, use_graphs=True,
-                 hbm_budget_bytes=0, tile_k=None, regs_profile=None):
+                 hbm_budget_bytes=0, tile_k=None, regs_profile=None, tuned=True):
         L = load_library()
+        if tuned and tile_k is None and regs_profile is None:
+            tile_k, regs_profile = _tuned(precision)
         self._L = L
         o = abi.BatchOptions()
         _check(L.edus_batch_options_default(C.byref(o)), "edus_batch_options_default")
@@ -398,8 +407,10 @@ class Server:
 
     def __init__(self, device=0, precision=abi.EDUS_PREC_FP64, max_instances=1024, chunk_steps=16,
                  hbm_budget_bytes=0, setup_threads=4, drop_decoupled_core=True, max_bypass_s=2.0, tile_k=None,
-                 regs_profile=None):
+                 regs_profile=None, tuned=True):
         L = load_library()
+        if tuned and tile_k is None and regs_profile is None:
+            tile_k, regs_profile = _tuned(precision)
         self._L = L
         o = abi.ServerOptions()
         _check(L.edus_server_options_default(C.byref(o)), "edus_server_options_default")

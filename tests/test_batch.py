@@ -152,3 +152,33 @@ def test_device_built_wannier_model_matches_host_build(workdir, nw, nside, name)
     assert rel(J1(ld), J1(lh)) < 1e-10
     ph, pd = np.array([x["pop"] for x in lh]), np.array([x["pop"] for x in ld])
     assert np.abs(ph - pd).max() < 1e-12
+
+
+@pytest.mark.parametrize("kt", [8, 16])
+def test_matrix_product_form_matches_single_solve(workdir, kt):
+    """Register profile 2 (C = P H~^T in register blocks) against the single-solve path."""
+    d = f"{workdir}/w8mm"
+    p = E.parse_input(W.wannier(d, n=12, t_fin_fs=0.4, it_res=4))
+    pb = E.Problem(p, d)
+    rho, log = single(pb)
+    for prec, tol_rho, tol_j in [(abi.EDUS_PREC_FP64, 1e-13, 1e-11), (abi.EDUS_PREC_MIXED, 1e-6, 1e-6)]:
+        b = E.Batch(precision=prec, chunk_steps=8, tile_k={8: kt}, regs_profile={8: 2})
+        s = b.add(pb)
+        drain(b, [s], 8)
+        assert np.abs(b.get_state(s) - rho).max() < tol_rho
+        assert rel(J1(b.obs(s)), J1(log)) < tol_j
+
+
+def test_matrix_product_form_16_bands(workdir):
+    d = f"{workdir}/w16mm"
+    p = E.parse_input(W.wannier(d, nw=16, nside=13, n=10, t_fin_fs=0.2, it_res=5, name="W16"))
+    out = {}
+    for prof, kt in [(0, 2), (2, 2), (2, 4), (2, 8)]:
+        b = E.Batch(chunk_steps=8, tile_k={16: kt}, regs_profile={16: prof})
+        s = b.add(E.Problem(p, d))
+        drain(b, [s], 8)
+        out[(prof, kt)] = (b.get_state(s), J1(b.obs(s)))
+    ref_rho, ref_j = out[(0, 2)]
+    for key, (rho, j) in out.items():
+        assert np.abs(rho - ref_rho).max() < 1e-13, key
+        assert rel(j, ref_j) < 1e-11, key
