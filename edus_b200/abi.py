@@ -190,6 +190,8 @@ class BatchOptions(C.Structure):
         ("use_graphs", C.c_int32),
         ("tile_k", C.c_int32 * (EDUS_MAX_BANDS + 1)),
         ("regs_profile", C.c_int32 * (EDUS_MAX_BANDS + 1)),
+        ("tc_contraction", C.c_int32),
+        ("pad", C.c_int32),
         ("hbm_budget_bytes", C.c_int64),
     ]
 

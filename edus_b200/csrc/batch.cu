@@ -17,6 +17,7 @@
 
 #include "cuda/batch.cuh"
 #include "cuda/model_build.hpp"
+#include "cuda/tc_contract.hpp"
 #include "host/problem.hpp"
 
 namespace edus {
@@ -86,6 +87,7 @@ struct edus_batch {
   std::vector<Slot> slots;
   Inst* d_insts = nullptr;
   int* d_it[2] = {nullptr, nullptr};
+  int* d_err = nullptr;  // device error word of bounded waits
   std::map<int, ClassTab> classes;
   long long tick = 0;
   int64_t bytes_used = 0, budget = 0;
@@ -225,6 +227,150 @@ void detect_lattice(const Problem& P, Inst& I) {
   for (int b = 0; b < P.nnb; b++)
     if (I.off[b][0] <= -n1 || I.off[b][0] >= n1 || I.off[b][1] <= -n2 || I.off[b][1] >= n2) return;
   I.lattice = 1;
+}
+
+float tf32_round_host(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  u += 0x0FFFu + ((u >> 13) & 1u);
+  u &= 0xFFFFE000u;
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+// Mixed precision: H(k), D(k) on the tensor cores (cuda/tc_contract.cu, split
+// TF32), band energies in FP64, then the eigensolve and dH/dk on the FP64 matrix
+// the dynamics uses.
+int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
+  const int n = P.ncv, nt = n * (n + 1) / 2, nk = P.nk, nr = P.nrpts;
+  // H and D on the tensor cores; dH/dk, an observable-only table whose k sums
+  // cancel strongly, is the reference's stencil over an FP64 H(k) (CUDA cores)
+  const int ncomp = 4;
+  const int kp = tc_pad_k(nr), ncols = 2 * ncomp * nt, K = 2 * nr;
+  std::vector<float> Bw((size_t)ncols * kp, 0.f);
+  for (int i = 0; i < n; i++)
+    for (int j = i; j < n; j++) {
+      const int e = tri_index(i, j, n);
+      for (int comp = 0; comp < ncomp; comp++) {
+        const int ce = comp * nt + e;
+        for (int r = 0; r < nr; r++) {
+          const cd h = P.HR[((size_t)i * n + j) * nr + r];
+          const cd c = comp == 0 ? h
+                                 : 0.5 * (P.rR[(((size_t)(comp - 1) * n + i) * n + j) * nr + r] +
+                                          P.rR[(((size_t)(comp - 1) * n + j) * n + i) * nr + r]);
+          // re column: [Re c ; -Im c], im column: [Im c ; Re c]
+          const float vals[2][2] = {{(float)c.real(), (float)-c.imag()}, {(float)c.imag(), (float)c.real()}};
+          for (int part = 0; part < 2; part++)
+            for (int hh = 0; hh < 2; hh++) {
+              const float x = vals[part][hh];
+              const float hi = tf32_round_host(x), lo = tf32_round_host(x - hi);
+              float* row = &Bw[(size_t)(2 * ce + part) * kp];
+              const int q = hh * nr + r;
+              row[q] = hi;          // pairs with A_hi
+              row[K + q] = lo;      // pairs with A_hi
+              row[2 * K + q] = hi;  // pairs with A_lo
+            }
+        }
+      }
+    }
+  std::vector<double2> hdr((size_t)n * nr);
+  for (int i = 0; i < n; i++)
+    for (int r = 0; r < nr; r++) hdr[(size_t)i * nr + r] = mkc<double2>(P.HR[((size_t)i * n + i) * nr + r]);
+  std::vector<double> gb((size_t)P.nnb * 3);
+  for (int bb = 0; bb < P.nnb; bb++)
+    for (int x = 0; x < 3; x++) gb[bb * 3 + x] = P.shell_w[P.bshell[bb]] * P.bvec[bb * 3 + x];
+  const size_t plane = (size_t)nt * nk;
+  const size_t bytes = align256(sizeof(double) * 3 * nk) + align256(sizeof(double) * 3 * nr) + align256(sizeof(float) * Bw.size()) +
+                       align256(sizeof(double2) * hdr.size()) + align256(sizeof(double) * gb.size()) +
+                       align256(sizeof(float) * (size_t)nk * kp) + align256(sizeof(float) * (size_t)nk * ncols) +
+                       align256(sizeof(double2) * plane) + align256(sizeof(double2) * n * n * nk) +
+                       (I.GE ? align256(sizeof(double2) * plane) + align256(sizeof(double2) * 3 * plane) +
+                                   align256(sizeof(double2) * 4 * nt * nr)
+                             : 0);
+  char* base = nullptr;
+  if (cudaMallocAsync((void**)&base, bytes, b->pool, b->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(EDUS_ENOMEM, "batch: tensor-core model build scratch of %zu bytes", bytes);
+  }
+  char* p = base;
+  auto carve = [&](size_t sz) {
+    char* r = p;
+    p += align256(sz);
+    return r;
+  };
+  double* dk = (double*)carve(sizeof(double) * 3 * nk);
+  double* dR = (double*)carve(sizeof(double) * 3 * nr);
+  float* dB = (float*)carve(sizeof(float) * Bw.size());
+  double2* dh = (double2*)carve(sizeof(double2) * hdr.size());
+  double* dg = (double*)carve(sizeof(double) * gb.size());
+  int rc;
+  if ((rc = put(b, dk, P.kpt)) || (rc = put(b, dR, P.Rvec)) || (rc = put(b, dB, Bw)) || (rc = put(b, dh, hdr)) || (rc = put(b, dg, gb))) {
+    cudaFreeAsync(base, b->stream);
+    return rc;
+  }
+  TcArgs t;
+  t.n = n;
+  t.ntri = nt;
+  t.nk = nk;
+  t.nr = nr;
+  t.kpt = dk;
+  t.Rvec = dR;
+  t.Bw = dB;
+  t.hdiagR = dh;
+  t.Aw = (float*)carve(sizeof(float) * (size_t)nk * kp);
+  t.Cw = (float*)carve(sizeof(float) * (size_t)nk * ncols);
+  t.H32 = (float2*)I.H;
+  t.D32 = (float2*)I.D;
+  t.GE32 = nullptr;
+  t.Hdiag = (double*)I.Hdiag;
+  t.Hused = (double2*)carve(sizeof(double2) * plane);
+  t.err = b->d_err;
+  ModelBuildArgs a;
+  memset(&a, 0, sizeof(a));
+  a.n = n;
+  a.ntri = nt;
+  a.nk = nk;
+  a.nr = nr;
+  a.nnb = P.nnb;
+  a.nbands = P.nbands;
+  a.nv = P.p.nb[1];
+  a.scissor = 0.;
+  a.kpt = dk;
+  a.Rvec = dR;
+  a.nbr = I.nbr;
+  a.gb = dg;
+  a.H = t.Hused;
+  a.U = (double2*)carve(sizeof(double2) * n * n * nk);
+  a.GE = nullptr;
+  a.P0 = I.P0;
+  cudaError_t e = tc_contract(t, b->stream);
+  if (e == cudaSuccess) e = finish_wannier_model(a, b->stream);
+  if (e == cudaSuccess) e = planes_to_float(a.U, (float2*)I.U, (size_t)n * n * nk, b->stream);
+  if (e == cudaSuccess && I.GE) {
+    // dH/dk: FP64 H(k) (coefficients: H(R) upper elements) and the stencil
+    std::vector<double2> hc((size_t)nt * nr);
+    for (int i = 0; i < n; i++)
+      for (int j = i; j < n; j++)
+        for (int r = 0; r < nr; r++) hc[(size_t)tri_index(i, j, n) * nr + r] = mkc<double2>(P.HR[((size_t)i * n + j) * nr + r]);
+    ModelBuildArgs g = a;
+    g.only_h = 1;
+    g.H = (double2*)carve(sizeof(double2) * plane);
+    g.GE = (double2*)carve(sizeof(double2) * 3 * plane);
+    double2* dhc = (double2*)carve(sizeof(double2) * 4 * nt * nr);
+    int prc = put(b, dhc, hc);
+    if (prc) {
+      cudaFreeAsync(base, b->stream);
+      return prc;
+    }
+    g.coef = dhc;
+    e = wannier_h_and_gradient(g, b->stream);
+    if (e == cudaSuccess) e = planes_to_float(g.GE, (float2*)I.GE, 3 * plane, b->stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync((void*)I.Peq, I.P0, sizeof(double2) * plane, cudaMemcpyDeviceToDevice, b->stream);
+  cudaFreeAsync(base, b->stream);
+  if (e != cudaSuccess) return fail(EDUS_ECUDA, "batch: tensor-core model build: %s", cudaGetErrorString(e));
+  return 0;
 }
 
 // Deferred Wannier model: tabulate H, D, U, dH/dk and the initial state on the
@@ -405,6 +551,9 @@ int run_chunk(edus_batch* b) {
   }
   BCK(cudaEventRecord(b->e1, b->stream));
   BCK(cudaEventSynchronize(b->e1));
+  int derr = 0;
+  BCK(cudaMemcpy(&derr, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (derr) return fail(EDUS_ETIMEOUT, "batch: a bounded device wait ran out (error %d)", derr);
   float ms = 0;
   BCK(cudaEventElapsedTime(&ms, b->e0, b->e1));
   b->device_ms += ms;
@@ -449,6 +598,7 @@ int edus_batch_options_default(edus_batch_options* o) {
   o->max_instances = 1024;
   o->chunk_steps = 16;
   o->use_graphs = 1;
+  o->tc_contraction = 1;
   o->hbm_budget_bytes = 0;
   return 0;
 }
@@ -482,8 +632,9 @@ int edus_batch_create(const edus_batch_options* o, edus_batch** out) {
   const int cap = o->max_instances;
   b->slots.resize(cap);
   if (cudaMalloc(&b->d_insts, sizeof(Inst) * cap) != cudaSuccess || cudaMalloc(&b->d_it[0], sizeof(int) * cap) != cudaSuccess ||
-      cudaMalloc(&b->d_it[1], sizeof(int) * cap) != cudaSuccess)
+      cudaMalloc(&b->d_it[1], sizeof(int) * cap) != cudaSuccess || cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess)
     return bail(fail(EDUS_ENOMEM, "batch tables"));
+  cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream);
   cudaMemsetAsync(b->d_insts, 0, sizeof(Inst) * cap, b->stream);
   cudaMemsetAsync(b->d_it[0], 0xff, sizeof(int) * cap, b->stream);
   cudaMemsetAsync(b->d_it[1], 0xff, sizeof(int) * cap, b->stream);
@@ -508,6 +659,7 @@ void edus_batch_destroy(edus_batch* b) {
   cudaFree(b->d_insts);
   cudaFree(b->d_it[0]);
   cudaFree(b->d_it[1]);
+  cudaFree(b->d_err);
   if (b->pool) cudaMemPoolDestroy(b->pool);
   if (b->e0) cudaEventDestroy(b->e0);
   if (b->e1) cudaEventDestroy(b->e1);
@@ -616,7 +768,8 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
     if ((rc = put(b, (void*)I.nbr, nb))) return undo(rc);
   }
   if (P.model_deferred) {
-    if ((rc = build_model_on_device(b, P, I))) return undo(rc);
+    const bool tc = b->mixed && b->opt.tc_contraction && P.p.conduction_shift <= 1e-16;
+    if ((rc = tc ? build_model_tc(b, P, I) : build_model_on_device(b, P, I))) return undo(rc);
   } else {
     rc = b->mixed ? upload_model<float2>(b, P, I) : upload_model<double2>(b, P, I);
     if (rc) return undo(rc);

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(kContractThreads) k_wan_contract(ModelBuildArg
     ph[q] = make_double2(c, s);
   }
   __syncthreads();
-  const int nout = 4 * ntri * kContractKT;
+  const int nout = (a.only_h ? 1 : 4) * ntri * kContractKT;
   for (int o = threadIdx.x; o < nout; o += blockDim.x) {
     const int kl = o % kContractKT, ce = o / kContractKT;  // ce = comp * ntri + e
     const int k = k0 + kl;
@@ -135,6 +135,11 @@ cudaError_t build_wannier_model(const ModelBuildArgs& a, cudaStream_t s) {
   k_wan_contract<<<(a.nk + kContractKT - 1) / kContractKT, kContractThreads, smem, s>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  return finish_wannier_model(a, s);
+}
+
+cudaError_t finish_wannier_model(const ModelBuildArgs& a, cudaStream_t s) {
+  cudaError_t e;
   const int blocks = (a.nk + 63) / 64;
   switch (a.n) {
     case 2: k_wan_eig<2><<<blocks, 64, 0, s>>>(a); break;
@@ -151,6 +156,19 @@ cudaError_t build_wannier_model(const ModelBuildArgs& a, cudaStream_t s) {
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+cudaError_t wannier_h_and_gradient(const ModelBuildArgs& a, cudaStream_t s) {
+  const size_t smem = sizeof(double2) * kContractKT * a.nr;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_wan_contract, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_wan_contract<<<(a.nk + kContractKT - 1) / kContractKT, kContractThreads, smem, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !a.GE) return e;
+  k_wan_ge<<<dim3((a.nk + 127) / 128, a.ntri), 128, 0, s>>>(a);
+  return cudaGetLastError();
 }
 
 cudaError_t planes_to_float(const double2* src, float2* dst, size_t count, cudaStream_t s) {

@@ -307,7 +307,7 @@ class Batch:
     """Many solves advanced together on one GPU (edus_batch_* of the C ABI)."""
 
     def __init__(self, device=0, precision=abi.EDUS_PREC_FP64, max_instances=1024, chunk_steps=16, use_graphs=True,
-                 hbm_budget_bytes=0, tile_k=None, regs_profile=None, tuned=True):
+                 hbm_budget_bytes=0, tile_k=None, regs_profile=None, tuned=True, tc_contraction=True):
         L = load_library()
         if tuned and tile_k is None and regs_profile is None:
             tile_k, regs_profile = _tuned(precision)
@@ -324,6 +324,7 @@ class Batch:
             o.tile_k[n] = k
         for n, r in (regs_profile or {}).items():
             o.regs_profile[n] = r
+        o.tc_contraction = 1 if tc_contraction else 0
         self._h = C.c_void_p()
         _check(L.edus_batch_create(C.byref(o), C.byref(self._h)), "edus_batch_create")
         self._n = {}

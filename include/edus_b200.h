@@ -294,7 +294,13 @@ typedef struct {
   int32_t max_instances;    /* slots */
   int32_t chunk_steps;      /* time steps per graph replay (even) */
   int32_t use_graphs;
-  int32_t tile_k[EDUS_MAX_BANDS + 1]; /* k points per tile by band count; 0 = tuned default */
+  int32_t tile_k[EDUS_MAX_BANDS + 1]; /* k points per tile by band count; 0 = default */
+  int32_t regs_profile[EDUS_MAX_BANDS + 1]; /* stage-kernel form by band count: 0 = element-parallel,
+                                               56 registers; 1 = element-parallel, more registers;
+                                               2 = matrix-product form (8 and 16 bands) */
+  int32_t tc_contraction;   /* mixed precision: deferred Wannier models contracted on the tensor
+                               cores (split TF32, FP32 accumulate; band energies FP64) */
+  int32_t pad;
   int64_t hbm_budget_bytes; /* admission limit; 0 = 90 % of the free device memory at create */
 } edus_batch_options;
 
