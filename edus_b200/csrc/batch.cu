@@ -270,6 +270,7 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
               row[q] = hi;          // pairs with A_hi
               row[K + q] = lo;      // pairs with A_hi
               row[2 * K + q] = hi;  // pairs with A_lo
+              row[3 * K + q] = lo;  // pairs with A_lo
             }
         }
       }
@@ -283,7 +284,7 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
   const size_t plane = (size_t)nt * nk;
   const size_t bytes = align256(sizeof(double) * 3 * nk) + align256(sizeof(double) * 3 * nr) + align256(sizeof(float) * Bw.size()) +
                        align256(sizeof(double2) * hdr.size()) + align256(sizeof(double) * gb.size()) +
-                       align256(sizeof(float) * (size_t)nk * kp) + align256(sizeof(float) * (size_t)nk * ncols) +
+                       align256(sizeof(float) * (size_t)nk * kp) + align256(sizeof(double) * (size_t)nk * ncols) +
                        align256(sizeof(double2) * plane) + align256(sizeof(double2) * n * n * nk) +
                        (I.GE ? align256(sizeof(double2) * plane) + align256(sizeof(double2) * 3 * plane) +
                                    align256(sizeof(double2) * 4 * nt * nr)
@@ -319,10 +320,9 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
   t.Bw = dB;
   t.hdiagR = dh;
   t.Aw = (float*)carve(sizeof(float) * (size_t)nk * kp);
-  t.Cw = (float*)carve(sizeof(float) * (size_t)nk * ncols);
+  t.Cw = (double*)carve(sizeof(double) * (size_t)nk * ncols);
   t.H32 = (float2*)I.H;
   t.D32 = (float2*)I.D;
-  t.GE32 = nullptr;
   t.Hdiag = (double*)I.Hdiag;
   t.Hused = (double2*)carve(sizeof(double2) * plane);
   t.err = b->d_err;

@@ -1,29 +1,25 @@
 // tc_contract.cu — the Wannier Fourier sums H(k), D(k) on the tcgen05 tensor
 // cores (split TF32, FP32 accumulation) for mixed-precision batch instances.
 //
-// dH/dk, the reference's b-vector stencil of H (save_HUD.cpp:96-137), is the
-// same kind of sum: every k + b is a grid point of the periodic H(k), so
-//   sum_b w_b b_x (H(k+b) - H(k)) = sum_r e^{2 pi i k.R_r} H(R_r) W_x(R_r),
-//   W_x(R) = sum_b w_b b_x (e^{2 pi i dk_b.R} - 1),
-// three more output components that carry no finite-difference cancellation.
-//
 // Real form of the complex sums: with A[k][.] = [cos(2 pi k.R_r) | sin(2 pi k.R_r)]
 // (K = 2 nr) and, per output element, the column pair
 //   re: [ Re c_r ; -Im c_r ],   im: [ Im c_r ; Re c_r ],
 // out = A . B^T gives Re / Im of sum_r e^{2 pi i k.R_r} c_r. The compensated
-// split x = x_hi + x_lo (both exactly TF32) enters as one GEMM of three times
-// the depth: A' = [A_hi | A_hi | A_lo], B' = [B_hi | B_lo | B_hi] (per row), so
-// A'.B'^T = A_hi B_hi + A_hi B_lo + A_lo B_hi, accumulated in FP32 in TMEM.
+// split x = x_hi + x_lo (both exactly TF32) enters as one GEMM of four times
+// the depth: A' = [A_hi | A_hi | A_lo | A_lo], B' = [B_hi | B_lo | B_hi | B_lo]
+// (per row), so A'.B'^T = (A_hi + A_lo)(B_hi + B_lo). Products of two TF32
+// values are exact in FP32; the tensor core sums each 32-deep slice in FP32 in
+// TMEM and the slices are added in FP64 registers.
 //
-// GEMM kernel: one CTA (4 warps) per 128 x 128 tile of C; per 32-deep slice of
+// GEMM kernel: one CTA (4 warps) per 128 x 32 tile of C; per 32-deep slice of
 // K the block stages A and B in shared memory in the K-major canonical layout
 // without swizzle (16-byte rows of 4 TF32, 8-row core matrices 128 bytes
 // apart, the two 16-byte halves of one MMA's K = 8 slice one whole operand
 // apart), one elected thread issues four tcgen05.mma (M 128, N 128, K 8) and
 // commits them to an mbarrier that the block waits on (bounded) before the
-// next slice overwrites shared memory. The accumulator (128 lanes x 128 FP32
-// columns of TMEM) is read back with tcgen05.ld.32x32b by each warp's lane
-// quarter.
+// next slice overwrites shared memory. The slice's accumulator (128 lanes x 32
+// FP32 columns of TMEM) is read back with tcgen05.ld.32x32b by each warp's lane
+// quarter into FP64 registers.
 #include <stdint.h>
 
 #include "batch.cuh"
@@ -34,9 +30,10 @@ namespace edus {
 namespace batch {
 namespace {
 
-constexpr int TM = 128, TN = 128, TK = 32;  // CTA tile and K slice (TF32 elements)
+constexpr int TM = 128, TN = 32, TK = 32;  // CTA tile and K slice (TF32 elements)
 constexpr int kThreads = 128;
-constexpr uint32_t kTmemCols = 128;
+constexpr uint32_t kTmemCols = 32;
+constexpr int kSplit = 4;                  // hi.hi + hi.lo + lo.hi + lo.lo
 
 // nearest TF32 (10 explicit mantissa bits) of a finite float
 __device__ __forceinline__ float tf32_round(float x) {
@@ -46,15 +43,15 @@ __device__ __forceinline__ float tf32_round(float x) {
   return __uint_as_float(u);
 }
 
-// A' rows: phases of k point m over the R vectors, split hi / lo.
+// A' rows: phases of k point m over the R vectors, [hi | hi | lo | lo].
 __global__ void k_phase_split(const double* __restrict__ kpt, const double* __restrict__ Rvec, int nk, int nr, int kpad,
                               float* __restrict__ A) {
   const int m = blockIdx.x;
   const int K = 2 * nr;
   for (int c = threadIdx.x; c < kpad; c += blockDim.x) {
     float v = 0.f;
-    if (m < nk && c < 3 * K) {
-      const int part = c / K, q = c - part * K;  // part 0, 1: hi; 2: lo
+    if (m < nk && c < kSplit * K) {
+      const int part = c / K, q = c - part * K;  // parts 0, 1: hi; 2, 3: lo
       const int r = q < nr ? q : q - nr;
       const double kR = kpt[m * 3 + 0] * Rvec[r * 3 + 0] + kpt[m * 3 + 1] * Rvec[r * 3 + 1] + kpt[m * 3 + 2] * Rvec[r * 3 + 2];
       double s, co;
@@ -77,10 +74,12 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo_bytes,
   return d;
 }
 
-// kind::tf32, D FP32, A and B TF32 K-major, M = 128, N = 128
+// kind::tf32, D FP32, A and B TF32 K-major, M = 128, N = 32
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
 
-__global__ void __launch_bounds__(kThreads, 1) k_tc_gemm(const float* __restrict__ A, const float* __restrict__ B, float* __restrict__ C,
+// C (FP64) = A' B'^T. Every 32-deep slice starts a fresh TMEM accumulator and is
+// added into FP64 registers, so FP32 rounding spans only 32 exact products.
+__global__ void __launch_bounds__(kThreads, 1) k_tc_gemm(const float* __restrict__ A, const float* __restrict__ B, double* __restrict__ C,
                                                          int M, int N, int Kp, int* err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   float* sA = reinterpret_cast<float*>(smem);              // [TK / 4 chunks][TM rows][4]
@@ -99,6 +98,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_gemm(const float* __restrict
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_base;
   const uint32_t aBase = smem_u32(sA), bBase = smem_u32(sB);
+  double acc[TN];
+#pragma unroll
+  for (int c = 0; c < TN; c++) acc[c] = 0.;
   bool ok = true;
   uint32_t phase = 0;
   for (int k0 = 0; k0 < Kp; k0 += TK) {
@@ -125,25 +127,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_gemm(const float* __restrict
         // K = 8 slice j: chunks 2j, 2j+1; LBO = one chunk plane, SBO = 8 rows x 16 bytes
         const uint64_t da = smem_desc(aBase + (uint32_t)(2 * j * TM * 16), TM * 16, 128);
         const uint64_t db = smem_desc(bBase + (uint32_t)(2 * j * TN * 16), TN * 16, 128);
-        const uint32_t acc = (k0 > 0 || j > 0) ? 1u : 0u;
+        const uint32_t accum = j > 0 ? 1u : 0u;  // each slice starts from zero
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-            "l"(da), "l"(db), "r"(kIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            "l"(da), "l"(db), "r"(kIdesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&bar)) : "memory");
     }
-    // the MMAs have read this slice once the barrier completes its phase
-    ok = ok && mbar_wait(&bar, phase, err);
+    // the MMAs have read this slice and written TMEM once the barrier completes its phase
+    const bool done = mbar_wait(&bar, phase, err);
     phase ^= 1;
-    __syncthreads();
-    if (!ok) break;
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;");
-  if (ok) {
-    // warp w reads TMEM lanes 32w..32w+31 = rows m0 + 32w + lane
-    const int row = m0 + warp * 32 + lane;
+    if (__syncthreads_or(!done)) {  // a wait that ran out ends the block, uniformly
+      ok = false;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    // warp w reads TMEM lanes 32w..32w+31 (rows m0 + 32w + lane), all TN columns
+#pragma unroll
     for (int c0 = 0; c0 < TN; c0 += 8) {
       uint32_t v[8];
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
@@ -151,39 +153,45 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_gemm(const float* __restrict
                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                    : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < M)
-        for (int u = 0; u < 8; u++)
-          if (n0 + c0 + u < N) C[(size_t)row * N + n0 + c0 + u] = __uint_as_float(v[u]);
+#pragma unroll
+      for (int u = 0; u < 8; u++) acc[c0 + u] += (double)__uint_as_float(v[u]);
     }
+    // the next slice's MMAs overwrite TMEM and its staging overwrites shared memory
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+  }
+  if (ok) {
+    const int row = m0 + warp * 32 + lane;
+    if (row < M)
+#pragma unroll
+      for (int c = 0; c < TN; c++)
+        if (n0 + c < N) C[(size_t)row * N + n0 + c] = acc[c];
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
-// C[k][col] (col = (comp * ntri + e) * 2 + re/im) -> FP32 planes H [ntri][nk], D [3][ntri][nk],
-// dH/dk [3][ntri][nk] (comps 4..6 when present); diagonal imaginary parts are zero
-// (Wannier.h:489-492, and dH/dk of a real diagonal)
-__global__ void k_scatter(const float* __restrict__ C, int nk, int n, int ntri, int ncols, float2* __restrict__ H,
-                          float2* __restrict__ D, float2* __restrict__ GE) {
+// C[k][col] (col = (comp * ntri + e) * 2 + re/im) -> FP32 planes H [ntri][nk], D [3][ntri][nk];
+// diagonal imaginary parts are zero (Wannier.h:489-492)
+__global__ void k_scatter(const double* __restrict__ C, int nk, int n, int ntri, int ncols, float2* __restrict__ H,
+                          float2* __restrict__ D) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int ce = blockIdx.y;  // comp * ntri + e
   if (k >= nk) return;
   const int comp = ce / ntri, e = ce - comp * ntri;
-  float2 v = make_float2(C[(size_t)k * ncols + 2 * ce], C[(size_t)k * ncols + 2 * ce + 1]);
+  float2 v = make_float2((float)C[(size_t)k * ncols + 2 * ce], (float)C[(size_t)k * ncols + 2 * ce + 1]);
   bool diag = false;
   for (int i = 0; i < n; i++) diag = diag || (e == i * n - (i * (i - 1)) / 2);
   if (diag) v.y = 0.f;
   if (comp == 0)
     H[(size_t)e * nk + k] = v;
-  else if (comp < 4)
-    D[((size_t)(comp - 1) * ntri + e) * nk + k] = v;
   else
-    GE[((size_t)(comp - 4) * ntri + e) * nk + k] = v;
+    D[((size_t)(comp - 1) * ntri + e) * nk + k] = v;
 }
 
 // FP64 band energies: Re sum_r e^{2 pi i k.R_r} H_ii(R_r), and the FP64 matrix the
-// eigensolve uses: off-diagonal from the tensor-core result, diagonal from here.
+// eigensolve uses: the tensor-core off-diagonal (as stored, FP32), diagonal from here.
 __global__ void k_diag64(const double* __restrict__ kpt, const double* __restrict__ Rvec, const double2* __restrict__ hdiagR,
                          const float2* __restrict__ H32, int nk, int n, int nr, double* __restrict__ Hdiag,
                          double2* __restrict__ Hused) {
@@ -199,7 +207,6 @@ __global__ void k_diag64(const double* __restrict__ kpt, const double* __restric
     acc += c * h.x - s * h.y;
   }
   Hdiag[(size_t)i * nk + k] = acc;
-  // row i of the upper triangle of Hused
   for (int j = i; j < n; j++) {
     const int e = i * n - (i * (i - 1)) / 2 + (j - i);
     Hused[(size_t)e * nk + k] = (j == i) ? make_double2(acc, 0.) : make_double2(H32[(size_t)e * nk + k].x, H32[(size_t)e * nk + k].y);
@@ -210,12 +217,11 @@ __global__ void k_diag64(const double* __restrict__ kpt, const double* __restric
 
 size_t tc_gemm_smem() { return sizeof(float) * (TM + TN) * TK + 1024; }
 
-int tc_pad_k(int nr) { return ((6 * nr + TK - 1) / TK) * TK; }
+int tc_pad_k(int nr) { return ((2 * kSplit * nr + TK - 1) / TK) * TK; }
 
 cudaError_t tc_contract(const TcArgs& a, cudaStream_t s) {
   const int kpad = tc_pad_k(a.nr);
-  const int ncomp = a.GE32 ? 7 : 4;
-  const int ncols = 2 * ncomp * a.ntri;
+  const int ncols = 8 * a.ntri;
   k_phase_split<<<a.nk, 256, 0, s>>>(a.kpt, a.Rvec, a.nk, a.nr, kpad, a.Aw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
@@ -225,7 +231,7 @@ cudaError_t tc_contract(const TcArgs& a, cudaStream_t s) {
   dim3 grid((a.nk + TM - 1) / TM, (ncols + TN - 1) / TN);
   k_tc_gemm<<<grid, kThreads, smem, s>>>(a.Aw, a.Bw, a.Cw, a.nk, ncols, kpad, a.err);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  k_scatter<<<dim3((a.nk + 255) / 256, ncomp * a.ntri), 256, 0, s>>>(a.Cw, a.nk, a.n, a.ntri, ncols, a.H32, a.D32, a.GE32);
+  k_scatter<<<dim3((a.nk + 255) / 256, 4 * a.ntri), 256, 0, s>>>(a.Cw, a.nk, a.n, a.ntri, ncols, a.H32, a.D32);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_diag64<<<dim3((a.nk + 127) / 128, a.n), 128, 0, s>>>(a.kpt, a.Rvec, a.hdiagR, a.H32, a.nk, a.n, a.nr, a.Hdiag, a.Hused);
   return cudaGetLastError();

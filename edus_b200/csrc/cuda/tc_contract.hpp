@@ -12,20 +12,18 @@ struct TcArgs {
   int n, ntri, nk, nr;
   const double* kpt;     // [nk][3]
   const double* Rvec;    // [nr][3]
-  const float* Bw;       // [2 ncomp ntri][Kp] split coefficients (host-built, tc_pad_k columns per row);
-                         // ncomp = 4 (H, D) or 7 (H, D, dH/dk)
+  const float* Bw;       // [8 ntri][Kp] split coefficients [hi | lo | hi | lo] (host-built)
   const double2* hdiagR; // [n][nr] H_ii(R) for the FP64 band energies
   float* Aw;             // scratch [nk][Kp] split phases
-  float* Cw;             // scratch [nk][8 ntri] GEMM result
+  double* Cw;            // scratch [nk][8 ntri] GEMM result (FP64 sum of FP32 slices)
   float2* H32;           // out [ntri][nk]
   float2* D32;           // out [3][ntri][nk]
-  float2* GE32;          // out [3][ntri][nk] dH/dk, or null
   double* Hdiag;         // out [n][nk] FP64 band energies
   double2* Hused;        // out [ntri][nk] FP64 matrix the dynamics uses (for the eigensolve)
   int* err;              // device error word (bounded waits)
 };
 
-// K depth of the split GEMM (3 x 2 nr, padded to the K slice)
+// K depth of the split GEMM (4 x 2 nr, padded to the K slice)
 int tc_pad_k(int nr);
 cudaError_t tc_contract(const TcArgs& a, cudaStream_t s);
 
