@@ -114,7 +114,7 @@ struct StageSmem {
   C X[MIX ? SZ : 1];                // mixed: E^w . D
   double Ed[MIX ? N * KT : 1];      // mixed: diagonal of H~ in FP64
   double E[2][3];                   // field of the stage: pump, probe / 2
-  double G[kBatchMaxNb][3];         // w_b E_pump,x b_x per neighbour
+  double G[kBatchMaxNb];            // w_b (E_pump . b) per neighbour
   int nb[kBatchMaxNb][KT];          // k + b of the tile's k points
   int on;                           // k-gradient on (E_non0)
   int active;                       // the tile's instance is inside its time grid
@@ -146,7 +146,7 @@ __device__ __forceinline__ void tile_setup(StageSmem<N, KT, MIX>& s, const View&
   const double* Es = stage == 0 ? fr->Et : (stage == 3 ? fr[1].Et : fr->Eh);
   if (tid < nnb) {
     const int b = tid;
-    for (int x = 0; x < 3; x++) s.G[b][x] = I->wb[b] * Es[x] * I->bvec[b][x];
+    s.G[b] = I->wb[b] * (Es[0] * I->bvec[b][0] + Es[1] * I->bvec[b][1] + Es[2] * I->bvec[b][2]);
   }
   if (tid == 0) {
     for (int q = 0; q < 6; q++) s.E[q / 3][q % 3] = Es[q];
@@ -218,15 +218,8 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
 #pragma unroll
           for (int q = 0; q < GB; q++) {
             if (b0 + q >= nnb) break;
-            const int b = b0 + q;
             const C pq = cvt<C>(pn[q]);
-            if (MIX) {
-              G = xadd(G, xscale(pq, (R)(s.G[b][0] + s.G[b][1] + s.G[b][2])));
-            } else {
-              G = xadd(G, xscale(pq, (R)s.G[b][0]));
-              G = xadd(G, xscale(pq, (R)s.G[b][1]));
-              G = xadd(G, xscale(pq, (R)s.G[b][2]));
-            }
+            G = xadd(G, xscale(pq, (R)s.G[b0 + q]));
           }
         }
       }

@@ -68,7 +68,7 @@ struct MMLayout {
 
 struct Setup {
   double E[2][3];
-  double G[kBatchMaxNb][3];
+  double G[kBatchMaxNb];  // w_b (E_pump . b)
   int on, active;
 };
 
@@ -118,8 +118,7 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
     const FieldRow* fr = I->field + it;
     const double* Es = stage == 0 ? fr->Et : (stage == 3 ? fr[1].Et : fr->Eh);
     const int nnb = I->nnb, nk = I->nk;
-    if (tid < nnb)
-      for (int x = 0; x < 3; x++) su[slot].G[tid][x] = I->wb[tid] * Es[x] * I->bvec[tid][x];
+    if (tid < nnb) su[slot].G[tid] = I->wb[tid] * (Es[0] * I->bvec[tid][0] + Es[1] * I->bvec[tid][1] + Es[2] * I->bvec[tid][2]);
     if (tid == 0) {
       for (int q = 0; q < 6; q++) su[slot].E[q / 3][q % 3] = Es[q];
       su[slot].on = (it == 0) || field_nonzero(fr->Et);
@@ -183,17 +182,9 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
 #pragma unroll
             for (int u = 0; u < GB; u++) {
               if (b0 + u >= nnb) break;
-              const int b = b0 + u;
               const C pq = cv<C>(pn[u]);
-              if (MIX) {
-                const R c = (R)(su[cur].G[b][0] + su[cur].G[b][1] + su[cur].G[b][2]);
-                G = mk<C>(G.x + pq.x * c, G.y + pq.y * c);
-              } else {
-                for (int x = 0; x < 3; x++) {
-                  const R c = (R)su[cur].G[b][x];
-                  G = mk<C>(G.x + pq.x * c, G.y + pq.y * c);
-                }
-              }
+              const R c = (R)su[cur].G[b0 + u];
+              G = mk<C>(G.x + pq.x * c, G.y + pq.y * c);
             }
           }
         }

@@ -42,13 +42,16 @@ __global__ void __launch_bounds__(kRowThreads) k_coul_rows(const double2* __rest
   double* st = reinterpret_cast<double*>(srow + (size_t)ntri * n2);
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
+  const uint32_t row_bytes = (uint32_t)n2 * sizeof(double2);
   if (threadIdx.x == 0) {
-    const uint32_t row_bytes = (uint32_t)n2 * sizeof(double2);
+    // the trig table does not depend on the previous kernel: in flight before the wait
     const uint32_t trig_bytes = ((uint32_t)(n2 * nq * sizeof(double)) + 15u) & ~15u;
     mbar_expect_tx(&bar, (uint32_t)ntri * row_bytes + trig_bytes);
-    for (int e = 0; e < ntri; e++) bulk_g2s(srow + (size_t)e * n2, rho + (size_t)e * nk + (size_t)i1 * n2, row_bytes, &bar);
     bulk_g2s(st, t2T, trig_bytes, &bar);
   }
+  pdl_wait();
+  if (threadIdx.x == 0)
+    for (int e = 0; e < ntri; e++) bulk_g2s(srow + (size_t)e * n2, rho + (size_t)e * nk + (size_t)i1 * n2, row_bytes, &bar);
   mbar_wait(&bar, 0, err);
   for (int o = threadIdx.x; o < ntri * nq; o += kRowThreads) {
     const int e = o / nq, q = o - e * nq;
@@ -98,13 +101,17 @@ __global__ void __launch_bounds__(kModeThreads) k_coul_modes(const double2* __re
   __shared__ unsigned long long bar;
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
+  const uint32_t col_bytes = (uint32_t)n1 * sizeof(double2);
   if (threadIdx.x == 0) {
-    const uint32_t col_bytes = (uint32_t)n1 * sizeof(double2);
+    // the trig table does not depend on the previous kernel: in flight before the wait
     const uint32_t trig_bytes = ((uint32_t)(2 * ncut * ld * sizeof(double)) + 15u) & ~15u;
     mbar_expect_tx(&bar, 2 * col_bytes + trig_bytes);
+    bulk_g2s(tc, t1P, trig_bytes, &bar);
+  }
+  pdl_wait();
+  if (threadIdx.x == 0) {
     bulk_g2s(gc, g + ((size_t)n * ntri + e) * n1, col_bytes, &bar);
     bulk_g2s(gc + n1, g + ((size_t)(ncut + n) * ntri + e) * n1, col_bytes, &bar);
-    bulk_g2s(tc, t1P, trig_bytes, &bar);
   }
   mbar_wait(&bar, 0, err);
   for (int o = threadIdx.x; o < 4 * ncut; o += kModeThreads) {
@@ -231,6 +238,7 @@ __global__ void __launch_bounds__(kObsThreads) k_obs(DevTables tb, const DevCons
   obs_zero(my);
   const double2* rho = a.rho;
   const double2* hr = a.hr;
+  pdl_wait();
   if (k < nk) {
     double2 P[NT];
 #pragma unroll
@@ -406,14 +414,14 @@ cudaError_t coulomb_prepare(const DevTables& tb) {
 
 cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2* rho, double2* h, double2* Xout,
                            const double2* X0, cudaStream_t s) {
-  k_coul_rows<<<tb.n1, kRowThreads, coulomb_rows_smem(tb), s>>>(rho, tb.nk, tb.n1, tb.n2, tb.ntri, tb.ncut, c.t2T, c.g, tb.err);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_pdl(k_coul_rows, dim3(tb.n1), dim3(kRowThreads), coulomb_rows_smem(tb), s, rho, tb.nk, tb.n1, tb.n2,
+                             tb.ntri, tb.ncut, (const double*)c.t2T, c.g, tb.err);
   if (e != cudaSuccess) return e;
   dim3 grid(tb.ncut, tb.ntri);
-  k_coul_modes<<<grid, kModeThreads, coulomb_modes_smem(tb), s>>>(c.g, tb.n1, tb.ntri, tb.ncut, 1.0 / tb.nk, c.t1P, tb.err,
-                                                                   c.A, c.B, c.C, c.D, X0, c.is_diag, h, Xout, c.fdiag,
-                                                                   c.diag_of);
-  return cudaGetLastError();
+  return launch_pdl(k_coul_modes, grid, dim3(kModeThreads), coulomb_modes_smem(tb), s, (const double2*)c.g, tb.n1, tb.ntri,
+                    tb.ncut, 1.0 / tb.nk, (const double*)c.t1P, tb.err, (const double2*)c.A, (const double2*)c.B,
+                    (const double2*)c.C, (const double2*)c.D, X0, (const unsigned char*)c.is_diag, h, Xout, c.fdiag,
+                    (const int*)c.diag_of);
 }
 
 int obs_parts(int nk) { return (nk + kObsThreads - 1) / kObsThreads; }
@@ -421,8 +429,7 @@ size_t obs_part_bytes() { return sizeof(ObsPart); }
 
 template <int N>
 static cudaError_t launch_obs_n(const DevTables& tb, const DevConsts* cst, const ObsArgs& a, cudaStream_t s) {
-  k_obs<N><<<obs_parts(tb.nk), kObsThreads, 0, s>>>(tb, cst, a);
-  return cudaGetLastError();
+  return launch_pdl(k_obs<N>, dim3(obs_parts(tb.nk)), dim3(kObsThreads), 0, s, tb, cst, a);
 }
 
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,

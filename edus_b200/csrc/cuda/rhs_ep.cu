@@ -49,18 +49,12 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
   __shared__ unsigned long long bar;
   const bool staged = tb.h && a.stage_rows > 0;
   if (staged) {
-    // the inverse-transform rows this block touches arrive by one bulk copy while
-    // the threads load their own planes; the k2 trig values are gathered by hand
+    // the k2 trig values do not depend on the previous kernel: gathered before
+    // the wait; the inverse-transform rows this block touches (written by the
+    // previous kernel) then arrive by one bulk copy while the threads load
+    // their own planes
     const int n2 = tb.n2, nc = tb.ncut;
     const int tid = threadIdx.y * KT + threadIdx.x, nthr = KT * NT;
-    if (tid == 0) {
-      const int r0 = k0 / n2;
-      const int r1 = (min(k0 + KT, nk) - 1) / n2;
-      const uint32_t hbytes = (uint32_t)((r1 - r0 + 1) * 2 * nc * NT * sizeof(double2));
-      mbar_init(&bar, 1);
-      mbar_expect_tx(&bar, hbytes);
-      bulk_g2s(dyn, tb.h + (size_t)r0 * 2 * nc * NT, hbytes, &bar);
-    }
     double* ts = reinterpret_cast<double*>(dyn + a.stage_rows * 2 * nc * NT);
 #pragma unroll 4
     for (int t = tid; t < 2 * nc * KT; t += nthr) {
@@ -69,6 +63,17 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
       const int i2 = kk - (kk / n2) * n2;
       ts[t] = __ldg((cs == 0 ? tb.t2c : tb.t2s) + m * n2 + i2);
     }
+    pdl_wait();
+    if (tid == 0) {
+      const int r0 = k0 / n2;
+      const int r1 = (min(k0 + KT, nk) - 1) / n2;
+      const uint32_t hbytes = (uint32_t)((r1 - r0 + 1) * 2 * nc * NT * sizeof(double2));
+      mbar_init(&bar, 1);
+      mbar_expect_tx(&bar, hbytes);
+      bulk_g2s(dyn, tb.h + (size_t)r0 * 2 * nc * NT, hbytes, &bar);
+    }
+  } else {
+    pdl_wait();
   }
   double2 Pe = cz(), He = cz(), G = cz();
   double2 De[3] = {cz(), cz(), cz()};
@@ -276,8 +281,7 @@ static cudaError_t launch_ep(const DevTables& tb, const DevConsts* cst, const St
       dyn = bytes;
     }
   }
-  k_rhs_ep<N, KT><<<(tb.nk + KT - 1) / KT, block, dyn, s>>>(tb, cst, b);
-  return cudaGetLastError();
+  return launch_pdl(k_rhs_ep<N, KT>, dim3((tb.nk + KT - 1) / KT), block, dyn, s, tb, cst, b);
 }
 
 cudaError_t launch_rhs(const DevTables& tb, const DevConsts* cst, const StageArgs& a, cudaStream_t s) {
