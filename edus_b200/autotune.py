@@ -107,6 +107,10 @@ def tune(bands=(2, 3, 8, 16), precisions=("fp64", "mixed"), grid=96, steps=96, v
         for pn in precisions:
             best = None
             for kt, prof in VARIANTS[nb]:
+                if prof == 2 and pn == "mixed":
+                    continue  # the matrix-product form is built for FP64 only
+                if nb == 3 and pn == "mixed":
+                    continue  # mixed instances carry no core band: 3-band hBN runs as 2 bands
                 t0 = time.perf_counter()
                 rate = time_variant(problems, PREC[pn], nb, kt, prof, steps)
                 if verbose:
@@ -114,6 +118,8 @@ def tune(bands=(2, 3, 8, 16), precisions=("fp64", "mixed"), grid=96, steps=96, v
                           f"({time.perf_counter() - t0:.1f} s)", flush=True)
                 if best is None or rate > best[0]:
                     best = (rate, kt, prof)
+            if best is None:
+                continue
             entry.setdefault(pn, {})[str(nb)] = {"tile_k": best[1], "regs_profile": best[2], "kpoint_steps_per_s": best[0],
                                                  "instances": count}
         for p in problems:

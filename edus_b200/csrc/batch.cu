@@ -68,7 +68,8 @@ struct Layout {
   size_t state, H, D, GE, U, nbr, field, log, part;
   size_t eq;     // initial state kept for the mixed-precision deviation form
   size_t hdiag;  // FP64 band energies of the mixed-precision commutator
-  size_t total() const { return 4 * state + eq + hdiag + H + D + GE + U + nbr + field + log + part + 256; }
+  size_t w;      // E-linear rho_eq terms of the mixed-precision deviation form
+  size_t total() const { return 4 * state + eq + hdiag + w + H + D + GE + U + nbr + field + log + part + 256; }
 };
 
 }  // namespace
@@ -113,6 +114,7 @@ Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
   L.state = align256(nt * nk * sizeof(double2));
   L.eq = b->mixed ? L.state : 0;
   L.hdiag = b->mixed ? align256(n * nk * sizeof(double)) : 0;
+  L.w = b->mixed ? align256(3 * nt * nk * sizeof(float2)) : 0;
   L.H = align256(nt * nk * s);
   L.D = align256(3 * nt * nk * s);
   L.GE = P.p.current ? align256(3 * nt * nk * s) : 0;
@@ -125,7 +127,11 @@ Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
   return L;
 }
 
-int profile_of(const edus_batch* b, int n) { return (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.regs_profile[n] : 0; }
+// register profile / kernel form of a band count; the matrix-product form is built for FP64 only
+int profile_of(const edus_batch* b, int n) {
+  const int p = (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.regs_profile[n] : 0;
+  return (p == 2 && b->mixed) ? 0 : p;
+}
 
 int check_problem(const edus_batch* b, const Problem& P) {
   const int n = P.ncv;
@@ -134,6 +140,9 @@ int check_problem(const edus_batch* b, const Problem& P) {
     return fail(EDUS_EUNSUPPORTED, "batch: %d bands with %d k points per tile (profile %d) is not built", n, tile_len(b, n),
                 profile_of(b, n));
   if (P.p.coulomb) return fail(EDUS_EUNSUPPORTED, "batch: the Coulomb mean field runs only in single-solve contexts");
+  if (b->mixed && P.nch > 0)
+    return fail(EDUS_EUNSUPPORTED,
+                "batch: mixed precision needs a problem without core bands (edus_problem_drop_decoupled_core, or FP64)");
   if (!P.diss_i.empty()) return fail(EDUS_EUNSUPPORTED, "batch: dissipation runs only in single-solve contexts");
   if (P.p.solver != EDUS_SOLVER_RK4 || P.p.dynamical_dt)
     return fail(EDUS_EUNSUPPORTED, "batch: instances integrate with RK4 at constant dt");
@@ -368,6 +377,7 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
     if (e == cudaSuccess) e = planes_to_float(g.GE, (float2*)I.GE, 3 * plane, b->stream);
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync((void*)I.Peq, I.P0, sizeof(double2) * plane, cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(I.P0, 0, sizeof(double2) * plane, b->stream);  // deviation = 0
   cudaFreeAsync(base, b->stream);
   if (e != cudaSuccess) return fail(EDUS_ECUDA, "batch: tensor-core model build: %s", cudaGetErrorString(e));
   return 0;
@@ -453,6 +463,7 @@ int build_model_on_device(edus_batch* b, const Problem& P, const Inst& I) {
     if (e == cudaSuccess) e = planes_to_float(a.U, (float2*)I.U, (size_t)n * n * nk, b->stream);
     if (e == cudaSuccess && I.GE) e = planes_to_float(a.GE, (float2*)I.GE, 3 * plane, b->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync((void*)I.Peq, I.P0, sizeof(double2) * plane, cudaMemcpyDeviceToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(I.P0, 0, sizeof(double2) * plane, b->stream);  // deviation = 0
   }
   cudaFreeAsync(base, b->stream);
   if (e != cudaSuccess) return fail(EDUS_ECUDA, "batch: device model build: %s", cudaGetErrorString(e));
@@ -741,6 +752,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   I.Pb = (double2*)carve(L.state);
   I.Peq = (const double2*)carve(L.eq);
   I.Hdiag = (const double*)carve(L.hdiag);
+  I.W = carve(L.w);
   I.H = carve(L.H);
   I.D = carve(L.D);
   I.GE = carve(L.GE);
@@ -775,8 +787,14 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
     if (rc) return undo(rc);
     std::vector<double2> st;
     planes<double2>(P.P0.data(), nk, n, 1, st);
-    if ((rc = put(b, I.P0, st))) return undo(rc);
-    if (I.Peq && (rc = put(b, (void*)I.Peq, st))) return undo(rc);
+    if (I.Peq) {
+      // mixed precision: the state is the deviation from rho_eq
+      if ((rc = put(b, (void*)I.Peq, st))) return undo(rc);
+      if (cudaMemsetAsync(I.P0, 0, sizeof(double2) * st.size(), b->stream) != cudaSuccess)
+        return undo(fail(EDUS_ECUDA, "batch: clear deviation"));
+    } else if ((rc = put(b, I.P0, st))) {
+      return undo(rc);
+    }
   }
   {
     // field table: the single-solve loop's times (t += dt) and fields
@@ -797,6 +815,8 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   if (cudaMemsetAsync(I.done, 0, sizeof(unsigned int), b->stream) != cudaSuccess ||
       cudaMemcpyAsync(b->d_insts + q, &I, sizeof(Inst), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
     return undo(fail(EDUS_ECUDA, "batch: upload of the instance descriptor"));
+  if (b->mixed && launch_weq(b->d_insts, q, nt, nk, b->stream) != cudaSuccess)
+    return undo(fail(EDUS_ECUDA, "batch: equilibrium terms"));
   const int zero = 0;
   if (cudaMemcpyAsync(b->d_it[b->tick & 1] + q, &zero, sizeof(int), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
     return undo(fail(EDUS_ECUDA, "batch: clock"));
@@ -865,7 +885,14 @@ int edus_batch_get_state(edus_batch* b, int32_t slot, double* rho) {
   const int n = s->n, nk = s->nk;
   std::vector<double2> pl((size_t)s->ntri * nk);
   BCK(cudaMemcpyAsync(pl.data(), s->inst.P0, sizeof(double2) * pl.size(), cudaMemcpyDeviceToHost, b->stream));
+  std::vector<double2> eq;
+  if (s->inst.Peq) {
+    // mixed precision keeps the deviation from rho_eq
+    eq.resize(pl.size());
+    BCK(cudaMemcpyAsync(eq.data(), s->inst.Peq, sizeof(double2) * eq.size(), cudaMemcpyDeviceToHost, b->stream));
+  }
   BCK(cudaStreamSynchronize(b->stream));
+  for (size_t q = 0; q < eq.size(); q++) pl[q] = cadd(pl[q], eq[q]);
   cd* o = (cd*)rho;
   for (int k = 0; k < nk; k++)
     for (int i = 0; i < n; i++)

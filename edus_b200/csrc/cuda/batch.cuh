@@ -47,9 +47,12 @@ struct Inst {
   const void* D;           // [3][ntri][nk]
   const void* GE;          // [3][ntri][nk] or null
   const void* U;           // [n*n][nk]
+  // FP64: P0 = rho, Pa / Pb = RK4 stage inputs. Mixed precision: P0 = rho - rho_eq
+  // (FP64), Pa / Pb hold FP32 deviations (float2 at the same plane index).
   double2 *P0, *P1, *Pa, *Pb;
-  const double2* Peq;      // mixed precision: initial state [ntri][nk]
+  const double2* Peq;      // mixed precision: rho_eq, the initial state [ntri][nk]
   const double* Hdiag;     // mixed precision: diagonal of H in FP64 [n][nk]
+  const void* W;           // mixed precision: E-linear rho_eq terms [3][ntri][nk] (float2)
   const FieldRow* field;   // [itfi + 2]
   edus_obs* log;           // [itfi / res + 1]
   void* part;              // [ntiles] observable partials
@@ -89,6 +92,8 @@ bool mm_supported(int N, int kt);
 cudaError_t launch_stage_mm(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
 int stage_grid_mm(int N, int kt, bool mixed);
 size_t obs_part_bytes();
+// Mixed precision: W of one instance (after its D and rho_eq are on the device).
+cudaError_t launch_weq(const Inst* insts, int slot, int ntri, int nk, cudaStream_t s);
 
 }  // namespace batch
 }  // namespace edus

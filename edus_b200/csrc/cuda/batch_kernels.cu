@@ -109,9 +109,7 @@ struct StageSmem {
   using C = typename Types<MIX>::C;
   static constexpr int SZ = Rows<N, KT>::SIZE;
   C P[SZ];                          // FP64: rho; mixed: rho - rho_eq
-  C H[SZ];                          // H~ = H + E^w . D (mixed: off-diagonal part)
-  C Q[MIX ? SZ : 1];                // mixed: rho_eq
-  C X[MIX ? SZ : 1];                // mixed: E^w . D
+  C H[SZ];                          // H~ = H + E . D (mixed: off-diagonal part)
   double Ed[MIX ? N * KT : 1];      // mixed: diagonal of H~ in FP64
   double E[2][3];                   // field of the stage: pump, probe / 2
   double G[kBatchMaxNb];            // w_b (E_pump . b) per neighbour
@@ -188,38 +186,46 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
     const int k = tl.k0 + kl;
     const bool valid = active && lane_ok && k < nk;
     const double2* src = stage == 0 ? I->P0 : (stage == 2 ? I->Pb : I->Pa);
+    // mixed: the stage inputs of stages 1-3 are FP32 deviations in the same planes
+    const float2* src32 = reinterpret_cast<const float2*>(stage == 2 ? I->Pb : I->Pa);
     const size_t o = (size_t)e * nk + k;
-    double2 p1v = cz(), p0v = cz(), Pe = cz(), Qe = cz();
+    double2 p1v = cz(), p0v = cz(), Pe = cz();
     double Hii = 0.;
     S He = xmk<S>(0, 0), De[3] = {xmk<S>(0, 0), xmk<S>(0, 0), xmk<S>(0, 0)};
+    S We[3] = {xmk<S>(0, 0), xmk<S>(0, 0), xmk<S>(0, 0)};
     C G = xmk<C>(0, 0);
     if (valid) {
       // every global load of the tile is issued here, the stencil gathers included
-      Pe = src[o];
+      Pe = (!MIX || stage == 0) ? src[o] : cvt<double2>(src32[o]);
       He = reinterpret_cast<const S*>(I->H)[o];
       const S* Dp = reinterpret_cast<const S*>(I->D);
 #pragma unroll
       for (int x = 0; x < 3; x++) De[x] = Dp[(size_t)x * NT * nk + o];
       if (MIX) {
-        Qe = I->Peq[o];
+#pragma unroll
+        for (int x = 0; x < 3; x++) We[x] = reinterpret_cast<const S*>(I->W)[(size_t)x * NT * nk + o];
         if (i == j) Hii = I->Hdiag[(size_t)i * nk + k];
       }
       if (stage > 0) p1v = I->P1[o];
       if (stage == 1 || stage == 2) p0v = I->P0[o];
       if (s.on) {
         // k-gradient: sum_b (w_b E_pump . b) rho_e(k + b) (headers/RungeKutta.h:258-276),
-        // gathers four at a time, summed in b order
-        const double2* row = src + (size_t)e * nk;
+        // gathers four at a time, summed in b order (mixed: of the deviation; the
+        // rho_eq part is in W)
         constexpr int GB = 4;
         for (int b0 = 0; b0 < nnb; b0 += GB) {
-          double2 pn[GB];
+          C pn[GB];
 #pragma unroll
-          for (int q = 0; q < GB; q++) pn[q] = (b0 + q < nnb) ? row[s.nb[b0 + q][kl]] : cz();
+          for (int q = 0; q < GB; q++) {
+            const int kb = s.nb[b0 + q < nnb ? b0 + q : 0][kl];
+            pn[q] = (b0 + q >= nnb) ? xmk<C>(0, 0)
+                    : (!MIX || stage == 0) ? cvt<C>(src[(size_t)e * nk + kb])
+                                           : cvt<C>(src32[(size_t)e * nk + kb]);
+          }
 #pragma unroll
           for (int q = 0; q < GB; q++) {
             if (b0 + q >= nnb) break;
-            const C pq = cvt<C>(pn[q]);
-            G = xadd(G, xscale(pq, (R)s.G[b0 + q]));
+            G = xadd(G, xscale(pn[q], (R)s.G[b0 + q]));
           }
         }
       }
@@ -232,49 +238,47 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
       tile_setup(sn, v, tl, it, stage);
     }
     if (valid) {
+      constexpr int RS = Rows<N, KT>::RS;
+      const int oij = i * RS + j * KT + kl, oji = j * RS + i * KT + kl;
+      const C pc = cvt<C>(Pe);
+      s.P[oij] = pc;
+      s.P[oji] = xconj(pc);
       // H~ = H + E^w . D, w = probe when exactly one index is a core band; the
       // lower entry is conj(H) + E^w . D (D symmetric)
       const int w = (i < nch) != (j < nch);
-      C hu = cvt<C>(He), hl = xconj(cvt<C>(He)), xd = xmk<C>(0, 0);
+      C hu = cvt<C>(He), hl = xconj(cvt<C>(He));
 #pragma unroll
       for (int x = 0; x < 3; x++) {
         const C d = cvt<C>(De[x]);
         hu = xadd(hu, xscale(d, (R)s.E[w][x]));
         hl = xadd(hl, xscale(d, (R)s.E[w][x]));
-        if (MIX) xd = xadd(xd, xscale(d, (R)s.E[w][x]));
       }
-      constexpr int RS = Rows<N, KT>::RS;
-      const int oij = i * RS + j * KT + kl, oji = j * RS + i * KT + kl;
-      const C pc = MIX ? cvt<C>(csub(Pe, Qe)) : cvt<C>(Pe);
-      s.P[oij] = pc;
-      s.P[oji] = xconj(pc);
-      if (MIX && i == j) {
-        // the band energies enter in FP64: their FP32 rounding would be the same
-        // at every k and turn into a coherent phase drift
-        double ed = Hii;
+      if (MIX) {
+        if (i == j) {
+          // the band energies enter in FP64: their FP32 rounding would be the same
+          // at every k and turn into a coherent phase drift
+          double ed = Hii;
 #pragma unroll
-        for (int x = 0; x < 3; x++) ed += (double)De[x].x * s.E[0][x];
-        s.Ed[i * KT + kl] = ed;
-        hu = hl = xmk<C>(0, 0);
+          for (int x = 0; x < 3; x++) ed += (double)De[x].x * s.E[0][x];
+          s.Ed[i * KT + kl] = ed;
+          hu = hl = xmk<C>(0, 0);
+        }
+        // field-driven equilibrium terms, linear in E: -i[E.D, rho_eq] + k-gradient of rho_eq
+#pragma unroll
+        for (int x = 0; x < 3; x++) G = xadd(G, xscale(cvt<C>(We[x]), (R)s.E[0][x]));
       }
       s.H[oij] = hu;
       s.H[oji] = hl;
-      if (MIX) {
-        const C qc = cvt<C>(Qe);
-        s.Q[oij] = qc;
-        s.Q[oji] = xconj(qc);
-        s.X[oij] = xd;
-        s.X[oji] = xd;
-      }
     }
     __syncthreads();
     if (valid) {
       // -i[H~, rho]_ij in the reference's transposed convention
       // (headers/RungeKutta.h:158-208): beta = sum_l H~_jl P_il - conj(H~_il P_jl);
       // on the diagonal this is 2i Im sum_l H~_il P_il, the reference's Pv_ii.
-      // Mixed: -i([H~, rho - rho_eq] + [E.D, rho_eq]); the dropped [H, rho_eq]
-      // vanishes for the ground-state projector, so every FP32 rounding is
-      // relative to the driven part instead of the O(1) background.
+      // Mixed: P = rho - rho_eq, H~ without its diagonal (added below in FP64);
+      // [H, rho_eq] vanishes for the ground-state projector and the E-linear
+      // rho_eq terms come precomputed (W), so every FP32 rounding is relative to
+      // the driven part instead of the O(1) background.
       constexpr int RS = Rows<N, KT>::RS;
       const C* Hi = s.H + i * RS + kl;
       const C* Hj = s.H + j * RS + kl;
@@ -287,47 +291,105 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
         const C y = xmul(Hi[l * KT], Pj[l * KT]);
         beta = xadd(beta, xsub(x, xconj(y)));
       }
-      if constexpr (MIX) {
-        const C* Xi = s.X + i * RS + kl;
-        const C* Xj = s.X + j * RS + kl;
-        const C* Qi = s.Q + i * RS + kl;
-        const C* Qj = s.Q + j * RS + kl;
-#pragma unroll
-        for (int l = 0; l < N; l++) {
-          const C x = xmul(Xj[l * KT], Qi[l * KT]);
-          const C y = xmul(Xi[l * KT], Qj[l * KT]);
-          beta = xadd(beta, xsub(x, xconj(y)));
-        }
-      }
       C vv = xmi(beta);
-      if (i < nch && j >= nch) vv = xadd(vv, xmi(xscale(cvt<C>(Pe), (R)(-I->wx2))));
+      if (!MIX && i < nch && j >= nch) vv = xadd(vv, xmi(xscale(cvt<C>(Pe), (R)(-I->wx2))));
       vv = xadd(vv, G);
       double2 d = cvt<double2>(vv);
       if constexpr (MIX) {
         // diagonal part of [H~, rho - rho_eq]: (H~_jj - H~_ii) (rho - rho_eq)_ij in FP64
         const double dE = s.Ed[j * KT + kl] - s.Ed[i * KT + kl];
-        d = cadd(d, cmi(cscale(csub(Pe, Qe), dE)));
+        d = cadd(d, cmi(cscale(Pe, dE)));
       }
       if (i == j) d.y = 0;
       const double dt = I->dt, dt6 = dt / 6.0, dt3 = dt / 3.0, dt2 = dt / 2.0;
-      switch (stage) {
-        case 0:
-          I->P1[o] = cadd(Pe, cscale(d, dt6));
-          I->Pa[o] = cadd(Pe, cscale(d, dt2));
-          break;
-        case 1:
-          I->P1[o] = cadd(p1v, cscale(d, dt3));
-          I->Pb[o] = cadd(p0v, cscale(d, dt2));
-          break;
-        case 2:
-          I->P1[o] = cadd(p1v, cscale(d, dt3));
-          I->Pa[o] = cadd(p0v, cscale(d, dt));
-          break;
-        default:
-          I->P0[o] = cadd(p1v, cscale(d, dt6));
-          break;
+      if constexpr (MIX) {
+        // FP64 accumulation of the deviation; FP32 stage inputs
+        float2* Pa32 = reinterpret_cast<float2*>(I->Pa);
+        float2* Pb32 = reinterpret_cast<float2*>(I->Pb);
+        switch (stage) {
+          case 0:
+            I->P1[o] = cadd(Pe, cscale(d, dt6));
+            Pa32[o] = cvt<float2>(cadd(Pe, cscale(d, dt2)));
+            break;
+          case 1:
+            I->P1[o] = cadd(p1v, cscale(d, dt3));
+            Pb32[o] = cvt<float2>(cadd(p0v, cscale(d, dt2)));
+            break;
+          case 2:
+            I->P1[o] = cadd(p1v, cscale(d, dt3));
+            Pa32[o] = cvt<float2>(cadd(p0v, cscale(d, dt)));
+            break;
+          default:
+            I->P0[o] = cadd(p1v, cscale(d, dt6));
+            break;
+        }
+      } else {
+        switch (stage) {
+          case 0:
+            I->P1[o] = cadd(Pe, cscale(d, dt6));
+            I->Pa[o] = cadd(Pe, cscale(d, dt2));
+            break;
+          case 1:
+            I->P1[o] = cadd(p1v, cscale(d, dt3));
+            I->Pb[o] = cadd(p0v, cscale(d, dt2));
+            break;
+          case 2:
+            I->P1[o] = cadd(p1v, cscale(d, dt3));
+            I->Pa[o] = cadd(p0v, cscale(d, dt));
+            break;
+          default:
+            I->P0[o] = cadd(p1v, cscale(d, dt6));
+            break;
+        }
       }
     }
+  }
+}
+
+// Equilibrium terms of the mixed-precision deviation form, linear in the
+// field: W_x = -i [D_x, rho_eq] (transposed convention, as the commutator above)
+// + sum_b w_b b_x rho_eq(k + b). Thread per (k, element); FP64 from the stored D.
+template <class S>
+__global__ void k_weq(const Inst* __restrict__ insts, int slot) {
+  const Inst* I = insts + slot;
+  const int n = I->n, nk = I->nk, nt = I->ntri;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = blockIdx.y;
+  if (k >= nk) return;
+  int i = 0, r = e;
+  while (r >= n - i) {
+    r -= n - i;
+    i++;
+  }
+  const int j = i + r;
+  auto up = [&](int a, int b) { return a * n - (a * (a - 1)) / 2 + (b - a); };
+  auto Q = [&](int a, int b) -> double2 {
+    return a <= b ? I->Peq[(size_t)up(a, b) * nk + k] : cconj(I->Peq[(size_t)up(b, a) * nk + k]);
+  };
+  const S* D = reinterpret_cast<const S*>(I->D);
+  auto Dx = [&](int x, int a, int b) -> double2 {
+    const S v = D[((size_t)x * nt + (a <= b ? up(a, b) : up(b, a))) * nk + k];
+    return make_double2((double)v.x, (double)v.y);
+  };
+  S* W = reinterpret_cast<S*>(const_cast<void*>(I->W));
+  const int i1 = k / I->n2, i2 = k - (k / I->n2) * I->n2;
+  for (int x = 0; x < 3; x++) {
+    double2 beta = cz();
+    for (int l = 0; l < n; l++) beta = cadd(beta, csub(cmul(Dx(x, j, l), Q(i, l)), cconj(cmul(Dx(x, i, l), Q(j, l)))));
+    double2 w = cmi(beta);
+    for (int b = 0; b < I->nnb; b++) {
+      int kb;
+      if (I->lattice) {
+        int j1 = i1 + I->off[b][0], j2 = i2 + I->off[b][1];
+        j1 += j1 < 0 ? I->n1 : (j1 >= I->n1 ? -I->n1 : 0);
+        j2 += j2 < 0 ? I->n2 : (j2 >= I->n2 ? -I->n2 : 0);
+        kb = j1 * I->n2 + j2;
+      } else {
+        kb = I->nbr[(size_t)b * nk + k];
+      }
+      w = cadd(w, cscale(I->Peq[(size_t)e * nk + kb], I->wb[b] * I->bvec[b][x]));
+    }
+    W[((size_t)x * nt + e) * nk + k] = cvt<S>(w);
   }
 }
 
@@ -445,7 +507,7 @@ __global__ void __launch_bounds__(pad32(KO* TriB<N>::NT)) k_bobs(View v, int par
       const bool valid = lane_ok && k < kend;
       if (lane_ok) {
         const size_t o = (size_t)e * nk + k;
-        sP[e][kl] = valid ? I->P0[o] : cz();
+        sP[e][kl] = valid ? (MIX ? cadd(I->P0[o], I->Peq[o]) : I->P0[o]) : cz();
         sH[e][kl] = valid ? cvt<double2>(H[o]) : cz();
         for (int x = 0; x < 3; x++) sD[x][e][kl] = valid ? cvt<double2>(D[(size_t)x * NT * nk + o]) : cz();
       }
@@ -662,6 +724,11 @@ int obs_grid(int N, int kt, bool mixed) {
 }
 
 size_t obs_part_bytes() { return sizeof(Part); }
+
+cudaError_t launch_weq(const Inst* insts, int slot, int ntri, int nk, cudaStream_t s) {
+  k_weq<float2><<<dim3((nk + 127) / 128, ntri), 128, 0, s>>>(insts, slot);
+  return cudaGetLastError();
+}
 
 }  // namespace batch
 }  // namespace edus
