@@ -63,3 +63,24 @@ def test_missing_library_raises(monkeypatch, tmp_path):
     monkeypatch.setattr(lib, "library_path", lambda: str(tmp_path / "nope.so"))
     with pytest.raises(E.EdusError):
         lib.load_library()
+
+
+def test_edus_run_driver_reports_input_errors(tmp_path):
+    """The drop-in executable: usage, a missing input and a grammar error end
+    with the reference's exit status 1 (usage errors 2) before any GPU work."""
+    import subprocess
+
+    from edus_b200 import build
+
+    if not os.path.exists(build.EXE):
+        build.build()
+    r = subprocess.run([build.EXE, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "usage: edus_run" in r.stdout
+    r = subprocess.run([build.EXE, "--no-such-flag"], capture_output=True, text=True)
+    assert r.returncode == 2
+    r = subprocess.run([build.EXE, str(tmp_path / "missing.txt")], capture_output=True, text=True)
+    assert r.returncode == 1 and "missing.txt" in r.stderr
+    bad = tmp_path / "input.txt"
+    bad.write_text("#SYSTEM\nthis is not an input file\n")
+    r = subprocess.run([build.EXE, str(bad)], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 1 and "edus_run:" in r.stderr

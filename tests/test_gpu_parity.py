@@ -184,3 +184,23 @@ def test_write_outputs_format(workdir, tmp_path):
     np.testing.assert_allclose(vals[:, 1::2], J1.real, rtol=1e-14, atol=1e-300)
     losses = open(os.path.join(out, "Losses.txt")).read().splitlines()
     assert losses[0].split()[0] == "-0.21" and len(losses[0].split()) == 4
+
+
+def test_edus_run_writes_the_reference_outputs(tmp_path):
+    """The drop-in executable on the shipped AB5 input: Output/J1.txt and
+    Output/Losses.txt against the golden run, as a user of the reference reads them."""
+    import shutil
+    import subprocess
+
+    from edus_b200 import build
+
+    shutil.copy(GOLDEN_INPUT, tmp_path / "input.txt")
+    r = subprocess.run([build.EXE], capture_output=True, text=True, cwd=tmp_path, timeout=600)
+    assert r.returncode == 0, r.stderr
+    G = np.load(os.path.join(GOLDEN, "ab5_golden.npz"))
+    rows = G["rows"]
+    J1 = np.loadtxt(tmp_path / "Output" / "J1.txt")
+    assert len(J1) == int(G["nrows"])
+    assert rel(J1[rows, 1:], G["J1"][:, 1:]) < 1e-12
+    L = np.loadtxt(tmp_path / "Output" / "Losses.txt")
+    assert np.abs(L[rows, 1:4] - G["Losses"][:, 1:4]).max() < 1e-13
