@@ -55,11 +55,15 @@ struct Slot {
 };
 
 struct ClassTab {
-  int n = 0, kt = 0, occ = 0;
+  int n = 0, kt = 0, occ = 0;  // occ: requested register profile / kernel form
+  int form = -1;               // form in use (profile 3 falls back to 0 when an instance does not fit it)
+  int psel = 0, pcomp = 0;     // profile 3: most stencil vectors / field components in use per instance
   std::vector<Tile> tiles;
   Tile* d_tiles = nullptr;
   size_t cap = 0;
-  int* d_ntiles = nullptr;
+  int* d_ntiles = nullptr;         // [0] tiles, [1] instances of the class
+  std::vector<ClassInst> insts;    // instance table (observable kernel)
+  ClassInst* d_cinst = nullptr;    // capacity: the batch's max_instances
   int sgrid = 0, ogrid = 0;
   bool dirty = false;
 };
@@ -130,7 +134,34 @@ Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
 // register profile / kernel form of a band count; the matrix-product form is built for FP64 only
 int profile_of(const edus_batch* b, int n) {
   const int p = (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.regs_profile[n] : 0;
-  return (p == 2 && b->mixed) ? 0 : p;
+  if (p == 2 && b->mixed) return 0;
+  if (p == 3 && !b->mixed) return 0;  // asynchronous staging is built for mixed precision
+  return p;
+}
+
+// Kernel form a class runs: profile 3 needs every running instance of the
+// class on a lattice stencil, otherwise the element-parallel form. Also the
+// staging sizes of profile 3 (at least one slot each).
+int form_of(const edus_batch* b, const ClassTab& c, int& psel, int& pcomp) {
+  psel = pcomp = 1;
+  if (c.occ != 3) return c.occ;
+  if (!pipe_supported(c.n, c.kt)) return 0;
+  for (const Slot& s : b->slots) {
+    if (s.status != EDUS_INST_RUNNING || s.n != c.n) continue;
+    const Inst& I = s.inst;
+    if (!I.lattice) return 0;
+    psel = std::max(psel, I.nsel);
+    pcomp = std::max(pcomp, ((I.fmask >> 0) & 1) + ((I.fmask >> 1) & 1) + ((I.fmask >> 2) & 1));
+  }
+  return 3;
+}
+
+int grid_of(const edus_batch* b, const ClassTab& c) {
+  switch (c.form) {
+    case 2: return stage_grid_mm(c.n, c.kt, b->mixed);
+    case 3: return stage_grid_pipe(c.n, c.kt, c.psel, c.pcomp);
+    default: return stage_grid(c.n, c.kt, c.form ? 1 : 0, b->mixed);
+  }
 }
 
 int check_problem(const edus_batch* b, const Problem& P) {
@@ -199,6 +230,29 @@ int upload_model(edus_batch* b, const Problem& P, const Inst& I) {
     if ((rc = put(b, (void*)I.Hdiag, hd))) return rc;
   }
   return 0;
+}
+
+// Field components and stencil vectors that contribute for the whole run. A
+// component that is zero in every field-table row (pump and probe, at t and
+// t + dt/2) adds E_x D_x = 0 and E_x W_x = 0 exactly; a stencil vector with
+// w_b = 0, or orthogonal to every pump component in use, has a gradient
+// coefficient w_b (E_pump . b) that is exactly 0. The stage kernels skip
+// both; the remaining terms are summed in the same order, so the result is
+// the same to the last bit.
+void select_terms(const Problem& P, const std::vector<FieldRow>& fr, Inst& I) {
+  int fmask = 0, pmask = 0;
+  for (const FieldRow& r : fr)
+    for (int x = 0; x < 3; x++) {
+      if (r.Et[x] != 0. || r.Eh[x] != 0.) pmask |= 1 << x;
+      if (r.Et[3 + x] != 0. || r.Eh[3 + x] != 0.) fmask |= 1 << x;
+    }
+  I.fmask = fmask | pmask;
+  I.nsel = 0;
+  for (int b = 0; b < P.nnb; b++) {
+    bool on = false;
+    for (int x = 0; x < 3; x++) on = on || ((pmask >> x) & 1 && P.bvec[b * 3 + x] != 0.);
+    if (on && P.shell_w[P.bshell[b]] != 0.) I.bsel[I.nsel++] = b;
+  }
 }
 
 // The k-gradient neighbours of a Monkhorst-Pack grid are fixed lattice steps
@@ -489,9 +543,30 @@ int sync_tiles(edus_batch* b) {
       c.cap = cap;
     }
     if (!c.tiles.empty()) BCK(cudaMemcpyAsync(c.d_tiles, c.tiles.data(), c.tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, b->stream));
-    const int nt = (int)c.tiles.size();
-    BCK(cudaMemcpyAsync(c.d_ntiles, &nt, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-    // pageable source: the copy has left nt before the call returns
+    // instance table: the runs of equal slots in the tile table
+    c.insts.clear();
+    for (size_t t = 0; t < c.tiles.size();) {
+      size_t u = t;
+      while (u < c.tiles.size() && c.tiles[u].inst == c.tiles[t].inst) u++;
+      const Slot& sl = b->slots[c.tiles[t].inst];
+      const int uk = obs_unit(c.n);
+      c.insts.push_back(ClassInst{c.tiles[t].inst, (sl.nk + uk - 1) / uk, sl.itfi, sl.res});
+      t = u;
+    }
+    if (!c.insts.empty())
+      BCK(cudaMemcpyAsync(c.d_cinst, c.insts.data(), c.insts.size() * sizeof(ClassInst), cudaMemcpyHostToDevice, b->stream));
+    const int counts[2] = {(int)c.tiles.size(), (int)c.insts.size()};
+    BCK(cudaMemcpyAsync(c.d_ntiles, counts, sizeof(counts), cudaMemcpyHostToDevice, b->stream));
+    // pageable sources: the copies have left the host buffers before the calls return
+    int psel = 1, pcomp = 1;
+    const int form = form_of(b, c, psel, pcomp);
+    if (form != c.form || psel != c.psel || pcomp != c.pcomp) {
+      c.form = form;
+      c.psel = psel;
+      c.pcomp = pcomp;
+      c.sgrid = grid_of(b, c);
+      if (c.sgrid <= 0) return fail(EDUS_ECUDA, "batch: no resident block for %d bands (form %d)", c.n, c.form);
+    }
     c.dirty = false;
   }
   return 0;
@@ -501,7 +576,8 @@ std::string graph_key(const edus_batch* b) {
   std::string k;
   for (const auto& kv : b->classes) {
     char buf[96];
-    snprintf(buf, sizeof(buf), "%d:%d:%p;", kv.second.n, kv.second.kt, (const void*)kv.second.d_tiles);
+    snprintf(buf, sizeof(buf), "%d:%d:%d:%d:%d:%p;", kv.second.n, kv.second.kt, kv.second.form, kv.second.psel, kv.second.pcomp,
+             (const void*)kv.second.d_tiles);
     k += buf;
   }
   return k;
@@ -513,17 +589,19 @@ int record_chunk(edus_batch* b) {
     const int parity = s & 1;
     for (auto& kv : b->classes) {
       ClassTab& c = kv.second;
-      View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles};
-      BCK(launch_obs(c.n, c.kt, b->mixed, v, parity, c.ogrid, b->stream));
+      View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles, c.d_cinst, c.d_ntiles + 1};
+      BCK(launch_obs(c.n, c.kt, b->mixed, v, parity, (int)b->slots.size(), c.ogrid, b->stream));
     }
     for (int st = 0; st < 4; st++)
       for (auto& kv : b->classes) {
         ClassTab& c = kv.second;
-        View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles};
-        if (c.occ == 2)
+        View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles, c.d_cinst, c.d_ntiles + 1};
+        if (c.form == 3)
+          BCK(launch_stage_pipe(c.n, c.kt, v, st, parity, c.psel, c.pcomp, c.sgrid, b->stream));
+        else if (c.form == 2)
           BCK(launch_stage_mm(c.n, c.kt, b->mixed, v, st, parity, c.sgrid, b->stream));
         else
-          BCK(launch_stage(c.n, c.kt, c.occ, b->mixed, v, st, parity, c.sgrid, b->stream));
+          BCK(launch_stage(c.n, c.kt, c.form, b->mixed, v, st, parity, c.sgrid, b->stream));
       }
   }
   return 0;
@@ -665,6 +743,7 @@ void edus_batch_destroy(edus_batch* b) {
   for (auto& kv : b->classes) {
     if (kv.second.d_tiles) cudaFreeAsync(kv.second.d_tiles, b->stream);
     if (kv.second.d_ntiles) cudaFree(kv.second.d_ntiles);
+    if (kv.second.d_cinst) cudaFree(kv.second.d_cinst);
   }
   if (b->stream) cudaStreamSynchronize(b->stream);
   cudaFree(b->d_insts);
@@ -796,6 +875,10 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
       return undo(rc);
     }
   }
+  // mixed precision: Pb starts as the FP32 copy of the deviation P0 = 0 that
+  // stage 0 reads (stage 3 refreshes it every step)
+  if (b->mixed && cudaMemsetAsync(I.Pb, 0, L.state, b->stream) != cudaSuccess)
+    return undo(fail(EDUS_ECUDA, "batch: clear stage input"));
   {
     // field table: the single-solve loop's times (t += dt) and fields
     std::vector<FieldRow> fr((size_t)P.itfi + 2);
@@ -811,6 +894,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
       t += P.p.dt;
     }
     if ((rc = put(b, (void*)I.field, fr))) return undo(rc);
+    select_terms(P, fr, I);
   }
   if (cudaMemsetAsync(I.done, 0, sizeof(unsigned int), b->stream) != cudaSuccess ||
       cudaMemcpyAsync(b->d_insts + q, &I, sizeof(Inst), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
@@ -826,9 +910,12 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
     c.n = n;
     c.kt = kt;
     c.occ = profile_of(b, n);
-    c.sgrid = c.occ == 2 ? stage_grid_mm(n, kt, b->mixed) : stage_grid(n, kt, c.occ ? 1 : 0, b->mixed);
-    c.ogrid = obs_grid(n, kt, b->mixed);
-    if (cudaMalloc(&c.d_ntiles, sizeof(int)) != cudaSuccess) return undo(fail(EDUS_ENOMEM, "tile count"));
+    c.form = -1;  // chosen with the tile table, before the next chunk
+    c.ogrid = obs_grid(n, b->mixed, (int)b->slots.size());
+    if (c.ogrid <= 0) return undo(fail(EDUS_ECUDA, "batch: no resident block of the observable kernel for %d bands", n));
+    if (cudaMalloc(&c.d_ntiles, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c.d_cinst, b->slots.size() * sizeof(ClassInst)) != cudaSuccess)
+      return undo(fail(EDUS_ENOMEM, "tile count"));
   }
   for (int t = 0; t < s.ntiles; t++) c.tiles.push_back(Tile{q, t * kt, t, 0});
   c.dirty = true;

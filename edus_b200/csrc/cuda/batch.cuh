@@ -60,6 +60,13 @@ struct Inst {
   double wb[kMaxNb];
   double bvec[kMaxNb][3];
   int off[kBatchMaxNb][2];   // lattice step (d1, d2) of each b when lattice != 0
+  // Terms that are exact zeros for the whole run, skipped by the stage kernels:
+  // bit x of fmask is set when field component x (pump or probe) is nonzero at
+  // some step (D_x, W_x are read only then); bsel[0..nsel) lists, in b order,
+  // the stencil vectors whose gradient coefficient w_b (E_pump . b) can be
+  // nonzero (w_b != 0 and b not orthogonal to every pump component in use).
+  int fmask, nsel;
+  int bsel[kBatchMaxNb];
 };
 
 struct Tile {
@@ -69,11 +76,20 @@ struct Tile {
   int pad;
 };
 
+// One instance of a class for the observable kernel: its slot, its number of
+// observable units (obs_unit(N) consecutive k points each), its last step and
+// output resolution.
+struct ClassInst {
+  int slot, nunits, itfi, res;
+};
+
 struct View {
   const Inst* insts;
   int* it[2];            // step counter per slot, by tick parity
   const Tile* tiles;     // tile table of one class
   const int* ntiles;     // its length (device scalar)
+  const ClassInst* cinst;  // instance table of the class
+  const int* ninst;        // its length (device scalar)
 };
 
 // One RK4 stage (0..3, Source_Main/RungeKutta.cpp schedule) over every tile of
@@ -81,17 +97,27 @@ struct View {
 // occ the register profile (0: 56 registers, more resident warps; 1: more registers).
 cudaError_t launch_stage(int N, int kt, int occ, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
 // Observables of the instances due at this tick (it % res == 0) and the
-// step-counter advance of every instance of the class.
-cudaError_t launch_obs(int N, int kt, bool mixed, const View& v, int parity, int grid, cudaStream_t s);
+// step-counter advance of every instance of the class (batch_obs.cu);
+// max_inst bounds the class's instance table.
+cudaError_t launch_obs(int N, int kt, bool mixed, const View& v, int parity, int max_inst, int grid, cudaStream_t s);
 // Persistent grid sizes (SMs x resident blocks) of the two kernels.
 int stage_grid(int N, int kt, int occ, bool mixed);
-int obs_grid(int N, int kt, bool mixed);
+int obs_grid(int N, bool mixed, int max_inst);
 bool class_supported(int N, int kt);
 // Matrix-product form of the stage kernel (batch_mm.cu), register profile 2.
 bool mm_supported(int N, int kt);
 cudaError_t launch_stage_mm(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
 int stage_grid_mm(int N, int kt, bool mixed);
+// Mixed-precision stage kernel with asynchronous staging (batch_pipe.cu),
+// register profile 3, for lattice-stencil instances: classes it is built for,
+// launch and persistent grid; nsel / ncomp are the most stencil vectors and
+// field components in use by an instance of the class (they size the staging).
+bool pipe_supported(int N, int kt);
+cudaError_t launch_stage_pipe(int N, int kt, const View& v, int stage, int parity, int nsel, int ncomp, int grid, cudaStream_t s);
+int stage_grid_pipe(int N, int kt, int nsel, int ncomp);
 size_t obs_part_bytes();
+// k points per observable unit (one partial per unit; the partials are sized per tile)
+int obs_unit(int N);
 // Mixed precision: W of one instance (after its D and rho_eq are on the device).
 cudaError_t launch_weq(const Inst* insts, int slot, int ntri, int nk, cudaStream_t s);
 

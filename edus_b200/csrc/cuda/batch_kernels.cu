@@ -60,6 +60,33 @@ __device__ __forceinline__ C xmi(C a) { return xmk<C>(a.y, -a.x); }
 template <class To, class From>
 __device__ __forceinline__ To cvt(From a) { return xmk<To>((decltype(To::x))a.x, (decltype(To::x))a.y); }
 
+// Commutator sum beta = sum_l H~_jl P_il - conj(H~_il P_jl) as fused
+// multiply-adds into eight independent partial sums (products with H~_j and
+// with H~_i, real and imaginary parts, even and odd l), so that no dependency
+// chain is longer than N multiply-adds; batch_pipe.cu uses the same order.
+template <class C>
+struct CommAcc {
+  using R = decltype(C::x);
+  R ax[2] = {0, 0}, ay[2] = {0, 0}, bx[2] = {0, 0}, by[2] = {0, 0};
+  __device__ __forceinline__ void add(int par, C hj, C pi, C hi, C pj) {
+    ax[par] = fma(hj.x, pi.x, ax[par]);
+    ax[par] = fma(-hj.y, pi.y, ax[par]);
+    ay[par] = fma(hj.x, pi.y, ay[par]);
+    ay[par] = fma(hj.y, pi.x, ay[par]);
+    bx[par] = fma(hi.x, pj.x, bx[par]);
+    bx[par] = fma(-hi.y, pj.y, bx[par]);
+    by[par] = fma(hi.x, pj.y, by[par]);
+    by[par] = fma(hi.y, pj.x, by[par]);
+  }
+  // H~_j.P_i - conj(H~_i.P_j)
+  __device__ __forceinline__ C sum() const {
+    C r;
+    r.x = (ax[0] + ax[1]) - (bx[0] + bx[1]);
+    r.y = (ay[0] + ay[1]) + (by[0] + by[1]);
+    return r;
+  }
+};
+
 template <bool MIX>
 struct Types {
   using S = double2;  // storage of H, D, GE, U
@@ -96,11 +123,13 @@ constexpr int min_blocks(int nthr, int occ) {
 // [r * RS + c * KT + kl], so every operand of the commutator is a constant
 // offset from a per-thread row pointer. The tile's field, gradient
 // coefficients and neighbour indices are written one tile ahead.
-// Row r of a shared matrix starts at r * RS(N, KT): one entry of padding per
-// row keeps the rows of a warp's elements on different banks.
+// Row r of a shared matrix starts at r * RS(N, KT), RS = KT mod 2 KT: the
+// elements (i, j), (i, j + 1), ... that one bank phase of a warp serves (16
+// threads of 8-byte entries, 8 threads of 16-byte entries) then read their
+// KT-long runs of row j from disjoint banks.
 template <int N, int KT>
 struct Rows {
-  static constexpr int RS = N * KT + 1;
+  static constexpr int RS = N * KT + ((N % 2) ? 0 : KT);
   static constexpr int SIZE = N * RS;
 };
 
@@ -139,20 +168,20 @@ __device__ __forceinline__ void tile_setup(StageSmem<N, KT, MIX>& s, const View&
   const int tid = threadIdx.x;
   if (tid == 0) s.active = active;
   if (!active) return;
-  const int nk = I->nk, nnb = I->nnb;
+  const int nk = I->nk, nsel = I->nsel;
   const FieldRow* fr = I->field + it;
   const double* Es = stage == 0 ? fr->Et : (stage == 3 ? fr[1].Et : fr->Eh);
-  if (tid < nnb) {
-    const int b = tid;
-    s.G[b] = I->wb[b] * (Es[0] * I->bvec[b][0] + Es[1] * I->bvec[b][1] + Es[2] * I->bvec[b][2]);
+  if (tid < nsel) {
+    const int b = I->bsel[tid];
+    s.G[tid] = I->wb[b] * (Es[0] * I->bvec[b][0] + Es[1] * I->bvec[b][1] + Es[2] * I->bvec[b][2]);
   }
   if (tid == 0) {
     for (int q = 0; q < 6; q++) s.E[q / 3][q % 3] = Es[q];
     s.on = (it == 0) || field_on(fr->Et);
   }
-  for (int q = tid; q < nnb * KT; q += blockDim.x) {
-    const int b = q / KT, kq = tl.k0 + q % KT;
-    s.nb[b][q % KT] = kq < nk ? neighbour(I, kq, b) : 0;
+  for (int q = tid; q < nsel * KT; q += blockDim.x) {
+    const int c = q / KT, kq = tl.k0 + q % KT;
+    s.nb[c][q % KT] = kq < nk ? neighbour(I, kq, I->bsel[c]) : 0;
   }
 }
 
@@ -182,7 +211,7 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
     buf ^= 1;
     const Inst* I = v.insts + tl.inst;
     const bool active = s.active;
-    const int nk = I->nk, nch = I->nch, nnb = I->nnb;
+    const int nk = I->nk, nch = I->nch, nsel = I->nsel, fmask = I->fmask;
     const int k = tl.k0 + kl;
     const bool valid = active && lane_ok && k < nk;
     const double2* src = stage == 0 ? I->P0 : (stage == 2 ? I->Pb : I->Pa);
@@ -199,32 +228,35 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
       Pe = (!MIX || stage == 0) ? src[o] : cvt<double2>(src32[o]);
       He = reinterpret_cast<const S*>(I->H)[o];
       const S* Dp = reinterpret_cast<const S*>(I->D);
+      // components of the field that are zero for the whole run are not read
 #pragma unroll
-      for (int x = 0; x < 3; x++) De[x] = Dp[(size_t)x * NT * nk + o];
+      for (int x = 0; x < 3; x++)
+        if ((fmask >> x) & 1) De[x] = Dp[(size_t)x * NT * nk + o];
       if (MIX) {
 #pragma unroll
-        for (int x = 0; x < 3; x++) We[x] = reinterpret_cast<const S*>(I->W)[(size_t)x * NT * nk + o];
+        for (int x = 0; x < 3; x++)
+          if ((fmask >> x) & 1) We[x] = reinterpret_cast<const S*>(I->W)[(size_t)x * NT * nk + o];
         if (i == j) Hii = I->Hdiag[(size_t)i * nk + k];
       }
       if (stage > 0) p1v = I->P1[o];
       if (stage == 1 || stage == 2) p0v = I->P0[o];
       if (s.on) {
-        // k-gradient: sum_b (w_b E_pump . b) rho_e(k + b) (headers/RungeKutta.h:258-276),
-        // gathers four at a time, summed in b order (mixed: of the deviation; the
-        // rho_eq part is in W)
+        // k-gradient: sum_b (w_b E_pump . b) rho_e(k + b) (headers/RungeKutta.h:258-276)
+        // over the b whose coefficient is not identically zero, gathers four at a
+        // time, summed in b order (mixed: of the deviation; the rho_eq part is in W)
         constexpr int GB = 4;
-        for (int b0 = 0; b0 < nnb; b0 += GB) {
+        for (int b0 = 0; b0 < nsel; b0 += GB) {
           C pn[GB];
 #pragma unroll
           for (int q = 0; q < GB; q++) {
-            const int kb = s.nb[b0 + q < nnb ? b0 + q : 0][kl];
-            pn[q] = (b0 + q >= nnb) ? xmk<C>(0, 0)
+            const int kb = s.nb[b0 + q < nsel ? b0 + q : 0][kl];
+            pn[q] = (b0 + q >= nsel) ? xmk<C>(0, 0)
                     : (!MIX || stage == 0) ? cvt<C>(src[(size_t)e * nk + kb])
                                            : cvt<C>(src32[(size_t)e * nk + kb]);
           }
 #pragma unroll
           for (int q = 0; q < GB; q++) {
-            if (b0 + q >= nnb) break;
+            if (b0 + q >= nsel) break;
             G = xadd(G, xscale(pn[q], (R)s.G[b0 + q]));
           }
         }
@@ -284,13 +316,10 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
       const C* Hj = s.H + j * RS + kl;
       const C* Pi = s.P + i * RS + kl;
       const C* Pj = s.P + j * RS + kl;
-      C beta = xmk<C>(0, 0);
+      CommAcc<C> acc;
 #pragma unroll
-      for (int l = 0; l < N; l++) {
-        const C x = xmul(Hj[l * KT], Pi[l * KT]);
-        const C y = xmul(Hi[l * KT], Pj[l * KT]);
-        beta = xadd(beta, xsub(x, xconj(y)));
-      }
+      for (int l = 0; l < N; l++) acc.add(l & 1, Hj[l * KT], Pi[l * KT], Hi[l * KT], Pj[l * KT]);
+      const C beta = acc.sum();
       C vv = xmi(beta);
       if (!MIX && i < nch && j >= nch) vv = xadd(vv, xmi(xscale(cvt<C>(Pe), (R)(-I->wx2))));
       vv = xadd(vv, G);
@@ -319,9 +348,13 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
             I->P1[o] = cadd(p1v, cscale(d, dt3));
             Pa32[o] = cvt<float2>(cadd(p0v, cscale(d, dt)));
             break;
-          default:
-            I->P0[o] = cadd(p1v, cscale(d, dt6));
+          default: {
+            // the new deviation, and its FP32 copy that the next stage 0 reads
+            const double2 pn = cadd(p1v, cscale(d, dt6));
+            I->P0[o] = pn;
+            Pb32[o] = cvt<float2>(pn);
             break;
+          }
         }
       } else {
         switch (stage) {
@@ -393,237 +426,6 @@ __global__ void k_weq(const Inst* __restrict__ insts, int slot) {
   }
 }
 
-// ------------------------------------------------------------------ observables
-struct Part {
-  double pop[kMaxBands];
-  double2 J1[3], J2[3], TA[3];
-  double pmax, pmin;
-};
-__device__ __forceinline__ void part_zero(Part& p) {
-  for (int c = 0; c < kMaxBands; c++) p.pop[c] = 0;
-  for (int x = 0; x < 3; x++) p.J1[x] = p.J2[x] = p.TA[x] = cz();
-  p.pmax = 0;
-  p.pmin = 1.0;
-}
-__device__ __forceinline__ void part_add(Part& d, const Part& o, int n) {
-  for (int c = 0; c < n; c++) d.pop[c] += o.pop[c];
-  for (int x = 0; x < 3; x++) {
-    d.J1[x] = cadd(d.J1[x], o.J1[x]);
-    d.J2[x] = cadd(d.J2[x], o.J2[x]);
-    d.TA[x] = cadd(d.TA[x], o.TA[x]);
-  }
-  d.pmax = fmax(d.pmax, o.pmax);
-  d.pmin = fmin(d.pmin, o.pmin);
-}
-
-__device__ __forceinline__ double warp_sum(double x) {
-  for (int s = 16; s > 0; s >>= 1) x += __shfl_xor_sync(0xffffffffu, x, s);
-  return x;
-}
-
-constexpr int kRedVals = kMaxBands + 20;
-
-// Sums (max / min for pmax / pmin) one Part per thread over the block into
-// out, in a fixed order: warp butterflies, then warps in index order.
-template <int N, int NW>
-__device__ __forceinline__ void block_reduce(Part& my, Part& out, double (*sW)[kRedVals]) {
-  const int lane = threadIdx.x % 32, w = threadIdx.x / 32;
-  double vals[N + 20];
-  for (int c = 0; c < N; c++) vals[c] = my.pop[c];
-  for (int x = 0; x < 3; x++) {
-    vals[N + 6 * x + 0] = my.J1[x].x;
-    vals[N + 6 * x + 1] = my.J1[x].y;
-    vals[N + 6 * x + 2] = my.J2[x].x;
-    vals[N + 6 * x + 3] = my.J2[x].y;
-    vals[N + 6 * x + 4] = my.TA[x].x;
-    vals[N + 6 * x + 5] = my.TA[x].y;
-  }
-  for (int q = 0; q < N + 18; q++) vals[q] = warp_sum(vals[q]);
-  double pmax = my.pmax, pmin = my.pmin;
-  for (int s = 16; s > 0; s >>= 1) {
-    pmax = fmax(pmax, __shfl_xor_sync(0xffffffffu, pmax, s));
-    pmin = fmin(pmin, __shfl_xor_sync(0xffffffffu, pmin, s));
-  }
-  vals[N + 18] = pmax;
-  vals[N + 19] = pmin;
-  if (lane == 0)
-    for (int q = 0; q < N + 20; q++) sW[w][q] = vals[q];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    part_zero(out);
-    for (int ww = 0; ww < NW; ww++) {
-      for (int c = 0; c < N; c++) out.pop[c] += sW[ww][c];
-      for (int x = 0; x < 3; x++) {
-        out.J1[x] = cadd(out.J1[x], cmk(sW[ww][N + 6 * x], sW[ww][N + 6 * x + 1]));
-        out.J2[x] = cadd(out.J2[x], cmk(sW[ww][N + 6 * x + 2], sW[ww][N + 6 * x + 3]));
-        out.TA[x] = cadd(out.TA[x], cmk(sW[ww][N + 6 * x + 4], sW[ww][N + 6 * x + 5]));
-      }
-      out.pmax = fmax(out.pmax, sW[ww][N + 18]);
-      out.pmin = fmin(out.pmin, sW[ww][N + 19]);
-    }
-  }
-  __syncthreads();
-}
-
-// Observables at one output instant (headers/Observables_MPI.h:217-484,559-598,
-// 668-775) of every instance due at this tick; the tile's k points are taken
-// KO at a time. Also advances the step counter of every instance of the class.
-template <int N, int KO, bool MIX>
-__global__ void __launch_bounds__(pad32(KO* TriB<N>::NT)) k_bobs(View v, int parity, int kt) {
-  constexpr int NT = TriB<N>::NT;
-  constexpr int NTHR = pad32(KO * NT);
-  constexpr int NW = NTHR / 32;
-  using S = typename Types<MIX>::S;
-  __shared__ double2 sP[NT][KO];
-  __shared__ double2 sH[NT][KO];
-  __shared__ double2 sD[3][NT][KO];
-  __shared__ double2 sU[N * N][KO];
-  __shared__ double sW[NW][kRedVals];
-  __shared__ Part sT;
-  __shared__ bool sLast;
-  const int tid = threadIdx.x;
-  const int kl = tid % KO, e = tid / KO;
-  const bool lane_ok = e < NT;
-  int i = 0, j = 0;
-  if (lane_ok) TriB<N>::ij(e, i, j);
-  const int ntiles = *v.ntiles;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const Tile tl = v.tiles[t];
-    const int it = v.it[parity][tl.inst];
-    const Inst* I = v.insts + tl.inst;
-    const int itfi = I->itfi;
-    if (tl.t_in == 0 && tid == 0) v.it[parity ^ 1][tl.inst] = it <= itfi ? it + 1 : it;
-    if (it < 0 || it > itfi || it % I->res != 0) continue;
-    const int nk = I->nk, nch = I->nch;
-    const S* H = reinterpret_cast<const S*>(I->H);
-    const S* D = reinterpret_cast<const S*>(I->D);
-    const S* GE = reinterpret_cast<const S*>(I->GE);
-    const S* U = reinterpret_cast<const S*>(I->U);
-    Part my;
-    part_zero(my);
-    const int kend = min(tl.k0 + kt, nk);
-    for (int k0 = tl.k0; k0 < kend; k0 += KO) {
-      const int k = k0 + kl;
-      const bool valid = lane_ok && k < kend;
-      if (lane_ok) {
-        const size_t o = (size_t)e * nk + k;
-        sP[e][kl] = valid ? (MIX ? cadd(I->P0[o], I->Peq[o]) : I->P0[o]) : cz();
-        sH[e][kl] = valid ? cvt<double2>(H[o]) : cz();
-        for (int x = 0; x < 3; x++) sD[x][e][kl] = valid ? cvt<double2>(D[(size_t)x * NT * nk + o]) : cz();
-      }
-      for (int q = tid; q < N * N * KO; q += NTHR) {
-        const int u = q / KO, kq = k0 + q % KO;
-        sU[u][q % KO] = kq < kend ? cvt<double2>(U[(size_t)u * nk + kq]) : cz();
-      }
-      __syncthreads();
-      if (valid) {
-        auto Pf = [&](int r, int c) -> double2 { return (r <= c) ? sP[TriB<N>::idx(r, c)][kl] : cconj(sP[TriB<N>::idx(c, r)][kl]); };
-        auto Hf = [&](int r, int c) -> double2 { return (r <= c) ? sH[TriB<N>::idx(r, c)][kl] : cconj(sH[TriB<N>::idx(c, r)][kl]); };
-        auto Df = [&](int x, int r, int c) -> double2 {
-          return r <= c ? sD[x][TriB<N>::idx(r, c)][kl] : sD[x][TriB<N>::idx(c, r)][kl];
-        };
-        const double2 pe = sP[e][kl];
-        if (I->want_current) {
-          const size_t o = (size_t)e * nk + k;
-          for (int x = 0; x < 3; x++) {
-            const double2 ge = cvt<double2>(GE[(size_t)x * NT * nk + o]);
-            my.J1[x] = cadd(my.J1[x], cmul(pe, ge));
-            if (i != j) my.J1[x] = cadd(my.J1[x], cmul(cconj(pe), cconj(ge)));
-          }
-          // J2: sum_l P_ab H_al conj(D_bl) for (a, b) = (i, j) and, off the diagonal, (j, i)
-          for (int pass = 0; pass < (i == j ? 1 : 2); pass++) {
-            const int a = pass ? j : i, b = pass ? i : j;
-            const double2 pab = pass ? cconj(pe) : pe;
-            for (int l = 0; l < N; l++) {
-              const double2 ph = cmul(pab, Hf(a, l));
-              for (int x = 0; x < 3; x++) my.J2[x] = cadd(my.J2[x], cmulc(ph, Df(x, b, l)));
-            }
-          }
-        }
-        if (I->want_tabs && i < nch && j >= nch)
-          for (int x = 0; x < 3; x++) my.TA[x] = csub(my.TA[x], cmul(cscale(sD[x][e][kl], 2.), pe));
-        if (e < N) {
-          // population of band c = e in the model eigenbasis: sum_ij conj(U_ci) P_ij U_cj
-          const int c = e;
-          double2 acc = cz();
-          for (int ii = 0; ii < N; ii++) {
-            double2 m = cz();
-            for (int jj = 0; jj < N; jj++) m = cadd(m, cmul(Pf(ii, jj), sU[c * N + jj][kl]));
-            acc = cadd(acc, cmul(cconj(sU[c * N + ii][kl]), m));
-          }
-          const double Pk = acc.x;
-          my.pop[c] += Pk;
-          if (c < I->nbands) {
-            my.pmax = fmax(my.pmax, fabs(1. - Pk));
-            my.pmin = fmin(my.pmin, 1. - Pk);
-          } else {
-            my.pmax = fmax(my.pmax, fabs(Pk));
-            my.pmin = fmin(my.pmin, Pk);
-          }
-        }
-      }
-      __syncthreads();
-    }
-    block_reduce<N, NW>(my, sT, sW);
-    if (tid == 0) {
-      reinterpret_cast<Part*>(I->part)[tl.t_in] = sT;
-      __threadfence();
-      sLast = atomicAdd(I->done, 1u) == (unsigned)(I->ntiles - 1);
-    }
-    __syncthreads();
-    if (sLast) {
-      // last tile of the instance to finish: fixed-order reduction over its tiles
-      __threadfence();
-      const Part* part = reinterpret_cast<const Part*>(I->part);
-      Part acc;
-      part_zero(acc);
-      for (int q = tid; q < I->ntiles; q += NTHR) {
-        // written by other blocks of this launch: read past L1
-        Part pq;
-        const double* src = reinterpret_cast<const double*>(part + q);
-        double* dst = reinterpret_cast<double*>(&pq);
-        for (int w = 0; w < (int)(sizeof(Part) / sizeof(double)); w++) dst[w] = __ldcg(src + w);
-        part_add(acc, pq, N);
-      }
-      block_reduce<N, NW>(acc, sT, sW);
-      if (tid == 0) {
-        edus_obs rec;
-        memset(&rec, 0, sizeof(rec));
-        rec.t = I->field[it].t;
-        if (it > 0)
-          for (int x = 0; x < 3; x++) {
-            rec.EF_pump[x] = I->field[it].Et[x];
-            rec.EF_probe[x] = I->field[it].Et[3 + x];
-          }
-        rec.dt = I->dt;
-        const double inv = 1. / nk;
-        double trace = -(double)I->nbands, ncd = 0;
-        for (int c = 0; c < N; c++) {
-          double val = sT.pop[c] * inv;
-          trace += val;
-          if (c < I->nbands) val = 1.0 - val;
-          rec.pop[c] = val;
-          if (val > ncd) ncd = val;
-        }
-        for (int x = 0; x < 3; x++) {
-          rec.J1[2 * x] = sT.J1[x].x * I->scaleJ;
-          rec.J1[2 * x + 1] = sT.J1[x].y * I->scaleJ;
-          rec.J2[x] = -2. * (sT.J2[x].y * I->scaleJ);
-          rec.tabs[2 * x] = sT.TA[x].x * I->scaleTA * inv;
-          rec.tabs[2 * x + 1] = sT.TA[x].y * I->scaleTA * inv;
-        }
-        rec.trace_dev = trace;
-        rec.p_cond_max = sT.pmax;
-        rec.p_min = sT.pmin;
-        rec.n_cond = ncd;
-        I->log[it / I->res] = rec;
-        *I->done = 0u;
-      }
-    }
-    __syncthreads();
-  }
-}
-
 // ------------------------------------------------------------------ dispatch
 template <int N, int KT, bool MIX, int OCC>
 cudaError_t stage_n(const View& v, int stage, int parity, int grid, cudaStream_t s) {
@@ -637,29 +439,6 @@ int stage_grid_n() {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bstage<N, KT, MIX, OCC>, pad32(KT * TriB<N>::NT), 0);
-  return sms * (per > 0 ? per : 1);
-}
-
-// observable sub-tile length per band count
-template <int N>
-struct ObsKO {
-  static constexpr int v = N <= 2 ? 32 : (N <= 3 ? 16 : (N <= 4 ? 8 : (N <= 8 ? 4 : 1)));
-};
-
-template <int N, bool MIX>
-cudaError_t obs_n(const View& v, int parity, int kt, int grid, cudaStream_t s) {
-  constexpr int KO = ObsKO<N>::v;
-  k_bobs<N, KO, MIX><<<grid, pad32(KO * TriB<N>::NT), 0, s>>>(v, parity, kt);
-  return cudaGetLastError();
-}
-
-template <int N, bool MIX>
-int obs_grid_n() {
-  constexpr int KO = ObsKO<N>::v;
-  int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bobs<N, KO, MIX>, pad32(KO * TriB<N>::NT), 0);
   return sms * (per > 0 ? per : 1);
 }
 
@@ -698,32 +477,6 @@ int stage_grid(int N, int kt, int occ, bool mixed) {
   return 0;
 }
 
-cudaError_t launch_obs(int N, int kt, bool mixed, const View& v, int parity, int grid, cudaStream_t s) {
-  switch (N) {
-    case 2: return mixed ? obs_n<2, true>(v, parity, kt, grid, s) : obs_n<2, false>(v, parity, kt, grid, s);
-    case 3: return mixed ? obs_n<3, true>(v, parity, kt, grid, s) : obs_n<3, false>(v, parity, kt, grid, s);
-    case 4: return mixed ? obs_n<4, true>(v, parity, kt, grid, s) : obs_n<4, false>(v, parity, kt, grid, s);
-    case 5: return mixed ? obs_n<5, true>(v, parity, kt, grid, s) : obs_n<5, false>(v, parity, kt, grid, s);
-    case 8: return mixed ? obs_n<8, true>(v, parity, kt, grid, s) : obs_n<8, false>(v, parity, kt, grid, s);
-    case 16: return mixed ? obs_n<16, true>(v, parity, kt, grid, s) : obs_n<16, false>(v, parity, kt, grid, s);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
-int obs_grid(int N, int kt, bool mixed) {
-  (void)kt;
-  switch (N) {
-    case 2: return mixed ? obs_grid_n<2, true>() : obs_grid_n<2, false>();
-    case 3: return mixed ? obs_grid_n<3, true>() : obs_grid_n<3, false>();
-    case 4: return mixed ? obs_grid_n<4, true>() : obs_grid_n<4, false>();
-    case 5: return mixed ? obs_grid_n<5, true>() : obs_grid_n<5, false>();
-    case 8: return mixed ? obs_grid_n<8, true>() : obs_grid_n<8, false>();
-    case 16: return mixed ? obs_grid_n<16, true>() : obs_grid_n<16, false>();
-    default: return 0;
-  }
-}
-
-size_t obs_part_bytes() { return sizeof(Part); }
 
 cudaError_t launch_weq(const Inst* insts, int slot, int ntri, int nk, cudaStream_t s) {
   k_weq<float2><<<dim3((nk + 127) / 128, ntri), 128, 0, s>>>(insts, slot);

@@ -117,15 +117,18 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
     if (!active) return;
     const FieldRow* fr = I->field + it;
     const double* Es = stage == 0 ? fr->Et : (stage == 3 ? fr[1].Et : fr->Eh);
-    const int nnb = I->nnb, nk = I->nk;
-    if (tid < nnb) su[slot].G[tid] = I->wb[tid] * (Es[0] * I->bvec[tid][0] + Es[1] * I->bvec[tid][1] + Es[2] * I->bvec[tid][2]);
+    const int nsel = I->nsel, nk = I->nk;
+    if (tid < nsel) {
+      const int b = I->bsel[tid];
+      su[slot].G[tid] = I->wb[b] * (Es[0] * I->bvec[b][0] + Es[1] * I->bvec[b][1] + Es[2] * I->bvec[b][2]);
+    }
     if (tid == 0) {
       for (int q = 0; q < 6; q++) su[slot].E[q / 3][q % 3] = Es[q];
       su[slot].on = (it == 0) || field_nonzero(fr->Et);
     }
-    for (int q = tid; q < nnb * KT; q += NTHR) {
-      const int b = q / KT, kq = tl.k0 + q % KT;
-      snb[slot][b][q % KT] = kq < nk ? nb_of(I, kq, b) : 0;
+    for (int q = tid; q < nsel * KT; q += NTHR) {
+      const int c = q / KT, kq = tl.k0 + q % KT;
+      snb[slot][c][q % KT] = kq < nk ? nb_of(I, kq, I->bsel[c]) : 0;
     }
   };
 
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
     buf ^= 1;
     const Inst* I = v.insts + tl.inst;
     const bool active = su[cur].active;
-    const int nk = I->nk, nch = I->nch, nnb = I->nnb, k0 = tl.k0;
+    const int nk = I->nk, nch = I->nch, nsel = I->nsel, fmask = I->fmask, k0 = tl.k0;
     const double2* src = stage == 0 ? I->P0 : (stage == 2 ? I->Pb : I->Pa);
     // ---- (A) element items
     if (active) {
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
         const S He = Hg[o];
         S De[3];
 #pragma unroll
-        for (int x = 0; x < 3; x++) De[x] = Dg[(size_t)x * NT * nk + o];
+        for (int x = 0; x < 3; x++) De[x] = ((fmask >> x) & 1) ? Dg[(size_t)x * NT * nk + o] : mk<S>(0, 0);
         double2 Qe = make_double2(0., 0.);
         double Hii = 0.;
         if (MIX) {
@@ -175,13 +178,13 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
         if (su[cur].on) {
           const double2* row = src + (size_t)e * nk;
           constexpr int GB = 4;
-          for (int b0 = 0; b0 < nnb; b0 += GB) {
+          for (int b0 = 0; b0 < nsel; b0 += GB) {
             double2 pn[GB];
 #pragma unroll
-            for (int u = 0; u < GB; u++) pn[u] = (b0 + u < nnb) ? row[snb[cur][b0 + u][kl]] : make_double2(0., 0.);
+            for (int u = 0; u < GB; u++) pn[u] = (b0 + u < nsel) ? row[snb[cur][b0 + u][kl]] : make_double2(0., 0.);
 #pragma unroll
             for (int u = 0; u < GB; u++) {
-              if (b0 + u >= nnb) break;
+              if (b0 + u >= nsel) break;
               const C pq = cv<C>(pn[u]);
               const R c = (R)su[cur].G[b0 + u];
               G = mk<C>(G.x + pq.x * c, G.y + pq.y * c);

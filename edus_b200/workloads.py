@@ -165,7 +165,7 @@ def write_wannier_tb(path, nw=8, nside=11, seed=12345, a_ang=2.5, decay_h=1.5, d
 
 
 def wannier(workdir, nw=8, nside=11, n=96, field=0.4, photon=0.3, duration=40.0, dt_fs=0.01, t_fin_fs=None, it_res=10,
-            seed=12345, name="W8", phase=0.0, write_model=True):
+            seed=12345, name="W8", phase=0.0, write_model=True, pol="0 0 1"):
     os.makedirs(workdir, exist_ok=True)
     if write_model or not os.path.exists(os.path.join(workdir, f"{name}_tb.dat")):
         write_wannier_tb(os.path.join(workdir, f"{name}_tb.dat"), nw=nw, nside=nside, seed=seed)
@@ -180,7 +180,7 @@ def wannier(workdir, nw=8, nside=11, n=96, field=0.4, photon=0.3, duration=40.0,
         f"t_fin {t_fin} fs\n"
         "}\n\n"
         f"nkpt{{\n1 {n} {n}\n}}\n\n"
-        + _pump(photon, field, duration, phase=phase)
+        + _pump(photon, field, duration, pol=pol, phase=phase)
         + "\nobservables{\nCurrent\n"
         f"it_resolution {it_res}\n"
         "}\n"

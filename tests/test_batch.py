@@ -63,6 +63,8 @@ def test_fp64_batch_matches_single_solves(workdir):
         assert len(lb) == len(log)
         assert all(x["t"] == y["t"] for x, y in zip(lb, log))
         assert rel(J1(lb), J1(log)) < 1e-11
+        J2b, J2s = np.array([x["J2"] for x in lb]), np.array([x["J2"] for x in log])
+        assert rel(J2b, J2s) < 1e-10
         pg, po = np.array([x["pop"] for x in lb]), np.array([x["pop"] for x in log])
         assert np.abs(pg - po).max() < 1e-14
     st = b.stats()
@@ -220,3 +222,31 @@ def test_tensor_core_model_build(workdir, nw, nside, name):
         drain(b, [s], 8)
         assert np.abs(b.get_state(s) - rho64).max() < 1e-5
         assert rel(J1(b.obs(s)), j64) < 1e-5
+
+
+def test_staged_form_equals_element_parallel_form(workdir):
+    """Register profile 3 (operands staged with cp.async, one tile ahead) does
+    the arithmetic of profile 0 in the same order: the same state and
+    observables for 2-, 8- and 16-band instances, and a fallback to profile 0
+    for an instance whose field uses all three components."""
+    reqs = []
+    d = f"{workdir}/h"
+    hb = E.Problem(E.parse_input(W.hbn_rk4(d, n=20, t_fin_fs=0.5, it_res=3, field=0.4)), d).drop_decoupled_core()
+    reqs.append(hb)
+    d = f"{workdir}/w8"
+    reqs.append(E.Problem(E.parse_input(W.wannier(d, n=12, t_fin_fs=0.4, it_res=4)), d))
+    d = f"{workdir}/w16"
+    reqs.append(E.Problem(E.parse_input(W.wannier(d, nw=16, nside=13, n=10, t_fin_fs=0.2, it_res=5, name="W16")), d))
+    d = f"{workdir}/w8xyz"
+    reqs.append(E.Problem(E.parse_input(W.wannier(d, n=12, t_fin_fs=0.3, it_res=4, pol="0.3 0.5 0.8")), d))
+    out = {0: [], 3: []}
+    for prof in (0, 3):
+        # the three-component instance runs in a batch of its own: it sends its whole class to profile 0
+        for group in (reqs[:3], reqs[3:]):
+            b = E.Batch(precision=abi.EDUS_PREC_MIXED, chunk_steps=8, regs_profile={2: prof, 8: prof, 16: prof})
+            slots = [b.add(p) for p in group]
+            drain(b, slots, 8)
+            out[prof] += [(b.get_state(s), J1(b.obs(s))) for s in slots]
+    for (r0, j0), (r3, j3) in zip(out[0], out[3]):
+        assert np.array_equal(r0, r3)
+        assert np.array_equal(j0, j3)
