@@ -255,6 +255,21 @@ void select_terms(const Problem& P, const std::vector<FieldRow>& fr, Inst& I) {
   }
 }
 
+// A tile is interior when its k points lie in one grid row and every selected
+// stencil step stays inside the grid without wrapping: then k + b = k + d1 n2 + d2.
+int interior_tile(const Inst& I, int k0, int kt) {
+  if (!I.lattice) return 0;
+  const int k1 = std::min(k0 + kt, I.nk) - 1;
+  const int i1 = k0 / I.n2, i2a = k0 % I.n2, i2b = k1 % I.n2;
+  if (k1 / I.n2 != i1) return 0;
+  for (int c = 0; c < I.nsel; c++) {
+    const int b = I.bsel[c];
+    const int j1 = i1 + I.off[b][0];
+    if (j1 < 0 || j1 >= I.n1 || i2a + I.off[b][1] < 0 || i2b + I.off[b][1] >= I.n2) return 0;
+  }
+  return 1;
+}
+
 // The k-gradient neighbours of a Monkhorst-Pack grid are fixed lattice steps
 // with periodic wrap. Find the step of every b from k = 0 and keep the table
 // path unless every k agrees.
@@ -917,7 +932,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
         cudaMalloc(&c.d_cinst, b->slots.size() * sizeof(ClassInst)) != cudaSuccess)
       return undo(fail(EDUS_ENOMEM, "tile count"));
   }
-  for (int t = 0; t < s.ntiles; t++) c.tiles.push_back(Tile{q, t * kt, t, 0});
+  for (int t = 0; t < s.ntiles; t++) c.tiles.push_back(Tile{q, t * kt, t, interior_tile(I, t * kt, kt)});
   c.dirty = true;
   s.status = EDUS_INST_RUNNING;
   s.tick_admit = b->tick;

@@ -70,10 +70,10 @@ struct Inst {
 };
 
 struct Tile {
-  int inst;     // slot
-  int k0;       // first k point
-  int t_in;     // index of the tile within its instance
-  int pad;
+  int inst;      // slot
+  int k0;        // first k point
+  int t_in;      // index of the tile within its instance
+  int interior;  // lattice stencil: every k + b of the tile's k points is k + (d1 n2 + d2), no wrap
 };
 
 // One instance of a class for the observable kernel: its slot, its number of

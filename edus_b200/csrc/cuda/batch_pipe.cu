@@ -75,6 +75,7 @@ struct alignas(16) PipeMeta {
   const float2* DW[3][2];        // (D_x, W_x) of the field components in use
   double E[3][2];                // (pump, probe / 2) of the components in use
   int off[kBatchMaxNb][2];       // lattice steps of the stencil vectors in use
+  int delta[kBatchMaxNb];        // d1 n2 + d2: k + b on an interior tile
   float G[kBatchMaxNb];          // their w_b (E_pump . b), in FP32 as the commutator uses it
   double dt;
   int inst, pad;
@@ -190,13 +191,14 @@ __device__ __forceinline__ void pipe_meta(PipeMeta& M, const View& v, int inst, 
     M.G[lane] = (float)(I->wb[b] * (Es[0] * I->bvec[b][0] + Es[1] * I->bvec[b][1] + Es[2] * I->bvec[b][2]));
     M.off[lane][0] = I->off[b][0];
     M.off[lane][1] = I->off[b][1];
+    M.delta[lane] = I->off[b][0] * I->n2 + I->off[b][1];
   }
 }
 
 // Copies of this thread's operands of tile k0 (element e, k = k0 + kl).
 template <int N, int KT, int STAGE>
-__device__ __forceinline__ void pipe_issue(const PipeCarve<N, KT>& S, const PipeMeta& M, int k0, int tid, int kl, int e, int i,
-                                           int j) {
+__device__ __forceinline__ void pipe_issue(const PipeCarve<N, KT>& S, const PipeMeta& M, int k0, bool interior, int tid, int kl,
+                                           int e, int i, int j) {
   constexpr int NTHR = PipeCarve<N, KT>::NTHR;
   const int4 a = ldv<int4>(&M.active);  // active, nk, on, nsel
   const int k = k0 + kl, nk = a.y;
@@ -219,7 +221,16 @@ __device__ __forceinline__ void pipe_issue(const PipeCarve<N, KT>& S, const Pipe
     cp_async8(&S.sW[c * NTHR + tid], (const float2*)dw.y + o);
   }
   if (i == j) cp_async8(&S.sHii[tid], M.Hdiag + i * nk + k);
-  if (a.z) {
+  if (a.z && interior) {
+    const float2* at = src + o;
+    for (int c = 0; c < a.w; c += 4) {
+      const int4 d = ldv<int4>(&M.delta[c]);
+      cp_async8(&S.sG[c * NTHR + tid], at + d.x);
+      if (c + 1 < a.w) cp_async8(&S.sG[(c + 1) * NTHR + tid], at + d.y);
+      if (c + 2 < a.w) cp_async8(&S.sG[(c + 2) * NTHR + tid], at + d.z);
+      if (c + 3 < a.w) cp_async8(&S.sG[(c + 3) * NTHR + tid], at + d.w);
+    }
+  } else if (a.z) {
     const int n1 = b.y, n2 = b.z;
     const int i1 = k / n2, i2 = k - i1 * n2;
     const float2* row = src + e * nk;
@@ -260,7 +271,7 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
   int ms = 0;
   if (warp == 0) pipe_meta<N, STAGE>(S.meta[0], v, cur.inst, parity, lane);
   __syncthreads();
-  pipe_issue<N, KT, STAGE>(S, S.meta[0], cur.k0, tid, kl, e, i, j);
+  pipe_issue<N, KT, STAGE>(S, S.meta[0], cur.k0, cur.interior, tid, kl, e, i, j);
   cp_async_commit();
   Tile nxt = t0 + 1 < t1 ? v.tiles[t0 + 1] : cur;
 
@@ -321,7 +332,7 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
     __syncthreads();
     // ---- copies of the next tile, in flight during this tile's commutator
     if (more) {
-      pipe_issue<N, KT, STAGE>(S, S.meta[msn], nxt.k0, tid, kl, e, i, j);
+      pipe_issue<N, KT, STAGE>(S, S.meta[msn], nxt.k0, nxt.interior, tid, kl, e, i, j);
       cp_async_commit();
     }
     const Tile after = t + 2 < t1 ? v.tiles[t + 2] : nxt;
