@@ -20,14 +20,15 @@ from edus_b200 import abi
 from edus_b200 import workloads as W
 
 # built variants per band count: (tile length, register profile); profile 2
-# is the matrix-product form (FP64), profile 3 the staged form (mixed)
+# is the matrix-product form (FP64), profiles 3 and 4 the staged forms
+# (mixed; 4 with the register-blocked commutator)
 VARIANTS = {
     2: [(16, 0), (16, 1), (32, 0), (32, 1), (32, 3)],
     3: [(16, 0), (16, 1), (32, 0), (32, 1), (32, 3)],
     4: [(16, 0), (16, 1), (16, 3)],
     5: [(16, 0), (16, 1), (16, 3)],
-    8: [(4, 0), (8, 0), (8, 1), (8, 2), (16, 2), (8, 3)],
-    16: [(2, 0), (2, 1), (2, 2), (4, 2), (8, 2), (2, 3)],
+    8: [(4, 0), (8, 0), (8, 1), (8, 2), (16, 2), (8, 3), (8, 4), (16, 4)],
+    16: [(2, 0), (2, 1), (2, 2), (4, 2), (8, 2), (2, 3), (2, 4), (4, 4)],
 }
 PREC = {"fp64": abi.EDUS_PREC_FP64, "mixed": abi.EDUS_PREC_MIXED}
 
@@ -110,8 +111,8 @@ def tune(bands=(2, 3, 8, 16), precisions=("fp64", "mixed"), grid=96, steps=96, v
             for kt, prof in VARIANTS[nb]:
                 if prof == 2 and pn == "mixed":
                     continue  # the matrix-product form is built for FP64 only
-                if prof == 3 and pn == "fp64":
-                    continue  # the staged form is built for mixed precision only
+                if prof >= 3 and pn == "fp64":
+                    continue  # the staged forms are built for mixed precision only
                 if nb == 3 and pn == "mixed":
                     continue  # mixed instances carry no core band: 3-band hBN runs as 2 bands
                 t0 = time.perf_counter()

@@ -135,17 +135,17 @@ Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
 int profile_of(const edus_batch* b, int n) {
   const int p = (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.regs_profile[n] : 0;
   if (p == 2 && b->mixed) return 0;
-  if (p == 3 && !b->mixed) return 0;  // asynchronous staging is built for mixed precision
+  if (p >= 3 && !b->mixed) return 0;  // asynchronous staging is built for mixed precision
   return p;
 }
 
-// Kernel form a class runs: profile 3 needs every running instance of the
-// class on a lattice stencil, otherwise the element-parallel form. Also the
-// staging sizes of profile 3 (at least one slot each).
+// Kernel form a class runs: profiles 3 and 4 need every running instance of
+// the class on a lattice stencil, otherwise the element-parallel form. Also
+// the staging sizes of profiles 3 and 4 (at least one slot each).
 int form_of(const edus_batch* b, const ClassTab& c, int& psel, int& pcomp) {
   psel = pcomp = 1;
-  if (c.occ != 3) return c.occ;
-  if (!pipe_supported(c.n, c.kt)) return 0;
+  if (c.occ != 3 && c.occ != 4) return c.occ;
+  if (!pipe_supported(c.n, c.kt, c.occ == 4)) return 0;
   for (const Slot& s : b->slots) {
     if (s.status != EDUS_INST_RUNNING || s.n != c.n) continue;
     const Inst& I = s.inst;
@@ -153,20 +153,24 @@ int form_of(const edus_batch* b, const ClassTab& c, int& psel, int& pcomp) {
     psel = std::max(psel, I.nsel);
     pcomp = std::max(pcomp, ((I.fmask >> 0) & 1) + ((I.fmask >> 1) & 1) + ((I.fmask >> 2) & 1));
   }
-  return 3;
+  return c.occ;
 }
 
 int grid_of(const edus_batch* b, const ClassTab& c) {
   switch (c.form) {
     case 2: return stage_grid_mm(c.n, c.kt, b->mixed);
-    case 3: return stage_grid_pipe(c.n, c.kt, c.psel, c.pcomp);
+    case 3:
+    case 4: return stage_grid_pipe(c.n, c.kt, c.form == 4, c.psel, c.pcomp);
     default: return stage_grid(c.n, c.kt, c.form ? 1 : 0, b->mixed);
   }
 }
 
 int check_problem(const edus_batch* b, const Problem& P) {
   const int n = P.ncv;
-  const bool ok = profile_of(b, n) == 2 ? mm_supported(n, tile_len(b, n)) : class_supported(n, tile_len(b, n));
+  const int prof = profile_of(b, n), kt = tile_len(b, n);
+  // the staged forms also run tile lengths the element-parallel form is not built for
+  // (their instances must then be on a lattice stencil, checked at admission)
+  const bool ok = prof == 2 ? mm_supported(n, kt) : (class_supported(n, kt) || (prof >= 3 && pipe_supported(n, kt, prof == 4)));
   if (!ok)
     return fail(EDUS_EUNSUPPORTED, "batch: %d bands with %d k points per tile (profile %d) is not built", n, tile_len(b, n),
                 profile_of(b, n));
@@ -611,8 +615,8 @@ int record_chunk(edus_batch* b) {
       for (auto& kv : b->classes) {
         ClassTab& c = kv.second;
         View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles, c.d_cinst, c.d_ntiles + 1};
-        if (c.form == 3)
-          BCK(launch_stage_pipe(c.n, c.kt, v, st, parity, c.psel, c.pcomp, c.sgrid, b->stream));
+        if (c.form == 3 || c.form == 4)
+          BCK(launch_stage_pipe(c.n, c.kt, c.form == 4, v, st, parity, c.psel, c.pcomp, c.sgrid, b->stream));
         else if (c.form == 2)
           BCK(launch_stage_mm(c.n, c.kt, b->mixed, v, st, parity, c.sgrid, b->stream));
         else
@@ -861,6 +865,8 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
     for (int x = 0; x < 3; x++) I.bvec[bb][x] = P.bvec[bb * 3 + x];
   }
   detect_lattice(P, I);
+  if (!I.lattice && !class_supported(n, kt))
+    return fail(EDUS_EUNSUPPORTED, "batch: %d k points per tile needs a lattice stencil for %d bands", kt, n);
   auto undo = [&](int code) {
     free_slot_mem(b, s);
     return code;

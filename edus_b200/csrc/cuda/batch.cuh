@@ -108,13 +108,16 @@ bool class_supported(int N, int kt);
 bool mm_supported(int N, int kt);
 cudaError_t launch_stage_mm(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
 int stage_grid_mm(int N, int kt, bool mixed);
-// Mixed-precision stage kernel with asynchronous staging (batch_pipe.cu),
-// register profile 3, for lattice-stencil instances: classes it is built for,
-// launch and persistent grid; nsel / ncomp are the most stencil vectors and
-// field components in use by an instance of the class (they size the staging).
-bool pipe_supported(int N, int kt);
-cudaError_t launch_stage_pipe(int N, int kt, const View& v, int stage, int parity, int nsel, int ncomp, int grid, cudaStream_t s);
-int stage_grid_pipe(int N, int kt, int nsel, int ncomp);
+// Mixed-precision stage kernel with asynchronous staging (batch_pipe.cu) for
+// lattice-stencil instances: register profile 3 (element-parallel
+// commutator, cb = 0) and 4 (commutator from register blocks of C = P H~^T,
+// cb = 1). Classes it is built for, launch and persistent grid; nsel / ncomp
+// are the most stencil vectors and field components in use by an instance of
+// the class (they size the staging).
+bool pipe_supported(int N, int kt, int cb);
+cudaError_t launch_stage_pipe(int N, int kt, int cb, const View& v, int stage, int parity, int nsel, int ncomp, int grid,
+                              cudaStream_t s);
+int stage_grid_pipe(int N, int kt, int cb, int nsel, int ncomp);
 size_t obs_part_bytes();
 // k points per observable unit (one partial per unit; the partials are sized per tile)
 int obs_unit(int N);

@@ -74,6 +74,7 @@ struct alignas(16) PipeMeta {
   float2* dst;                   // FP32 stage input written: stage 0 Pa, 1 Pb, 2 Pa, 3 Pb
   const float2* DW[3][2];        // (D_x, W_x) of the field components in use
   double E[3][2];                // (pump, probe / 2) of the components in use
+  float Ef[3][4];                // the same in FP32 (pump, probe / 2, -, -) as the commutator uses them
   int off[kBatchMaxNb][2];       // lattice steps of the stencil vectors in use
   int delta[kBatchMaxNb];        // d1 n2 + d2: k + b on an interior tile
   float G[kBatchMaxNb];          // their w_b (E_pump . b), in FP32 as the commutator uses it
@@ -102,13 +103,14 @@ struct PipeCarve {
   double* sHii;
   float2 *sPin, *sH, *sD, *sW, *sG;  // sD, sW: [ncomp][NTHR]; sG: [nsel][NTHR]
   float2 *xP, *xH;                    // [2][SIZE]
+  float2* xC;                         // blocked commutator only: C = P H~^T [SIZE]
   double* xEd;                        // [2][N * KT]
   PipeMeta* meta;                     // [3]
-  static __host__ __device__ size_t bytes(int nsel, int ncomp) {
-    return (size_t)NTHR * (16 + 16 + 8 + 8 + 8 + 16 * ncomp + 8 * nsel) + 2 * 2 * PipeRows<N, KT>::SIZE * sizeof(float2) +
+  static __host__ __device__ size_t bytes(int nsel, int ncomp, int cb) {
+    return (size_t)NTHR * (16 + 16 + 8 + 8 + 8 + 16 * ncomp + 8 * nsel) + (4 + (cb ? 1 : 0)) * PipeRows<N, KT>::SIZE * sizeof(float2) +
            2 * N * KT * sizeof(double) + 3 * sizeof(PipeMeta);
   }
-  __device__ PipeCarve(unsigned char* base, int nsel, int ncomp) {
+  __device__ PipeCarve(unsigned char* base, int nsel, int ncomp, int cb) {
     unsigned char* p = base;
     auto take = [&](size_t b) {
       unsigned char* r = p;
@@ -125,6 +127,7 @@ struct PipeCarve {
     sG = (float2*)take((size_t)NTHR * 8 * nsel);
     xP = (float2*)take(2 * PipeRows<N, KT>::SIZE * sizeof(float2));
     xH = (float2*)take(2 * PipeRows<N, KT>::SIZE * sizeof(float2));
+    xC = (float2*)take(cb ? PipeRows<N, KT>::SIZE * sizeof(float2) : 0);
     xEd = (double*)take(2 * N * KT * sizeof(double));
     meta = (PipeMeta*)take(3 * sizeof(PipeMeta));
   }
@@ -184,6 +187,8 @@ __device__ __forceinline__ void pipe_meta(PipeMeta& M, const View& v, int inst, 
       M.DW[c][1] = reinterpret_cast<const float2*>(I->W) + x * plane;
       M.E[c][0] = Es[x];
       M.E[c][1] = Es[3 + x];
+      M.Ef[c][0] = (float)Es[x];
+      M.Ef[c][1] = (float)Es[3 + x];
     }
   }
   if (lane < I->nsel) {
@@ -248,7 +253,15 @@ __device__ __forceinline__ void pipe_issue(const PipeCarve<N, KT>& S, const Pipe
   }
 }
 
-template <int N, int KT, int STAGE>
+// Register blocks of the blocked commutator (C = P H~^T, BR x BC entries of C
+// per thread and k point): 2 x 2 for 8 bands, 4 x 2 for 16.
+template <int N>
+struct CBlk {
+  static constexpr int BR = N >= 16 ? 4 : 2, BC = 2;
+  static constexpr int NB = (N / BR) * (N / BC);
+};
+
+template <int N, int KT, int STAGE, int CB>
 __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad32(KT * TriP<N>::NT)) > 0 ? 1152 / pipe_pad32(KT * TriP<N>::NT) : 1)
     k_bpipe(View v, int parity, int nsel_max, int ncomp_max) {
   constexpr int NT = TriP<N>::NT;
@@ -256,7 +269,7 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
   constexpr int SIZE = PipeRows<N, KT>::SIZE;
   constexpr int NTHR = PipeCarve<N, KT>::NTHR;
   extern __shared__ __align__(16) unsigned char pipe_smem[];
-  const PipeCarve<N, KT> S(pipe_smem, nsel_max, ncomp_max);
+  const PipeCarve<N, KT> S(pipe_smem, nsel_max, ncomp_max, CB);
   const int tid = threadIdx.x, lane = tid % 32, warp = tid / 32;
   const int kl = tid % KT, e = tid / KT;
   const bool lane_ok = e < NT;
@@ -288,7 +301,9 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
     double2 Pe = cz(), p1v = cz(), p0v = cz();
     float2 G = fmk(0.f, 0.f);
     if (valid) {
-      Pe = STAGE == 0 ? S.sP0[tid] : to_d(S.sPin[tid]);
+      // stages 1-3: the FP32 stage input feeds the exchange rows as it is
+      const float2 pin = S.sPin[tid];
+      Pe = STAGE == 0 ? S.sP0[tid] : to_d(pin);
       if (STAGE >= 1) p1v = S.sP1[tid];
       if (STAGE == 1 || STAGE == 2) p0v = S.sP0[tid];
       if (a.z)
@@ -301,7 +316,7 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
         }
       const int4 b = ldv<int4>(&M.nch);  // nch, n1, n2, ncomp
       const int oij = i * RS + j * KT + kl, oji = j * RS + i * KT + kl;
-      const float2 pc = to_f(Pe);
+      const float2 pc = STAGE == 0 ? to_f(Pe) : pin;
       xP[oij] = pc;
       xP[oji] = fconj(pc);
       const int w = (i < b.x) != (j < b.x);
@@ -309,18 +324,18 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
       float2 hu = h0, hl = fconj(h0);
       double ed = i == j ? S.sHii[tid] : 0.;
       for (int c = 0; c < b.w; c++) {
-        const double2 Ec = ldv<double2>(&M.E[c][0]);  // pump, probe / 2
+        const float2 ef = ldv<float2>(&M.Ef[c][0]);  // pump, probe / 2
         const float2 d = S.sD[c * NTHR + tid];
-        const float ew = (float)(w ? Ec.y : Ec.x);
+        const float ew = w ? ef.y : ef.x;
         hu = fadd(hu, fscale(d, ew));
         hl = fadd(hl, fscale(d, ew));
-        if (i == j) ed += (double)d.x * Ec.x;
+        if (i == j) ed += (double)d.x * M.E[c][0];
       }
       if (i == j) {
         xEd[i * KT + kl] = ed;
         hu = hl = fmk(0.f, 0.f);
       }
-      for (int c = 0; c < b.w; c++) G = fadd(G, fscale(S.sW[c * NTHR + tid], (float)M.E[c][0]));
+      for (int c = 0; c < b.w; c++) G = fadd(G, fscale(S.sW[c * NTHR + tid], M.Ef[c][0]));
       xH[oij] = hu;
       xH[oji] = hl;
     }
@@ -336,6 +351,43 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
       cp_async_commit();
     }
     const Tile after = t + 2 < t1 ? v.tiles[t + 2] : nxt;
+    if (CB) {
+      // C = P H~^T in register blocks: C_rc = sum_l P_rl H~_cl (rows of the
+      // exchange matrices), BR x BC entries per thread, then beta_ij = C_ij -
+      // conj(C_ji) below
+      constexpr int BR = CBlk<N>::BR, BC = CBlk<N>::BC, NBC = N / BC;
+      if (a.x && tid < KT * CBlk<N>::NB) {
+        const int kc = tid % KT, blk = tid / KT;
+        const int r0 = (blk / NBC) * BR, c0 = (blk % NBC) * BC;
+        float2 acc[BR][BC];
+#pragma unroll
+        for (int x = 0; x < BR; x++)
+#pragma unroll
+          for (int y = 0; y < BC; y++) acc[x][y] = fmk(0.f, 0.f);
+#pragma unroll
+        for (int l = 0; l < N; l++) {
+          float2 pr[BR], hc[BC];
+#pragma unroll
+          for (int x = 0; x < BR; x++) pr[x] = xP[(r0 + x) * RS + l * KT + kc];
+#pragma unroll
+          for (int y = 0; y < BC; y++) hc[y] = xH[(c0 + y) * RS + l * KT + kc];
+#pragma unroll
+          for (int x = 0; x < BR; x++)
+#pragma unroll
+            for (int y = 0; y < BC; y++) {
+              acc[x][y].x = fmaf(pr[x].x, hc[y].x, acc[x][y].x);
+              acc[x][y].x = fmaf(-pr[x].y, hc[y].y, acc[x][y].x);
+              acc[x][y].y = fmaf(pr[x].x, hc[y].y, acc[x][y].y);
+              acc[x][y].y = fmaf(pr[x].y, hc[y].x, acc[x][y].y);
+            }
+        }
+#pragma unroll
+        for (int x = 0; x < BR; x++)
+#pragma unroll
+          for (int y = 0; y < BC; y++) S.xC[(r0 + x) * RS + (c0 + y) * KT + kc] = acc[x][y];
+      }
+      __syncthreads();
+    }
     if (valid) {
       // -i[H~, rho - rho_eq] in the reference's transposed convention
       // (headers/RungeKutta.h:158-208), as k_bstage
@@ -346,7 +398,7 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
       // sum_l H~_jl P_il - conj(H~_il P_jl) in eight partial sums, as k_bstage
       float ax[2] = {0.f, 0.f}, ay[2] = {0.f, 0.f}, bx[2] = {0.f, 0.f}, by[2] = {0.f, 0.f};
 #pragma unroll
-      for (int l = 0; l < N; l++) {
+      for (int l = 0; l < (CB ? 0 : N); l++) {
         const int q = l & 1;
         const float2 hj = Hj[l * KT], pi = Pi[l * KT], hi = Hi[l * KT], pj = Pj[l * KT];
         ax[q] = fmaf(hj.x, pi.x, ax[q]);
@@ -358,7 +410,11 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
         by[q] = fmaf(hi.x, pj.y, by[q]);
         by[q] = fmaf(hi.y, pj.x, by[q]);
       }
-      const float2 beta = fmk((ax[0] + ax[1]) - (bx[0] + bx[1]), (ay[0] + ay[1]) + (by[0] + by[1]));
+      float2 beta = fmk((ax[0] + ax[1]) - (bx[0] + bx[1]), (ay[0] + ay[1]) + (by[0] + by[1]));
+      if (CB) {
+        const float2 cij = S.xC[i * RS + j * KT + kl], cji = S.xC[j * RS + i * KT + kl];
+        beta = fmk(cij.x - cji.x, cij.y + cji.y);
+      }
       float2 vv = fmi(beta);
       vv = fadd(vv, G);
       double2 d = to_d(vv);
@@ -393,65 +449,85 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
 
 // (the dynamic shared-memory limit of the four kernels is raised by
 // stage_grid_pipe on the batch's device before the first launch)
-template <int N, int KT, int STAGE>
+template <int N, int KT, int STAGE, int CB>
 cudaError_t pipe_launch(const View& v, int parity, int nsel, int ncomp, int grid, cudaStream_t s) {
   constexpr int NTHR = PipeCarve<N, KT>::NTHR;
-  k_bpipe<N, KT, STAGE><<<grid, NTHR, PipeCarve<N, KT>::bytes(nsel, ncomp), s>>>(v, parity, nsel, ncomp);
+  k_bpipe<N, KT, STAGE, CB><<<grid, NTHR, PipeCarve<N, KT>::bytes(nsel, ncomp, CB), s>>>(v, parity, nsel, ncomp);
   return cudaGetLastError();
 }
 
-template <int N, int KT>
+template <int N, int KT, int CB>
 cudaError_t pipe_stage(const View& v, int stage, int parity, int nsel, int ncomp, int grid, cudaStream_t s) {
   switch (stage) {
-    case 0: return pipe_launch<N, KT, 0>(v, parity, nsel, ncomp, grid, s);
-    case 1: return pipe_launch<N, KT, 1>(v, parity, nsel, ncomp, grid, s);
-    case 2: return pipe_launch<N, KT, 2>(v, parity, nsel, ncomp, grid, s);
-    default: return pipe_launch<N, KT, 3>(v, parity, nsel, ncomp, grid, s);
+    case 0: return pipe_launch<N, KT, 0, CB>(v, parity, nsel, ncomp, grid, s);
+    case 1: return pipe_launch<N, KT, 1, CB>(v, parity, nsel, ncomp, grid, s);
+    case 2: return pipe_launch<N, KT, 2, CB>(v, parity, nsel, ncomp, grid, s);
+    default: return pipe_launch<N, KT, 3, CB>(v, parity, nsel, ncomp, grid, s);
   }
 }
 
-template <int N, int KT>
+template <int N, int KT, int CB>
 int pipe_grid_n(int nsel, int ncomp) {
   constexpr int NTHR = PipeCarve<N, KT>::NTHR;
-  const size_t smem = PipeCarve<N, KT>::bytes(nsel, ncomp);
+  const size_t smem = PipeCarve<N, KT>::bytes(nsel, ncomp, CB);
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaFuncSetAttribute(k_bpipe<N, KT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-      cudaFuncSetAttribute(k_bpipe<N, KT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-      cudaFuncSetAttribute(k_bpipe<N, KT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-      cudaFuncSetAttribute(k_bpipe<N, KT, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_bpipe<N, KT, 0, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_bpipe<N, KT, 1, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_bpipe<N, KT, 2, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_bpipe<N, KT, 3, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return 0;
-
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bpipe<N, KT, 0>, NTHR, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bpipe<N, KT, 0, CB>, NTHR, smem) != cudaSuccess) return 0;
   return sms * per;
 }
 
 #define EDUS_PIPE_CLASSES(X) X(2, 32) X(3, 32) X(4, 16) X(5, 16) X(8, 8) X(16, 2)
+// classes with the blocked commutator (register profile 4)
+#define EDUS_PIPE_CB_CLASSES(X) X(8, 8) X(8, 16) X(16, 2) X(16, 4)
 
 }  // namespace
 
-bool pipe_supported(int N, int kt) {
+bool pipe_supported(int N, int kt, int cb) {
 #define X(n, k) \
   if (N == n && kt == k) return true;
-  EDUS_PIPE_CLASSES(X)
+  if (cb) {
+    EDUS_PIPE_CB_CLASSES(X)
+  } else {
+    EDUS_PIPE_CLASSES(X)
+  }
 #undef X
   return false;
 }
 
-cudaError_t launch_stage_pipe(int N, int kt, const View& v, int stage, int parity, int nsel, int ncomp, int grid, cudaStream_t s) {
+cudaError_t launch_stage_pipe(int N, int kt, int cb, const View& v, int stage, int parity, int nsel, int ncomp, int grid,
+                              cudaStream_t s) {
 #define X(n, k) \
-  if (N == n && kt == k) return pipe_stage<n, k>(v, stage, parity, nsel, ncomp, grid, s);
-  EDUS_PIPE_CLASSES(X)
+  if (N == n && kt == k) return pipe_stage<n, k, 0>(v, stage, parity, nsel, ncomp, grid, s);
+#define Y(n, k) \
+  if (N == n && kt == k) return pipe_stage<n, k, 1>(v, stage, parity, nsel, ncomp, grid, s);
+  if (cb) {
+    EDUS_PIPE_CB_CLASSES(Y)
+  } else {
+    EDUS_PIPE_CLASSES(X)
+  }
 #undef X
+#undef Y
   return cudaErrorInvalidValue;
 }
 
-int stage_grid_pipe(int N, int kt, int nsel, int ncomp) {
+int stage_grid_pipe(int N, int kt, int cb, int nsel, int ncomp) {
 #define X(n, k) \
-  if (N == n && kt == k) return pipe_grid_n<n, k>(nsel, ncomp);
-  EDUS_PIPE_CLASSES(X)
+  if (N == n && kt == k) return pipe_grid_n<n, k, 0>(nsel, ncomp);
+#define Y(n, k) \
+  if (N == n && kt == k) return pipe_grid_n<n, k, 1>(nsel, ncomp);
+  if (cb) {
+    EDUS_PIPE_CB_CLASSES(Y)
+  } else {
+    EDUS_PIPE_CLASSES(X)
+  }
 #undef X
+#undef Y
   return 0;
 }
 

@@ -250,3 +250,21 @@ def test_staged_form_equals_element_parallel_form(workdir):
     for (r0, j0), (r3, j3) in zip(out[0], out[3]):
         assert np.array_equal(r0, r3)
         assert np.array_equal(j0, j3)
+
+
+@pytest.mark.parametrize("nw,nside,name,kt", [(8, 11, "W8", 8), (8, 11, "W8", 16), (16, 13, "W16", 2), (16, 13, "W16", 4)])
+def test_blocked_commutator_form(workdir, nw, nside, name, kt):
+    """Register profile 4 (commutator from register blocks of C = P H~^T), also
+    with tiles the element-parallel form is not built for, against profile 3:
+    the same dynamics to FP32 rounding."""
+    d = f"{workdir}/{name}"
+    p = E.parse_input(W.wannier(d, nw=nw, nside=nside, n=12, t_fin_fs=0.4, it_res=4, name=name))
+    out = {}
+    for prof in (3, 4):
+        b = E.Batch(precision=abi.EDUS_PREC_MIXED, chunk_steps=8, regs_profile={nw: prof},
+                    tile_k={nw: kt if prof == 4 else (8 if nw == 8 else 2)})
+        s = b.add(E.Problem(p, d))
+        drain(b, [s], 8)
+        out[prof] = (b.get_state(s), J1(b.obs(s)))
+    assert np.abs(out[4][0] - out[3][0]).max() < 1e-6
+    assert rel(out[4][1], out[3][1]) < 1e-6
