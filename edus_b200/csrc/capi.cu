@@ -739,8 +739,8 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   c->ntri = nt;
   c->nk = nk;
   c->plane = (size_t)nt * nk;
-  if (n != 1 && n != 2 && n != 3 && n != 4 && n != 5 && n != 8)
-    return bail(fail(EDUS_EUNSUPPORTED, "band count %d has no FP64 kernel instance (1-5, 8)", n));
+  if (n != 1 && n != 2 && n != 3 && n != 4 && n != 5 && n != 8 && n != 16)
+    return bail(fail(EDUS_EUNSUPPORTED, "band count %d has no FP64 kernel instance (1-5, 8, 16)", n));
   if (P.nnb > kMaxNb) return bail(fail(EDUS_EUNSUPPORTED, "stencil with %d neighbours (max %d)", P.nnb, kMaxNb));
   c->solver = P.p.solver;
   c->order = P.p.solver == EDUS_SOLVER_RK4 ? 0 : P.p.order;

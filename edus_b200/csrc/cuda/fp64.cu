@@ -456,6 +456,7 @@ cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const 
     case 4: return launch_obs_n<4>(tb, cst, a, s);
     case 5: return launch_obs_n<5>(tb, cst, a, s);
     case 8: return launch_obs_n<8>(tb, cst, a, s);
+    case 16: return launch_obs_n<16>(tb, cst, a, s);
     default: return cudaErrorInvalidValue;
   }
 }

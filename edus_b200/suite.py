@@ -12,7 +12,8 @@ one GPU; inputs are synthetic (edus_b200.workloads).
                 sample of the same instances.
   serve_line    Poisson stream of requests (2, 8 or 16 bands, grids 32^2-192^2,
                 10-100 fs) through the served engine (continuous batching),
-                against the FP64 path run request by request on a sample.
+                against the plain FP64 single-solve path run request by request
+                on the first requests of the stream.
 
 The error of the mixed path is the relative L2 norm over t of J1(t) against
 the FP64 single-solve path (which matches the reference's CPU output to 1e-12).
@@ -168,7 +169,7 @@ def serve_requests(count, seed=7, nmin=32, nmax=192, dmin=10.0, dmax=100.0):
     return out
 
 
-def serve_line(count=2000, rate=None, fp64_sample=6, seed=7, max_s=None, **kw):
+def serve_line(count=2000, rate=None, fp64_sample=9, seed=7, max_s=None, **kw):
     D = _Dirs()
     specs = serve_requests(count, seed=seed, **kw)
     reqs = [(E.parse_input(p), d) for p, d in (D.instance(s, i) for i, s in enumerate(specs))]
@@ -190,21 +191,17 @@ def serve_line(count=2000, rate=None, fp64_sample=6, seed=7, max_s=None, **kw):
     for q in range(min(fp64_sample, count)):
         logs[q] = s.obs(ids[q])
     s.close()
-    # FP64, request by request (one request on the GPU at a time), on the first requests
+    # plain FP64 single-solve path, request by request (one request on the GPU at
+    # a time), on the first requests of the stream
     units = secs = 0.0
     lat = []
     errs = []
     for q in range(min(fp64_sample, count)):
-        f = E.Server(precision=abi.EDUS_PREC_FP64)
-        t0 = f.clock()
-        rid = f.submit(*reqs[q])
-        f.drain(3600)
-        info = f.info(rid)
-        ref = f.obs(rid)
-        f.close()
-        lat.append(info["t_done"] - t0)
-        units += info["nk"] * info["steps"]
-        secs += info["t_done"] - t0
+        path, d = D.instance(specs[q], q)
+        u, sec, ref = _single_fp64(path, d)
+        lat.append(sec)
+        units += u
+        secs += sec
         errs.append(_rel(_J1(logs[q]), _J1(ref)))
     fp64_rate = units / secs
     return {

@@ -268,3 +268,15 @@ def test_blocked_commutator_form(workdir, nw, nside, name, kt):
         out[prof] = (b.get_state(s), J1(b.obs(s)))
     assert np.abs(out[4][0] - out[3][0]).max() < 1e-6
     assert rel(out[4][1], out[3][1]) < 1e-6
+
+
+def test_16_band_single_solve_matches_batch(workdir):
+    """The single-solve FP64 path for 16 bands against the FP64 batch engine."""
+    d = f"{workdir}/w16s"
+    pb = E.Problem(E.parse_input(W.wannier(d, nw=16, nside=13, n=10, t_fin_fs=0.2, it_res=5, name="W16")), d)
+    rho, log = single(pb)
+    b = E.Batch(precision=abi.EDUS_PREC_FP64, chunk_steps=8)
+    s = b.add(pb)
+    drain(b, [s], 8)
+    assert np.abs(b.get_state(s) - rho).max() < 1e-13
+    assert rel(J1(b.obs(s)), J1(log)) < 1e-11
