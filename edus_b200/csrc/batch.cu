@@ -311,16 +311,6 @@ void detect_lattice(const Problem& P, Inst& I) {
   I.lattice = 1;
 }
 
-float tf32_round_host(float x) {
-  uint32_t u;
-  memcpy(&u, &x, 4);
-  u += 0x0FFFu + ((u >> 13) & 1u);
-  u &= 0xFFFFE000u;
-  float r;
-  memcpy(&r, &u, 4);
-  return r;
-}
-
 // Mixed precision: H(k), D(k) on the tensor cores (cuda/tc_contract.cu, split
 // TF32), band energies in FP64, then the eigensolve and dH/dk on the FP64 matrix
 // the dynamics uses.
@@ -329,31 +319,30 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
   // H and D on the tensor cores; dH/dk, an observable-only table whose k sums
   // cancel strongly, is the reference's stencil over an FP64 H(k) (CUDA cores)
   const int ncomp = 4;
-  const int kp = tc_pad_k(nr), ncols = 2 * ncomp * nt, K = 2 * nr;
+  const int kp = tc_pad_k(nr), kseg = tc_seg_k(nr), ncols = 2 * ncomp * nt, K = 2 * nr;
   std::vector<float> Bw((size_t)ncols * kp, 0.f);
+  std::vector<double> col(K);
   for (int i = 0; i < n; i++)
     for (int j = i; j < n; j++) {
       const int e = tri_index(i, j, n);
       for (int comp = 0; comp < ncomp; comp++) {
         const int ce = comp * nt + e;
-        for (int r = 0; r < nr; r++) {
-          const cd h = P.HR[((size_t)i * n + j) * nr + r];
-          const cd c = comp == 0 ? h
-                                 : 0.5 * (P.rR[(((size_t)(comp - 1) * n + i) * n + j) * nr + r] +
-                                          P.rR[(((size_t)(comp - 1) * n + j) * n + i) * nr + r]);
+        for (int part = 0; part < 2; part++) {
           // re column: [Re c ; -Im c], im column: [Im c ; Re c]
-          const float vals[2][2] = {{(float)c.real(), (float)-c.imag()}, {(float)c.imag(), (float)c.real()}};
-          for (int part = 0; part < 2; part++)
-            for (int hh = 0; hh < 2; hh++) {
-              const float x = vals[part][hh];
-              const float hi = tf32_round_host(x), lo = tf32_round_host(x - hi);
-              float* row = &Bw[(size_t)(2 * ce + part) * kp];
-              const int q = hh * nr + r;
-              row[q] = hi;          // pairs with A_hi
-              row[K + q] = lo;      // pairs with A_hi
-              row[2 * K + q] = hi;  // pairs with A_lo
-              row[3 * K + q] = lo;  // pairs with A_lo
-            }
+          double amax = 0.;
+          for (int r = 0; r < nr; r++) {
+            const cd c = comp == 0 ? P.HR[((size_t)i * n + j) * nr + r]
+                                   : 0.5 * (P.rR[(((size_t)(comp - 1) * n + i) * n + j) * nr + r] +
+                                            P.rR[(((size_t)(comp - 1) * n + j) * n + i) * nr + r]);
+            col[r] = part == 0 ? c.real() : c.imag();
+            col[nr + r] = part == 0 ? -c.imag() : c.real();
+            amax = std::max(amax, std::max(std::fabs(col[r]), std::fabs(col[nr + r])));
+          }
+          // power-of-two scale of the column: every y = value / scale in [-1, 1]
+          const double scale = amax > 0. ? std::ldexp(1.0, std::ilogb(amax) + 1) : 1.0;
+          float* row = &Bw[(size_t)(2 * ce + part) * kp];
+          for (int p = 0; p < kTcPairs; p++)
+            for (int q = 0; q < K; q++) row[(size_t)p * kseg + q] = (float)(scale * tc_slice(col[q] / scale, tc_pair_b(p)));
         }
       }
     }

@@ -1,21 +1,24 @@
 // tc_contract.cu — the Wannier Fourier sums H(k), D(k) on the tcgen05 tensor
-// cores (split TF32, FP32 accumulation) for mixed-precision batch instances.
+// cores (kind::tf32 with exact integer slices) for mixed-precision batch
+// instances.
 //
 // Real form of the complex sums: with A[k][.] = [cos(2 pi k.R_r) | sin(2 pi k.R_r)]
 // (K = 2 nr) and, per output element, the column pair
 //   re: [ Re c_r ; -Im c_r ],   im: [ Im c_r ; Re c_r ],
-// out = A . B^T gives Re / Im of sum_r e^{2 pi i k.R_r} c_r. The compensated
-// split x = x_hi + x_lo (both exactly TF32) enters as one GEMM of four times
-// the depth: A' = [A_hi | A_hi | A_lo | A_lo], B' = [B_hi | B_lo | B_hi | B_lo]
-// (per row), so A'.B'^T = (A_hi + A_lo)(B_hi + B_lo). Products of two TF32
-// values are exact in FP32; the tensor core sums each 32-deep slice in FP32 in
-// TMEM and the slices are added in FP64 registers.
+// out = A . B^T gives Re / Im of sum_r e^{2 pi i k.R_r} c_r. Both operands are
+// cut into 9-bit slices on a power-of-two scale (tc_contract.hpp): the GEMM
+// depth holds one segment of 2 nr (padded to 32) per slice pair (a, b) with
+// a + b <= 3. Within a 32-deep K slice every product is an integer times a
+// common power of two and at most 2^16, so the tensor core's FP32 sums are
+// exact; the slices are added in FP64 registers. The result is the FP64 sum to
+// about 2^-32 of the terms, so the FP32 tables stored from it equal those of
+// the FP64 CUDA-core build up to the last rounding.
 //
 // GEMM kernel: one CTA (4 warps) per 128 x 32 tile of C; per 32-deep slice of
 // K the block stages A and B in shared memory in the K-major canonical layout
 // without swizzle (16-byte rows of 4 TF32, 8-row core matrices 128 bytes
 // apart, the two 16-byte halves of one MMA's K = 8 slice one whole operand
-// apart), one elected thread issues four tcgen05.mma (M 128, N 128, K 8) and
+// apart), one elected thread issues four tcgen05.mma (M 128, N 32, K 8) and
 // commits them to an mbarrier that the block waits on (bounded) before the
 // next slice overwrites shared memory. The slice's accumulator (128 lanes x 32
 // FP32 columns of TMEM) is read back with tcgen05.ld.32x32b by each warp's lane
@@ -33,32 +36,22 @@ namespace {
 constexpr int TM = 128, TN = 32, TK = 32;  // CTA tile and K slice (TF32 elements)
 constexpr int kThreads = 128;
 constexpr uint32_t kTmemCols = 32;
-constexpr int kSplit = 4;                  // hi.hi + hi.lo + lo.hi + lo.lo
 
-// nearest TF32 (10 explicit mantissa bits) of a finite float
-__device__ __forceinline__ float tf32_round(float x) {
-  uint32_t u = __float_as_uint(x);
-  u += 0x0FFFu + ((u >> 13) & 1u);  // round half to even on the 13 dropped bits
-  u &= 0xFFFFE000u;
-  return __uint_as_float(u);
-}
-
-// A' rows: phases of k point m over the R vectors, [hi | hi | lo | lo].
-__global__ void k_phase_split(const double* __restrict__ kpt, const double* __restrict__ Rvec, int nk, int nr, int kpad,
-                              float* __restrict__ A) {
+// A' rows: phases of k point m over the R vectors; segment p holds slice
+// tc_pair_a(p) of [cos | sin], zero padded to the segment length.
+__global__ void k_phase_split(const double* __restrict__ kpt, const double* __restrict__ Rvec, int nk, int nr, int kseg,
+                              int kpad, float* __restrict__ A) {
   const int m = blockIdx.x;
   const int K = 2 * nr;
   for (int c = threadIdx.x; c < kpad; c += blockDim.x) {
     float v = 0.f;
-    if (m < nk && c < kSplit * K) {
-      const int part = c / K, q = c - part * K;  // parts 0, 1: hi; 2, 3: lo
+    const int p = c / kseg, q = c - p * kseg;
+    if (m < nk && q < K) {
       const int r = q < nr ? q : q - nr;
       const double kR = kpt[m * 3 + 0] * Rvec[r * 3 + 0] + kpt[m * 3 + 1] * Rvec[r * 3 + 1] + kpt[m * 3 + 2] * Rvec[r * 3 + 2];
-      double s, co;
-      sincospi(2.0 * kR, &s, &co);
-      const float x = (float)(q < nr ? co : s);
-      const float hi = tf32_round(x);
-      v = part < 2 ? hi : tf32_round(x - hi);
+      double sn, co;
+      sincospi(2.0 * kR, &sn, &co);
+      v = (float)tc_slice(q < nr ? co : sn, tc_pair_a(p));  // at most 9 significant bits: exact in TF32
     }
     A[(size_t)m * kpad + c] = v;
   }
@@ -217,12 +210,13 @@ __global__ void k_diag64(const double* __restrict__ kpt, const double* __restric
 
 size_t tc_gemm_smem() { return sizeof(float) * (TM + TN) * TK + 1024; }
 
-int tc_pad_k(int nr) { return ((2 * kSplit * nr + TK - 1) / TK) * TK; }
+int tc_seg_k(int nr) { return ((2 * nr + TK - 1) / TK) * TK; }
+int tc_pad_k(int nr) { return kTcPairs * tc_seg_k(nr); }
 
 cudaError_t tc_contract(const TcArgs& a, cudaStream_t s) {
   const int kpad = tc_pad_k(a.nr);
   const int ncols = 8 * a.ntri;
-  k_phase_split<<<a.nk, 256, 0, s>>>(a.kpt, a.Rvec, a.nk, a.nr, kpad, a.Aw);
+  k_phase_split<<<a.nk, 256, 0, s>>>(a.kpt, a.Rvec, a.nk, a.nr, tc_seg_k(a.nr), kpad, a.Aw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   // about 55 KB of shared memory per CTA keeps at most four CTAs, 512 TMEM columns, per SM

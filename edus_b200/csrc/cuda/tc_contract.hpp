@@ -12,9 +12,9 @@ struct TcArgs {
   int n, ntri, nk, nr;
   const double* kpt;     // [nk][3]
   const double* Rvec;    // [nr][3]
-  const float* Bw;       // [8 ntri][Kp] split coefficients [hi | lo | hi | lo] (host-built)
+  const float* Bw;       // [8 ntri][Kp] coefficient slices, one K segment per slice pair (host-built)
   const double2* hdiagR; // [n][nr] H_ii(R) for the FP64 band energies
-  float* Aw;             // scratch [nk][Kp] split phases
+  float* Aw;             // scratch [nk][Kp] phase slices, one K segment per slice pair
   double* Cw;            // scratch [nk][8 ntri] GEMM result (FP64 sum of FP32 slices)
   float2* H32;           // out [ntri][nk]
   float2* D32;           // out [3][ntri][nk]
@@ -23,7 +23,35 @@ struct TcArgs {
   int* err;              // device error word (bounded waits)
 };
 
-// K depth of the split GEMM (4 x 2 nr, padded to the K slice)
+// Exact-slice form of the contraction. Every operand y (a phase cos / sin, or
+// a coefficient divided by its column's power-of-two scale) lies in [-1, 1]
+// and is cut into kTcSlices slices of at most 9 significant bits, slice s a
+// multiple of 2^-(8 s + 8): y = sum_s slice_s(y) + O(2^-33). The GEMM runs one
+// K segment per slice pair (a, b) with a + b < kTcSlices; inside a 32-deep K
+// slice every product is an integer times one power of two, at most 2^16 in
+// magnitude, so the tensor core's FP32 sums of 32 of them are exact and the
+// FP64 sum of the slices is the contraction to about 2^-32 of its terms.
+constexpr int kTcSlices = 4;
+constexpr int kTcPairs = 10;  // (a, b) with a + b <= 3
+__host__ __device__ constexpr int tc_pair_a(int p) {
+  return p == 0 ? 0 : p == 1 ? 0 : p == 2 ? 1 : p == 3 ? 0 : p == 4 ? 1 : p == 5 ? 2 : p == 6 ? 0 : p == 7 ? 1 : p == 8 ? 2 : 3;
+}
+__host__ __device__ constexpr int tc_pair_b(int p) {
+  return p == 0 ? 0 : p == 1 ? 1 : p == 2 ? 0 : p == 3 ? 2 : p == 4 ? 1 : p == 5 ? 0 : p == 6 ? 3 : p == 7 ? 2 : p == 8 ? 1 : 0;
+}
+// slice s of y in [-1, 1] (FP64 arithmetic, exact at every step)
+__host__ __device__ inline double tc_slice(double y, int s) {
+  double r = y, v = 0.;
+  double scale = 256.;
+  for (int t = 0; t <= s; t++) {
+    v = rint(r * scale) / scale;
+    r -= v;
+    scale *= 256.;
+  }
+  return v;
+}
+// K segment length (2 nr padded to the 32-deep K slice) and the GEMM depth
+int tc_seg_k(int nr);
 int tc_pad_k(int nr);
 cudaError_t tc_contract(const TcArgs& a, cudaStream_t s);
 
