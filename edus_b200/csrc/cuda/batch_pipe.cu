@@ -354,11 +354,13 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
     if (CB) {
       // C = P H~^T in register blocks: C_rc = sum_l P_rl H~_cl (rows of the
       // exchange matrices), BR x BC entries per thread, then beta_ij = C_ij -
-      // conj(C_ji) below
-      constexpr int BR = CBlk<N>::BR, BC = CBlk<N>::BC, NBC = N / BC;
+      // conj(C_ji) below. Block (rb, cb) holds rows rb + x N/BR and columns
+      // cb + y N/BC, so the blocks of one warp read consecutive rows (the
+      // padded row stride puts them on different banks).
+      constexpr int BR = CBlk<N>::BR, BC = CBlk<N>::BC, NBC = N / BC, NBR = N / BR;
       if (a.x && tid < KT * CBlk<N>::NB) {
         const int kc = tid % KT, blk = tid / KT;
-        const int r0 = (blk / NBC) * BR, c0 = (blk % NBC) * BC;
+        const int r0 = blk / NBC, c0 = blk % NBC;
         float2 acc[BR][BC];
 #pragma unroll
         for (int x = 0; x < BR; x++)
@@ -368,9 +370,9 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
         for (int l = 0; l < N; l++) {
           float2 pr[BR], hc[BC];
 #pragma unroll
-          for (int x = 0; x < BR; x++) pr[x] = xP[(r0 + x) * RS + l * KT + kc];
+          for (int x = 0; x < BR; x++) pr[x] = xP[(r0 + x * NBR) * RS + l * KT + kc];
 #pragma unroll
-          for (int y = 0; y < BC; y++) hc[y] = xH[(c0 + y) * RS + l * KT + kc];
+          for (int y = 0; y < BC; y++) hc[y] = xH[(c0 + y * NBC) * RS + l * KT + kc];
 #pragma unroll
           for (int x = 0; x < BR; x++)
 #pragma unroll
@@ -384,7 +386,7 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
 #pragma unroll
         for (int x = 0; x < BR; x++)
 #pragma unroll
-          for (int y = 0; y < BC; y++) S.xC[(r0 + x) * RS + (c0 + y) * KT + kc] = acc[x][y];
+          for (int y = 0; y < BC; y++) S.xC[(r0 + x * NBR) * RS + (c0 + y * NBC) * KT + kc] = acc[x][y];
       }
       __syncthreads();
     }

@@ -38,22 +38,26 @@ constexpr int kThreads = 128;
 constexpr uint32_t kTmemCols = 32;
 
 // A' rows: phases of k point m over the R vectors; segment p holds slice
-// tc_pair_a(p) of [cos | sin], zero padded to the segment length.
+// tc_pair_a(p) of [cos | sin], zero padded to the segment length. One phase
+// is evaluated once and written to every segment.
 __global__ void k_phase_split(const double* __restrict__ kpt, const double* __restrict__ Rvec, int nk, int nr, int kseg,
                               int kpad, float* __restrict__ A) {
   const int m = blockIdx.x;
   const int K = 2 * nr;
-  for (int c = threadIdx.x; c < kpad; c += blockDim.x) {
-    float v = 0.f;
-    const int p = c / kseg, q = c - p * kseg;
+  float* row = A + (size_t)m * kpad;
+  for (int q = threadIdx.x; q < kseg; q += blockDim.x) {
+    float sl[kTcSlices] = {0.f, 0.f, 0.f, 0.f};
     if (m < nk && q < K) {
       const int r = q < nr ? q : q - nr;
       const double kR = kpt[m * 3 + 0] * Rvec[r * 3 + 0] + kpt[m * 3 + 1] * Rvec[r * 3 + 1] + kpt[m * 3 + 2] * Rvec[r * 3 + 2];
       double sn, co;
       sincospi(2.0 * kR, &sn, &co);
-      v = (float)tc_slice(q < nr ? co : sn, tc_pair_a(p));  // at most 9 significant bits: exact in TF32
+      const double y = q < nr ? co : sn;
+#pragma unroll
+      for (int t = 0; t < kTcSlices; t++) sl[t] = (float)tc_slice(y, t);  // at most 9 significant bits: exact in TF32
     }
-    A[(size_t)m * kpad + c] = v;
+#pragma unroll
+    for (int p = 0; p < kTcPairs; p++) row[(size_t)p * kseg + q] = sl[tc_pair_a(p)];
   }
 }
 
