@@ -238,11 +238,13 @@ int upload_model(edus_batch* b, const Problem& P, const Inst& I) {
 
 // Field components and stencil vectors that contribute for the whole run. A
 // component that is zero in every field-table row (pump and probe, at t and
-// t + dt/2) adds E_x D_x = 0 and E_x W_x = 0 exactly; a stencil vector with
-// w_b = 0, or orthogonal to every pump component in use, has a gradient
-// coefficient w_b (E_pump . b) that is exactly 0. The stage kernels skip
-// both; the remaining terms are summed in the same order, so the result is
-// the same to the last bit.
+// t + dt/2) adds E_x D_x = 0 and E_x W_x = 0 exactly; a stencil vector
+// orthogonal to every pump component in use has a gradient coefficient
+// w_b (E_pump . b) that is exactly 0. A shell weight below 1e-12 of the
+// largest is least-squares noise of the weight fit (headers/CalculateWeigths.h:
+// the diagonal shell of a square grid comes out near 1e-21 against 1e3) and
+// its terms lie below the FP64 resolution of the sum. The stage kernels skip
+// all of these; the remaining terms are summed in the same order.
 void select_terms(const Problem& P, const std::vector<FieldRow>& fr, Inst& I) {
   int fmask = 0, pmask = 0;
   for (const FieldRow& r : fr)
@@ -252,10 +254,12 @@ void select_terms(const Problem& P, const std::vector<FieldRow>& fr, Inst& I) {
     }
   I.fmask = fmask | pmask;
   I.nsel = 0;
+  double wmax = 0.;
+  for (int b = 0; b < P.nnb; b++) wmax = std::max(wmax, std::fabs(P.shell_w[P.bshell[b]]));
   for (int b = 0; b < P.nnb; b++) {
     bool on = false;
     for (int x = 0; x < 3; x++) on = on || ((pmask >> x) & 1 && P.bvec[b * 3 + x] != 0.);
-    if (on && P.shell_w[P.bshell[b]] != 0.) I.bsel[I.nsel++] = b;
+    if (on && std::fabs(P.shell_w[P.bshell[b]]) > 1e-12 * wmax) I.bsel[I.nsel++] = b;
   }
 }
 
