@@ -211,6 +211,7 @@ def serve_line(count=2000, rate=None, fp64_sample=9, seed=7, max_s=None, **kw):
                    "coulomb": "not in the served mix (batch instances run without the mean field)"},
         "kpoint_steps_per_s": st["kpoint_steps_per_s"], "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
         "max_latency_s": st["max_latency_s"], "completed": st["completed"], "failed": st["failed"], "span_s": st["span_s"],
+        "device_busy_s": st["device_ms"] * 1e-3,
         "peak_active": st["peak_active"], "peak_bytes": st["peak_bytes"],
         "fp64_request_by_request_sample": {"kpoint_steps_per_s": fp64_rate, "requests": len(lat),
                                            "mean_latency_s": float(np.mean(lat))},
