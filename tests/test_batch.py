@@ -286,3 +286,38 @@ def test_16_band_single_solve_matches_batch(workdir):
     drain(b, [s], 8)
     assert np.abs(b.get_state(s) - rho).max() < 1e-13
     assert rel(J1(b.obs(s)), J1(log)) < 1e-11
+
+
+@pytest.mark.parametrize("kind,n", [("w8", 10), ("w8", 6), ("hbn", 10), ("w16", 6)])
+def test_staged_forms_on_ragged_grids(workdir, kind, n):
+    """Grids whose rows are not whole tiles (tiles crossing rows, the wrap-around
+    stencil path, instances smaller than a tile): the staged forms (profile 3
+    for 2 bands, 4 for 8 and 16) against the element-parallel form (profile 0)
+    and the FP64 single solve."""
+    d = f"{workdir}/{kind}{n}"
+    if kind == "hbn":
+        p = E.parse_input(W.hbn_rk4(d, n=n, t_fin_fs=0.3, it_res=3, field=0.5))
+        nb, prof, kts = 2, 3, (32,)
+    elif kind == "w8":
+        p = E.parse_input(W.wannier(d, n=n, t_fin_fs=0.3, it_res=4))
+        nb, prof, kts = 8, 4, (8, 16)
+    else:
+        p = E.parse_input(W.wannier(d, nw=16, nside=13, n=n, t_fin_fs=0.2, it_res=5, name="W16"))
+        nb, prof, kts = 16, 4, (2, 4)
+    rho64, log64 = single(E.Problem(p, d))
+
+    def run(profile, kt):
+        pb = E.Problem(p, d)
+        if kind == "hbn":
+            pb.drop_decoupled_core()
+        b = E.Batch(precision=abi.EDUS_PREC_MIXED, chunk_steps=8, regs_profile={nb: profile}, tile_k={nb: kt})
+        s = b.add(pb)
+        drain(b, [s], 8)
+        return b.get_state(s), J1(b.obs(s))
+
+    ref_rho, ref_j = run(0, 32 if nb == 2 else (8 if nb == 8 else 2))
+    assert rel(ref_j, J1(log64)) < 1e-5
+    for kt in kts:
+        rho, j = run(prof, kt)
+        assert np.abs(rho - ref_rho).max() < 1e-6
+        assert rel(j, ref_j) < 1e-6
