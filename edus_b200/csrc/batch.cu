@@ -324,7 +324,7 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
   // cancel strongly, is the reference's stencil over an FP64 H(k) (CUDA cores)
   const int ncomp = 4;
   const int kp = tc_pad_k(nr), kseg = tc_seg_k(nr), ncols = 2 * ncomp * nt, K = 2 * nr;
-  std::vector<float> Bw((size_t)ncols * kp, 0.f);
+  std::vector<uint16_t> Bw((size_t)ncols * kp, 0);
   std::vector<double> col(K);
   for (int i = 0; i < n; i++)
     for (int j = i; j < n; j++) {
@@ -342,11 +342,13 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
             col[nr + r] = part == 0 ? -c.imag() : c.real();
             amax = std::max(amax, std::max(std::fabs(col[r]), std::fabs(col[nr + r])));
           }
-          // power-of-two scale of the column: every y = value / scale in [-1, 1]
-          const double scale = amax > 0. ? std::ldexp(1.0, std::ilogb(amax) + 1) : 1.0;
-          float* row = &Bw[(size_t)(2 * ce + part) * kp];
+          // power-of-two scale of the column: every y = value / scale in [-1/2, 1/2), so every
+          // slice is at most 128 in magnitude; the phases enter halved, so the stored
+          // slices carry 2 scale
+          const double scale = amax > 0. ? std::ldexp(1.0, std::ilogb(amax) + 2) : 1.0;
+          uint16_t* row = &Bw[(size_t)(2 * ce + part) * kp];
           for (int p = 0; p < kTcPairs; p++)
-            for (int q = 0; q < K; q++) row[(size_t)p * kseg + q] = (float)(scale * tc_slice(col[q] / scale, tc_pair_b(p)));
+            for (int q = 0; q < K; q++) row[(size_t)p * kseg + q] = tc_bf16(2.0 * scale * tc_slice(col[q] / scale, tc_pair_b(p)));
         }
       }
     }
@@ -357,9 +359,9 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
   for (int bb = 0; bb < P.nnb; bb++)
     for (int x = 0; x < 3; x++) gb[bb * 3 + x] = P.shell_w[P.bshell[bb]] * P.bvec[bb * 3 + x];
   const size_t plane = (size_t)nt * nk;
-  const size_t bytes = align256(sizeof(double) * 3 * nk) + align256(sizeof(double) * 3 * nr) + align256(sizeof(float) * Bw.size()) +
+  const size_t bytes = align256(sizeof(double) * 3 * nk) + align256(sizeof(double) * 3 * nr) + align256(sizeof(uint16_t) * Bw.size()) +
                        align256(sizeof(double2) * hdr.size()) + align256(sizeof(double) * gb.size()) +
-                       align256(sizeof(float) * (size_t)nk * kp) + align256(sizeof(double) * (size_t)nk * ncols) +
+                       align256(sizeof(uint16_t) * (size_t)nk * kp) + align256(sizeof(double) * (size_t)nk * ncols) +
                        align256(sizeof(double2) * plane) + align256(sizeof(double2) * n * n * nk) +
                        (I.GE ? align256(sizeof(double2) * plane) + align256(sizeof(double2) * 3 * plane) +
                                    align256(sizeof(double2) * 4 * nt * nr)
@@ -377,7 +379,7 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
   };
   double* dk = (double*)carve(sizeof(double) * 3 * nk);
   double* dR = (double*)carve(sizeof(double) * 3 * nr);
-  float* dB = (float*)carve(sizeof(float) * Bw.size());
+  uint16_t* dB = (uint16_t*)carve(sizeof(uint16_t) * Bw.size());
   double2* dh = (double2*)carve(sizeof(double2) * hdr.size());
   double* dg = (double*)carve(sizeof(double) * gb.size());
   int rc;
@@ -394,7 +396,7 @@ int build_model_tc(edus_batch* b, const Problem& P, const Inst& I) {
   t.Rvec = dR;
   t.Bw = dB;
   t.hdiagR = dh;
-  t.Aw = (float*)carve(sizeof(float) * (size_t)nk * kp);
+  t.Aw = (uint16_t*)carve(sizeof(uint16_t) * (size_t)nk * kp);
   t.Cw = (double*)carve(sizeof(double) * (size_t)nk * ncols);
   t.H32 = (float2*)I.H;
   t.D32 = (float2*)I.D;
@@ -873,7 +875,8 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
     if ((rc = put(b, (void*)I.nbr, nb))) return undo(rc);
   }
   if (P.model_deferred) {
-    const bool tc = b->mixed && b->opt.tc_contraction && P.p.conduction_shift <= 1e-16;
+    // (the exact segment sums hold up to 1024-deep segments, 512 R vectors)
+    const bool tc = b->mixed && b->opt.tc_contraction && P.p.conduction_shift <= 1e-16 && tc_seg_k(P.nrpts) <= 1024;
     if ((rc = tc ? build_model_tc(b, P, I) : build_model_on_device(b, P, I))) return undo(rc);
   } else {
     rc = b->mixed ? upload_model<float2>(b, P, I) : upload_model<double2>(b, P, I);

@@ -1,6 +1,7 @@
-// tc_contract.hpp — tensor-core (tcgen05, split TF32) Wannier contraction.
+// tc_contract.hpp — tensor-core (tcgen05, exact BF16 slices) Wannier contraction.
 #pragma once
 #include <cuda_runtime.h>
+#include <cstring>
 #include <stddef.h>
 
 #include <algorithm>
@@ -12,9 +13,9 @@ struct TcArgs {
   int n, ntri, nk, nr;
   const double* kpt;     // [nk][3]
   const double* Rvec;    // [nr][3]
-  const float* Bw;       // [8 ntri][Kp] coefficient slices, one K segment per slice pair (host-built)
+  const uint16_t* Bw;    // [8 ntri][Kp] coefficient slices (BF16), one K segment per slice pair (host-built)
   const double2* hdiagR; // [n][nr] H_ii(R) for the FP64 band energies
-  float* Aw;             // scratch [nk][Kp] phase slices, one K segment per slice pair
+  uint16_t* Aw;          // scratch [nk][Kp] phase slices (BF16), one K segment per slice pair
   double* Cw;            // scratch [nk][8 ntri] GEMM result (FP64 sum of FP32 slices)
   float2* H32;           // out [ntri][nk]
   float2* D32;           // out [3][ntri][nk]
@@ -23,14 +24,16 @@ struct TcArgs {
   int* err;              // device error word (bounded waits)
 };
 
-// Exact-slice form of the contraction. Every operand y (a phase cos / sin, or
-// a coefficient divided by its column's power-of-two scale) lies in [-1, 1]
-// and is cut into kTcSlices slices of at most 9 significant bits, slice s a
-// multiple of 2^-(8 s + 8): y = sum_s slice_s(y) + O(2^-33). The GEMM runs one
-// K segment per slice pair (a, b) with a + b < kTcSlices; inside a 32-deep K
-// slice every product is an integer times one power of two, at most 2^16 in
-// magnitude, so the tensor core's FP32 sums of 32 of them are exact and the
-// FP64 sum of the slices is the contraction to about 2^-32 of its terms.
+// Exact-slice form of the contraction. Every operand y (half a phase cos / sin,
+// or a coefficient divided by its column's power-of-two scale) lies in
+// [-1/2, 1/2] and is cut into kTcSlices slices of at most 8 significant bits,
+// slice s a multiple of 2^-(8 s + 8) and at most 128 in magnitude:
+// y = sum_s slice_s(y) + O(2^-33); every slice is exact in BF16. The GEMM runs
+// one K segment per slice pair
+// (a, b) with a + b < kTcSlices; inside a segment every product is an integer
+// times one power of two, at most 2^14 in magnitude, so the tensor core's FP32
+// sums over a segment of up to 1024 are exact and the FP64 sum of the segments
+// is the contraction to about 2^-32 of its terms.
 constexpr int kTcSlices = 4;
 constexpr int kTcPairs = 10;  // (a, b) with a + b <= 3
 __host__ __device__ constexpr int tc_pair_a(int p) {
@@ -50,7 +53,15 @@ __host__ __device__ inline double tc_slice(double y, int s) {
   }
   return v;
 }
-// K segment length (2 nr padded to the 32-deep K slice) and the GEMM depth
+// BF16 bit pattern of a value with at most 8 significant bits (exact: the low
+// 16 bits of its FP32 pattern are zero)
+__host__ __device__ inline uint16_t tc_bf16(double v) {
+  const float f = (float)v;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  return (uint16_t)(u >> 16);
+}
+// K segment length (2 nr padded to the 64-deep K slice) and the GEMM depth
 int tc_seg_k(int nr);
 int tc_pad_k(int nr);
 cudaError_t tc_contract(const TcArgs& a, cudaStream_t s);
