@@ -297,9 +297,14 @@ typedef struct {
   int32_t tile_k[EDUS_MAX_BANDS + 1]; /* k points per tile by band count; 0 = default */
   int32_t regs_profile[EDUS_MAX_BANDS + 1]; /* stage-kernel form by band count: 0 = element-parallel,
                                                56 registers; 1 = element-parallel, more registers;
-                                               2 = matrix-product form (8 and 16 bands) */
+                                               2 = matrix-product form (FP64; 8 and 16 bands);
+                                               3 = staged (cp.async one tile ahead; mixed);
+                                               4 = staged with the register-blocked commutator
+                                               (mixed; 8 and 16 bands). 3 and 4 fall back to 0 for
+                                               an instance without a lattice stencil */
   int32_t tc_contraction;   /* mixed precision: deferred Wannier models contracted on the tensor
-                               cores (split TF32, FP32 accumulate; band energies FP64) */
+                               cores (exact BF16 slices, FP32 sums exact per segment, FP64 across
+                               segments; band energies FP64) */
   int32_t pad;
   int64_t hbm_budget_bytes; /* admission limit; 0 = 90 % of the free device memory at create */
 } edus_batch_options;
