@@ -55,7 +55,9 @@ def parse_args():
 
 
 def dist_env():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+    from edus_b200.replicas import dist_env as env
+
+    return env()
 
 
 def make_workload(workdir):
@@ -182,12 +184,11 @@ def run_reference(args):
 def run_ours(args):
     import torch
 
-    rank, world, local = dist_env()
-    if world > 1:
-        import datetime
+    from edus_b200.replicas import ReplicaGroup, whole_job_rate
 
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rank, world, local = dist_env()
     torch.cuda.set_device(local)
+    group = ReplicaGroup("nccl", device=f"cuda:{local}")
     import edus_b200 as E
 
     d = tempfile.mkdtemp(prefix="edus_bench_")
@@ -199,10 +200,7 @@ def run_ours(args):
     units = nk * nsteps  # k-point·steps per solve
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > 126 MB L2
 
-    def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
+    barrier = group.barrier
 
     for _ in range(max(args.warmup, 1)):  # the first run captures the CUDA graph
         ctx.reset()
@@ -222,12 +220,8 @@ def run_ours(args):
         launches += l
     barrier()
     clocks = sampler.stop()
-    total_ms = sum(dev_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * units * args.steps / (max_ms * 1e-3)
+    max_ms = group.max(sum(dev_ms))
+    value = whole_job_rate(world, units, args.steps, max_ms * 1e-3)
 
     # end to end through the C ABI with host buffers: H2D of the initial state,
     # the solve, D2H of the observable log and of the final state
@@ -244,11 +238,7 @@ def run_ours(args):
         host_rho[...] = ctx.get_state()
         nobs = len(obs)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * units * args.steps / float(te.item())
+    e2e_value = whole_job_rate(world, units, args.steps, group.max(time.perf_counter() - t0))
     obs_bytes = nobs * C.sizeof(E.abi.Obs)
 
     # live roofline of the dominant kernel (fused RHS + AB update), CUDA events on its stream
@@ -290,8 +280,7 @@ def run_ours(args):
         }
         print(json.dumps(line), flush=True)
     ctx.close()
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    group.close()
     return 0
 
 
