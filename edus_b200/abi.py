@@ -220,6 +220,7 @@ class ServerOptions(C.Structure):
         ("setup_threads", C.c_int32),
         ("drop_decoupled_core", C.c_int32),
         ("max_bypass_s", C.c_double),
+        ("trace_tol", C.c_double),
     ]
 
 

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -178,6 +179,29 @@ void admit(edus_server* s, edus_batch_stats& st) {
   }
 }
 
+// Health check of a finished request's observable log: 0, EDUS_ENONFINITE
+// for a record with a non-finite value, or EDUS_ETRACE for a trace that
+// drifted past trace_tol (the reference prints the trace check only,
+// headers/Observables_MPI.h:396-410; a served request fails instead).
+int log_health(const std::vector<edus_obs>& obs, double trace_tol, std::string& why) {
+  for (size_t q = 0; q < obs.size(); q++) {
+    const edus_obs& o = obs[q];
+    bool finite = std::isfinite(o.trace_dev) && std::isfinite(o.p_cond_max) && std::isfinite(o.p_min);
+    for (int x = 0; x < 6; x++) finite = finite && std::isfinite(o.J1[x]);
+    for (int x = 0; x < 3; x++) finite = finite && std::isfinite(o.J2[x]);
+    for (int c = 0; c < EDUS_MAX_BANDS; c++) finite = finite && std::isfinite(o.pop[c]);
+    if (!finite) {
+      why = "non-finite observables at output instant " + std::to_string(q);
+      return EDUS_ENONFINITE;
+    }
+    if (trace_tol > 0 && std::fabs(o.trace_dev) > trace_tol) {
+      why = "trace drift " + std::to_string(o.trace_dev) + " at output instant " + std::to_string(q);
+      return EDUS_ETRACE;
+    }
+  }
+  return 0;
+}
+
 int retire(edus_server* s) {
   std::vector<std::pair<int, int64_t>> run;
   {
@@ -195,11 +219,19 @@ int retire(edus_server* s) {
     std::vector<edus_obs> obs(n);
     if (n && (rc = edus_batch_obs_get(s->batch, sr.first, 0, n, obs.data()))) return rc;
     if ((rc = edus_batch_release(s->batch, sr.first))) return rc;
+    std::string why;
+    const int health = log_health(obs, s->opt.trace_tol, why);
     std::lock_guard<std::mutex> lk(s->mu);
     Request* r = s->reqs[sr.second].get();
-    r->obs.swap(obs);
     s->running.erase(sr.first);
     s->bytes_in_use -= r->footprint;
+    if (health) {
+      r->error = health;
+      r->message = "request " + std::to_string(sr.second) + ": " + why;
+      finish(s, *r, EDUS_REQ_FAILED);
+      continue;
+    }
+    r->obs.swap(obs);
     finish(s, *r, EDUS_REQ_DONE);
   }
   return 0;
@@ -254,6 +286,7 @@ int edus_server_options_default(edus_server_options* o) {
   o->setup_threads = 4;
   o->drop_decoupled_core = 1;
   o->max_bypass_s = 2.0;
+  o->trace_tol = 1e-3;
   return 0;
 }
 

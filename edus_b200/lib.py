@@ -408,7 +408,7 @@ class Server:
 
     def __init__(self, device=0, precision=abi.EDUS_PREC_FP64, max_instances=1024, chunk_steps=16,
                  hbm_budget_bytes=0, setup_threads=4, drop_decoupled_core=True, max_bypass_s=2.0, tile_k=None,
-                 regs_profile=None, tuned=True):
+                 regs_profile=None, tuned=True, trace_tol=None):
         L = load_library()
         if tuned and tile_k is None and regs_profile is None:
             tile_k, regs_profile = _tuned(precision)
@@ -427,6 +427,8 @@ class Server:
         o.setup_threads = setup_threads
         o.drop_decoupled_core = 1 if drop_decoupled_core else 0
         o.max_bypass_s = max_bypass_s
+        if trace_tol is not None:
+            o.trace_tol = trace_tol
         self._h = C.c_void_p()
         _check(L.edus_server_create(C.byref(o), C.byref(self._h)), "edus_server_create")
         self._keep = {}

@@ -359,6 +359,10 @@ typedef struct {
   int32_t setup_threads;        /* host threads building problems */
   int32_t drop_decoupled_core;  /* apply edus_problem_drop_decoupled_core where it holds */
   double max_bypass_s;          /* how long younger requests may pass one that does not fit */
+  double trace_tol;             /* health check of every finished request's observable log:
+                                   a non-finite record fails it with EDUS_ENONFINITE, a record with
+                                   |trace - (Nch + Nv)| > trace_tol with EDUS_ETRACE (0: no trace
+                                   check); default 1e-3 */
 } edus_server_options;
 
 enum { EDUS_REQ_QUEUED = 0, EDUS_REQ_SETUP = 1, EDUS_REQ_READY = 2, EDUS_REQ_RUNNING = 3, EDUS_REQ_DONE = 4, EDUS_REQ_FAILED = 5 };

@@ -111,3 +111,22 @@ def test_unsupported_request_fails_alone(workdir):
     with pytest.raises(E.EdusError):
         s.obs(ids[1])
     s.close()
+
+
+@pytest.mark.parametrize("precision", [abi.EDUS_PREC_FP64, abi.EDUS_PREC_MIXED])
+def test_diverging_request_fails_alone(workdir, precision):
+    """Health check at retirement: an RK4 step 100x past its stability limit
+    overflows (floating point only, nothing faults); that request fails with
+    EDUS_ENONFINITE or EDUS_ETRACE while the others complete."""
+    reqs = requests(workdir)[:2]
+    d = f"{workdir}/unstable"
+    bad = (E.parse_input(W.hbn_rk4(d, n=12, t_fin_fs=120.0, it_res=5, dt_fs=1.0, field=0.5)), d)
+    s = E.Server(precision=precision, chunk_steps=8)
+    ids = [s.submit(*reqs[0]), s.submit(*bad), s.submit(*reqs[1])]
+    s.drain(300)
+    st = [s.info(i)["status"] for i in ids]
+    assert st == [abi.EDUS_REQ_DONE, abi.EDUS_REQ_FAILED, abi.EDUS_REQ_DONE]
+    assert s.info(ids[1])["error"] in (abi.EDUS_ENONFINITE, abi.EDUS_ETRACE)
+    with pytest.raises(E.EdusError):
+        s.obs(ids[1])
+    s.close()
