@@ -683,6 +683,24 @@ int edus_problem_get(const edus_problem* pb, const char* name, void* dst, size_t
 
 void edus_problem_free(edus_problem* pb) { delete pb; }
 
+// Output/k_grid.txt: the crystal coordinates of every k point in grid order,
+// one "k0 k1 k2" line each with the default stream format, as the reference
+// writes it at its first output step (headers/Observables_MPI.h:492-550,
+// called from Source_Main/if_resolution.cpp:100-102).
+static int write_kgrid(const Problem& P, const char* outdir) {
+  mkdir(outdir, 0755);
+  std::ofstream f(std::string(outdir) + "/k_grid.txt");
+  if (!f) return fail(EDUS_EIO, "cannot write into %s", outdir);
+  const std::vector<double>& k = P.kpt;
+  for (size_t ik = 0; ik + 2 < k.size(); ik += 3) f << k[ik] << " " << k[ik + 1] << " " << k[ik + 2] << std::endl;
+  return f ? 0 : fail(EDUS_EIO, "write error in %s/k_grid.txt", outdir);
+}
+
+int edus_problem_write_kgrid(const edus_problem* pb, const char* outdir) {
+  if (!pb || !outdir) return fail(EDUS_EINVAL, "null argument");
+  return write_kgrid(pb->P, outdir);
+}
+
 int edus_model_hud(const edus_problem* pb, const double kcrys[3], double* H, double* U, double* D) {
   if (!pb || !kcrys || !H || !U || !D) return fail(EDUS_EINVAL, "null argument");
   return model_hud(pb->P, kcrys, (cd*)H, (cd*)U, (cd*)D);
@@ -1169,8 +1187,9 @@ int edus_last_timing(edus_ctx* c, double* ms, int64_t* launches) {
   return 0;
 }
 
-// Output/{EF,J1,J2,Losses,TransientAbs}.txt with the reference's stream formats
-// (headers/Observables_MPI.h:134-140, 398-406, 586-595, 707-712, 766-771).
+// Output/{EF,J1,J2,Losses,TransientAbs,k_grid}.txt with the reference's stream
+// formats (headers/Observables_MPI.h:134-140, 398-406, 492-550, 586-595,
+// 707-712, 766-771).
 int edus_write_outputs(edus_ctx* c, const char* outdir) {
   if (!c || !outdir) return fail(EDUS_EINVAL, "null argument");
   int32_t n = 0;
@@ -1178,7 +1197,7 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
   std::vector<edus_obs> log(n);
   int rc = edus_obs_get(c, 0, n, log.data());
   if (rc) return rc;
-  mkdir(outdir, 0755);
+  if ((rc = write_kgrid(c->P, outdir))) return rc;
   std::string d = outdir;
   std::ofstream fe(d + "/EF.txt"), fl(d + "/Losses.txt");
   std::ofstream f1, f2, ft;

@@ -40,6 +40,7 @@ def load_library():
         "edus_problem_create_deferred": (C.c_int, [P(abi.Params), cp, P(vp)]),
         "edus_problem_get": (C.c_int, [vp, cp, vp, sz]),
         "edus_problem_free": (None, [vp]),
+        "edus_problem_write_kgrid": (C.c_int, [vp, cp]),
         "edus_model_hud": (C.c_int, [vp, P(dbl), vp, vp, vp]),
         "edus_struct_sizes": (C.c_int, [P(C.c_int64)]),
         "edus_options_default": (C.c_int, [P(abi.Options)]),
@@ -167,6 +168,10 @@ class Problem:
         a = np.zeros(shp, dtype=dt)
         _check(self._L.edus_problem_get(self._h, name.encode(), a.ctypes.data, a.nbytes), f"edus_problem_get({name})")
         return a
+
+    def write_kgrid(self, outdir):
+        """outdir/k_grid.txt in the reference's format (edus_problem_write_kgrid)."""
+        _check(self._L.edus_problem_write_kgrid(self._h, os.fsencode(outdir)), "edus_problem_write_kgrid")
 
     def model_hud(self, kcrys):
         """H, U, D of the model at one crystal k point (gHUD)."""

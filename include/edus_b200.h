@@ -184,6 +184,11 @@ int edus_problem_drop_decoupled_core(edus_problem* pb);
  * "HR","rR","Rvec"); nbytes must match exactly. */
 int edus_problem_get(const edus_problem* pb, const char* name, void* dst, size_t nbytes);
 void edus_problem_free(edus_problem* pb);
+/* Write outdir/k_grid.txt (outdir created if missing): the crystal
+ * coordinates of every k point, one "k0 k1 k2" line each in the default C++
+ * stream format, as the reference's print_k_MPI (headers/Observables_MPI.h:
+ * 492-550) writes Output/k_grid.txt. edus_write_outputs writes it too. */
+int edus_problem_write_kgrid(const edus_problem* pb, const char* outdir);
 /* H(k), U(k) and D(k) of the problem's model at one crystal k point, as
  * gHUD (headers/HUD.h:5-20) returns them: H, U [n][n], D [n][n][3] interleaved
  * complex. */
@@ -246,7 +251,7 @@ int edus_observables(edus_ctx* ctx, edus_obs* out);
  * on a device: calls that overlap in time (two host threads, or two streams)
  * race on it and must be serialised by the caller. */
 int edus_observables_static(edus_ctx* ctx, edus_obs* out);
-/* Write Output/{EF,J1,J2,Losses,TransientAbs}.txt in the reference's format. */
+/* Write Output/{EF,J1,J2,Losses,TransientAbs,k_grid}.txt in the reference's format. */
 int edus_write_outputs(edus_ctx* ctx, const char* outdir);
 /* Device time (ms, CUDA events) of the last edus_step/edus_run call and the
  * number of kernel launches it issued. */

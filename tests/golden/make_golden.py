@@ -7,6 +7,8 @@ Writes (all small, committed):
   ab5_input.txt          input.txt of the shipped Adams–Bashforth run
   ab5_golden.npz         its Output/{J1,J2,Losses,EF,TransientAbs}.txt, every
                          4th output row (830 of 3319), at printed precision
+  ab5_kgrid.json         its Output/k_grid.txt: SHA-256 of the bytes, line
+                         count and the first and last lines
   test_matrices.npz      H, U, dx, dy at k=(0,0.3,0.1) from Test_matrices.txt
   ../../edus_b200/data/coulomb_ncut20.npz
                          Output/Coulomb/{A,B,C,D}_coeff, Screen_const and
@@ -57,7 +59,22 @@ def test_matrices(path):
     return blocks
 
 
+def kgrid(ref):
+    """Fingerprint of the shipped Output/k_grid.txt (byte-exact comparison)."""
+    import hashlib
+    import json
+
+    with open(os.path.join(ref, AB5, "Output", "k_grid.txt"), "rb") as f:
+        raw = f.read()
+    lines = raw.decode().splitlines()
+    out = {"sha256": hashlib.sha256(raw).hexdigest(), "bytes": len(raw), "lines": len(lines),
+           "head": lines[:3], "tail": lines[-3:]}
+    with open(os.path.join(HERE, "ab5_kgrid.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 def main(ref):
+    kgrid(ref)
     g = os.path.join(ref, AB5)
     with open(os.path.join(g, "input.txt")) as f, open(os.path.join(HERE, "ab5_input.txt"), "w") as o:
         o.write(f.read())

@@ -204,3 +204,8 @@ def test_edus_run_writes_the_reference_outputs(tmp_path):
     assert rel(J1[rows, 1:], G["J1"][:, 1:]) < 1e-12
     L = np.loadtxt(tmp_path / "Output" / "Losses.txt")
     assert np.abs(L[rows, 1:4] - G["Losses"][:, 1:4]).max() < 1e-13
+    import hashlib
+    import json
+
+    kg = json.load(open(os.path.join(GOLDEN, "ab5_kgrid.json")))
+    assert hashlib.sha256((tmp_path / "Output" / "k_grid.txt").read_bytes()).hexdigest() == kg["sha256"]

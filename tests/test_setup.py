@@ -49,6 +49,22 @@ def test_golden_shells_match_reference_log():
     assert np.sum(np.isclose(np.linalg.norm(b, axis=1), 0.02194, atol=1e-5)) == 6
 
 
+def test_golden_kgrid_file_byte_exact(tmp_path):
+    """Output/k_grid.txt of the shipped AB5 run (headers/Observables_MPI.h:492-550),
+    byte for byte: the k grid in the reference's order and stream format."""
+    import hashlib
+    import json
+
+    ref = json.load(open(os.path.join(GOLDEN, "ab5_kgrid.json")))
+    pb = E.Problem(E.parse_input(GOLDEN_INPUT))
+    out = tmp_path / "Output"
+    pb.write_kgrid(str(out))
+    raw = (out / "k_grid.txt").read_bytes()
+    lines = raw.decode().splitlines()
+    assert lines[:3] == ref["head"] and lines[-3:] == ref["tail"] and len(lines) == ref["lines"]
+    assert len(raw) == ref["bytes"] and hashlib.sha256(raw).hexdigest() == ref["sha256"]
+
+
 def test_test_matrices_known_answer():
     """Source_Main/test_matrix_k.cpp prints H, U, dx, dy at k = (0, 0.3, 0.1)."""
     p = E.parse_input(GOLDEN_INPUT)
