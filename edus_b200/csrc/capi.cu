@@ -13,8 +13,10 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <iomanip>
 #include <mutex>
+#include <sstream>
 #include <string>
 #include <sys/stat.h>
 #include <vector>
@@ -103,6 +105,15 @@ struct edus_ctx {
   int log_cap = 0, nlog = 0;
   double* d_ncond = nullptr;
   double* d_pcmax = nullptr;
+  // per-k snapshots (PrintPopulation / Print_new_band_dispersion): icont and
+  // the times as the reference counts them; with PrintPopulation, slot m of
+  // d_snap holds snapshot m's three eigenbasis elements [3][nk]; with the
+  // Coulomb mean field, slot m of d_edia its band energies [n][nk]
+  bool snap_on = false;
+  int icont = -1, snap_cap = 0, snap_ic = 0, snap_jc = 0;
+  double2* d_snap = nullptr;
+  double* d_edia = nullptr;
+  std::vector<double> snap_t;
   unsigned long long* d_maxdp = nullptr;
   // loop state (host mirror of the reference's scalars)
   int it = 0, itfi = 0, res = 1;
@@ -139,6 +150,8 @@ struct edus_ctx {
     bool e_non0;
     int ring_idx[kMaxOrder];
     double2 *P0, *Pa;
+    int icont;
+    std::vector<double> snap_t;
   } after_graph{};
 };
 
@@ -432,12 +445,37 @@ int sync_scalars(edus_ctx* c) {
   return 0;
 }
 
+// Snapshot switch of an output step (Source_Main/if_resolution.cpp:18-33):
+// a snapshot is due when t > start + icont * step and t < end (icont counted
+// from -1); then icont advances and, with PrintPopulation, the state's
+// eigenbasis elements go to slot icont (Source_Main/if_resolution.cpp:231-270).
+int snapshot(edus_ctx* c) {
+  const edus_params& p = c->P.p;
+  if (!(c->time_loop > p.print_start + c->icont * p.print_step && c->time_loop < p.print_end)) return 0;
+  c->icont++;
+  c->snap_t.push_back(c->time_loop * kTimeAuFs);
+  if (!c->d_snap && !c->d_edia) return 0;
+  if (c->icont >= c->snap_cap) return fail(EDUS_EINVAL, "snapshot %d exceeds the %d slots", c->icont, c->snap_cap);
+  if (c->d_snap) {
+    CK(launch_snapshot(c->tb, c->d_P0, c->snap_ic, c->snap_jc, c->d_snap + (size_t)c->icont * 3 * c->nk, c->stream));
+    c->launches++;
+  }
+  if (c->d_edia) {
+    // the renormalised H of the last RHS evaluation, as the populations use it
+    // (headers/Observables_MPI.h:282-303, 440-478)
+    CK(launch_band_energies(c->tb, c->d_hr, c->d_edia + (size_t)c->icont * c->n * c->nk, c->stream));
+    c->launches++;
+  }
+  return 0;
+}
+
 int run_steps(edus_ctx* c, int nsteps, bool all) {
   int done = 0;
   if (!c->dyn) {
     while (c->it <= c->itfi && (all || done < nsteps)) {
       if (c->it % c->res == 0) {
         int rc = observe(c);
+        if (!rc && c->snap_on) rc = snapshot(c);
         if (rc) return rc;
       }
       int rc = do_step(c);
@@ -452,6 +490,7 @@ int run_steps(edus_ctx* c, int nsteps, bool all) {
         int rc = observe(c);
         if (rc) return rc;
         if ((rc = sync_scalars(c))) return rc;
+        if (c->snap_on && (rc = snapshot(c))) return rc;
       }
       int rc = do_step(c);
       if (rc) return rc;
@@ -494,6 +533,8 @@ int timed(edus_ctx* c, int nsteps, bool all) {
     memcpy(h.ring_idx, c->ring_idx, sizeof(h.ring_idx));
     h.P0 = c->d_P0;
     h.Pa = c->d_Pa;
+    h.icont = c->icont;
+    h.snap_t = c->snap_t;
     CK(cudaEventRecord(c->ev0, c->stream));
     CK(cudaGraphLaunch(c->gexec, c->stream));
   } else if (graph) {
@@ -511,6 +552,8 @@ int timed(edus_ctx* c, int nsteps, bool all) {
     memcpy(c->ring_idx, h.ring_idx, sizeof(h.ring_idx));
     c->d_P0 = h.P0;
     c->d_Pa = h.Pa;
+    c->icont = h.icont;
+    c->snap_t = h.snap_t;
   } else {
     CK(cudaEventRecord(c->ev0, c->stream));
     int rc = run_steps(c, nsteps, all);
@@ -683,11 +726,15 @@ int edus_problem_get(const edus_problem* pb, const char* name, void* dst, size_t
 
 void edus_problem_free(edus_problem* pb) { delete pb; }
 
+}  // extern "C"
+
+namespace {
+
 // Output/k_grid.txt: the crystal coordinates of every k point in grid order,
 // one "k0 k1 k2" line each with the default stream format, as the reference
 // writes it at its first output step (headers/Observables_MPI.h:492-550,
 // called from Source_Main/if_resolution.cpp:100-102).
-static int write_kgrid(const Problem& P, const char* outdir) {
+int write_kgrid(const Problem& P, const char* outdir) {
   mkdir(outdir, 0755);
   std::ofstream f(std::string(outdir) + "/k_grid.txt");
   if (!f) return fail(EDUS_EIO, "cannot write into %s", outdir);
@@ -695,6 +742,155 @@ static int write_kgrid(const Problem& P, const char* outdir) {
   for (size_t ik = 0; ik + 2 < k.size(); ik += 3) f << k[ik] << " " << k[ik + 1] << " " << k[ik + 2] << std::endl;
   return f ? 0 : fail(EDUS_EIO, "write error in %s/k_grid.txt", outdir);
 }
+
+// Print order of the per-k files: the rows of the grid (nk_x consecutive k
+// points) sorted by their first k point's coordinate along the row axis, the
+// first of equal values first (Create_sorted_indices_k_MPI and find_index_min,
+// headers/Observables_MPI.h:600-660; the reordering of Print_vec3x_MPI,
+// :44-62). Returns the source k of every printed line.
+std::vector<int> print_order(const Problem& P) {
+  const int* Nk = P.p.nk;
+  const int nk = P.nk;
+  int pol = 1, nk_x = Nk[1] * Nk[0];
+  if (Nk[1] > Nk[2]) {
+    pol = 0;
+    nk_x = Nk[1] * Nk[2];
+  }
+  const int nk_y = nk / nk_x;
+  std::vector<double> kt(nk_y, 0.0);
+  for (int ik = 0; ik < nk; ik++)
+    if (ik % nk_x == 0 && ik / nk_x < nk_y) kt[ik / nk_x] = P.kpt[(size_t)ik * 3 + pol];
+  std::vector<int> idx(nk_y);
+  for (int r = 0; r < nk_y; r++) {
+    int m = 0;
+    double mv = 1e15;
+    for (int q = 0; q < nk_y; q++)
+      if (kt[q] < mv) {
+        mv = kt[q];
+        m = q;
+      }
+    kt[m] = 1e15;
+    idx[r] = m;
+  }
+  std::vector<int> order(nk);
+  for (int ik = 0; ik < nk; ik++) {
+    const int ikx = ik / nk_x, iky = ik % nk_x;
+    order[ik] = ikx < nk_y ? idx[ikx] * nk_x + iky : ik;
+  }
+  return order;
+}
+
+// Output/t_Ek.txt (time of every snapshot, fs), with the Coulomb mean field
+// Edia_<m>.txt, and with PrintPopulation the
+// three per-k files of every snapshot m: P_val_cond_in_Eigenstate_<v><c>_<m>,
+// P_val_in_Eigenstate_<v><v>_<m>, P_cond_in_Eigenstate_<c><c>_<m>, one "re im"
+// line per k (Source_Main/if_resolution.cpp:18-33, 231-270, Source_Main/
+// open_files.cpp:57-63, headers/Observables_MPI.h:3-130).
+int write_snapshots(edus_ctx* c, const std::string& d) {
+  std::ofstream ft(d + "/t_Ek.txt");
+  if (!ft) return fail(EDUS_EIO, "cannot write into %s", d.c_str());
+  for (double t : c->snap_t) ft << t << std::endl;
+  const int nk = c->nk, nsnap = std::min(c->icont + 1, c->snap_cap);
+  if (c->d_edia) {
+    // Output/Edia_<m>.txt: the band energies of every k in grid order, 20 digits
+    std::vector<double> e((size_t)c->n * nk);
+    for (int m = 0; m < nsnap; m++) {
+      CK(cudaMemcpy(e.data(), c->d_edia + (size_t)m * c->n * nk, sizeof(double) * e.size(), cudaMemcpyDeviceToHost));
+      std::ostringstream name;
+      name << d << "/Edia_" << m << ".txt";
+      std::ofstream f(name.str());
+      if (!f) return fail(EDUS_EIO, "cannot write %s", name.str().c_str());
+      for (int ik = 0; ik < nk; ik++) {
+        for (int i = 0; i < c->n; i++) f << std::setprecision(20) << e[(size_t)i * nk + ik] << " ";
+        f << std::endl;
+      }
+    }
+  }
+  if (!c->d_snap) return 0;
+  const std::vector<int> order = print_order(c->P);
+  std::vector<double2> buf((size_t)3 * nk);
+  const char* label[3] = {"P_val_cond_in_Eigenstate", "P_val_in_Eigenstate", "P_cond_in_Eigenstate"};
+  const int ii[3] = {c->snap_ic, c->snap_ic, c->snap_jc}, jj[3] = {c->snap_jc, c->snap_ic, c->snap_jc};
+  for (int m = 0; m < nsnap; m++) {
+    CK(cudaMemcpy(buf.data(), c->d_snap + (size_t)m * 3 * nk, sizeof(double2) * buf.size(), cudaMemcpyDeviceToHost));
+    for (int q = 0; q < 3; q++) {
+      std::ostringstream name;
+      name << d << "/" << label[q] << "_" << ii[q] << jj[q] << "_" << m << ".txt";
+      std::ofstream f(name.str());
+      if (!f) return fail(EDUS_EIO, "cannot write %s", name.str().c_str());
+      for (int ik = 0; ik < nk; ik++) {
+        const double2 v = buf[(size_t)q * nk + order[ik]];
+        f << v.x << " ";
+        f << v.y << std::endl;
+      }
+    }
+  }
+  return 0;
+}
+
+// The files the reference writes once, at its first output step
+// (Print_initial_H_P, Source_Main/if_resolution.cpp:275-328), one "re im" line
+// per k in print order, v / c the top valence and bottom conduction band:
+// H_Eigen_{cond,val,val_cond} (eigenvalues of the model H on the diagonal,
+// zero elsewhere: Diagonalize_unitary_vec3x, headers/InitialPopulation.h:45-96),
+// H_Wannier_cond (model H), P_initial_Wannier_ (the initial state) and Uk_
+// (elements cc and cv of U), named <label>_<i><j>_0.txt.
+int write_initial(edus_ctx* c, const std::string& d) {
+  const int n = c->n, nk = c->nk, v = c->P.nbands - 1, cb = c->P.nbands;
+  if (v < 0 || cb >= n) return 0;
+  auto tri = [n](int i, int j) { return i * n - (i * (i - 1)) / 2 + (j - i); };
+  std::vector<double> eps((size_t)n * nk);
+  {
+    double* d_eps = nullptr;
+    CK(cudaMalloc(&d_eps, sizeof(double) * eps.size()));
+    cudaError_t e = launch_band_energies(c->tb, c->tb.H, d_eps, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(eps.data(), d_eps, sizeof(double) * eps.size(), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_eps);
+    CK(e);
+  }
+  auto plane = [&](const double2* src, std::vector<double2>& out) -> int {
+    out.resize(nk);
+    CK(cudaMemcpy(out.data(), src, sizeof(double2) * nk, cudaMemcpyDeviceToHost));
+    return 0;
+  };
+  std::vector<double2> hcc, pcc, ucc, ucv;
+  int rc;
+  if ((rc = plane(c->tb.H + (size_t)tri(cb, cb) * nk, hcc)) || (rc = plane(c->d_Pinit + (size_t)tri(cb, cb) * nk, pcc)) ||
+      (rc = plane(c->tb.U + (size_t)(cb * n + cb) * nk, ucc)) || (rc = plane(c->tb.U + (size_t)(cb * n + v) * nk, ucv)))
+    return rc;
+  const std::vector<int> order = print_order(c->P);
+  struct Out {
+    const char* label;
+    int i, j;
+    std::function<double2(int)> at;
+  };
+  const Out files[] = {
+      {"H_Eigen_cond", cb, cb, [&](int k) { return make_double2(eps[(size_t)cb * nk + k], 0.0); }},
+      {"H_Eigen_val", v, v, [&](int k) { return make_double2(eps[(size_t)v * nk + k], 0.0); }},
+      {"H_Eigen_val_cond", v, cb, [&](int) { return make_double2(0.0, 0.0); }},
+      {"H_Wannier_cond", cb, cb, [&](int k) { return hcc[k]; }},
+      {"P_initial_Wannier_", cb, cb, [&](int k) { return pcc[k]; }},
+      {"Uk_", cb, cb, [&](int k) { return ucc[k]; }},
+      {"Uk_", cb, v, [&](int k) { return ucv[k]; }},
+  };
+  for (const Out& o : files) {
+    std::ostringstream name;
+    name << d << "/" << o.label << "_" << o.i << o.j << "_0.txt";
+    std::ofstream f(name.str());
+    if (!f) return fail(EDUS_EIO, "cannot write %s", name.str().c_str());
+    for (int ik = 0; ik < nk; ik++) {
+      const double2 x = o.at(order[ik]);
+      f << x.x << " ";
+      f << x.y << std::endl;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
 
 int edus_problem_write_kgrid(const edus_problem* pb, const char* outdir) {
   if (!pb || !outdir) return fail(EDUS_EINVAL, "null argument");
@@ -842,6 +1038,34 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   cudaMemsetAsync(c->d_pcmax, 0, sizeof(double), c->stream);
   c->log_cap = P.p.dynamical_dt ? 1 << 16 : P.nprint + 2;
   if ((rc = dalloc(c, &c->d_log, c->log_cap))) return bail(rc);
+  // ---- per-k snapshots: slots for every snapshot the run can take
+  c->snap_on = P.p.print_population || P.p.print_band_dispersion;
+  if (c->snap_on && (P.p.print_population || c->coul)) {
+    c->snap_ic = P.nbands - 1;  // top valence and bottom conduction band (Nb[0] + Nb[1] - 1, Nb[0] + Nb[1])
+    c->snap_jc = P.nbands;
+    if (P.p.print_population && (c->snap_ic < 0 || c->snap_jc >= n))
+      return bail(fail(EDUS_EUNSUPPORTED, "PrintPopulation needs a valence and a conduction band"));
+    int cap = 0;
+    if (!c->dyn) {
+      // the snapshot switch along the constant-dt clock of the run loop
+      double t = P.t_start;
+      int ic = -1;
+      for (int it = 0; it <= P.itfi; it++) {
+        if (it % c->res == 0 && t > P.p.print_start + ic * P.p.print_step && t < P.p.print_end) ic++;
+        t += P.p.dt;
+      }
+      cap = ic + 1;
+    } else if (P.p.print_step > 0) {
+      cap = (int)std::min<double>(c->log_cap, std::floor((P.p.print_end - P.p.print_start) / P.p.print_step) + 2);
+    } else {
+      return bail(fail(EDUS_EUNSUPPORTED, "PrintPopulation with step <= 0 under a dynamical dt"));
+    }
+    if ((double)cap * (3 * sizeof(double2) + n * sizeof(double)) * nk > 16e9)
+      return bail(fail(EDUS_EUNSUPPORTED, "%d snapshots exceed 16 GB", cap));
+    c->snap_cap = cap;
+    if (cap > 0 && P.p.print_population && (rc = dalloc(c, &c->d_snap, (size_t)cap * 3 * nk))) return bail(rc);
+    if (cap > 0 && c->coul && (rc = dalloc(c, &c->d_edia, (size_t)cap * n * nk))) return bail(rc);
+  }
   // ---- tables struct
   DevTables& tb = c->tb;
   memset(&tb, 0, sizeof(tb));
@@ -1024,6 +1248,8 @@ int edus_reset(edus_ctx* c) {
   c->n_cond = c->dyn ? std::pow(10, -16) : 0;
   c->P_cond_max = 0;
   c->nlog = 0;
+  c->icont = -1;
+  c->snap_t.clear();
   return 0;
 }
 
@@ -1199,6 +1425,8 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
   if (rc) return rc;
   if ((rc = write_kgrid(c->P, outdir))) return rc;
   std::string d = outdir;
+  if (c->snap_on && (rc = write_snapshots(c, d))) return rc;
+  if ((rc = write_initial(c, d))) return rc;
   std::ofstream fe(d + "/EF.txt"), fl(d + "/Losses.txt");
   std::ofstream f1, f2, ft;
   if (c->P.p.current) {

@@ -424,6 +424,72 @@ cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2*
                     (const int*)c.diag_of);
 }
 
+// Per-k snapshot: elements (ic, jc), (ic, ic) and (jc, jc) of the state in
+// the model's eigenbasis, P_dia_rc = sum_ii sum_jj conj(U_r,ii) P_ii,jj U_c,jj
+// in the reference's summation order (headers/InitParameters.h:232-255), for
+// the snapshots of Source_Main/if_resolution.cpp:231-270. One thread per k.
+__global__ void k_snapshot(DevTables tb, const double2* __restrict__ rho, int ic, int jc, double2* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nk = tb.nk, n = tb.n;
+  if (k >= nk) return;
+  auto tri = [n](int i, int j) { return i * n - (i * (i - 1)) / 2 + (j - i); };
+  const int rows[3] = {ic, ic, jc}, cols[3] = {jc, ic, jc};
+  for (int q = 0; q < 3; q++) {
+    const int r = rows[q], c = cols[q];
+    double2 acc = cz();
+    for (int ii = 0; ii < n; ii++) {
+      const double2 ur = cconj(tb.U[(size_t)(r * n + ii) * nk + k]);
+      for (int jj = 0; jj < n; jj++) {
+        const double2 p = ii <= jj ? rho[(size_t)tri(ii, jj) * nk + k] : cconj(rho[(size_t)tri(jj, ii) * nk + k]);
+        acc = cadd(acc, cmul(cmul(ur, p), tb.U[(size_t)(c * n + jj) * nk + k]));
+      }
+    }
+    out[(size_t)q * nk + k] = acc;
+  }
+}
+
+cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int jc, double2* out, cudaStream_t s) {
+  if (!tb.U || ic < 0 || jc < 0 || ic >= tb.n || jc >= tb.n) return cudaErrorInvalidValue;
+  k_snapshot<<<(tb.nk + 127) / 128, 128, 0, s>>>(tb, rho, ic, jc, out);
+  return cudaGetLastError();
+}
+
+// Band energies of the renormalised Hamiltonian at every k (ascending, as
+// eig_sym returns them; headers/Observables_MPI.h:282-303), for the Edia
+// snapshot files. One thread per k.
+template <int N>
+__global__ void k_band_energies(int nk, const double2* __restrict__ hr, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nk) return;
+  double2 A[N * N], Z[N * N];
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = i; j < N; j++) {
+      const double2 v = hr[(size_t)Tri<N>::idx(i, j) * nk + k];
+      A[i * N + j] = v;
+      A[j * N + i] = cconj(v);
+    }
+  eig_herm_dev<N>(A, Z);
+#pragma unroll
+  for (int i = 0; i < N; i++) out[(size_t)i * nk + k] = A[i * N + i].x;
+}
+
+cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double* out, cudaStream_t s) {
+  const dim3 g((tb.nk + 63) / 64), b(64);
+  switch (tb.n) {
+    case 1: k_band_energies<1><<<g, b, 0, s>>>(tb.nk, hr, out); break;
+    case 2: k_band_energies<2><<<g, b, 0, s>>>(tb.nk, hr, out); break;
+    case 3: k_band_energies<3><<<g, b, 0, s>>>(tb.nk, hr, out); break;
+    case 4: k_band_energies<4><<<g, b, 0, s>>>(tb.nk, hr, out); break;
+    case 5: k_band_energies<5><<<g, b, 0, s>>>(tb.nk, hr, out); break;
+    case 8: k_band_energies<8><<<g, b, 0, s>>>(tb.nk, hr, out); break;
+    case 16: k_band_energies<16><<<g, b, 0, s>>>(tb.nk, hr, out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 int obs_parts(int nk) { return (nk + kObsThreads - 1) / kObsThreads; }
 size_t obs_part_bytes() { return sizeof(ObsPart); }
 

@@ -33,6 +33,11 @@ size_t coulomb_t2T_count(int n2, int ncut);
 size_t coulomb_t1P_count(int n1, int ncut);
 cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2* rho, double2* h, double2* Xout,
                            const double2* X0, cudaStream_t s);
+// Elements (ic, jc), (ic, ic), (jc, jc) of rho in the eigenbasis of tb.U for
+// every k: out[3][nk].
+cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int jc, double2* out, cudaStream_t s);
+// Ascending eigenvalues of the Hermitian planes hr at every k: out[n][nk].
+cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double* out, cudaStream_t s);
 int obs_parts(int nk);
 size_t obs_part_bytes();
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,

@@ -251,7 +251,10 @@ int edus_observables(edus_ctx* ctx, edus_obs* out);
  * on a device: calls that overlap in time (two host threads, or two streams)
  * race on it and must be serialised by the caller. */
 int edus_observables_static(edus_ctx* ctx, edus_obs* out);
-/* Write Output/{EF,J1,J2,Losses,TransientAbs,k_grid}.txt in the reference's format. */
+/* Write Output/{EF,J1,J2,Losses,TransientAbs,k_grid}.txt in the reference's
+ * format, the per-k files of the first output step (H_Eigen_*, H_Wannier_cond,
+ * P_initial_Wannier_, Uk_) and, when the input asks for them, the snapshot
+ * files (P_*_in_Eigenstate_*, Edia_*, t_Ek.txt) taken during edus_run. */
 int edus_write_outputs(edus_ctx* ctx, const char* outdir);
 /* Device time (ms, CUDA events) of the last edus_step/edus_run call and the
  * number of kernel launches it issued. */

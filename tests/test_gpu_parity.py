@@ -209,3 +209,125 @@ def test_edus_run_writes_the_reference_outputs(tmp_path):
 
     kg = json.load(open(os.path.join(GOLDEN, "ab5_kgrid.json")))
     assert hashlib.sha256((tmp_path / "Output" / "k_grid.txt").read_bytes()).hexdigest() == kg["sha256"]
+
+
+def _snapshot_schedule(t0, dt, itfi, res, start, end, step):
+    """Output steps that take a snapshot: t > start + icont * step and t < end,
+    icont counted from -1 (Source_Main/if_resolution.cpp:18-33)."""
+    out, icont, t = [], -1, t0
+    for it in range(itfi + 1):
+        if it % res == 0 and t > start + icont * step and t < end:
+            icont += 1
+            out.append((it, t))
+        t += dt
+    return out
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_per_k_snapshots_match_oracle(workdir, graphs):
+    """PrintPopulation snapshots: Output/t_Ek.txt holds the reference's schedule and
+    every snapshot's three files hold, per k, the top-valence / bottom-conduction
+    elements of the state in the model's eigenbasis (get_P_in_dia,
+    headers/InitParameters.h:232-255) of the oracle's state at that step, to the
+    6 printed digits; a replay after edus_reset writes the same files."""
+    d = f"{workdir}/snap{int(graphs)}"
+    path = W.hbn_rk4(d, n=12, t_fin_fs=1.5, it_res=10)
+    txt = open(path).read().replace("Current\n", "Current\nPrintPopulation 0 60 15\n")
+    open(path, "w").write(txt)
+    p = E.parse_input(path)
+    pb = E.Problem(p, d)
+    ctx = E.Context(pb, use_graphs=graphs)
+    ctx.run()
+    out = f"{d}/Output"
+    ctx.write_outputs(out)
+    sched = _snapshot_schedule(pb.info.t_start, p.dt, pb.info.nsteps - 1, 10, 0.0, 60.0, 15.0)
+    assert len(sched) == 5
+    t_ek = [float(x) for x in open(f"{out}/t_Ek.txt").read().split()]
+    np.testing.assert_allclose(t_ek, [t * TIME_AU_FS for _, t in sched], rtol=1e-5)
+    nb = pb.info.nch + pb.info.nv
+    v, c = nb - 1, nb
+    o = Oracle(p, d)
+    U = o.get("U")
+    done = 0
+    files = {}
+    for m, (it, _) in enumerate(sched):
+        o.run(it - done)
+        done = it
+        P = o.get("P0")
+        Pd = np.einsum("kri,kij,kcj->krc", U.conj(), P, U)
+        for label, (r, cc) in [("P_val_cond_in_Eigenstate", (v, c)), ("P_val_in_Eigenstate", (v, v)),
+                               ("P_cond_in_Eigenstate", (c, c))]:
+            name = f"{out}/{label}_{r}{cc}_{m}.txt"
+            files[name] = open(name).read()
+            got = np.loadtxt(name)
+            assert got.shape == (pb.info.nk, 2)
+            want = np.stack([Pd[:, r, cc].real, Pd[:, r, cc].imag], axis=1)
+            assert np.all(np.abs(got - want) <= 1e-5 * np.abs(want) + 1e-12), (label, m)
+    assert not os.path.exists(f"{out}/P_val_in_Eigenstate_{v}{v}_5.txt")
+    ctx.reset()
+    ctx.run()
+    ctx.write_outputs(out)
+    for name, text in files.items():
+        assert open(name).read() == text
+
+
+def test_coulomb_band_energy_snapshots_match_oracle(workdir):
+    """Print_new_band_dispersion with the Coulomb mean field: Output/Edia_<m>.txt
+    holds, per k, the ascending eigenvalues of the renormalised Hamiltonian of
+    the last RHS evaluation (headers/Observables_MPI.h:282-303, 440-478) at each
+    snapshot of the default print window, against the oracle's."""
+    d = f"{workdir}/edia"
+    path = W.hbn_coulomb(d, n=24, t_fin_fs=0.3, it_res=10)
+    txt = open(path).read().replace("Rytova_Keldysh\n", "Rytova_Keldysh\nPrint_new_band_dispersion\n")
+    open(path, "w").write(txt)
+    p = E.parse_input(path)
+    pb = E.Problem(p, d)
+    ctx = E.Context(pb)
+    ctx.run()
+    out = f"{d}/Output"
+    ctx.write_outputs(out)
+    sched = _snapshot_schedule(pb.info.t_start, p.dt, pb.info.nsteps - 1, 10, p.print_start, p.print_end, p.print_step)
+    assert len(sched) == 2
+    t_ek = [float(x) for x in open(f"{out}/t_Ek.txt").read().split()]
+    np.testing.assert_allclose(t_ek, [t * TIME_AU_FS for _, t in sched], rtol=1e-5)
+    o = Oracle(p, d)
+    done = 0
+    for m, (it, _) in enumerate(sched):
+        o.run(it - done)
+        done = it
+        want = np.linalg.eigvalsh(o.get("Hr"))
+        got = np.loadtxt(f"{out}/Edia_{m}.txt")
+        assert got.shape == want.shape
+        assert np.abs(got - want).max() < 1e-11
+    assert not os.path.exists(f"{out}/Edia_2.txt")
+    assert not any(f.startswith("P_val") for f in os.listdir(out))
+
+
+def test_first_output_step_files_match_oracle(workdir):
+    """The files every reference run writes at its first output step
+    (Print_initial_H_P, Source_Main/if_resolution.cpp:275-328): eigenvalues of
+    the model H (H_Eigen_*), H_cc, the initial state's cc element and U_cc, U_cv,
+    per k, against the oracle's tables to the 6 printed digits."""
+    d = f"{workdir}/init"
+    path = W.hbn_rk4(d, n=12, t_fin_fs=0.05, it_res=1)
+    p = E.parse_input(path)
+    pb = E.Problem(p, d)
+    ctx = E.Context(pb)
+    ctx.run()
+    out = f"{d}/Output"
+    ctx.write_outputs(out)
+    o = Oracle(p, d)
+    H, U, P0 = o.get("H"), o.get("U"), o.get("P0")
+    eps = np.linalg.eigvalsh(H)
+    nb = pb.info.nch + pb.info.nv
+    v, c = nb - 1, nb
+    want = {
+        f"H_Eigen_cond_{c}{c}_0": eps[:, c], f"H_Eigen_val_{v}{v}_0": eps[:, v],
+        f"H_Eigen_val_cond_{v}{c}_0": np.zeros(pb.info.nk), f"H_Wannier_cond_{c}{c}_0": H[:, c, c],
+        f"P_initial_Wannier__{c}{c}_0": P0[:, c, c], f"Uk__{c}{c}_0": U[:, c, c], f"Uk__{c}{v}_0": U[:, c, v],
+    }
+    for name, w in want.items():
+        got = np.loadtxt(f"{out}/{name}.txt")
+        wv = np.stack([np.real(w), np.imag(w)], axis=1)
+        assert got.shape == wv.shape, name
+        assert np.all(np.abs(got - wv) <= 1e-5 * np.abs(wv) + 1e-12), name
