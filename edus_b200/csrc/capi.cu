@@ -1304,12 +1304,9 @@ int edus_runge_kutta_ad(edus_ctx* c, int32_t src, int32_t dst, double dt) {
   // P_dst = P_src + dt * Pv as an element-wise device update
   double2 *s = c ? slot_ptr(c, src) : nullptr, *d = c ? slot_ptr(c, dst) : nullptr;
   if (!s || !d || src == EDUS_SLOT_PV || dst == EDUS_SLOT_PV) return fail(EDUS_EINVAL, "bad slot");
-  std::vector<double2> a(c->plane), v(c->plane);
-  CK(cudaMemcpyAsync(a.data(), s, sizeof(double2) * c->plane, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(v.data(), c->d_Pb, sizeof(double2) * c->plane, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  for (size_t i = 0; i < c->plane; i++) a[i] = cadd(a[i], cscale(v[i], dt));
-  CK(cudaMemcpyAsync(d, a.data(), sizeof(double2) * c->plane, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaSetDevice(c->device));
+  CK(launch_axpy(s, c->d_Pb, dt, d, c->plane, c->stream));
+  c->launches++;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }

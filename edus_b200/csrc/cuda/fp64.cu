@@ -14,6 +14,8 @@
 #include <cstdio>
 
 #include "dev.cuh"
+#include <algorithm>
+
 #include "eig.cuh"
 #include "kernels.hpp"
 
@@ -487,6 +489,22 @@ cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double*
     case 16: k_band_energies<16><<<g, b, 0, s>>>(tb.nk, hr, out); break;
     default: return cudaErrorInvalidValue;
   }
+  return cudaGetLastError();
+}
+
+// d = a + dt * v over n complex entries, multiply then add without
+// contraction, as Runge_Kutta_Ad / Runge_Kutta_Ac (headers/RungeKutta.h:301-355).
+__global__ void k_axpy(const double2* a, const double2* __restrict__ v, double dt, double2* d,
+                       size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 x = a[i], y = v[i];
+    d[i] = make_double2(__dadd_rn(x.x, __dmul_rn(y.x, dt)), __dadd_rn(x.y, __dmul_rn(y.y, dt)));
+  }
+}
+
+cudaError_t launch_axpy(const double2* a, const double2* v, double dt, double2* d, size_t n, cudaStream_t s) {
+  const size_t blocks = std::min<size_t>((n + 255) / 256, 148 * 8);
+  k_axpy<<<(unsigned)(blocks ? blocks : 1), 256, 0, s>>>(a, v, dt, d, n);
   return cudaGetLastError();
 }
 

@@ -38,6 +38,8 @@ cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2*
 cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int jc, double2* out, cudaStream_t s);
 // Ascending eigenvalues of the Hermitian planes hr at every k: out[n][nk].
 cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double* out, cudaStream_t s);
+// d = a + dt * v elementwise (n complex entries; d may alias a).
+cudaError_t launch_axpy(const double2* a, const double2* v, double dt, double2* d, size_t n, cudaStream_t s);
 int obs_parts(int nk);
 size_t obs_part_bytes();
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,

@@ -170,6 +170,12 @@ def serve_requests(count, seed=7, nmin=32, nmax=192, dmin=10.0, dmax=100.0):
 
 
 def serve_line(count=2000, rate=None, fp64_sample=9, seed=7, max_s=None, **kw):
+    """Served mixed-precision stream against the plain FP64 single-solve path on
+    the same work: the FP64 path runs, request by request, a sample stratified by
+    band count (the first fp64_sample / 3 requests of each class, in stream
+    order); its per-class rates give the FP64 time of the whole stream (sum over
+    classes of the class's k-point steps / its rate), and the speed-up is that
+    time over the served span."""
     D = _Dirs()
     specs = serve_requests(count, seed=seed, **kw)
     reqs = [(E.parse_input(p), d) for p, d in (D.instance(s, i) for i, s in enumerate(specs))]
@@ -187,23 +193,32 @@ def serve_line(count=2000, rate=None, fp64_sample=9, seed=7, max_s=None, **kw):
         ids.append(s.submit(p, d))
     s.drain(max_s or 7200)
     st = s.stats()
-    logs = {}
-    for q in range(min(fp64_sample, count)):
-        logs[q] = s.obs(ids[q])
+    infos = [s.info(i) for i in ids]
+    nb_of = [int(x["nbands"]) for x in infos]
+    stream_units = {}
+    for x in infos:
+        stream_units[int(x["nbands"])] = stream_units.get(int(x["nbands"]), 0.0) + float(x["nk"]) * float(x["steps"])
+    per_class = max(1, fp64_sample // max(1, len(stream_units)))
+    sample = []
+    for nb in sorted(stream_units):
+        sample += [q for q in range(count) if nb_of[q] == nb][:per_class]
+    logs = {q: s.obs(ids[q]) for q in sample}
     s.close()
-    # plain FP64 single-solve path, request by request (one request on the GPU at
-    # a time), on the first requests of the stream
-    units = secs = 0.0
+    # plain FP64 single-solve path, request by request (one request on the GPU at a time)
+    cls = {}
     lat = []
     errs = []
-    for q in range(min(fp64_sample, count)):
+    for q in sample:
         path, d = D.instance(specs[q], q)
         u, sec, ref = _single_fp64(path, d)
         lat.append(sec)
-        units += u
-        secs += sec
+        c = cls.setdefault(nb_of[q], [0.0, 0.0, 0])
+        c[0] += u
+        c[1] += sec
+        c[2] += 1
         errs.append(_rel(_J1(logs[q]), _J1(ref)))
-    fp64_rate = units / secs
+    fp64_stream_s = sum(stream_units[nb] / (cls[nb][0] / cls[nb][1]) for nb in stream_units)
+    fp64_sample_rate = sum(c[0] for c in cls.values()) / sum(c[1] for c in cls.values())
     return {
         "metric": "solves/s", "value": st["solves_per_s"], "unit": "solves/s", "higher_is_better": True,
         "dtype": "mixed (fp32 commutator, fp64 rho)", "data": "synthetic",
@@ -213,8 +228,11 @@ def serve_line(count=2000, rate=None, fp64_sample=9, seed=7, max_s=None, **kw):
         "max_latency_s": st["max_latency_s"], "completed": st["completed"], "failed": st["failed"], "span_s": st["span_s"],
         "device_busy_s": st["device_ms"] * 1e-3,
         "peak_active": st["peak_active"], "peak_bytes": st["peak_bytes"],
-        "fp64_request_by_request_sample": {"kpoint_steps_per_s": fp64_rate, "requests": len(lat),
-                                           "mean_latency_s": float(np.mean(lat))},
-        "speedup_vs_fp64_request_by_request": st["kpoint_steps_per_s"] / fp64_rate,
+        "stream_kpoint_steps_by_bands": {str(k): v for k, v in sorted(stream_units.items())},
+        "fp64_request_by_request_sample": {
+            "requests": len(lat), "mean_latency_s": float(np.mean(lat)), "kpoint_steps_per_s": fp64_sample_rate,
+            "by_bands": {str(nb): {"requests": c[2], "kpoint_steps_per_s": c[0] / c[1]} for nb, c in sorted(cls.items())},
+            "stream_seconds": fp64_stream_s},
+        "speedup_vs_fp64_request_by_request": fp64_stream_s / st["span_s"],
         "j1_rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "requests": len(errs)},
     }

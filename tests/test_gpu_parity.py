@@ -81,9 +81,10 @@ def test_stage_updates_match_reference_formulae():
     ctx.get_derivative(abi.SLOT_P0, [0, 1e-3, 0, 0, 0, 0], 0.0, 1)
     Pv = ctx.slot_get(abi.SLOT_PV)
     ctx.runge_kutta_ad(abi.SLOT_P0, abi.SLOT_P1, 0.05)  # Runge_Kutta_Ad: P1 = P0 + dt Pv
-    np.testing.assert_allclose(ctx.slot_get(abi.SLOT_P1), P0 + Pv * 0.05, rtol=0, atol=1e-16)
+    # (multiply, then add: bit for bit the unfused arithmetic of the reference's loops)
+    np.testing.assert_array_equal(ctx.slot_get(abi.SLOT_P1), P0 + Pv * 0.05)
     ctx.runge_kutta_ac(abi.SLOT_P1, 0.05)  # Runge_Kutta_Ac: P1 += dt Pv
-    np.testing.assert_allclose(ctx.slot_get(abi.SLOT_P1), (P0 + Pv * 0.05) + Pv * 0.05, rtol=0, atol=1e-16)
+    np.testing.assert_array_equal(ctx.slot_get(abi.SLOT_P1), (P0 + Pv * 0.05) + Pv * 0.05)
 
 
 def test_golden_run_on_gpu():
