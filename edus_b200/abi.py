@@ -31,6 +31,7 @@ EDUS_PREC_FP64 = 0
 EDUS_PREC_MIXED = 1
 
 EDUS_MAX_PUMPS = 8
+EDUS_MAX_TABSK = 64
 EDUS_MAX_HOPPING = 8
 EDUS_MAX_BANDS = 16
 EDUS_STRLEN = 256
@@ -109,6 +110,9 @@ class Params(C.Structure):
         ("sample_110", C.c_int32),
         ("vectorization", C.c_int32),
         ("precision", C.c_int32),
+        ("tabs_k", C.c_int32),
+        ("n_tabs_k", C.c_int32),
+        ("tabs_k_pts", (C.c_double * 3) * EDUS_MAX_TABSK),
     ]
 
 

@@ -1431,6 +1431,14 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
     f2.open(d + "/J2.txt");
   }
   if (c->P.p.tabs) ft.open(d + "/TransientAbs.txt");
+  // k-resolved transient absorption: one file per TAbsK point, opened and left
+  // empty as the reference leaves it (Source_Main/open_files.cpp:43-55)
+  for (int i = 0; c->P.p.tabs_k && i < c->P.p.n_tabs_k; i++) {
+    std::ostringstream name;
+    name << d << "/TAbsK_" << c->P.p.tabs_k_pts[i][0] << "_" << c->P.p.tabs_k_pts[i][1] << "_" << c->P.p.tabs_k_pts[i][2] << ".txt";
+    std::ofstream fk(name.str());
+    if (!fk) return fail(EDUS_EIO, "cannot write %s", name.str().c_str());
+  }
   if (!fe || !fl) return fail(EDUS_EIO, "cannot write into %s", outdir);
   const int ncv = c->n;
   for (const edus_obs& o : log) {

@@ -658,14 +658,34 @@ extern "C" int edus_parse_input(const char* path, edus_params* out) {
           else if (ieq(k, "TransientAbsorption") || ieq(k, "TAbs"))
             P.tabs = 1;
           else if (ieq(k, "kresolvedTAbs") || ieq(k, "kTAbs") || ieq(k, "kTransientAbsorption"))
-            return fail(EDUS_EUNSUPPORTED, "k-resolved transient absorption is not built");
+            P.tabs_k = 1;
           else
             return fail(EDUS_EPARSE, "option %s not available in the observables.", k.c_str());
         }
         if (!r.next(s)) return fail(EDUS_EPARSE, "Can't find the end of observables section.");
       }
     } else if (ieq(key, "TAbsK")) {
-      return fail(EDUS_EUNSUPPORTED, "TAbsK section is not built");
+      // headers/ReadInput.h:1047-1083: the number of k points, then one
+      // "k0 k1 k2" line each (crystal coordinates)
+      if (!P.tabs_k)
+        return fail(EDUS_EPARSE,
+                    "Error in the input. You defined the section TAbsK without putting it in the observables.");
+      s.clear();
+      while (s.empty())
+        if (!r.next(s)) return fail(EDUS_EPARSE, "Can't find the end of TAbsK section.");
+      auto t = split(s, s.size());
+      if (t.size() != 1) return fail(EDUS_EPARSE, "Error in TAbsK. you didn't define in the first line the number of k points.");
+      const int nt = std::atoi(t[0].c_str());
+      if (nt < 0) return fail(EDUS_EPARSE, "Error in TAbsK: %d k points", nt);
+      if (nt > EDUS_MAX_TABSK) return fail(EDUS_EUNSUPPORTED, "TAbsK: %d k points (at most %d)", nt, EDUS_MAX_TABSK);
+      P.n_tabs_k = nt;
+      for (int i = 0; i < nt; i++) {
+        if (!r.next(s)) s.clear();
+        auto q = split(s, s.size());
+        if (q.size() != 3) return fail(EDUS_EPARSE, "Error in defining k points in TAbsK. Please review your input.");
+        for (int j = 0; j < 3; j++) P.tabs_k_pts[i][j] = to_d(q, j);
+      }
+      rc = end_section(r, "TAbsK");
     } else if (ieq(key, "Coulomb")) {
       P.coulomb = 1;
       if (!r.next(s)) return fail(EDUS_EPARSE, "Can't find the end of Coulomb section.");

@@ -56,6 +56,7 @@ enum { EDUS_PREC_FP64 = 0, EDUS_PREC_MIXED = 1 };
 #define EDUS_MAX_PUMPS 8
 #define EDUS_MAX_HOPPING 8
 #define EDUS_MAX_BANDS 16
+#define EDUS_MAX_TABSK 64  /* k points of a TAbsK section */
 #define EDUS_STRLEN 256
 
 /* One laser pulse with every derived quantity resolved (headers/Laser.h:1-51).
@@ -119,6 +120,12 @@ typedef struct {
   int32_t vectorization;
   /* execution options (not in the reference) */
   int32_t precision;             /* EDUS_PREC_* */
+  /* k-resolved transient absorption (observables{kTAbs} and the TAbsK
+   * section): the reference reads the k points and opens one file per point,
+   * Output/TAbsK_<k0>_<k1>_<k2>.txt, that nothing writes into */
+  int32_t tabs_k;
+  int32_t n_tabs_k;
+  double tabs_k_pts[EDUS_MAX_TABSK][3];
 } edus_params;
 
 /* Observables at one output instant (headers/Observables_MPI.h). */

@@ -311,6 +311,9 @@ def test_first_output_step_files_match_oracle(workdir):
     per k, against the oracle's tables to the 6 printed digits."""
     d = f"{workdir}/init"
     path = W.hbn_rk4(d, n=12, t_fin_fs=0.05, it_res=1)
+    # with kTAbs: the reference opens one TAbsK file per listed k point and writes nothing into it
+    txt = open(path).read().replace("Current\n", "Current\nkTAbs\n") + "\nTAbsK{\n1\n0 0.1 0.2\n}\n"
+    open(path, "w").write(txt)
     p = E.parse_input(path)
     pb = E.Problem(p, d)
     ctx = E.Context(pb)
@@ -327,6 +330,7 @@ def test_first_output_step_files_match_oracle(workdir):
         f"H_Eigen_val_cond_{v}{c}_0": np.zeros(pb.info.nk), f"H_Wannier_cond_{c}{c}_0": H[:, c, c],
         f"P_initial_Wannier__{c}{c}_0": P0[:, c, c], f"Uk__{c}{c}_0": U[:, c, c], f"Uk__{c}{v}_0": U[:, c, v],
     }
+    assert os.path.getsize(f"{out}/TAbsK_0_0.1_0.2.txt") == 0
     for name, w in want.items():
         got = np.loadtxt(f"{out}/{name}.txt")
         wv = np.stack([np.real(w), np.imag(w)], axis=1)

@@ -112,13 +112,25 @@ def test_coulomb_and_decoherence(tmp_path):
         ("decoherence{\ncorehole 1 furlongs\n}\n", abi.EDUS_EPARSE),
         ("laserpump sin2 {\nsigma 2\n}\n", abi.EDUS_EPARSE),
         ("laserpump sin2 {\npolarization linear 0 0 1\n}\n", abi.EDUS_EPARSE),
-        ("observables{\nkTAbs\n}\n", abi.EDUS_EUNSUPPORTED),
+        ("TAbsK{\n1\n0 0.1 0.2\n}\nobservables{\nkTAbs\n}\n", abi.EDUS_EPARSE),
+        ("observables{\nkTAbs\n}\nTAbsK{\n2 3\n}\n", abi.EDUS_EPARSE),
+        ("observables{\nkTAbs\n}\nTAbsK{\n2\n0 0.1 0.2\n0 0.3\n}\n", abi.EDUS_EPARSE),
+        ("observables{\nkTAbs\n}\nTAbsK{\n65\n}\n", abi.EDUS_EUNSUPPORTED),
     ],
 )
 def test_errors_are_codes_not_exits(tmp_path, extra, code):
     with pytest.raises(E.EdusError) as ei:
         E.parse_input(_write(tmp_path, BASE.format(tdse="dt 0.1", extra=extra)))
     assert ei.value.code == code
+
+
+def test_tabsk_section(tmp_path):
+    """headers/ReadInput.h:1032, 1047-1083: kTAbs in the observables, then the
+    TAbsK section with the number of k points and one point per line."""
+    extra = "observables{\nCurrent\nkTAbs\n}\nTAbsK{\n\n2\n0 0.1 0.2\n0 -0.25 0.5\n}\n"
+    p = E.parse_input(_write(tmp_path, BASE.format(tdse="dt 0.1", extra=extra)))
+    assert p.tabs_k == 1 and p.n_tabs_k == 2 and p.current == 1
+    assert [list(p.tabs_k_pts[i]) for i in range(2)] == [[0.0, 0.1, 0.2], [0.0, -0.25, 0.5]]
 
 
 def test_missing_file():
