@@ -15,7 +15,8 @@ from .lib import (  # noqa: F401
     parse_input,
     default_params,
     library_path,
+    coulomb_generate,
 )
 from . import abi  # noqa: F401
 
-__all__ = ["EdusError", "Problem", "Context", "Batch", "Server", "load_library", "parse_input", "default_params", "abi", "library_path"]
+__all__ = ["EdusError", "Problem", "Context", "Batch", "Server", "load_library", "parse_input", "default_params", "abi", "library_path", "coulomb_generate"]

@@ -228,6 +228,10 @@ class ServerOptions(C.Structure):
     ]
 
 
+class CoulombGenOptions(C.Structure):
+    _fields_ = [("device", C.c_int32), ("n_sum", C.c_int32), ("n_sum_screen", C.c_int32)]
+
+
 class RequestInfo(C.Structure):
     _fields_ = [
         ("status", C.c_int32),

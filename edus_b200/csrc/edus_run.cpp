@@ -93,6 +93,21 @@ int main(int argc, char** argv) {
   edus_params p;
   int rc = edus_parse_input(input.c_str(), &p);
   if (rc) return die(input.c_str(), rc);
+  if (p.coulomb && !p.read_from_files) {
+    // the reference computes the Coulomb tables when it does not read them
+    // (Source_Main/Fourier_Coulomb.cpp:95-500): generate them on the device
+    // into Output/Coulomb and read them back as Read_Coulomb_from_files does
+    edus_coulomb_gen_options go;
+    edus_coulomb_gen_options_default(&go);
+    go.device = device;
+    char label[sizeof(p.coulomb_label)];
+    int32_t ng = 0;
+    rc = edus_coulomb_generate(&p, workdir.c_str(), &go, label, (int32_t)sizeof(label), &ng);
+    if (rc) return die("Coulomb coefficients", rc);
+    printf("edus_run: Coulomb tables %s (%d G vectors) in %s/Output/Coulomb\n", label, (int)ng, workdir.c_str());
+    p.read_from_files = 1;
+    snprintf(p.coulomb_label, sizeof(p.coulomb_label), "%s", label);
+  }
   edus_problem* pb = nullptr;
   rc = edus_problem_create(&p, workdir.c_str(), &pb);
   if (rc) return die("problem set-up", rc);

@@ -608,7 +608,8 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P, bool de
   if (p.coulomb) {
     if (p.diag_basis) return fail(EDUS_EUNSUPPORTED, "Coulomb_diag_basis is not built (Wannier-basis Coulomb is)");
     if (!p.read_from_files)
-      return fail(EDUS_EUNSUPPORTED, "Coulomb coefficients must be read from files (Read_Coulomb_from_files)");
+      return fail(EDUS_EUNSUPPORTED,
+                  "Coulomb coefficients are read from files (Read_Coulomb_from_files); edus_coulomb_generate computes them");
     if (p.ncut < 1 || p.ncut > 64) return fail(EDUS_EINVAL, "Ncut %d out of range", p.ncut);
     if (P.n1 != P.n2) return fail(EDUS_EINVAL, "Coulomb needs a square in-plane grid (Coulomb.h:285)");
     P.ncut = p.ncut;

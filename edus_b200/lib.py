@@ -65,6 +65,8 @@ def load_library():
         "edus_slot_set": (C.c_int, [vp, i32, vp]),
         "edus_slot_get": (C.c_int, [vp, i32, vp]),
         "edus_coulomb_hk": (C.c_int, [vp, i32, vp]),
+        "edus_coulomb_gen_options_default": (C.c_int, [P(abi.CoulombGenOptions)]),
+        "edus_coulomb_generate": (C.c_int, [P(abi.Params), cp, P(abi.CoulombGenOptions), C.c_char_p, i32, P(i32)]),
         "edus_observables_static": (C.c_int, [vp, P(abi.Obs)]),
         "edus_batch_options_default": (C.c_int, [P(abi.BatchOptions)]),
         "edus_batch_create": (C.c_int, [P(abi.BatchOptions), P(vp)]),
@@ -120,6 +122,24 @@ def parse_input(path):
     p = abi.Params()
     _check(L.edus_parse_input(os.fsencode(path), C.byref(p)), "edus_parse_input")
     return p
+
+
+def coulomb_generate(params, workdir, device=0, n_sum=None, n_sum_screen=None):
+    """Coulomb tables of a run computed on the GPU (edus_coulomb_generate):
+    writes workdir/Output/Coulomb/*<label>.txt; returns (label, number of G)."""
+    L = load_library()
+    o = abi.CoulombGenOptions()
+    _check(L.edus_coulomb_gen_options_default(C.byref(o)), "edus_coulomb_gen_options_default")
+    o.device = device
+    if n_sum is not None:
+        o.n_sum = n_sum
+    if n_sum_screen is not None:
+        o.n_sum_screen = n_sum_screen
+    lab = C.create_string_buffer(512)
+    ng = C.c_int32()
+    _check(L.edus_coulomb_generate(C.byref(params), os.fsencode(workdir), C.byref(o), lab, 512, C.byref(ng)),
+           "edus_coulomb_generate")
+    return lab.value.decode(), ng.value
 
 
 class Problem:

@@ -203,6 +203,27 @@ int edus_model_hud(const edus_problem* pb, const double kcrys[3], double* H, dou
 /* sizeof of the ABI structs: params, obs, problem_info, options (for bindings). */
 int edus_struct_sizes(int64_t out[4]);
 
+/* --------------------------------------------- Coulomb coefficient generator */
+typedef struct {
+  int32_t device;        /* CUDA device ordinal */
+  int32_t n_sum;         /* Simpson points per axis of the coefficient fit (reference: 4999) */
+  int32_t n_sum_screen;  /* ... of the screening constant (reference: 39999) */
+} edus_coulomb_gen_options;
+int edus_coulomb_gen_options_default(edus_coulomb_gen_options* o);
+/* Compute the Coulomb tables of a run on the GPU, as the reference does when
+ * its Coulomb section has no Read_Coulomb_from_files
+ * (Source_Main/Fourier_Coulomb.cpp:95-500): the Fourier coefficients A, B, C, D
+ * of the lattice-summed Thomas-Fermi / Rytova-Keldysh interaction (Simpson
+ * integrals over the zone, every reciprocal vector inside G_distance), the
+ * Hartree table and the screening constant. Writes
+ * workdir/Output/Coulomb/{A,B,C,D}_coeff<label>.txt, V_Hartree_<label>.txt and
+ * Screen_const_<label>.txt in the reference's formats, label =
+ * "G_num<G>_Ncut<Ncut><labelInput>" (returned in label_out, the number of G
+ * vectors in g_num_out); a run reads them with Read_Coulomb_from_files and
+ * labelInput <label>. Up to 4 bands; opt may be null (the reference's grids). */
+int edus_coulomb_generate(const edus_params* p, const char* workdir, const edus_coulomb_gen_options* opt, char* label_out,
+                          int32_t label_cap, int32_t* g_num_out);
+
 /* ------------------------------------------------------- device context */
 typedef struct edus_ctx edus_ctx;
 

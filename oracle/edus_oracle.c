@@ -1690,6 +1690,230 @@ int orc_clock(const orc* o, int* it, double* t, double* dt) {
   return 0;
 }
 
+/* ------------------------------------------------- Coulomb coefficient generator */
+
+/* headers/Coulomb.h:60-83 (Coloumb_THh_F) */
+static double gen_v(double q_mod, double qTF, double eps_area, double r0, int rk) {
+  double Num = 2 * PI, Den;
+  if (rk)
+    Den = eps_area * sqrt(q_mod + qTF * qTF) * (sqrt(q_mod) * r0 + 1.0);
+  else
+    Den = eps_area * sqrt(q_mod + qTF * qTF);
+  return Num / Den;
+}
+
+/* headers/Coulomb.h:87-157 (Create_Wq_with_G_sum): Wq[n][n] at (qx, qy) */
+static void gen_wq(const orc* o, double qx, double qy, const int* G, int ng, const double* disp, double qTF, double eps_area,
+                   int hartree, cplx* Wq) {
+  int n = o->ncv;
+  for (int i = 0; i < n * n; i++) Wq[i] = 0;
+  for (int g = 0; g < ng; g++) {
+    double c[3], x[3];
+    if (o->p.sample_110) {
+      c[0] = qx + G[2 * g];
+      c[1] = qy + G[2 * g + 1];
+      c[2] = 0.0;
+    } else {
+      c[0] = 0.0;
+      c[1] = qx + G[2 * g];
+      c[2] = qy + G[2 * g + 1];
+    }
+    crys_to_cart(o, c, x);
+    double Vq;
+    if (hartree && ((double)G[2 * g] + (double)G[2 * g + 1]) < 1e-16)
+      Vq = 0.0;
+    else
+      Vq = gen_v(x[0] * x[0] + x[1] * x[1] + x[2] * x[2], qTF, eps_area, o->p.r0, o->p.rytova_keldysh);
+    for (int ic = 0; ic < n; ic++)
+      for (int jc = ic; jc < n; jc++) {
+        if (ic + jc == 0) Wq[0] += Vq;
+        if (jc != ic) {
+          double phi = 0.0;
+          for (int i = 0; i < 3; i++) phi += x[i] * (disp[ic * 3 + i] - disp[jc * 3 + i]);
+          Wq[ic * n + jc] += Vq * cexp(I * phi);
+        }
+      }
+    for (int ic = 1; ic < n; ic++) Wq[ic * n + ic] = Wq[0];
+  }
+}
+
+/* Source_Main/Fourier_Coulomb.cpp:95-500 with the Simpson grid of
+ * headers/integrationWeight.h:5-15. what: bit 0 the Hartree table, bit 1 the
+ * Fourier coefficients A..D, bit 2 the screening constant (needs bit 1).
+ * n_sum / n_sum_screen: grid points per axis (the reference: 4999, 39999). */
+int orc_coulomb_generate(const edus_params* p, const char* workdir, int what, int n_sum, int n_sum_screen, double* A,
+                         double* B, double* C, double* D, double* screen, double* VH, int* g_num) {
+  edus_params q = *p;
+  q.coulomb = 0;
+  orc* o = NULL;
+  int rc = orc_create(&q, workdir, &o);
+  if (rc) return rc;
+  const int n = o->ncv, n2 = n * n, ncut = p->ncut;
+  /* Displacement_orb: diagonal dipoles at k = (0, 0.3, 0.1) (Fourier_Coulomb.cpp:41-67) */
+  double disp[EDUS_MAX_BANDS * 3];
+  {
+    double kc[3] = {0.0, 0.3, 0.1};
+    if (p->sample_110) {
+      kc[0] = 0.3;
+      kc[1] = 0.1;
+      kc[2] = 0.0;
+    }
+    for (int ic = 0; ic < n; ic++)
+      for (int x = 0; x < 3; x++) {
+        cplx d;
+        if (p->mode == EDUS_MODE_WANNIER) {
+          const cplx* R = x == 0 ? o->xR : (x == 1 ? o->yR : o->zR);
+          d = wannier_sum(o, R, ic, ic, kc);
+        } else {
+          d = tb_dipole(o, ic, ic, x);
+        }
+        disp[ic * 3 + x] = creal(d);
+      }
+  }
+  double det_b = p->sample_110 ? fabs(p->b[0][0] * p->b[1][1] - p->b[0][1] * p->b[1][0])
+                               : fabs(p->b[1][1] * p->b[2][2] - p->b[1][2] * p->b[2][1]);
+  double eps_area = p->epsilon_static * o->det_a;
+  double gdist = p->G_distance * sqrt(det_b);
+  /* G list (Fourier_Coulomb.cpp:113-136) */
+  int bord = (int)(sqrt(9999.0 * 9999.0) / 2);
+  int cap = 1 << 20, ng = 0;
+  int* G = malloc(sizeof(int) * 2 * cap);
+  for (int ix = -bord; ix <= bord; ix++)
+    for (int iy = -bord; iy <= bord; iy++) {
+      double c[3] = {0.0, (double)ix, (double)iy}, x[3];
+      if (p->sample_110) {
+        c[0] = ix;
+        c[1] = iy;
+        c[2] = 0.0;
+      }
+      crys_to_cart(o, c, x);
+      if (sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]) < gdist) {
+        if (ng == cap) {
+          cap *= 2;
+          G = realloc(G, sizeof(int) * 2 * cap);
+        }
+        G[2 * ng] = ix;
+        G[2 * ng + 1] = iy;
+        ng++;
+      }
+    }
+  if (g_num) *g_num = ng;
+  cplx Wq[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+  if (what & 1) {
+    /* Hartree table (Fourier_Coulomb.cpp:166-214) */
+    gen_wq(o, 0.0, 0.0, G, ng, disp, p->qTF, eps_area, 1, Wq);
+    cplx V[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+    memcpy(V, Wq, sizeof(cplx) * n2);
+    for (int ic = 0; ic < n; ic++) {
+      if (ic > 0) V[ic * n + ic] = V[0];
+      for (int jc = ic; jc < n; jc++) {
+        V[jc * n + ic] = creal(V[ic * n + jc]);
+        V[ic * n + jc] = V[jc * n + ic];
+      }
+    }
+    for (int i = 0; i < n2; i++) VH[i] = creal(V[i]);
+  }
+  cplx* cAc = calloc((size_t)ncut * ncut * n2, sizeof(cplx));
+  cplx* cBc = calloc((size_t)ncut * ncut * n2, sizeof(cplx));
+  cplx* cCc = calloc((size_t)ncut * ncut * n2, sizeof(cplx));
+  cplx* cDc = calloc((size_t)ncut * ncut * n2, sizeof(cplx));
+  if (what & 2) {
+    /* Simpson grid (headers/integrationWeight.h:5-15) and the coefficient sums (Fourier_Coulomb.cpp:233-275) */
+    double h = 1.0 / (n_sum - 1), hs = 3.0 * (n_sum - 1);
+    double* qg = malloc(sizeof(double) * n_sum);
+    double* sp = malloc(sizeof(double) * n_sum);
+    for (int i = 0; i < n_sum; i++) qg[i] = -0.5 + i * h;
+    sp[0] = 1 / hs;
+    for (int i = 1; i < n_sum; i += 2) sp[i] = 4.0 / hs;
+    for (int i = 2; i < n_sum; i += 2) sp[i] = 2.0 / hs;
+    sp[n_sum - 1] = 1 / hs;
+    for (long iq = 0; iq < (long)n_sum * n_sum; iq++) {
+      int ix = (int)(iq / n_sum), iy = (int)(iq % n_sum);
+      double spxy = sp[ix] * sp[iy], qx = qg[ix], qy = qg[iy];
+      gen_wq(o, qx, qy, G, ng, disp, p->qTF, eps_area, 0, Wq);
+      for (int mm = 0; mm < ncut * ncut; mm++) {
+        int m = mm / ncut, nn = mm % ncut;
+        double mq = 2 * PI * m * qx, nq = 2 * PI * nn * qy;
+        double tmc = cos(mq), tms = sin(mq), tnc = cos(nq), tns = sin(nq);
+        double dA = 4 * spxy * tmc * tnc, dD = 4 * spxy * tms * tns, dB = 4 * spxy * tmc * tns, dC = 4 * spxy * tms * tnc;
+        double fac = (m == 0 && nn == 0) ? 0.25 : ((m == 0 || nn == 0) ? 0.5 : 1.0);
+        for (int ic = 0; ic < n; ic++)
+          for (int jc = ic; jc < n; jc++) {
+            int il = ic * n + jc;
+            cplx Vq = Wq[il];
+            if (ic == 0 && jc == 0) {
+              cAc[(size_t)mm * n2] += creal(Vq * dA * fac);
+              cDc[(size_t)mm * n2] += creal(Vq * dD * fac);
+            }
+            if (jc != ic) {
+              cAc[(size_t)mm * n2 + il] += creal(dA * Vq * fac);
+              cBc[(size_t)mm * n2 + il] += I * cimag(dB * Vq * fac);
+              cCc[(size_t)mm * n2 + il] += I * cimag(dC * Vq * fac);
+              cDc[(size_t)mm * n2 + il] += creal(dD * Vq * fac);
+            }
+          }
+      }
+    }
+    free(qg);
+    free(sp);
+    for (size_t i = 0; i < (size_t)ncut * ncut * n2; i++) {
+      A[2 * i] = creal(cAc[i]);
+      A[2 * i + 1] = cimag(cAc[i]);
+      B[2 * i] = creal(cBc[i]);
+      B[2 * i + 1] = cimag(cBc[i]);
+      C[2 * i] = creal(cCc[i]);
+      C[2 * i + 1] = cimag(cCc[i]);
+      D[2 * i] = creal(cDc[i]);
+      D[2 * i + 1] = cimag(cDc[i]);
+    }
+  }
+  if ((what & 4) && (what & 2)) {
+    /* screening constant (Fourier_Coulomb.cpp:369-470), order 0 */
+    int N = n_sum_screen;
+    double h = 1.0 / (N - 1), dk2 = 1. / ((double)N * N);
+    double q_peak = p->qTF < 0.02 ? 0.02 : p->qTF;
+    cplx sum[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+    for (int i = 0; i < n2; i++) sum[i] = 0;
+    for (long iq = 0; iq < (long)N * N; iq++) {
+      double qx = -0.5 + (iq / N) * h, qy = -0.5 + (iq % N) * h;
+      double c[3] = {0.0, qx, qy}, x[3];
+      if (p->sample_110) {
+        c[0] = qx;
+        c[1] = qy;
+        c[2] = 0.0;
+      }
+      crys_to_cart(o, c, x);
+      double q_mod = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+      if (!(q_mod < q_peak * q_peak && q_mod > pow(10, -17))) continue;
+      gen_wq(o, qx, qy, G, ng, disp, 0.0, eps_area, 0, Wq);
+      for (int ic = 0; ic < n; ic++)
+        for (int jc = ic; jc < n; jc++) {
+          int il = ic * n + jc;
+          cplx VF = 0.0;
+          for (int m = 0; m < ncut; m++)
+            for (int nn = 0; nn < ncut; nn++) {
+              double tmc = cos(2 * PI * m * qx), tms = sin(2 * PI * m * qx);
+              double tnc = cos(2 * PI * nn * qy), tns = sin(2 * PI * nn * qy);
+              size_t ix = (size_t)(nn + ncut * m) * n2 + il;
+              VF += cAc[ix] * tmc * tnc + cBc[ix] * tmc * tns + cCc[ix] * tms * tnc + cDc[ix] * tms * tns;
+            }
+          sum[il] += (Wq[il] - VF) * dk2;
+        }
+    }
+    for (int i = 0; i < n2; i++) {
+      screen[2 * i] = creal(sum[i]);
+      screen[2 * i + 1] = cimag(sum[i]);
+    }
+  }
+  free(cAc);
+  free(cBc);
+  free(cCc);
+  free(cDc);
+  free(G);
+  orc_free(o);
+  return 0;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -41,6 +41,12 @@ int orc_observables(orc* o, const double* P, edus_obs* out);
 /* Time loop clock after orc_run. */
 int orc_clock(const orc* o, int* it, double* t, double* dt);
 int orc_num_threads(void);
+/* Coulomb coefficient generator (Source_Main/Fourier_Coulomb.cpp:95-500):
+ * what = 1 Hartree table VH[n][n], 2 coefficients A..D [ncut^2][n^2] complex,
+ * 4 screening constant [n^2] complex (with 2); grid points per axis n_sum,
+ * n_sum_screen (the reference uses 4999 and 39999). */
+int orc_coulomb_generate(const edus_params* p, const char* workdir, int what, int n_sum, int n_sum_screen, double* A,
+                         double* B, double* C, double* D, double* screen, double* VH, int* g_num);
 
 #ifdef __cplusplus
 }

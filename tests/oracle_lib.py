@@ -35,8 +35,30 @@ def load():
     L.orc_coulomb_hk.argtypes = [vp, vp, vp]
     L.orc_observables.argtypes = [vp, vp, P(abi.Obs)]
     L.orc_clock.argtypes = [vp, P(C.c_int), P(C.c_double), P(C.c_double)]
+    L.orc_coulomb_generate.argtypes = [P(abi.Params), C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp,
+                                       P(C.c_int)]
     _L = L
     return L
+
+
+def coulomb_generate(params, workdir, what, n_sum=4999, n_sum_screen=39999):
+    """The oracle's Coulomb coefficient generator (Source_Main/Fourier_Coulomb.cpp:95-500):
+    dict of VH [n][n], A..D [ncut^2][n^2], screen [n^2] (complex) and g_num."""
+    L = load()
+    n = params.nb[0] + params.nb[1] + params.nb[2]
+    nc = params.ncut * params.ncut * n * n
+    A, B, Cc, D = (np.zeros(nc, np.complex128) for _ in range(4))
+    sc = np.zeros(n * n, np.complex128)
+    VH = np.zeros(n * n, np.float64)
+    ng = C.c_int()
+    rc = L.orc_coulomb_generate(C.byref(params), os.fsencode(workdir), int(what), int(n_sum), int(n_sum_screen),
+                                A.ctypes.data, B.ctypes.data, Cc.ctypes.data, D.ctypes.data, sc.ctypes.data,
+                                VH.ctypes.data, C.byref(ng))
+    if rc != 0:
+        raise RuntimeError(f"orc_coulomb_generate failed: {rc}")
+    sh = (params.ncut * params.ncut, n * n)
+    return {"VH": VH.reshape(n, n), "A": A.reshape(sh), "B": B.reshape(sh), "C": Cc.reshape(sh), "D": D.reshape(sh),
+            "screen": sc, "g_num": ng.value}
 
 
 class Oracle:
