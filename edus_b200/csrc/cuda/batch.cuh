@@ -104,7 +104,7 @@ cudaError_t launch_obs(int N, int kt, bool mixed, const View& v, int parity, int
 int stage_grid(int N, int kt, int occ, bool mixed);
 int obs_grid(int N, bool mixed, int max_inst);
 bool class_supported(int N, int kt);
-// Matrix-product form of the stage kernel (batch_mm.cu), register profile 2.
+// Matrix-product form of the stage kernel (batch_mm.cu), register profile 2 (FP64 batches).
 bool mm_supported(int N, int kt);
 cudaError_t launch_stage_mm(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s);
 int stage_grid_mm(int N, int kt, bool mixed);

@@ -4,15 +4,14 @@
 // The commutator of headers/RungeKutta.h:158-208 in the reference's transposed
 // convention is beta_ij = sum_l H~_jl P_il - conj(H~_il P_jl) = C_ij - conj(C_ji)
 // with C = P H~^T. Per tile of KT k points:
-//   (A) element items (k, i <= j): loads, k-gradient gathers, H~ (and for mixed
-//       precision E.D, rho_eq, the FP64 band energies) into shared memory;
+//   (A) element items (k, i <= j): loads, k-gradient gathers and H~ into
+//       shared memory;
 //   (B) every thread accumulates a BR x BC block of C for one k point in
 //       registers: 1 / BR + 1 / BC shared loads per complex multiply-add,
 //       against 2 for the element-parallel form;
 //   (C) element items: beta from C, RWA, k-gradient, RK4 stage update.
-// Same arithmetic and precision rules as k_bstage (batch_kernels.cu).
-#include <type_traits>
-
+// Same arithmetic as the FP64 k_bstage (batch_kernels.cu). FP64 only: a
+// mixed-precision batch runs the element-parallel or the staged forms.
 #include "batch.cuh"
 
 namespace edus {
@@ -44,25 +43,23 @@ template <class To, class From>
 __device__ __forceinline__ To cv(From a) { return mk<To>((decltype(To::x))a.x, (decltype(To::x))a.y); }
 
 // shape of one instantiation
-template <int N, bool MIX>
+template <int N>
 struct MM {
-  using C = typename std::conditional<MIX, float2, double2>::type;
-  using S = C;
-  static constexpr int BR = MIX ? 4 : 2;      // rows of C per thread
+  using C = double2;
+  static constexpr int BR = 2;                // rows of C per thread
   static constexpr int BC = 4;                // columns of C per thread
   static constexpr int TPK = (N / BR) * (N / BC);  // threads per k point
 };
 
-template <int N, int KT, bool MIX>
+template <int N, int KT>
 struct MMLayout {
-  using C = typename MM<N, MIX>::C;
+  using C = typename MM<N>::C;
   static constexpr int RS = N * KT + 1;     // padded row of a shared matrix
   static constexpr int MAT = N * RS;        // one full matrix, all KT k points
   static constexpr int NT = TriM<N>::NT;
   static constexpr size_t bytes() {
-    return sizeof(C) * (size_t)MAT * (MIX ? 5 : 3)      // P, H, C (+ Q, X)
-           + sizeof(C) * (size_t)NT * KT                // k-gradient term per element
-           + (MIX ? sizeof(double) * (size_t)N * KT : 0);  // FP64 band energies
+    return sizeof(C) * (size_t)MAT * 3      // P, H, C
+           + sizeof(C) * (size_t)NT * KT;   // k-gradient term per element
   }
 };
 
@@ -87,23 +84,20 @@ __device__ __forceinline__ int nb_of(const Inst* I, int k, int b) {
   return j1 * I->n2 + j2;
 }
 
-template <int N, int KT, bool MIX>
-__global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int stage, int parity) {
-  using L = MMLayout<N, KT, MIX>;
-  using C = typename MM<N, MIX>::C;
-  using S = typename MM<N, MIX>::S;
+template <int N, int KT>
+__global__ void __launch_bounds__(KT* MM<N>::TPK) k_bstage_mm(View v, int stage, int parity) {
+  using L = MMLayout<N, KT>;
+  using C = typename MM<N>::C;
+  using S = C;
   using R = decltype(C::x);
   constexpr int NT = L::NT, RS = L::RS, MAT = L::MAT;
-  constexpr int BR = MM<N, MIX>::BR, BC = MM<N, MIX>::BC;
-  constexpr int NTHR = KT * MM<N, MIX>::TPK;
+  constexpr int BR = MM<N>::BR, BC = MM<N>::BC;
+  constexpr int NTHR = KT * MM<N>::TPK;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* sP = reinterpret_cast<C*>(smem_raw);
   C* sH = sP + MAT;
   C* sC = sH + MAT;
-  C* sQ = sC + MAT;                     // mixed only
-  C* sX = sQ + (MIX ? MAT : 0);         // mixed only
-  C* sG = sX + (MIX ? MAT : 0);         // [NT][KT]
-  double* sEd = reinterpret_cast<double*>(sG + NT * KT);  // mixed only: [N][KT]
+  C* sG = sC + MAT;  // [NT][KT]
   __shared__ Setup su[2];
   __shared__ int snb[2][kBatchMaxNb][KT];
   const int tid = threadIdx.x;
@@ -155,10 +149,6 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
         const int oij = i * RS + j * KT + kl, oji = j * RS + i * KT + kl;
         if (k >= nk) {
           sP[oij] = sP[oji] = sH[oij] = sH[oji] = mk<C>(0, 0);
-          if (MIX) {
-            sQ[oij] = sQ[oji] = sX[oij] = sX[oji] = mk<C>(0, 0);
-            if (i == j) sEd[i * KT + kl] = 0.;
-          }
           sG[e * KT + kl] = mk<C>(0, 0);
           continue;
         }
@@ -168,12 +158,6 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
         S De[3];
 #pragma unroll
         for (int x = 0; x < 3; x++) De[x] = ((fmask >> x) & 1) ? Dg[(size_t)x * NT * nk + o] : mk<S>(0, 0);
-        double2 Qe = make_double2(0., 0.);
-        double Hii = 0.;
-        if (MIX) {
-          Qe = I->Peq[o];
-          if (i == j) Hii = I->Hdiag[(size_t)i * nk + k];
-        }
         C G = mk<C>(0, 0);
         if (su[cur].on) {
           const double2* row = src + (size_t)e * nk;
@@ -193,35 +177,19 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
         }
         sG[e * KT + kl] = G;
         const int w = (i < nch) != (j < nch);
-        C hu = cv<C>(He), hl = mk<C>(hu.x, -hu.y), xd = mk<C>(0, 0);
+        C hu = cv<C>(He), hl = mk<C>(hu.x, -hu.y);
 #pragma unroll
         for (int x = 0; x < 3; x++) {
           const C d = cv<C>(De[x]);
           const R ex = (R)su[cur].E[w][x];
           hu = mk<C>(hu.x + d.x * ex, hu.y + d.y * ex);
           hl = mk<C>(hl.x + d.x * ex, hl.y + d.y * ex);
-          if (MIX) xd = mk<C>(xd.x + d.x * ex, xd.y + d.y * ex);
         }
-        const C pc = MIX ? cv<C>(make_double2(Pe.x - Qe.x, Pe.y - Qe.y)) : cv<C>(Pe);
+        const C pc = cv<C>(Pe);
         sP[oij] = pc;
         sP[oji] = mk<C>(pc.x, -pc.y);
-        if (MIX && i == j) {
-          // band energies in FP64 (a k-independent FP32 rounding would drift coherently)
-          double ed = Hii;
-#pragma unroll
-          for (int x = 0; x < 3; x++) ed += (double)De[x].x * su[cur].E[0][x];
-          sEd[i * KT + kl] = ed;
-          hu = hl = mk<C>(0, 0);
-        }
         sH[oij] = hu;
         sH[oji] = hl;
-        if (MIX) {
-          const C qc = cv<C>(Qe);
-          sQ[oij] = qc;
-          sQ[oji] = mk<C>(qc.x, -qc.y);
-          sX[oij] = xd;
-          sX[oji] = xd;
-        }
       }
     }
     // set-up of the next tile, published by the barrier below
@@ -232,7 +200,7 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
       setup(buf, tl, it);
     }
     __syncthreads();
-    // ---- (B) C = P H~^T (+ rho_eq (E.D)^T for mixed precision), BR x BC per thread
+    // ---- (B) C = P H~^T, BR x BC per thread
     if (active) {
       const int kl = tid % KT, blk = tid / KT;
       const int i0 = (blk / (N / BC)) * BR, j0 = (blk % (N / BC)) * BC;
@@ -259,7 +227,6 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
         }
       };
       product(sP, sH);
-      if (MIX) product(sQ, sX);
 #pragma unroll
       for (int r = 0; r < BR; r++)
 #pragma unroll
@@ -278,8 +245,7 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
         double2 p1v = make_double2(0., 0.), p0v = make_double2(0., 0.);
         if (stage > 0) p1v = I->P1[o];
         if (stage == 1 || stage == 2) p0v = I->P0[o];
-        double2 Pe = src[o], Qe = make_double2(0., 0.);
-        if (MIX) Qe = I->Peq[o];
+        const double2 Pe = src[o];
         const C cij = sC[i * RS + j * KT + kl], cji = sC[j * RS + i * KT + kl];
         C beta = mk<C>(cij.x - cji.x, cij.y + cji.y);
         C vv = mk<C>(beta.y, -beta.x);  // -i beta
@@ -291,11 +257,6 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
         const C G = sG[e * KT + kl];
         vv = mk<C>(vv.x + G.x, vv.y + G.y);
         double2 d = cv<double2>(vv);
-        if (MIX) {
-          const double dE = sEd[j * KT + kl] - sEd[i * KT + kl];
-          const double2 dp = make_double2(Pe.x - Qe.x, Pe.y - Qe.y);
-          d = make_double2(d.x + dp.y * dE, d.y - dp.x * dE);  // -i dE (rho - rho_eq)
-        }
         if (i == j) d.y = 0;
         switch (stage) {
           case 0:
@@ -320,27 +281,27 @@ __global__ void __launch_bounds__(KT* MM<N, MIX>::TPK) k_bstage_mm(View v, int s
   }
 }
 
-template <int N, int KT, bool MIX>
+template <int N, int KT>
 cudaError_t mm_launch(const View& v, int stage, int parity, int grid, cudaStream_t s) {
-  const size_t smem = MMLayout<N, KT, MIX>::bytes();
+  const size_t smem = MMLayout<N, KT>::bytes();
   static bool attr = false;  // per instantiation, per process
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_bstage_mm<N, KT, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_bstage_mm<N, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  k_bstage_mm<N, KT, MIX><<<grid, KT * MM<N, MIX>::TPK, smem, s>>>(v, stage, parity);
+  k_bstage_mm<N, KT><<<grid, KT * MM<N>::TPK, smem, s>>>(v, stage, parity);
   return cudaGetLastError();
 }
 
-template <int N, int KT, bool MIX>
+template <int N, int KT>
 int mm_grid() {
-  const size_t smem = MMLayout<N, KT, MIX>::bytes();
-  cudaFuncSetAttribute(k_bstage_mm<N, KT, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const size_t smem = MMLayout<N, KT>::bytes();
+  cudaFuncSetAttribute(k_bstage_mm<N, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bstage_mm<N, KT, MIX>, KT * MM<N, MIX>::TPK, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_bstage_mm<N, KT>, KT * MM<N>::TPK, smem);
   return sms * (per > 0 ? per : 1);
 }
 
@@ -352,16 +313,18 @@ bool mm_supported(int N, int kt) {
 }
 
 cudaError_t launch_stage_mm(int N, int kt, bool mixed, const View& v, int stage, int parity, int grid, cudaStream_t s) {
+  if (mixed) return cudaErrorInvalidValue;  // FP64 only
 #define MMX(n, k) \
-  if (N == n && kt == k) return mixed ? mm_launch<n, k, true>(v, stage, parity, grid, s) : mm_launch<n, k, false>(v, stage, parity, grid, s);
+  if (N == n && kt == k) return mm_launch<n, k>(v, stage, parity, grid, s);
   MMX(8, 8) MMX(8, 16) MMX(16, 2) MMX(16, 4) MMX(16, 8)
 #undef MMX
   return cudaErrorInvalidValue;
 }
 
 int stage_grid_mm(int N, int kt, bool mixed) {
+  if (mixed) return 0;  // FP64 only
 #define MMX(n, k) \
-  if (N == n && kt == k) return mixed ? mm_grid<n, k, true>() : mm_grid<n, k, false>();
+  if (N == n && kt == k) return mm_grid<n, k>();
   MMX(8, 8) MMX(8, 16) MMX(16, 2) MMX(16, 4) MMX(16, 8)
 #undef MMX
   return 0;
