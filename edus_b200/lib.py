@@ -58,6 +58,7 @@ def load_library():
         "edus_write_outputs": (C.c_int, [vp, cp]),
         "edus_last_timing": (C.c_int, [vp, P(dbl), P(C.c_int64)]),
         "edus_profile": (C.c_int, [vp, i32, P(dbl), P(C.c_int64), P(dbl), P(C.c_int64)]),
+        "edus_profile_ex": (C.c_int, [vp, i32, i32, P(dbl), P(C.c_int64), P(dbl), P(C.c_int64)]),
         "edus_get_derivative": (C.c_int, [vp, i32, P(dbl), dbl, i32]),
         "edus_runge_kutta_ad": (C.c_int, [vp, i32, i32, dbl]),
         "edus_runge_kutta_ac": (C.c_int, [vp, i32, dbl]),
@@ -278,10 +279,12 @@ class Context:
         _check(self._L.edus_last_timing(self._h, C.byref(ms), C.byref(launches)), "edus_last_timing")
         return ms.value, launches.value
 
-    def profile(self, nsteps):
-        """Device time of the fused RHS kernel and of the Coulomb pair over nsteps (eager)."""
+    def profile(self, nsteps, reps=1):
+        """Device time of the fused RHS kernel and of the Coulomb pair over nsteps (eager);
+        reps > 1 repeats each idempotent RHS launch back to back between its events."""
         a, b, c, d = C.c_double(), C.c_int64(), C.c_double(), C.c_int64()
-        _check(self._L.edus_profile(self._h, int(nsteps), C.byref(a), C.byref(b), C.byref(c), C.byref(d)), "edus_profile")
+        _check(self._L.edus_profile_ex(self._h, int(nsteps), int(reps), C.byref(a), C.byref(b), C.byref(c), C.byref(d)),
+               "edus_profile_ex")
         return {"rhs_ms": a.value, "rhs_launches": b.value, "coulomb_ms": c.value, "coulomb_launches": d.value}
 
     # ODE_solver-level mirror ---------------------------------------------

@@ -292,6 +292,13 @@ int edus_last_timing(edus_ctx* ctx, double* ms, int64_t* launches);
  * summed device times (ms) and launch counts. */
 int edus_profile(edus_ctx* ctx, int32_t nsteps, double* rhs_ms, int64_t* rhs_launches, double* coul_ms,
                  int64_t* coul_launches);
+/* As edus_profile, with every RHS launch whose result does not depend on its
+ * own output (AB, Taylor and Pv launches) repeated reps times back to back
+ * between its events: the launch-count-weighted average is the kernel's
+ * duration in a pipeline, without one event pair's overhead per launch. The
+ * repeats leave the state as one launch would. */
+int edus_profile_ex(edus_ctx* ctx, int32_t nsteps, int32_t reps, double* rhs_ms, int64_t* rhs_launches, double* coul_ms,
+                    int64_t* coul_launches);
 
 /* --------------------------------------------- ODE_solver-level mirror
  * Slots name device arrays of the state shape: 0 = P0, 1 = P1, 2 = P2,
