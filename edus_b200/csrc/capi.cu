@@ -97,6 +97,9 @@ struct edus_ctx {
   std::vector<void*> allocs;
   double2 *d_P0 = nullptr, *d_P1 = nullptr, *d_Pa = nullptr, *d_Pb = nullptr, *d_ring = nullptr, *d_hr = nullptr;
   double2 *d_h = nullptr, *d_X0 = nullptr;
+  // Coulomb in the diagonal basis: the state in the eigenbasis and the rotated term
+  bool diagb = false;
+  double2 *d_pdiag = nullptr, *d_xw = nullptr;
   CoulDev cd{};
   void* d_part = nullptr;
   unsigned int* d_done = nullptr;
@@ -228,6 +231,7 @@ StageArgs base_args(edus_ctx* c) {
   a.wx2 = c->P.p.probe.wl;
   a.order = c->order;
   a.dt = c->dt;
+  a.xw = c->diagb ? c->d_xw : nullptr;
   return a;
 }
 
@@ -248,8 +252,17 @@ int run_coulomb(edus_ctx* c, const double2* src) {
   if (!c->coul) return 0;
   int rc = prof_mark(c, 1, true);
   if (rc) return rc;
-  CK(launch_coulomb(c->tb, c->cd, src, c->d_h, nullptr, c->d_X0, c->stream));
-  c->launches += 2;
+  if (c->diagb) {
+    // headers/RungeKutta.h:35-55: coefficients of the state in the eigenbasis,
+    // then the screened term of that basis rotated back (:96-123)
+    CK(launch_pdiag(c->tb, src, c->d_pdiag, c->stream));
+    CK(launch_coulomb(c->tb, c->cd, c->d_pdiag, c->d_h, nullptr, c->d_X0, c->stream));
+    CK(launch_coulomb_xw(c->tb, c->d_cst, c->d_pdiag, c->d_xw, c->stream));
+    c->launches += 4;
+  } else {
+    CK(launch_coulomb(c->tb, c->cd, src, c->d_h, nullptr, c->d_X0, c->stream));
+    c->launches += 2;
+  }
   return prof_mark(c, 1, false);
 }
 
@@ -1164,6 +1177,10 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
         cd s = std::conj(P.screen[lin]);
         h.screen[e] = make_double2(s.real(), s.imag());
       }
+    // diagonal basis (headers/RungeKutta.h:96-108): Screen_const[0][0] on the
+    // diagonal, conj(Screen_const[0][1]) on every off-diagonal element
+    h.screen_d00 = make_double2(P.screen[0].real(), P.screen[0].imag());
+    if (n > 1) h.screen_d01c = make_double2(P.screen[1].real(), -P.screen[1].imag());
     for (int i = 0; i < n; i++)
       for (int j = 0; j < n; j++) h.VH[i * n + j] = P.VH[(size_t)i * n + j];
     double2* dcf[4];
@@ -1204,7 +1221,19 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
     if (cudaMemcpyAsync(c->d_hr, dH, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
       return bail(fail(EDUS_ECUDA, "copy Hr"));
     if (coulomb_prepare(tb) != cudaSuccess) return bail(fail(EDUS_EUNSUPPORTED, "Coulomb tables exceed shared memory"));
-    if (launch_coulomb(tb, c->cd, c->d_P0, nullptr, c->d_X0, nullptr, c->stream) != cudaSuccess)
+    const double2* eq = c->d_P0;
+    if (P.p.diag_basis) {
+      // the equilibrium state in the eigenbasis: 1 on the filled bands (main_MPI.cpp:291-304)
+      if (n > 4) return bail(fail(EDUS_EUNSUPPORTED, "Coulomb_diag_basis: up to 4 bands"));
+      c->diagb = true;
+      if ((rc = dalloc(c, &c->d_pdiag, c->plane)) || (rc = dalloc(c, &c->d_xw, c->plane))) return bail(rc);
+      std::vector<double2> pe(c->plane, make_double2(0, 0));
+      for (int i = 0; i < P.nbands && i < n; i++)
+        for (int k = 0; k < nk; k++) pe[(size_t)tri_index(i, i, n) * nk + k] = make_double2(1.0, 0.0);
+      if ((rc = upload(c, c->d_pdiag, pe))) return bail(rc);
+      eq = c->d_pdiag;
+    }
+    if (launch_coulomb(tb, c->cd, eq, nullptr, c->d_X0, nullptr, c->stream) != cudaSuccess)
       return bail(fail(EDUS_ECUDA, "equilibrium Coulomb pass"));
     std::vector<double2> fd(n);
     cudaMemcpyAsync(fd.data(), dfd, sizeof(double2) * n, cudaMemcpyDeviceToHost, c->stream);

@@ -142,6 +142,8 @@ struct DevConsts {
   double VH[kMaxBands * kMaxBands];
   double EH0[kMaxBands];
   double2 screen[kMaxTri];    // conj(Screen_const) per upper element (diag uses [0])
+  double2 screen_d00;         // diagonal basis: Screen_const[0][0]
+  double2 screen_d01c;        // diagonal basis: conj(Screen_const[0][1])
 };
 
 enum StageOp : int {
@@ -176,6 +178,9 @@ struct StageArgs {
   unsigned long long* maxdp;
   double pcond_plus_ncond;  // P_cond_max + n_cond
   int stage_rows;           // set by the launcher: k-grid rows of Coulomb tables staged per block
+  // Coulomb in the diagonal basis: the mean-field term already rotated back to
+  // the Wannier basis, [ntri][nk] (null: the Wannier-basis term from tb.h)
+  const double2* xw;
 };
 
 }  // namespace edus

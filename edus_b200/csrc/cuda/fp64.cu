@@ -492,6 +492,131 @@ cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double*
   return cudaGetLastError();
 }
 
+// Coulomb in the diagonal basis (headers/RungeKutta.h:35-55, 96-123).
+// The state in the model's eigenbasis, P_d = sum_ii,jj conj(U_c,ii) P_ii,jj U_c',jj
+// with a real diagonal (get_P_in_dia_vect, headers/InitParameters.h:264-333),
+// as upper planes for the forward transform. One thread per k.
+template <int N>
+__global__ void k_pdiag(DevTables tb, const double2* __restrict__ rho, double2* __restrict__ pd) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nk = tb.nk;
+  if (k >= nk) return;
+  double2 P[N * N], M[N * N];
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = i; j < N; j++) {
+      const double2 v = rho[(size_t)Tri<N>::idx(i, j) * nk + k];
+      P[i * N + j] = v;
+      P[j * N + i] = cconj(v);
+    }
+  // M[jc][ii] = sum_jj P[ii][jj] U[jc][jj]
+#pragma unroll
+  for (int ii = 0; ii < N; ii++)
+#pragma unroll
+    for (int jc = 0; jc < N; jc++) {
+      double2 m = cz();
+#pragma unroll
+      for (int jj = 0; jj < N; jj++) m = cadd(m, cmul(P[ii * N + jj], tb.U[(size_t)(jc * N + jj) * nk + k]));
+      M[jc * N + ii] = m;
+    }
+#pragma unroll
+  for (int ic = 0; ic < N; ic++)
+#pragma unroll
+    for (int jc = ic; jc < N; jc++) {
+      double2 v = cz();
+#pragma unroll
+      for (int ii = 0; ii < N; ii++) v = cadd(v, cmul(cconj(tb.U[(size_t)(ic * N + ii) * nk + k]), M[jc * N + ii]));
+      if (ic == jc) v.y = 0.;
+      pd[(size_t)Tri<N>::idx(ic, jc) * nk + k] = v;
+    }
+}
+
+// The mean-field term for the diagonal basis: X_d from the inverse-transform
+// rows of the P_d coefficients, the screening correction of that basis
+// (X_d,ii -= S00 (P_d,ii - [i < Nch + Nv]), X_d,ij -= conj(S01) conj(P_d,ij)),
+// then X_W = U^dagger X_d U (get_Xd_in_Wannier_vect, headers/InitParameters.h:
+// 339-373), written as upper planes. One thread per k.
+template <int N>
+__global__ void k_coulomb_xw(DevTables tb, const DevConsts* __restrict__ cst, const double2* __restrict__ pd,
+                             double2* __restrict__ xw) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nk = tb.nk;
+  if (k >= nk) return;
+  constexpr int NT = Tri<N>::NT;
+  const int n2 = tb.n2, nc = tb.ncut;
+  const int i1 = k / n2, i2 = k - i1 * n2;
+  double2 X[N * N];
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = i; j < N; j++) {
+      const int e = Tri<N>::idx(i, j);
+      const double2* hrow = tb.h + (size_t)i1 * 2 * nc * NT + e;
+      double yx = 0., yy = 0.;
+      for (int m = 0; m < nc; m++) {
+        const double cn = tb.t2c[m * n2 + i2], sn = tb.t2s[m * n2 + i2];
+        const double2 c = hrow[(size_t)m * NT], s = hrow[(size_t)(nc + m) * NT];
+        yx += c.x * cn + s.x * sn;
+        yy += c.y * cn + s.y * sn;
+      }
+      double2 x = cmk(-yx, yy);
+      const double2 p = pd[(size_t)e * nk + k];
+      if (i == j) {
+        const double pb = i < tb.nbands ? 1.0 : 0.0;
+        x = csub(x, cscale(cst->screen_d00, p.x - pb));
+      } else {
+        x = csub(x, cmul(cst->screen_d01c, cconj(p)));
+      }
+      X[i * N + j] = x;
+      if (i != j) X[j * N + i] = cconj(x);
+    }
+  // M[ii][jc] = sum_jj X[ii][jj] U[jj][jc]; X_W[ic][jc] = sum_ii conj(U[ii][ic]) M[ii][jc]
+  double2 M[N * N];
+#pragma unroll
+  for (int ii = 0; ii < N; ii++)
+#pragma unroll
+    for (int jc = 0; jc < N; jc++) {
+      double2 m = cz();
+#pragma unroll
+      for (int jj = 0; jj < N; jj++) m = cadd(m, cmul(X[ii * N + jj], tb.U[(size_t)(jj * N + jc) * nk + k]));
+      M[ii * N + jc] = m;
+    }
+#pragma unroll
+  for (int ic = 0; ic < N; ic++)
+#pragma unroll
+    for (int jc = ic; jc < N; jc++) {
+      double2 v = cz();
+#pragma unroll
+      for (int ii = 0; ii < N; ii++) v = cadd(v, cmul(cconj(tb.U[(size_t)(ii * N + ic) * nk + k]), M[ii * N + jc]));
+      xw[(size_t)Tri<N>::idx(ic, jc) * nk + k] = v;
+    }
+}
+
+cudaError_t launch_pdiag(const DevTables& tb, const double2* rho, double2* pd, cudaStream_t s) {
+  const dim3 g((tb.nk + 127) / 128), b(128);
+  switch (tb.n) {
+    case 1: k_pdiag<1><<<g, b, 0, s>>>(tb, rho, pd); break;
+    case 2: k_pdiag<2><<<g, b, 0, s>>>(tb, rho, pd); break;
+    case 3: k_pdiag<3><<<g, b, 0, s>>>(tb, rho, pd); break;
+    case 4: k_pdiag<4><<<g, b, 0, s>>>(tb, rho, pd); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_coulomb_xw(const DevTables& tb, const DevConsts* cst, const double2* pd, double2* xw, cudaStream_t s) {
+  const dim3 g((tb.nk + 127) / 128), b(128);
+  switch (tb.n) {
+    case 1: k_coulomb_xw<1><<<g, b, 0, s>>>(tb, cst, pd, xw); break;
+    case 2: k_coulomb_xw<2><<<g, b, 0, s>>>(tb, cst, pd, xw); break;
+    case 3: k_coulomb_xw<3><<<g, b, 0, s>>>(tb, cst, pd, xw); break;
+    case 4: k_coulomb_xw<4><<<g, b, 0, s>>>(tb, cst, pd, xw); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 // d = a + dt * v over n complex entries, multiply then add without
 // contraction, as Runge_Kutta_Ad / Runge_Kutta_Ac (headers/RungeKutta.h:301-355).
 __global__ void k_axpy(const double2* a, const double2* __restrict__ v, double dt, double2* d,

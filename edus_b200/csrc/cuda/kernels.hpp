@@ -40,6 +40,11 @@ cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int
 cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double* out, cudaStream_t s);
 // d = a + dt * v elementwise (n complex entries; d may alias a).
 cudaError_t launch_axpy(const double2* a, const double2* v, double dt, double2* d, size_t n, cudaStream_t s);
+// Coulomb in the diagonal basis, up to 4 bands: the state in the eigenbasis of
+// tb.U (upper planes), and the screened mean-field term rotated back to the
+// Wannier basis from the inverse-transform rows tb.h.
+cudaError_t launch_pdiag(const DevTables& tb, const double2* rho, double2* pd, cudaStream_t s);
+cudaError_t launch_coulomb_xw(const DevTables& tb, const DevConsts* cst, const double2* pd, double2* xw, cudaStream_t s);
 int obs_parts(int nk);
 size_t obs_part_bytes();
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,

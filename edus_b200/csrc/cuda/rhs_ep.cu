@@ -88,7 +88,22 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
     mbar_wait(&bar, 0, tb.err);
   }
   if (valid) {
-    if (tb.h) {
+    if (tb.h && a.xw) {
+      // diagonal basis: the term of k_coulomb_xw (screened, rotated back)
+      double2 X = a.xw[(size_t)e * nk + k];
+      if (i == j) {
+        X.y = 0.;
+        double eh = 0.;
+#pragma unroll
+        for (int jj = 0; jj < N; jj++) eh += tb.fdiag[jj].x * cst->VH[i * N + jj];
+        eh -= cst->EH0[i];
+        He = cadd(He, X);
+        He.x += eh;
+      } else {
+        He = cadd(He, X);
+      }
+      if (a.hr_out) a.hr_out[(size_t)e * nk + k] = He;
+    } else if (tb.h) {
       // X_e(k) = conj(-sum_n hc(i1,n,e) cos(2 pi n k2) + hs(i1,n,e) sin(2 pi n k2))
       const int n2 = tb.n2;
       const int i1 = k / n2, i2 = k - i1 * n2;
@@ -271,7 +286,7 @@ static cudaError_t launch_ep(const DevTables& tb, const DevConsts* cst, const St
   StageArgs b = a;
   size_t dyn = 0;
   b.stage_rows = 0;
-  if (tb.h) {
+  if (tb.h && !a.xw) {
     // rows of the k grid one block of KT consecutive k points can touch
     const int rows = (tb.n2 + KT - 2) / tb.n2 + 1;
     const size_t bytes = sizeof(double2) * ((size_t)rows * 2 * tb.ncut * NT + tb.ncut * KT);

@@ -606,7 +606,6 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P, bool de
       }
   // Coulomb
   if (p.coulomb) {
-    if (p.diag_basis) return fail(EDUS_EUNSUPPORTED, "Coulomb_diag_basis is not built (Wannier-basis Coulomb is)");
     if (!p.read_from_files)
       return fail(EDUS_EUNSUPPORTED,
                   "Coulomb coefficients are read from files (Read_Coulomb_from_files); edus_coulomb_generate computes them");

@@ -86,6 +86,7 @@ struct orc {
   double EH[EDUS_MAX_BANDS], EH0[EDUS_MAX_BANDS];
   double *cos_m1, *sin_m1, *cos_m2, *sin_m2; /* [ncut][nk] */
   cplx *PW0;                /* P_Wannier_0 */
+  cplx *Pd;                 /* diagonal basis: P in the eigenbasis [nk][n][n] */
   cplx *Hr;                 /* Hk_renorm [nk][n][n] */
   double n_cond_coul;       /* Coulomb_set.n_cond */
   /* time loop */
@@ -1011,17 +1012,102 @@ static void coulomb_hk(const orc* o, int ik, const cplx* P, cplx* Hk) {
   }
 }
 
+/* headers/InitParameters.h:264-333 (get_P_in_dia_vect): P_d = conj(U) P U^T
+ * with a real diagonal, for every k */
+static void p_in_dia(const orc* o, const cplx* P, cplx* Pd) {
+  int n = o->ncv;
+#pragma omp parallel for schedule(static)
+  for (int ik = 0; ik < o->nk; ik++) {
+    const cplx* U = &o->U[IDX3(ik, 0, 0, n)];
+    cplx Pf[EDUS_MAX_BANDS * EDUS_MAX_BANDS], M[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+    for (int ic = 0; ic < n; ic++)
+      for (int jc = ic; jc < n; jc++) {
+        Pf[ic * n + jc] = P[IDX3(ik, ic, jc, n)];
+        if (ic != jc) Pf[jc * n + ic] = conj(Pf[ic * n + jc]);
+      }
+    for (int ii = 0; ii < n; ii++)
+      for (int jc = 0; jc < n; jc++) {
+        cplx m = 0;
+        for (int jj = 0; jj < n; jj++) m += Pf[ii * n + jj] * U[jc * n + jj];
+        M[jc * n + ii] = m;
+      }
+    for (int ic = 0; ic < n; ic++)
+      for (int jc = 0; jc < n; jc++) {
+        cplx v = 0;
+        for (int ii = 0; ii < n; ii++) v += conj(U[ic * n + ii]) * M[jc * n + ii];
+        Pd[IDX3(ik, ic, jc, n)] = v;
+      }
+    for (int ic = 0; ic < n; ic++) Pd[IDX3(ik, ic, ic, n)] = creal(Pd[IDX3(ik, ic, ic, n)]);
+  }
+}
+
+/* headers/RungeKutta.h:96-138: renormalised H for one k, Coulomb in the
+ * diagonal basis (screening of that basis, then X_W = U^dagger X_d U,
+ * get_Xd_in_Wannier_vect, headers/InitParameters.h:339-373) */
+static void coulomb_hk_diag(const orc* o, int ik, cplx* Hk) {
+  int n = o->ncv;
+  cplx X[EDUS_MAX_BANDS * EDUS_MAX_BANDS], M[EDUS_MAX_BANDS * EDUS_MAX_BANDS], XW[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+  coulomb_X(o, ik, X);
+  const cplx* Pd = &o->Pd[IDX3(ik, 0, 0, n)];
+  for (int ic = 0; ic < n; ic++) {
+    double pb = ic < o->nbands ? 1.0 : 0.0;
+    X[ic * n + ic] -= o->screen[0] * (Pd[ic * n + ic] - pb);
+    for (int jc = ic + 1; jc < n; jc++) {
+      X[ic * n + jc] -= conj(o->screen[1]) * Pd[jc * n + ic];
+      X[jc * n + ic] = conj(X[ic * n + jc]);
+    }
+  }
+  const cplx* U = &o->U[IDX3(ik, 0, 0, n)];
+  for (int ii = 0; ii < n; ii++)
+    for (int jc = 0; jc < n; jc++) {
+      cplx m = 0;
+      for (int jj = 0; jj < n; jj++) m += X[ii * n + jj] * U[jj * n + jc];
+      M[ii * n + jc] = m;
+    }
+  for (int ic = 0; ic < n; ic++)
+    for (int jc = 0; jc < n; jc++) {
+      cplx v = 0;
+      for (int ii = 0; ii < n; ii++) v += conj(U[ii * n + ic]) * M[ii * n + jc];
+      XW[ic * n + jc] = v;
+    }
+  for (int ic = 0; ic < n; ic++) {
+    XW[ic * n + ic] = creal(XW[ic * n + ic]);
+    for (int jc = ic; jc < n; jc++) {
+      Hk[ic * n + jc] = o->H[IDX3(ik, ic, jc, n)] + XW[ic * n + jc];
+      if (ic == jc) Hk[ic * n + ic] += o->EH[ic];
+      if (ic != jc) Hk[jc * n + ic] = conj(Hk[ic * n + jc]);
+    }
+  }
+}
+
+/* Coulomb coefficients of the state (the eigenbasis state in the diagonal basis) */
+static void coulomb_update(orc* o, const cplx* P) {
+  if (o->p.diag_basis) {
+    p_in_dia(o, P, o->Pd);
+    coulomb_coeffs(o, o->Pd);
+  } else {
+    coulomb_coeffs(o, P);
+  }
+}
+
+static void coulomb_hk_any(const orc* o, int ik, const cplx* P, cplx* Hk) {
+  if (o->p.diag_basis)
+    coulomb_hk_diag(o, ik, Hk);
+  else
+    coulomb_hk(o, ik, P, Hk);
+}
+
 /* ------------------------------------------------------------ RHS */
 
 /* headers/RungeKutta.h:7-297 (get_derivative_Df), Wannier-basis Coulomb */
 static void rhs(orc* o, const cplx* P, cplx* Pv, double EF[2][3], double wx2, int e_non0) {
   int n = o->ncv, nch = o->nch;
-  if (o->p.coulomb) coulomb_coeffs(o, P);
+  if (o->p.coulomb) coulomb_update(o, P);
 #pragma omp parallel for schedule(static)
   for (int ik = 0; ik < o->nk; ik++) {
     cplx Hk[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
     if (o->p.coulomb) {
-      coulomb_hk(o, ik, P, Hk);
+      coulomb_hk_any(o, ik, P, Hk);
       for (int e = 0; e < n * n; e++) o->Hr[(size_t)ik * n * n + e] = Hk[e];
     } else {
       for (int ic = 0; ic < n; ic++)
@@ -1544,16 +1630,20 @@ int orc_create(const edus_params* p, const char* workdir, orc** out) {
       rc = EDUS_EUNSUPPORTED;
       goto fail;
     }
-    if (p->diag_basis) {
-      rc = EDUS_EUNSUPPORTED;
-      goto fail;
-    }
+    o->Pd = xcalloc(st, sizeof(cplx));
     rc = coulomb_read(o, workdir);
     if (rc) goto fail;
     trig_tables(o);
     memcpy(o->Hr, o->H, sizeof(cplx) * st);
-    /* main_MPI.cpp:276-337: equilibrium coefficients */
-    coulomb_coeffs(o, o->P0);
+    /* main_MPI.cpp:276-337: equilibrium coefficients (diagonal basis: of the
+     * equilibrium state in the eigenbasis, 1 on the filled bands) */
+    if (p->diag_basis) {
+      for (int ik = 0; ik < o->nk; ik++)
+        for (int ic = 0; ic < o->nbands; ic++) o->Pd[IDX3(ik, ic, ic, n)] = 1.0;
+      coulomb_coeffs(o, o->Pd);
+    } else {
+      coulomb_coeffs(o, o->P0);
+    }
     memcpy(o->Xcc0, o->Xcc, sizeof(cplx) * c2);
     memcpy(o->Xcs0, o->Xcs, sizeof(cplx) * c2);
     memcpy(o->Xsc0, o->Xsc, sizeof(cplx) * c2);
@@ -1573,7 +1663,7 @@ void orc_free(orc* o) {
   void* ptrs[] = {o->kpt, o->nbr, o->H, o->U, o->hU, o->D, o->GE, o->Rvec, o->HR, o->xR, o->yR, o->zR,
                   o->P0, o->P1, o->P2, o->Pv, o->Pgrad, o->ring, o->Pprev_diag, o->Psave_diag, o->cA, o->cB,
                   o->cC, o->cD, o->Xcc, o->Xcs, o->Xsc, o->Xss, o->Xcc0, o->Xcs0, o->Xsc0, o->Xss0,
-                  o->cos_m1, o->sin_m1, o->cos_m2, o->sin_m2, o->PW0, o->Hr};
+                  o->cos_m1, o->sin_m1, o->cos_m2, o->sin_m2, o->PW0, o->Hr, o->Pd};
   for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
   free(o);
 }
@@ -1671,10 +1761,10 @@ int orc_rhs(orc* o, const double* P, double* Pv, const double EF[6], double wx2,
 
 int orc_coulomb_hk(orc* o, const double* P, double* hk) {
   if (!o->p.coulomb) return EDUS_EINVAL;
-  coulomb_coeffs(o, (const cplx*)P);
+  coulomb_update(o, (const cplx*)P);
   int n = o->ncv;
 #pragma omp parallel for schedule(static)
-  for (int ik = 0; ik < o->nk; ik++) coulomb_hk(o, ik, (const cplx*)P, (cplx*)hk + (size_t)ik * n * n);
+  for (int ik = 0; ik < o->nk; ik++) coulomb_hk_any(o, ik, (const cplx*)P, (cplx*)hk + (size_t)ik * n * n);
   return 0;
 }
 
