@@ -134,3 +134,22 @@ def test_edus_run_generates_the_tables_it_needs(tmp_path):
         assert os.path.exists(tmp_path / "Output" / "Coulomb" / f"{f}{m.group(1)}.txt"), f
     J1 = np.loadtxt(tmp_path / "Output" / "J1.txt")
     assert J1.shape[1] == 7 and np.isfinite(J1).all()
+
+
+def test_generator_rejects_bad_grids_and_models_without_a_device(tmp_path):
+    """Argument errors come back as codes before any device work: Simpson grids
+    need an odd number of points, and the generator takes up to 4 bands."""
+    from edus_b200 import abi
+    from edus_b200 import workloads as W
+
+    p = _params(tmp_path, ncut=4, gdist=3)
+    for n_sum, n_scr in [(40, 401), (41, 400), (1, 401)]:
+        with pytest.raises(E.EdusError) as ei:
+            E.coulomb_generate(p, str(tmp_path), n_sum=n_sum, n_sum_screen=n_scr)
+        assert ei.value.code == abi.EDUS_EINVAL
+    d = tmp_path / "w8"
+    q = E.parse_input(W.wannier(str(d), n=12, t_fin_fs=0.1))
+    q.coulomb, q.ncut = 1, 4
+    with pytest.raises(E.EdusError) as ei:
+        E.coulomb_generate(q, str(d), n_sum=41, n_sum_screen=401)
+    assert ei.value.code == abi.EDUS_EUNSUPPORTED
