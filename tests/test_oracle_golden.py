@@ -65,3 +65,26 @@ def test_oracle_reproduces_golden_field_and_tabs(golden_run):
 def test_oracle_trace_is_conserved(golden_run):
     log, _ = golden_run
     assert max(abs(x["trace_dev"]) for x in log) < 1e-11
+
+
+@pytest.mark.parametrize("diag", [0, 1])
+def test_oracle_coulomb_equilibrium_is_stationary(workdir, diag):
+    """With no field, the Coulomb run starts in its own equilibrium in either
+    basis (main_MPI.cpp:276-337: the coefficients of the initial state, or in
+    the diagonal basis of the filled bands, are subtracted), so rho stays put
+    and the renormalised H stays Hermitian."""
+    from edus_b200 import workloads as W
+
+    path = W.hbn_coulomb(workdir, n=12, field=0.0, t_fin_fs=0.1, it_res=5)
+    txt = open(path).read()
+    if diag:
+        txt = txt.replace("Rytova_Keldysh\n", "Rytova_Keldysh\nCoulomb_diag_basis\n")
+    open(path, "w").write(txt)
+    p = E.parse_input(path)
+    o = Oracle(p, workdir)
+    rho0 = o.get("P0")
+    log = o.run(15)
+    assert np.abs(o.get("P0") - rho0).max() < 1e-13
+    hk = o.coulomb_hk(o.get("P0"))
+    assert np.array_equal(hk, np.conj(np.transpose(hk, (0, 2, 1))))
+    assert abs(log[-1]["trace_dev"]) < 1e-12
