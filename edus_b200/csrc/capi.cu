@@ -921,6 +921,24 @@ int edus_problem_write_kgrid(const edus_problem* pb, const char* outdir) {
   return write_kgrid(pb->P, outdir);
 }
 
+// <workdir>/kpt.txt: "ik i0 i1 i2 k0 k1 k2" per k point of the Monkhorst-Pack
+// grid, default stream format, as BZ_parameters writes it while it builds the
+// grid (headers/InitParameters.h:17-39).
+int edus_problem_write_kpt(const edus_problem* pb, const char* workdir) {
+  if (!pb || !workdir) return fail(EDUS_EINVAL, "null argument");
+  const Problem& P = pb->P;
+  std::ofstream f(std::string(workdir) + "/kpt.txt");
+  if (!f) return fail(EDUS_EIO, "cannot write into %s", workdir);
+  const int* Nk = P.p.nk;
+  for (int ik = 0; ik < P.nk; ik++) {
+    const int iik[3] = {(ik / (Nk[2] * Nk[1])) % Nk[0], (ik / Nk[2]) % Nk[1], ik % Nk[2]};
+    f << ik << " " << iik[0] << " " << iik[1] << " " << iik[2];
+    for (int c = 0; c < 3; c++) f << " " << P.kpt[(size_t)ik * 3 + c];
+    f << std::endl;
+  }
+  return f ? 0 : fail(EDUS_EIO, "write error in %s/kpt.txt", workdir);
+}
+
 int edus_model_hud(const edus_problem* pb, const double kcrys[3], double* H, double* U, double* D) {
   if (!pb || !kcrys || !H || !U || !D) return fail(EDUS_EINVAL, "null argument");
   return model_hud(pb->P, kcrys, (cd*)H, (cd*)U, (cd*)D);

@@ -196,6 +196,10 @@ void edus_problem_free(edus_problem* pb);
  * stream format, as the reference's print_k_MPI (headers/Observables_MPI.h:
  * 492-550) writes Output/k_grid.txt. edus_write_outputs writes it too. */
 int edus_problem_write_kgrid(const edus_problem* pb, const char* outdir);
+/* Write workdir/kpt.txt ("ik i0 i1 i2 k0 k1 k2" per k point), the grid listing
+ * the reference's BZ_parameters leaves in its working directory
+ * (headers/InitParameters.h:17-39); edus_run writes it at set-up. */
+int edus_problem_write_kpt(const edus_problem* pb, const char* workdir);
 /* H(k), U(k) and D(k) of the problem's model at one crystal k point, as
  * gHUD (headers/HUD.h:5-20) returns them: H, U [n][n], D [n][n][3] interleaved
  * complex. */

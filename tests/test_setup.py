@@ -65,6 +65,21 @@ def test_golden_kgrid_file_byte_exact(tmp_path):
     assert len(raw) == ref["bytes"] and hashlib.sha256(raw).hexdigest() == ref["sha256"]
 
 
+def test_kpt_listing(tmp_path):
+    """kpt.txt (headers/InitParameters.h:17-39): index, grid indices and crystal
+    coordinates per k point, the coordinates as k_grid.txt prints them."""
+    import json
+
+    pb = E.Problem(E.parse_input(GOLDEN_INPUT))
+    pb.write_kpt(str(tmp_path))
+    lines = (tmp_path / "kpt.txt").read_text().splitlines()
+    assert len(lines) == 4900
+    assert lines[0] == "0 0 0 0 0 -0.5 -0.5" and lines[71].startswith("71 0 1 1 ")
+    ref = json.load(open(os.path.join(GOLDEN, "ab5_kgrid.json")))
+    assert [" ".join(l.split()[4:]) for l in lines[:3]] == ref["head"]
+    assert [" ".join(l.split()[4:]) for l in lines[-3:]] == ref["tail"]
+
+
 def test_test_matrices_known_answer():
     """Source_Main/test_matrix_k.cpp prints H, U, dx, dy at k = (0, 0.3, 0.1)."""
     p = E.parse_input(GOLDEN_INPUT)
