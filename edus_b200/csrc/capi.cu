@@ -921,6 +921,68 @@ int edus_problem_write_kgrid(const edus_problem* pb, const char* outdir) {
   return write_kgrid(pb->P, outdir);
 }
 
+// <workdir>/Test_matrices.txt: H, U, U H U^dagger, U U^dagger and the dipoles
+// of the model at crystal k = (0, 0.3, 0.1), printed as the reference's
+// set-up prints them (Source_Main/test_matrix_k.cpp:1-105).
+int edus_problem_write_test_matrices(const edus_problem* pb, const char* workdir) {
+  if (!pb || !workdir) return fail(EDUS_EINVAL, "null argument");
+  const Problem& P = pb->P;
+  const int n = P.ncv;
+  const double k[3] = {0, 0.3, 0.1};
+  std::vector<cd> H((size_t)n * n), U((size_t)n * n), D((size_t)n * n * 3);
+  int rc = model_hud(P, k, H.data(), U.data(), D.data());
+  if (rc) return rc;
+  std::ofstream t(std::string(workdir) + "/Test_matrices.txt");
+  if (!t) return fail(EDUS_EIO, "cannot write into %s", workdir);
+  auto h = [&](int i, int j) { return H[(size_t)i * n + j]; };
+  auto u = [&](int i, int j) { return U[(size_t)i * n + j]; };
+  t << "k = " << k[0] << " " << k[1] << " " << k[2] << std::endl;
+  t << "Energy: \n";
+  for (int ic = 0; ic < n; ic++) {
+    for (int jc = 0; jc < n; jc++) t << h(ic, jc) << " ";
+    t << "\n";
+  }
+  t << "\n";
+  t << "Unitary: \n";
+  for (int ic = 0; ic < n; ic++) {
+    for (int jc = 0; jc < n; jc++) t << u(ic, jc) << " ";
+    t << "\n";
+  }
+  t << "\n";
+  t << "U E_W U_dagger (to compare with eq. 104 in notes).\n";
+  for (int ic = 0; ic < n; ic++) {
+    for (int jc = 0; jc < n; jc++) {
+      cd e2 = 0.;
+      for (int mc = 0; mc < n; mc++)
+        for (int nc = 0; nc < n; nc++) e2 += u(ic, mc) * h(mc, nc) * std::conj(u(jc, nc));
+      t << e2 << " ";
+    }
+    t << "\n";
+  }
+  t << "U  U_dagger (should be 1).\n";
+  for (int ic = 0; ic < n; ic++) {
+    for (int jc = 0; jc < n; jc++) {
+      cd e2 = 0.;
+      for (int mc = 0; mc < n; mc++) e2 += u(ic, mc) * std::conj(u(jc, mc));
+      t << e2 << " ";
+      if (std::abs(e2) > 1e-10 && ic != jc) t << "ERROR" << " ";
+      if (std::abs(e2 - 1.) > 1e-10 && ic == jc) t << "ERROR" << " ";
+    }
+    t << "\n";
+  }
+  t << "\n";
+  const char* lab[3] = {"dx: \n", "dy: \n", "dz: \n"};
+  for (int x = 0; x < 3; x++) {
+    t << lab[x];
+    for (int ic = 0; ic < n; ic++) {
+      for (int jc = 0; jc < n; jc++) t << D[((size_t)ic * n + jc) * 3 + x] << " ";
+      t << "\n";
+    }
+    t << "\n";
+  }
+  return t ? 0 : fail(EDUS_EIO, "write error in %s/Test_matrices.txt", workdir);
+}
+
 // <workdir>/kpt.txt: "ik i0 i1 i2 k0 k1 k2" per k point of the Monkhorst-Pack
 // grid, default stream format, as BZ_parameters writes it while it builds the
 // grid (headers/InitParameters.h:17-39).
@@ -1490,10 +1552,16 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
   if (c->snap_on && (rc = write_snapshots(c, d))) return rc;
   if ((rc = write_initial(c, d))) return rc;
   std::ofstream fe(d + "/EF.txt"), fl(d + "/Losses.txt");
+  // Exciton.txt receives one empty line per output instant, J3.txt and
+  // Jintra.txt are opened with the currents and left empty, as in the
+  // reference (Source_Main/open_files.cpp:22-36, headers/Observables_MPI.h:407)
+  std::ofstream fx(d + "/Exciton.txt");
   std::ofstream f1, f2, ft;
   if (c->P.p.current) {
     f1.open(d + "/J1.txt");
     f2.open(d + "/J2.txt");
+    std::ofstream(d + "/J3.txt");
+    std::ofstream(d + "/Jintra.txt");
   }
   if (c->P.p.tabs) ft.open(d + "/TransientAbs.txt");
   // k-resolved transient absorption: one file per TAbsK point, opened and left
@@ -1514,6 +1582,7 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
     fl << std::setprecision(16) << tfs << "   ";
     for (int i = 0; i < ncv; i++) fl << std::setprecision(16) << o.pop[i] << "   ";
     fl << std::endl;
+    fx << std::endl;
     if (c->P.p.current) {
       f1 << std::setw(15) << std::setprecision(8) << tfs;
       for (int x = 0; x < 3; x++) {

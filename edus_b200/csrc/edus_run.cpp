@@ -114,6 +114,7 @@ int main(int argc, char** argv) {
   edus_problem_info info;
   edus_problem_info_get(pb, &info);
   edus_problem_write_kpt(pb, workdir.c_str());
+  edus_problem_write_test_matrices(pb, workdir.c_str());
 
   edus_options o;
   edus_options_default(&o);

@@ -42,6 +42,7 @@ def load_library():
         "edus_problem_free": (None, [vp]),
         "edus_problem_write_kgrid": (C.c_int, [vp, cp]),
         "edus_problem_write_kpt": (C.c_int, [vp, cp]),
+        "edus_problem_write_test_matrices": (C.c_int, [vp, cp]),
         "edus_model_hud": (C.c_int, [vp, P(dbl), vp, vp, vp]),
         "edus_struct_sizes": (C.c_int, [P(C.c_int64)]),
         "edus_options_default": (C.c_int, [P(abi.Options)]),
@@ -198,6 +199,10 @@ class Problem:
     def write_kpt(self, workdir):
         """workdir/kpt.txt as the reference's BZ_parameters writes it (edus_problem_write_kpt)."""
         _check(self._L.edus_problem_write_kpt(self._h, os.fsencode(workdir)), "edus_problem_write_kpt")
+
+    def write_test_matrices(self, workdir):
+        """workdir/Test_matrices.txt as the reference's set-up prints it."""
+        _check(self._L.edus_problem_write_test_matrices(self._h, os.fsencode(workdir)), "edus_problem_write_test_matrices")
 
     def model_hud(self, kcrys):
         """H, U, D of the model at one crystal k point (gHUD)."""

@@ -200,6 +200,10 @@ int edus_problem_write_kgrid(const edus_problem* pb, const char* outdir);
  * the reference's BZ_parameters leaves in its working directory
  * (headers/InitParameters.h:17-39); edus_run writes it at set-up. */
 int edus_problem_write_kpt(const edus_problem* pb, const char* workdir);
+/* Write workdir/Test_matrices.txt: H, U, U H U^dagger, U U^dagger and the
+ * dipoles at crystal k = (0, 0.3, 0.1), as the reference's set-up prints them
+ * (Source_Main/test_matrix_k.cpp); edus_run writes it at set-up. */
+int edus_problem_write_test_matrices(const edus_problem* pb, const char* workdir);
 /* H(k), U(k) and D(k) of the problem's model at one crystal k point, as
  * gHUD (headers/HUD.h:5-20) returns them: H, U [n][n], D [n][n][3] interleaved
  * complex. */

@@ -9,6 +9,7 @@ Writes (all small, committed):
                          4th output row (830 of 3319), at printed precision
   ab5_kgrid.json         its Output/k_grid.txt: SHA-256 of the bytes, line
                          count and the first and last lines
+  ab5_test_matrices.txt  its Test_matrices.txt as shipped (byte comparison)
   test_matrices.npz      H, U, dx, dy at k=(0,0.3,0.1) from Test_matrices.txt
   ../../edus_b200/data/coulomb_ncut20.npz
                          Output/Coulomb/{A,B,C,D}_coeff, Screen_const and
@@ -73,8 +74,14 @@ def kgrid(ref):
         json.dump(out, f, indent=1)
 
 
+def test_matrices_text(ref):
+    with open(os.path.join(ref, AB5, "Test_matrices.txt"), "rb") as f, open(os.path.join(HERE, "ab5_test_matrices.txt"), "wb") as o:
+        o.write(f.read())
+
+
 def main(ref):
     kgrid(ref)
+    test_matrices_text(ref)
     g = os.path.join(ref, AB5)
     with open(os.path.join(g, "input.txt")) as f, open(os.path.join(HERE, "ab5_input.txt"), "w") as o:
         o.write(f.read())

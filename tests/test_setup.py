@@ -80,6 +80,16 @@ def test_kpt_listing(tmp_path):
     assert [" ".join(l.split()[4:]) for l in lines[-3:]] == ref["tail"]
 
 
+def test_test_matrices_file_byte_exact(tmp_path):
+    """Test_matrices.txt of the shipped AB5 run (Source_Main/test_matrix_k.cpp),
+    byte for byte, rounding residues of U H U^dagger included."""
+    pb = E.Problem(E.parse_input(GOLDEN_INPUT))
+    pb.write_test_matrices(str(tmp_path))
+    got = (tmp_path / "Test_matrices.txt").read_bytes()
+    ref = open(os.path.join(GOLDEN, "ab5_test_matrices.txt"), "rb").read()
+    assert got == ref
+
+
 def test_test_matrices_known_answer():
     """Source_Main/test_matrix_k.cpp prints H, U, dx, dy at k = (0, 0.3, 0.1)."""
     p = E.parse_input(GOLDEN_INPUT)
