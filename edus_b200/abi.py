@@ -113,6 +113,9 @@ class Params(C.Structure):
         ("tabs_k", C.c_int32),
         ("n_tabs_k", C.c_int32),
         ("tabs_k_pts", (C.c_double * 3) * EDUS_MAX_TABSK),
+        ("kpt_read", C.c_int32),
+        ("kpt_offset", C.c_int64),
+        ("input_path", C.c_char * EDUS_STRLEN),
     ]
 
 

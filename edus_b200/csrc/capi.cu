@@ -989,6 +989,7 @@ int edus_problem_write_test_matrices(const edus_problem* pb, const char* workdir
 int edus_problem_write_kpt(const edus_problem* pb, const char* workdir) {
   if (!pb || !workdir) return fail(EDUS_EINVAL, "null argument");
   const Problem& P = pb->P;
+  if (P.p.kpt_read) return 0;  // the reference writes it only for its own grid
   std::ofstream f(std::string(workdir) + "/kpt.txt");
   if (!f) return fail(EDUS_EIO, "cannot write into %s", workdir);
   const int* Nk = P.p.nk;

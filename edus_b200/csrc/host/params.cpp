@@ -435,6 +435,10 @@ extern "C" int edus_parse_input(const char* path, edus_params* out) {
   Reader r;
   r.in.open(path);
   if (!r.in.is_open()) return fail(EDUS_EIO, "error opening file %s", path);
+  {
+    char full[4096];
+    snprintf(P.input_path, sizeof(P.input_path), "%s", realpath(path, full) ? full : path);
+  }
   std::string ref;
   r.in >> ref;
   snprintf(P.ref_coord, sizeof(P.ref_coord), "%s", ref.c_str());
@@ -474,7 +478,18 @@ extern "C" int edus_parse_input(const char* path, edus_params* out) {
       rc = end_section(r, "unitcell");
     } else if (ieq(key, "nkpt")) {
       if (!(r.in >> P.nk[0] >> P.nk[1] >> P.nk[2])) return fail(EDUS_EPARSE, "Cannot read Nkpt because the file ended. Correct your input.");
-      if (str.size() == 2 && ieq(str[1], "read")) return fail(EDUS_EUNSUPPORTED, "nkpt read (explicit k list) is not built");
+      if (str.size() == 2) {
+        if (ieq(str[1], "read")) {
+          // the listed k points follow; set-up reads them again from the file
+          P.kpt_read = 1;
+          P.kpt_offset = (int64_t)r.in.tellg();
+          const long nl = (long)P.nk[0] * P.nk[1] * P.nk[2];
+          for (long q = 0; q < nl; q++) {
+            double k0, k1, k2;
+            if (!(r.in >> k0 >> k1 >> k2)) return fail(EDUS_EPARSE, "nkpt read: %ld k points expected", nl);
+          }
+        }
+      }
       rc = end_section(r, "nkpt");
     } else if (ieq(key, "bands")) {
       s.clear();

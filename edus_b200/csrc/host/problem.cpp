@@ -167,9 +167,19 @@ static int setup_geometry(Problem& P) {
   P.n2 = Nk[2];
   for (int c = 0; c < 3; c++) P.dk[c] = 1.0 / Nk[c];
   P.kpt.assign((size_t)P.nk * 3, 0.0);
-  for (int ik = 0; ik < P.nk; ik++) {
-    int iik[3] = {(ik / (Nk[2] * Nk[1])) % Nk[0], (ik / Nk[2]) % Nk[1], ik % Nk[2]};
-    for (int c = 0; c < 3; c++) P.kpt[ik * 3 + c] = (P.dk[c] != 1.0) ? -0.5 + P.dk[c] * iik[c] : 0.0;
+  if (P.p.kpt_read) {
+    // nkpt read: the listed crystal coordinates (headers/ReadInput.h:429-437)
+    std::ifstream f(P.p.input_path);
+    if (!f) return fail(EDUS_EIO, "nkpt read: cannot reopen %s", P.p.input_path);
+    f.seekg((std::streamoff)P.p.kpt_offset);
+    for (int ik = 0; ik < P.nk; ik++)
+      if (!(f >> P.kpt[ik * 3] >> P.kpt[ik * 3 + 1] >> P.kpt[ik * 3 + 2]))
+        return fail(EDUS_EPARSE, "nkpt read: %d k points expected in %s", P.nk, P.p.input_path);
+  } else {
+    for (int ik = 0; ik < P.nk; ik++) {
+      int iik[3] = {(ik / (Nk[2] * Nk[1])) % Nk[0], (ik / Nk[2]) % Nk[1], ik % Nk[2]};
+      for (int c = 0; c < 3; c++) P.kpt[ik * 3 + c] = (P.dk[c] != 1.0) ? -0.5 + P.dk[c] * iik[c] : 0.0;
+    }
   }
   // shells: each new shell is the next larger |k| over the grid points
   int plane = -1;
@@ -271,11 +281,25 @@ static int setup_geometry(Problem& P) {
       double x[3] = {kk[0] + P.bvec[b * 3], kk[1] + P.bvec[b * 3 + 1], kk[2] + P.bvec[b * 3 + 2]};
       double c[3];
       cart_to_crys(P, x, c);
-      bool ok = true;
-      for (int i = 0; i < 3 && ok; i++) {
-        double ci = std::fmod(c[i] + 0.5, 1.) - 0.5;
-        double d = ci - P.kpt[cand * 3 + i];
-        ok = std::fabs(d) < 1.e-08 || std::fabs(d - 1.) < 1.e-08 || std::fabs(d + 1.) < 1.e-08;
+      for (int i = 0; i < 3; i++) c[i] = std::fmod(c[i] + 0.5, 1.) - 0.5;
+      auto match = [&](int k1) {
+        for (int i = 0; i < 3; i++) {
+          const double d = c[i] - P.kpt[(size_t)k1 * 3 + i];
+          if (!(std::fabs(d) < 1.e-08 || std::fabs(d - 1.) < 1.e-08 || std::fabs(d + 1.) < 1.e-08)) return false;
+        }
+        return true;
+      };
+      // a listed grid: the first match in list order, as the reference searches
+      // (headers/CalculateWeigths.h:170-200); the grid: its index, checked
+      bool ok = false;
+      if (P.p.kpt_read) {
+        for (int k1 = 0; k1 < P.nk && !ok; k1++)
+          if (match(k1)) {
+            cand = k1;
+            ok = true;
+          }
+      } else {
+        ok = match(cand);
       }
       if (!ok) {
         bad++;
@@ -611,6 +635,7 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P, bool de
                   "Coulomb coefficients are read from files (Read_Coulomb_from_files); edus_coulomb_generate computes them");
     if (p.ncut < 1 || p.ncut > 64) return fail(EDUS_EINVAL, "Ncut %d out of range", p.ncut);
     if (P.n1 != P.n2) return fail(EDUS_EINVAL, "Coulomb needs a square in-plane grid (Coulomb.h:285)");
+    if (p.kpt_read) return fail(EDUS_EUNSUPPORTED, "Coulomb with nkpt read (the transforms run on the grid's rows)");
     P.ncut = p.ncut;
     rc = read_coulomb(P, workdir);
     if (rc) return rc;

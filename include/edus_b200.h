@@ -126,6 +126,11 @@ typedef struct {
   int32_t tabs_k;
   int32_t n_tabs_k;
   double tabs_k_pts[EDUS_MAX_TABSK][3];
+  /* nkpt read: the k points are listed in the input file after the grid
+   * sizes (headers/ReadInput.h:420-440); set-up reads them from input_path */
+  int32_t kpt_read;
+  int64_t kpt_offset;            /* byte offset of the first listed k point in input_path */
+  char input_path[EDUS_STRLEN];
 } edus_params;
 
 /* Observables at one output instant (headers/Observables_MPI.h). */

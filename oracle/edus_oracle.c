@@ -295,14 +295,28 @@ static void cart_to_crys(const orc* o, const double* x, double* c) {
 
 /* ------------------------------------------------------------ grid & stencil */
 
-/* headers/InitParameters.h:13-40 (BZ_parameters k grid) */
-static void make_grid(orc* o) {
+/* headers/InitParameters.h:13-40 (BZ_parameters k grid); with nkpt read the
+ * listed points (headers/ReadInput.h:429-437) */
+static int make_grid(orc* o) {
   const int* Nk = o->p.nk;
   for (int c = 0; c < 3; c++) o->dk[c] = 1.0 / Nk[c];
+  if (o->p.kpt_read) {
+    FILE* f = fopen(o->p.input_path, "r");
+    if (!f) return EDUS_EIO;
+    fseek(f, (long)o->p.kpt_offset, SEEK_SET);
+    for (int ik = 0; ik < o->nk; ik++)
+      if (fscanf(f, "%lf %lf %lf", &o->kpt[ik * 3], &o->kpt[ik * 3 + 1], &o->kpt[ik * 3 + 2]) != 3) {
+        fclose(f);
+        return EDUS_EPARSE;
+      }
+    fclose(f);
+    return 0;
+  }
   for (int ik = 0; ik < o->nk; ik++) {
     int iik[3] = {(ik / (Nk[2] * Nk[1])) % Nk[0], (ik / Nk[2]) % Nk[1], ik % Nk[2]};
     for (int c = 0; c < 3; c++) o->kpt[ik * 3 + c] = (o->dk[c] != 1.0) ? -0.5 + o->dk[c] * iik[c] : 0.0;
   }
+  return 0;
 }
 
 /* headers/CalculateWeigths.h:1-138 (b-vector shells and weights) */
@@ -413,7 +427,8 @@ static int calc_indices(orc* o) {
         cand[i] = (int)(((r % N) + N) % N);
       }
       int ck = (cand[0] * o->p.nk[1] + cand[1]) * o->p.nk[2] + cand[2];
-      for (int pass = 0; pass < 2 && found < 0; pass++) {
+      /* a listed grid: the reference's linear search only (first match in list order) */
+      for (int pass = o->p.kpt_read ? 1 : 0; pass < 2 && found < 0; pass++) {
         int lo = pass == 0 ? ck : 0, hi = pass == 0 ? ck + 1 : o->nk;
         for (int k1 = lo; k1 < hi; k1++) {
           int ok = 1;
@@ -1562,7 +1577,8 @@ int orc_create(const edus_params* p, const char* workdir, orc** out) {
   else
     o->det_a = fabs(p->a[0][0] * p->a[1][1] - p->a[0][1] * p->a[1][0]);
   o->kpt = xcalloc((size_t)o->nk * 3, sizeof(double));
-  make_grid(o);
+  rc = make_grid(o);
+  if (rc) goto fail;
   rc = calc_weights(o);
   if (rc) goto fail;
   o->nbr = xcalloc((size_t)o->nk * o->nnb, sizeof(int));

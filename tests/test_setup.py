@@ -147,3 +147,52 @@ def test_deferred_problem_is_refused_by_single_solve_contexts(workdir):
     with pytest.raises(E.EdusError) as ei:
         E.Context(pb)
     assert ei.value.code == E.abi.EDUS_EUNSUPPORTED
+
+
+def _listed_grid_input(workdir, order):
+    path = W.hbn_rk4(workdir, n=12, t_fin_fs=0.2, it_res=5)
+    dk = 1.0 / 12  # the grid's own arithmetic (headers/InitParameters.h:31-35)
+    pts = [(0.0, -0.5 + dk * i, -0.5 + dk * j) for i in range(12) for j in range(12)]
+    pts = [pts[q] for q in order]
+    lines = "".join(f"{a!r} {b!r} {c!r}\n" for a, b, c in pts)
+    txt = open(path).read().replace("nkpt{\n1 12 12\n}", "nkpt read{\n1 12 12\n" + lines + "}")
+    open(path, "w").write(txt)
+    return path
+
+
+def test_listed_grid_in_grid_order_equals_the_grid(workdir):
+    """nkpt read (headers/ReadInput.h:420-440) with the Monkhorst-Pack points in
+    grid order: the same tables as the generated grid."""
+    ref = E.Problem(E.parse_input(W.hbn_rk4(f"{workdir}/g", n=12, t_fin_fs=0.2, it_res=5)), f"{workdir}/g")
+    p = E.parse_input(_listed_grid_input(f"{workdir}/l", list(range(144))))
+    assert p.kpt_read == 1
+    pb = E.Problem(p, f"{workdir}/l")
+    for name in ["kpt", "nbr", "weights", "bvec", "H", "U", "D", "P0"]:
+        assert np.array_equal(pb.get(name), ref.get(name)), name
+
+
+def test_listed_grid_in_any_order_matches_oracle(workdir):
+    """A shuffled list: neighbours found by coordinates (the first match in list
+    order, headers/CalculateWeigths.h:140-226), against the oracle's search."""
+    order = list(np.random.default_rng(5).permutation(144))
+    p = E.parse_input(_listed_grid_input(workdir, order))
+    pb, o = compare_setup(p, workdir)
+    kpt = pb.get("kpt")
+    assert np.array_equal(kpt[0], [0.0, -0.5 + (1.0 / 12) * (order[0] // 12), -0.5 + (1.0 / 12) * (order[0] % 12)])
+    nbr = pb.get("nbr")
+    assert sorted(set(nbr.ravel().tolist())) == list(range(144))
+
+
+def test_listed_grid_in_any_order_propagates_as_the_grid(workdir):
+    """The oracle's time loop on the shuffled list and on the grid: the same
+    currents and populations (sums over k do not depend on the order beyond
+    rounding)."""
+    order = list(np.random.default_rng(9).permutation(144))
+    pl = E.parse_input(_listed_grid_input(f"{workdir}/l", order))
+    pg = E.parse_input(W.hbn_rk4(f"{workdir}/g", n=12, t_fin_fs=0.2, it_res=5))
+    ll = Oracle(pl, f"{workdir}/l").run(40)
+    lg = Oracle(pg, f"{workdir}/g").run(40)
+    J1l, J1g = np.array([x["J1"] for x in ll]), np.array([x["J1"] for x in lg])
+    # (the k sums run in another order: rounding at the 1e-18 floor of the early, near-zero currents)
+    assert np.abs(J1l - J1g).max() <= 1e-12 * np.abs(J1g).max() + 1e-17
+    assert np.abs(np.array([x["pop"] for x in ll]) - np.array([x["pop"] for x in lg])).max() < 1e-14
