@@ -316,7 +316,7 @@ static int setup_geometry(Problem& P) {
 
 namespace {
 
-enum TbKind { kHaldaneN = 1, kHaldaneB, kGen2d, kBN };
+enum TbKind { kHaldaneN = 1, kHaldaneB, kGen2d, kBN, kCoreBNN, kCoreBNB, kGraphene, kCoreGraphene };
 
 struct Tb {
   int kind = 0;
@@ -343,8 +343,19 @@ int tb_setup(const edus_params& p, Tb& t) {
     t.rchc = p.hopping[7];
   } else if (nm == "BoronNitride") {
     t.kind = kBN;
+  } else if (nm == "CoreBN_Nedge" || nm == "CoreBN_Bedge") {
+    t.kind = nm == "CoreBN_Nedge" ? kCoreBNN : kCoreBNB;
+  } else if (nm == "Graphene" || nm == "CoreGraphene") {
+    // headers/TightBinding.h:48-72: a = 2.46 A, b = 2.97 eV, no gap
+    t.kind = nm == "Graphene" ? kGraphene : kCoreGraphene;
+    t.a = 2.46 * kSpaceAAu;
+    t.b = 2.97 * kEnergyEvAu;
+    t.g = 0;
   } else {
-    return fail(EDUS_EUNSUPPORTED, "tight-binding model %s is not built (Haldane_CoreBN_Nedge/Bedge, gen2d_hexagonal, BoronNitride are)", nm.c_str());
+    return fail(EDUS_EUNSUPPORTED,
+                "tight-binding model %s is not built (Haldane_CoreBN_Nedge/Bedge, CoreBN_Nedge/Bedge, gen2d_hexagonal, "
+                "BoronNitride, Graphene, CoreGraphene are)",
+                nm.c_str());
   }
   return 0;
 }
@@ -360,6 +371,53 @@ void tb_eval(const Tb& t, int n, const double* k, cd* H, cd* U, cd* D) {
   }
   for (int e = 0; e < n * n * 3; e++) D[e] = 0;
   const double tp1 = 2. * kPi * k1, tp2 = 2. * kPi * k2;
+  auto d = [&](int i, int j, int x) -> cd& { return D[(i * n + j) * 3 + x]; };
+  if (t.kind == kCoreBNN || t.kind == kCoreBNB) {
+    // headers/TightBinding.h:177-207 (energy), :894-921 (unitary), dipoles as the Haldane edges
+    const cd f = (1. + eiphi(tp1)) + eiphi(tp2);
+    H[0] = t.kind == kCoreBNN ? -15.06 : -6.91;
+    H[1 * n + 1] = -t.g / 2.;
+    H[1 * n + 2] = t.b * std::conj(f);
+    H[2 * n + 1] = t.b * f;
+    H[2 * n + 2] = t.g / 2.;
+    const double E = std::sqrt(t.g * t.g + 4. * t.b * t.b * f * std::conj(f)).real() / 2.;
+    const double a = std::sqrt((t.g + 2. * E) / (4. * E)), h = std::sqrt((2. * E - t.g) / (4. * E));
+    U[0] = 1.;
+    U[1 * n + 1] = a;
+    U[1 * n + 2] = -h * std::conj(f) / std::abs(f);
+    U[2 * n + 1] = h;
+    U[2 * n + 2] = a * std::conj(f) / std::abs(f);
+    const double ay = t.a / std::sqrt(3.);
+    if (t.kind == kCoreBNN) {
+      d(0, 1, 0) = d(1, 0, 0) = 0.0697595094;
+      d(2, 2, 1) = ay;
+    } else {
+      d(0, 2, 0) = d(2, 0, 0) = 0.0869151662;
+      d(2, 2, 1) = ay;
+      d(0, 0, 1) = ay;
+    }
+    return;
+  }
+  if (t.kind == kGraphene || t.kind == kCoreGraphene) {
+    // headers/TightBinding.h:209-255 (energy), :1032-1059 (unitary), :1280-1285, 1345-1360 (dipoles)
+    const int o2 = t.kind == kCoreGraphene ? 2 : 0;
+    if (o2) {
+      H[0] = H[1 * n + 1] = -10.892178;
+      U[0] = U[1 * n + 1] = 1.;
+      d(0, 2, 0) = d(1, 3, 0) = d(2, 0, 0) = d(3, 1, 0) = 0.0780088;
+      d(1, 1, 1) = d(3, 3, 1) = -2.68341111;
+    } else {
+      d(1, 1, 1) = -2.68341111;
+    }
+    const cd f = (eiphi(tp1) + 1.) + eiphi(tp2);
+    H[o2 * n + o2 + 1] = std::conj(f) * t.b;
+    H[(o2 + 1) * n + o2] = f * t.b;
+    const cd fm = (eiphi(-tp1) + 1.) + eiphi(-tp2);
+    U[o2 * n + o2] = U[(o2 + 1) * n + o2] = 1. / std::sqrt(2.);
+    U[o2 * n + o2 + 1] = -fm / (std::sqrt(2.) * std::abs(fm));
+    U[(o2 + 1) * n + o2 + 1] = fm / (std::sqrt(2.) * std::abs(fm));
+    return;
+  }
   double Bx = t.b * (1. + std::cos(tp1) + std::cos(tp2));
   double By = t.b * (std::sin(tp1) + std::sin(tp2));
   double Bz = -t.g / 2.;
@@ -383,7 +441,6 @@ void tb_eval(const Tb& t, int n, const double* k, cd* H, cd* U, cd* D) {
     Bz = -t.g / 2. - 2. * t.t2 * std::sin(t.phi0) * (std::sin(-tp2 + tp1) + std::sin(tp2) + std::sin(-tp1));
     U[0] = 1.;
     double ay = t.a / std::sqrt(3.);
-    auto d = [&](int i, int j, int x) -> cd& { return D[(i * n + j) * 3 + x]; };
     if (t.kind == kHaldaneN) {
       d(0, 1, 0) = d(1, 0, 0) = 0.0697595094;
       d(2, 2, 1) = ay;

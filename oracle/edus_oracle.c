@@ -455,7 +455,7 @@ static int calc_indices(orc* o) {
 
 /* ------------------------------------------------------------ TB models */
 
-enum { TB_HALDANE_N = 1, TB_HALDANE_B, TB_GEN2D, TB_BN };
+enum { TB_HALDANE_N = 1, TB_HALDANE_B, TB_GEN2D, TB_BN, TB_COREBN_N, TB_COREBN_B, TB_GRAPHENE, TB_COREGRAPHENE };
 
 /* headers/TightBinding.h:43-173 (init / set_hopping) for the models built here */
 static int tb_init(orc* o) {
@@ -484,6 +484,14 @@ static int tb_init(orc* o) {
     o->tb_rchc = o->p.hopping[7];
   } else if (!strcmp(nm, "BoronNitride")) {
     o->tb_kind = TB_BN;
+  } else if (!strcmp(nm, "CoreBN_Nedge") || !strcmp(nm, "CoreBN_Bedge")) {
+    o->tb_kind = !strcmp(nm, "CoreBN_Nedge") ? TB_COREBN_N : TB_COREBN_B;
+  } else if (!strcmp(nm, "Graphene") || !strcmp(nm, "CoreGraphene")) {
+    /* TightBinding.h:48-72: a = 2.46 A, b = 2.97 eV, no gap */
+    o->tb_kind = !strcmp(nm, "Graphene") ? TB_GRAPHENE : TB_COREGRAPHENE;
+    o->tb_a = 2.46 * SPACE_A_AU;
+    o->tb_b = 2.97 * eV;
+    o->tb_g = 0;
   } else {
     return EDUS_EUNSUPPORTED;
   }
@@ -496,6 +504,29 @@ static cplx cexpi(double phase) { return cos(phase) + I * sin(phase); }
 static cplx tb_energy(const orc* o, int ic, int jc, const double* k) {
   double g = o->tb_g, b = o->tb_b, t2 = o->tb_t2, phi0 = o->tb_phi0;
   double k1 = k[1], k2 = k[2];
+  if (o->tb_kind == TB_COREBN_N || o->tb_kind == TB_COREBN_B) {
+    /* TightBinding.h:177-207 */
+    cplx f = (1. + cexpi(2. * PI * k1)) + cexpi(2. * PI * k2);
+    if (ic == 0) return jc == 0 ? (o->tb_kind == TB_COREBN_N ? -15.06 : -6.91) : 0;
+    if (ic == 1) return jc == 1 ? -g / 2. : (jc == 2 ? b * conj(f) : 0);
+    if (ic == 2) return jc == 1 ? b * f : (jc == 2 ? g / 2. : 0);
+    return 0;
+  }
+  if (o->tb_kind == TB_GRAPHENE) {
+    /* TightBinding.h:209-222 */
+    if (ic == jc) return 0.;
+    cplx f = (cexpi(2. * PI * k1) + 1.) + cexpi(2. * PI * k2);
+    return ic == 0 ? conj(f) * b : f * b;
+  }
+  if (o->tb_kind == TB_COREGRAPHENE) {
+    /* TightBinding.h:241-255 */
+    if (ic == jc && ic < 2) return -10.892178;
+    if (ic >= 2 && jc >= 2 && ic != jc) {
+      cplx f = (cexpi(2. * PI * k1) + 1.) + cexpi(2. * PI * k2);
+      return ic == 2 ? conj(f) * b : f * b;
+    }
+    return 0.;
+  }
   if (o->tb_kind == TB_BN) {
     if (ic == jc) return ic == 0 ? -g / 2 : (ic == 1 ? g / 2 : 0);
     cplx f = (cexpi(2. * PI * k1) + 1.) + cexpi(2. * PI * k2);
@@ -535,6 +566,29 @@ static cplx tb_energy(const orc* o, int ic, int jc, const double* k) {
 static cplx tb_unitary(const orc* o, int ic, int jc, const double* k) {
   double g = o->tb_g, b = o->tb_b, t2 = o->tb_t2, phi0 = o->tb_phi0;
   double k1 = k[1], k2 = k[2];
+  if (o->tb_kind == TB_COREBN_N || o->tb_kind == TB_COREBN_B) {
+    /* TightBinding.h:894-921 */
+    if (ic == 0) return jc == 0 ? 1. : 0.;
+    if (jc == 0) return 0.;
+    cplx f = (1. + cexpi(2. * PI * k1)) + cexpi(2. * PI * k2);
+    double E = creal(csqrt(g * g + 4. * b * b * f * conj(f))) / 2.;
+    double a = sqrt((g + 2. * E) / (4. * E));
+    double h = sqrt((2. * E - g) / (4. * E));
+    if (ic == 1) return jc == 1 ? (cplx)a : -h * conj(f) / cabs(f);
+    if (ic == 2) return jc == 1 ? (cplx)h : a * conj(f) / cabs(f);
+    return 0.;
+  }
+  if (o->tb_kind == TB_GRAPHENE || o->tb_kind == TB_COREGRAPHENE) {
+    /* TightBinding.h:1032-1059 */
+    int off2 = o->tb_kind == TB_COREGRAPHENE ? 2 : 0;
+    if (ic < off2) return ic == jc ? 1. : 0.;
+    if (jc == off2 + 1) {
+      cplx f = (cexpi(-2. * PI * k1) + 1.) + cexpi(-2. * PI * k2);
+      return ic == off2 ? -f / (sqrt(2.) * cabs(f)) : f / (sqrt(2.) * cabs(f));
+    }
+    if (jc == off2) return 1. / sqrt(2.);
+    return 0.;
+  }
   int off = 0;
   if (o->tb_kind != TB_BN) {
     if (ic == 0) return jc == 0 ? 1. : 0.;
@@ -581,6 +635,22 @@ static cplx tb_dipole(const orc* o, int ic, int jc, int x) {
       return 0.;
     case TB_BN:
       if (x == 1) return (ic == 1 && jc == 1) ? a / sqrt(3) : 0.;
+      return 0.;
+    case TB_COREBN_N:
+      if (x == 0) return ((ic == 0 && jc == 1) || (ic == 1 && jc == 0)) ? 0.0697595094 : 0.;
+      if (x == 1) return (ic == 2 && jc == 2) ? a / sqrt(3.) : 0.;
+      return 0.;
+    case TB_COREBN_B:
+      if (x == 0) return ((ic == 0 && jc == 2) || (ic == 2 && jc == 0)) ? 0.0869151662 : 0.;
+      if (x == 1) return ((ic == 2 && jc == 2) || (ic == 0 && jc == 0)) ? a / sqrt(3.) : 0.;
+      return 0.;
+    case TB_GRAPHENE:
+      if (x == 1) return (ic == 1 && jc == 1) ? -2.68341111 : 0.;
+      return 0.;
+    case TB_COREGRAPHENE:
+      if (x == 0)
+        return ((ic == 0 && jc == 2) || (ic == 1 && jc == 3) || (ic == 2 && jc == 0) || (ic == 3 && jc == 1)) ? 0.0780088 : 0.;
+      if (x == 1) return (ic == jc && ic % 2 == 1) ? -2.68341111 : 0.;
       return 0.;
   }
   return 0.;

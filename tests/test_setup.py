@@ -196,3 +196,23 @@ def test_listed_grid_in_any_order_propagates_as_the_grid(workdir):
     # (the k sums run in another order: rounding at the 1e-18 floor of the early, near-zero currents)
     assert np.abs(J1l - J1g).max() <= 1e-12 * np.abs(J1g).max() + 1e-17
     assert np.abs(np.array([x["pop"] for x in ll]) - np.array([x["pop"] for x in lg])).max() < 1e-14
+
+
+@pytest.mark.parametrize("model,nb", [("CoreBN_Nedge", 3), ("CoreBN_Bedge", 3), ("Graphene", 2), ("CoreGraphene", 4)])
+def test_more_tight_binding_models_match_oracle(workdir, model, nb):
+    """Tight-binding models with their closed-form H, U and dipoles
+    (headers/TightBinding.h:43-1421): the set-up tables against the oracle's,
+    U unitary and U H U^dagger diagonal (the reference's Test_matrices check)."""
+    path = W.hbn_rk4(workdir, n=12, t_fin_fs=0.2, it_res=5)
+    txt = open(path).read()
+    txt = txt.replace(txt.splitlines()[3] + "\n", f"tightbinding {model}\n")
+    open(path, "w").write(txt)
+    p = E.parse_input(path)
+    pb, o = compare_setup(p, workdir)
+    assert pb.info.ncv == nb
+    H, U = pb.get("H"), pb.get("U")
+    UU = np.einsum("kij,klj->kil", U, U.conj())
+    assert np.abs(UU - np.eye(nb)).max() < 1e-12
+    E2 = np.einsum("kim,kmn,kjn->kij", U, H, U.conj())
+    off = E2 - np.einsum("kii->ki", E2)[:, :, None] * np.eye(nb)
+    assert np.abs(off).max() < 1e-12 * max(1.0, np.abs(H).max())
