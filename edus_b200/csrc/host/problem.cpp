@@ -316,7 +316,19 @@ static int setup_geometry(Problem& P) {
 
 namespace {
 
-enum TbKind { kHaldaneN = 1, kHaldaneB, kGen2d, kBN, kCoreBNN, kCoreBNB, kGraphene, kCoreGraphene };
+enum TbKind {
+  kHaldaneN = 1,
+  kHaldaneB,
+  kGen2d,
+  kBN,
+  kCoreBNN,
+  kCoreBNB,
+  kGraphene,
+  kCoreGraphene,
+  kGrapheneCostD,
+  kGrapheneSymD,
+  kGrapheneZurron
+};
 
 struct Tb {
   int kind = 0;
@@ -345,16 +357,21 @@ int tb_setup(const edus_params& p, Tb& t) {
     t.kind = kBN;
   } else if (nm == "CoreBN_Nedge" || nm == "CoreBN_Bedge") {
     t.kind = nm == "CoreBN_Nedge" ? kCoreBNN : kCoreBNB;
-  } else if (nm == "Graphene" || nm == "CoreGraphene") {
-    // headers/TightBinding.h:48-72: a = 2.46 A, b = 2.97 eV, no gap
-    t.kind = nm == "Graphene" ? kGraphene : kCoreGraphene;
+  } else if (nm == "Graphene" || nm == "CoreGraphene" || nm == "Graphene_costD" || nm == "Graphene_symmetricD" ||
+             nm == "GrapheneZurron") {
+    // headers/TightBinding.h:48-80: a = 2.46 A, b = 2.97 eV, no gap
+    t.kind = nm == "Graphene"         ? kGraphene
+             : nm == "CoreGraphene"   ? kCoreGraphene
+             : nm == "Graphene_costD" ? kGrapheneCostD
+             : nm == "GrapheneZurron" ? kGrapheneZurron
+                                      : kGrapheneSymD;
     t.a = 2.46 * kSpaceAAu;
     t.b = 2.97 * kEnergyEvAu;
     t.g = 0;
   } else {
     return fail(EDUS_EUNSUPPORTED,
                 "tight-binding model %s is not built (Haldane_CoreBN_Nedge/Bedge, CoreBN_Nedge/Bedge, gen2d_hexagonal, "
-                "BoronNitride, Graphene, CoreGraphene are)",
+                "BoronNitride, Graphene, CoreGraphene, Graphene_costD, Graphene_symmetricD, GrapheneZurron are)",
                 nm.c_str());
   }
   return 0;
@@ -362,8 +379,8 @@ int tb_setup(const edus_params& p, Tb& t) {
 
 inline cd eiphi(double x) { return cd(std::cos(x), std::sin(x)); }
 
-// H, U and D of one k for the tight-binding models.
-void tb_eval(const Tb& t, int n, const double* k, cd* H, cd* U, cd* D) {
+// H, U and D of one k (crystal k, Cartesian kc) for the tight-binding models.
+void tb_eval(const Tb& t, int n, const double* k, const double* kc, cd* H, cd* U, cd* D) {
   const double k1 = k[1], k2 = k[2];
   for (int e = 0; e < n * n; e++) {
     H[e] = 0;
@@ -396,6 +413,38 @@ void tb_eval(const Tb& t, int n, const double* k, cd* H, cd* U, cd* D) {
       d(2, 2, 1) = ay;
       d(0, 0, 1) = ay;
     }
+    return;
+  }
+  if (t.kind == kGrapheneCostD || t.kind == kGrapheneSymD) {
+    // headers/TightBinding.h:225-239 (energy), :1064-1070 (unitary: 1),
+    // :1272-1283, 1349-1357, 1401-1405 (dipoles)
+    const double modf = std::abs((eiphi(tp1) + 1.) + eiphi(tp2));
+    H[0] = H[1 * n + 1] = -10.892178;
+    H[2 * n + 2] = -t.b * modf;
+    H[3 * n + 3] = t.b * modf;
+    for (int i = 0; i < n; i++) U[i * n + i] = 1.;
+    const double dx = 0.0780088 / std::sqrt(2.);
+    d(0, 2, 0) = d(0, 3, 0) = d(1, 2, 0) = dx;
+    d(1, 3, 0) = -dx;
+    d(2, 0, 0) = d(3, 0, 0) = d(2, 1, 0) = dx;
+    d(3, 1, 0) = -dx;
+    const int ny = t.kind == kGrapheneSymD ? 2 : 1;  // the symmetric variant repeats y in z
+    for (int x = 1; x <= ny; x++) {
+      d(1, 1, x) = -2.68341111;
+      d(2, 2, x) = d(3, 3, x) = -2.68341111 / 2;
+      d(2, 3, x) = d(3, 2, x) = 2.68341111 / 2;
+    }
+    return;
+  }
+  if (t.kind == kGrapheneZurron) {
+    // headers/TightBinding.h:257-269 (energy), :1072-1081 (unitary); no dipoles
+    const double a = t.a;
+    const cd f = eiphi(-a * kc[1] / std::sqrt(3.)) * (1. + 2. * eiphi(std::sqrt(3.) * a * kc[1] / 2.) * std::cos(a * kc[2] / 2.));
+    H[1] = f * t.b;
+    H[n] = std::conj(f) * t.b;
+    U[0] = U[n] = 1. / std::sqrt(2.);
+    U[1] = -f / (std::sqrt(2.) * std::abs(f));
+    U[n + 1] = f / (std::sqrt(2.) * std::abs(f));
     return;
   }
   if (t.kind == kGraphene || t.kind == kCoreGraphene) {
@@ -579,7 +628,9 @@ void eval_k(const Problem& P, const Tb& tb, const double* k, cd* H, cd* U, cd* D
     for (int i = 0; i < n; i++)
       for (int j = 0; j < n; j++) Uk[i * n + j] = std::conj(Z[j * n + i]);
   } else {
-    tb_eval(tb, n, k, Hk, Uk, Dk);
+    double kc[3];
+    crys_to_cart(P, k, kc);
+    tb_eval(tb, n, k, kc, Hk, Uk, Dk);
   }
   double S[EDUS_MAX_BANDS];
   const double gapc = P.p.conduction_shift;

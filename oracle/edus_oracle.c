@@ -455,7 +455,19 @@ static int calc_indices(orc* o) {
 
 /* ------------------------------------------------------------ TB models */
 
-enum { TB_HALDANE_N = 1, TB_HALDANE_B, TB_GEN2D, TB_BN, TB_COREBN_N, TB_COREBN_B, TB_GRAPHENE, TB_COREGRAPHENE };
+enum {
+  TB_HALDANE_N = 1,
+  TB_HALDANE_B,
+  TB_GEN2D,
+  TB_BN,
+  TB_COREBN_N,
+  TB_COREBN_B,
+  TB_GRAPHENE,
+  TB_COREGRAPHENE,
+  TB_GRAPHENE_COSTD,
+  TB_GRAPHENE_SYMD,
+  TB_GRAPHENE_ZURRON
+};
 
 /* headers/TightBinding.h:43-173 (init / set_hopping) for the models built here */
 static int tb_init(orc* o) {
@@ -486,9 +498,14 @@ static int tb_init(orc* o) {
     o->tb_kind = TB_BN;
   } else if (!strcmp(nm, "CoreBN_Nedge") || !strcmp(nm, "CoreBN_Bedge")) {
     o->tb_kind = !strcmp(nm, "CoreBN_Nedge") ? TB_COREBN_N : TB_COREBN_B;
-  } else if (!strcmp(nm, "Graphene") || !strcmp(nm, "CoreGraphene")) {
-    /* TightBinding.h:48-72: a = 2.46 A, b = 2.97 eV, no gap */
-    o->tb_kind = !strcmp(nm, "Graphene") ? TB_GRAPHENE : TB_COREGRAPHENE;
+  } else if (!strcmp(nm, "Graphene") || !strcmp(nm, "CoreGraphene") || !strcmp(nm, "Graphene_costD") ||
+             !strcmp(nm, "Graphene_symmetricD") || !strcmp(nm, "GrapheneZurron")) {
+    /* TightBinding.h:48-80: a = 2.46 A, b = 2.97 eV, no gap */
+    o->tb_kind = !strcmp(nm, "Graphene")         ? TB_GRAPHENE
+                 : !strcmp(nm, "CoreGraphene")   ? TB_COREGRAPHENE
+                 : !strcmp(nm, "Graphene_costD") ? TB_GRAPHENE_COSTD
+                 : !strcmp(nm, "GrapheneZurron") ? TB_GRAPHENE_ZURRON
+                                                 : TB_GRAPHENE_SYMD;
     o->tb_a = 2.46 * SPACE_A_AU;
     o->tb_b = 2.97 * eV;
     o->tb_g = 0;
@@ -511,6 +528,24 @@ static cplx tb_energy(const orc* o, int ic, int jc, const double* k) {
     if (ic == 1) return jc == 1 ? -g / 2. : (jc == 2 ? b * conj(f) : 0);
     if (ic == 2) return jc == 1 ? b * f : (jc == 2 ? g / 2. : 0);
     return 0;
+  }
+  if (o->tb_kind == TB_GRAPHENE_COSTD || o->tb_kind == TB_GRAPHENE_SYMD) {
+    /* TightBinding.h:225-239 */
+    if (ic == jc && ic < 2) return -10.892178;
+    if (ic >= 2 && jc >= 2 && ic == jc) {
+      double modf = cabs((cexpi(2. * PI * k1) + 1.) + cexpi(2. * PI * k2));
+      return ic == 2 ? -b * modf : b * modf;
+    }
+    return 0.;
+  }
+  if (o->tb_kind == TB_GRAPHENE_ZURRON) {
+    /* TightBinding.h:257-269, with the Cartesian k */
+    if (ic == jc) return 0.;
+    double kc[3];
+    crys_to_cart(o, k, kc);
+    double a = o->tb_a;
+    cplx f = cexpi(-a * kc[1] / sqrt(3.)) * (1. + 2. * cexpi(sqrt(3.) * a * kc[1] / 2.) * cos(a * kc[2] / 2.));
+    return ic == 0 ? f * b : conj(f) * b;
   }
   if (o->tb_kind == TB_GRAPHENE) {
     /* TightBinding.h:209-222 */
@@ -577,6 +612,16 @@ static cplx tb_unitary(const orc* o, int ic, int jc, const double* k) {
     if (ic == 1) return jc == 1 ? (cplx)a : -h * conj(f) / cabs(f);
     if (ic == 2) return jc == 1 ? (cplx)h : a * conj(f) / cabs(f);
     return 0.;
+  }
+  if (o->tb_kind == TB_GRAPHENE_COSTD || o->tb_kind == TB_GRAPHENE_SYMD) return ic == jc ? 1. : 0.; /* :1064-1070 */
+  if (o->tb_kind == TB_GRAPHENE_ZURRON) {
+    /* TightBinding.h:1072-1081 */
+    if (jc != 1) return 1. / sqrt(2.);
+    double kc[3];
+    crys_to_cart(o, k, kc);
+    double a = o->tb_a;
+    cplx f = cexpi(-a * kc[1] / sqrt(3.)) * (1. + 2. * cexpi(sqrt(3.) * a * kc[1] / 2.) * cos(a * kc[2] / 2.));
+    return ic == 0 ? -f / (sqrt(2.) * cabs(f)) : f / (sqrt(2.) * cabs(f));
   }
   if (o->tb_kind == TB_GRAPHENE || o->tb_kind == TB_COREGRAPHENE) {
     /* TightBinding.h:1032-1059 */
@@ -646,6 +691,22 @@ static cplx tb_dipole(const orc* o, int ic, int jc, int x) {
       return 0.;
     case TB_GRAPHENE:
       if (x == 1) return (ic == 1 && jc == 1) ? -2.68341111 : 0.;
+      return 0.;
+    case TB_GRAPHENE_COSTD:
+    case TB_GRAPHENE_SYMD: {
+      /* TightBinding.h:1272-1283, 1349-1357, 1401-1405 */
+      if (x == 0) {
+        cplx dx = 0.0780088 / sqrt(2.);
+        if (ic <= 1 && jc > 1) return (ic == 0 || (ic == 1 && jc == 2)) ? dx : -dx;
+        if (ic > 1 && jc <= 1) return conj((jc == 0 || (jc == 1 && ic == 2)) ? dx : -dx);
+        return 0.;
+      }
+      if (x == 2 && o->tb_kind == TB_GRAPHENE_COSTD) return 0.;
+      if (ic == 1 && jc == 1) return -2.68341111;
+      if (ic > 1 && jc > 1) return ic == jc ? -2.68341111 / 2 : 2.68341111 / 2;
+      return 0.;
+    }
+    case TB_GRAPHENE_ZURRON:
       return 0.;
     case TB_COREGRAPHENE:
       if (x == 0)

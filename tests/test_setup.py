@@ -198,7 +198,8 @@ def test_listed_grid_in_any_order_propagates_as_the_grid(workdir):
     assert np.abs(np.array([x["pop"] for x in ll]) - np.array([x["pop"] for x in lg])).max() < 1e-14
 
 
-@pytest.mark.parametrize("model,nb", [("CoreBN_Nedge", 3), ("CoreBN_Bedge", 3), ("Graphene", 2), ("CoreGraphene", 4)])
+@pytest.mark.parametrize("model,nb", [("CoreBN_Nedge", 3), ("CoreBN_Bedge", 3), ("Graphene", 2), ("CoreGraphene", 4),
+                                      ("Graphene_costD", 4), ("Graphene_symmetricD", 4), ("GrapheneZurron", 2)])
 def test_more_tight_binding_models_match_oracle(workdir, model, nb):
     """Tight-binding models with their closed-form H, U and dipoles
     (headers/TightBinding.h:43-1421): the set-up tables against the oracle's,
