@@ -102,38 +102,67 @@ void eig_herm(int n, cd* A, double* evals, cd* Z) {
   std::copy(Zs.begin(), Zs.end(), Z);
 }
 
-// Least squares min |A w - q| by Householder QR in long double (A: rows x cols).
+// Minimum-norm least squares w = A^+ q (A: rows x cols, row-major), the
+// pseudo-inverse with singular values at or below 1e-16 dropped, as the
+// reference solves for the b-shell weights (pinv(A, 1.e-16) * q,
+// headers/CalculateWeigths.h:100). The singular value decomposition is a
+// one-sided Jacobi one in long double: column rotations of A (accumulated in
+// V) until the columns are orthogonal, whose norms are then the singular
+// values. On a lattice whose shell equations are rank deficient (orthorhombic
+// cells) the minimum-norm choice is what fixes the weights.
 static void lstsq(int rows, int cols, const double* A, const double* q, double* w) {
-  std::vector<long double> R((size_t)rows * cols), b(q, q + rows);
-  for (int i = 0; i < rows * cols; i++) R[i] = A[i];
-  for (int c = 0; c < cols; c++) {
-    long double nrm = 0;
-    for (int r = c; r < rows; r++) nrm += R[r * cols + c] * R[r * cols + c];
-    nrm = std::sqrt(nrm);
-    if (nrm == 0) continue;
-    long double alpha = R[c * cols + c] > 0 ? -nrm : nrm;
-    std::vector<long double> v(rows, 0);
-    for (int r = c; r < rows; r++) v[r] = R[r * cols + c];
-    v[c] -= alpha;
-    long double vn = 0;
-    for (int r = c; r < rows; r++) vn += v[r] * v[r];
-    if (vn == 0) continue;
-    for (int j = c; j < cols; j++) {
-      long double d = 0;
-      for (int r = c; r < rows; r++) d += v[r] * R[r * cols + j];
-      d = 2 * d / vn;
-      for (int r = c; r < rows; r++) R[r * cols + j] -= d * v[r];
-    }
-    long double d = 0;
-    for (int r = c; r < rows; r++) d += v[r] * b[r];
-    d = 2 * d / vn;
-    for (int r = c; r < rows; r++) b[r] -= d * v[r];
+  std::vector<long double> U((size_t)rows * cols), V((size_t)cols * cols, 0.0L);
+  for (int i = 0; i < rows * cols; i++) U[i] = A[i];
+  for (int i = 0; i < cols; i++) V[(size_t)i * cols + i] = 1.0L;
+  for (int sweep = 0; sweep < 80; sweep++) {
+    long double worst = 0;
+    for (int p = 0; p < cols; p++)
+      for (int r = p + 1; r < cols; r++) {
+        long double app = 0, arr = 0, apr = 0;
+        for (int i = 0; i < rows; i++) {
+          const long double x = U[(size_t)i * cols + p], y = U[(size_t)i * cols + r];
+          app += x * x;
+          arr += y * y;
+          apr += x * y;
+        }
+        if (apr == 0 || app == 0 || arr == 0) continue;
+        const long double rel = std::fabs(apr) / std::sqrt(app * arr);
+        worst = std::max(worst, rel);
+        if (rel < 1e-19L) continue;
+        const long double zeta = (arr - app) / (2 * apr);
+        const long double t = (zeta >= 0 ? 1.0L : -1.0L) / (std::fabs(zeta) + std::sqrt(1 + zeta * zeta));
+        const long double c = 1 / std::sqrt(1 + t * t), sn = c * t;
+        for (int i = 0; i < rows; i++) {
+          long double& x = U[(size_t)i * cols + p];
+          long double& y = U[(size_t)i * cols + r];
+          const long double x0 = x;
+          x = c * x0 - sn * y;
+          y = sn * x0 + c * y;
+        }
+        for (int i = 0; i < cols; i++) {
+          long double& x = V[(size_t)i * cols + p];
+          long double& y = V[(size_t)i * cols + r];
+          const long double x0 = x;
+          x = c * x0 - sn * y;
+          y = sn * x0 + c * y;
+        }
+      }
+    if (worst < 1e-19L) break;
   }
-  for (int c = cols - 1; c >= 0; c--) {
-    long double acc = b[c];
-    for (int j = c + 1; j < cols; j++) acc -= R[c * cols + j] * (long double)w[j];
-    long double diag = R[c * cols + c];
-    w[c] = (std::fabs((double)diag) > 1e-300) ? (double)(acc / diag) : 0.0;
+  std::vector<long double> coef(cols, 0.0L);
+  for (int j = 0; j < cols; j++) {
+    long double s2 = 0, uq = 0;
+    for (int i = 0; i < rows; i++) {
+      s2 += U[(size_t)i * cols + j] * U[(size_t)i * cols + j];
+      uq += U[(size_t)i * cols + j] * q[i];
+    }
+    // column j of the rotated A is sigma_j u_j: (u_j . q) / sigma_j = (col . q) / sigma_j^2
+    if (std::sqrt(s2) > 1e-16L) coef[j] = uq / s2;
+  }
+  for (int i = 0; i < cols; i++) {
+    long double acc = 0;
+    for (int j = 0; j < cols; j++) acc += V[(size_t)i * cols + j] * coef[j];
+    w[i] = (double)acc;
   }
 }
 
@@ -327,12 +356,23 @@ enum TbKind {
   kCoreGraphene,
   kGrapheneCostD,
   kGrapheneSymD,
-  kGrapheneZurron
+  kGrapheneZurron,
+  kBN1b,
+  kVampa,
+  kGeS
 };
+
+// Vampa2015 model: cosine series of the two bands along each crystal axis,
+// E_c(k) = sum_x sum_j v[c][x][j] cos(j k_x) (+ the gap for the conduction
+// band); parameters as headers/TightBinding.h:98-122 tabulates them
+constexpr double kVampaCoeff[2][3][6] = {
+    {{-0.0928, 0.0705, 0.0200, -0.0012, 0.0029, 0.0006}, {-0.0307, 0.0307, 0, 0, 0, 0}, {-0.0059, 0.0059, 0, 0, 0, 0}},
+    {{0.0898, -0.0814, -0.0024, -0.0048, -0.0003, -0.0009}, {0.1147, -0.1147, 0, 0, 0, 0}, {0.0435, -0.0435, 0, 0, 0, 0}}};
 
 struct Tb {
   int kind = 0;
   double a = 2.5 * kSpaceAAu, b = 3.16 * kEnergyEvAu, g = 6.2 * kEnergyEvAu, t2 = 0, phi0 = 0, core = 0, rchv = 0, rchc = 0;
+  double c = 0, d = 0, f = 0;  // GeS second-neighbour hoppings and first-neighbour hopping
 };
 
 int tb_setup(const edus_params& p, Tb& t) {
@@ -355,6 +395,22 @@ int tb_setup(const edus_params& p, Tb& t) {
     t.rchc = p.hopping[7];
   } else if (nm == "BoronNitride") {
     t.kind = kBN;
+  } else if (nm == "BN1b") {
+    t.kind = kBN1b;
+  } else if (nm == "Vampa2015") {
+    t.kind = kVampa;
+    t.g = 0.1213;
+  } else if (nm == "GeS" || nm == "GeS_HSE06") {
+    // headers/TightBinding.h:135-154
+    const double eV = kEnergyEvAu;
+    t.kind = kGeS;
+    const bool hse = nm == "GeS_HSE06";
+    t.g = (hse ? 0.62 : 0.41) * eV;
+    t.f = (hse ? 2.91 : -2.33) * eV;
+    t.t2 = (hse ? -0.797 : 0.61) * eV;
+    t.b = (hse ? -0.05 : 0.13) * eV;
+    t.c = (hse ? -0.14 : 0.07) * eV;
+    t.d = (hse ? 0.106 : -0.09) * eV;
   } else if (nm == "CoreBN_Nedge" || nm == "CoreBN_Bedge") {
     t.kind = nm == "CoreBN_Nedge" ? kCoreBNN : kCoreBNB;
   } else if (nm == "Graphene" || nm == "CoreGraphene" || nm == "Graphene_costD" || nm == "Graphene_symmetricD" ||
@@ -371,7 +427,8 @@ int tb_setup(const edus_params& p, Tb& t) {
   } else {
     return fail(EDUS_EUNSUPPORTED,
                 "tight-binding model %s is not built (Haldane_CoreBN_Nedge/Bedge, CoreBN_Nedge/Bedge, gen2d_hexagonal, "
-                "BoronNitride, Graphene, CoreGraphene, Graphene_costD, Graphene_symmetricD, GrapheneZurron are)",
+                "BoronNitride, BN1b, Graphene, CoreGraphene, Graphene_costD, Graphene_symmetricD, GrapheneZurron, "
+                "Vampa2015, GeS, GeS_HSE06 are)",
                 nm.c_str());
   }
   return 0;
@@ -413,6 +470,47 @@ void tb_eval(const Tb& t, int n, const double* k, const double* kc, cd* H, cd* U
       d(2, 2, 1) = ay;
       d(0, 0, 1) = ay;
     }
+    return;
+  }
+  if (t.kind == kBN1b) {
+    // headers/TightBinding.h:307-311 (one band), :1147-1150 (U = 1), no dipoles
+    const cd f = (eiphi(tp1) + 1.) + eiphi(tp2);
+    H[0] = 0.5 * std::sqrt(t.g * t.g + 4. * t.b * t.b * f * std::conj(f)).real();
+    U[0] = 1.;
+    return;
+  }
+  if (t.kind == kVampa) {
+    // headers/TightBinding.h:312-326 (energy), :1151-1155 (U = 1), dipoles 3.46 in x, y and 3.94 in z off the diagonal
+    for (int c = 0; c < 2; c++) {
+      cd e = 0.;
+      for (int x = 0; x < 3; x++)
+        for (int j = 0; j < 6; j++) e += kVampaCoeff[c][x][j] * std::cos(j * k[x]);
+      if (c == 1) e += t.g;
+      H[c * n + c] = e;
+      U[c * n + c] = 1.;
+    }
+    d(0, 1, 0) = d(1, 0, 0) = d(0, 1, 1) = d(1, 0, 1) = 3.46;
+    d(0, 1, 2) = d(1, 0, 2) = 3.94;
+    return;
+  }
+  if (t.kind == kGeS) {
+    // headers/TightBinding.h:441-462 (energy), :1005-1030 (unitary), :1339-1343 (dipole)
+    const double tor = -2. * t.c * (std::cos(tp1) + std::cos(tp2)) - 2. * t.d * (std::cos(2. * kPi * (k1 - k2)));
+    H[0] = t.g + tor;
+    H[3] = -t.g + tor;
+    const cd phix = eiphi(tp1) + eiphi(tp2);
+    const cd tc = -t.f - t.t2 * phix - t.b * std::conj(phix);
+    H[1] = std::conj(tc);
+    H[2] = tc;
+    const double Bx = tc.real(), By = tc.imag(), Bz = t.g;
+    const double B = std::sqrt(Bx * Bx + By * By + Bz * Bz);
+    const double phi = std::atan2(By, Bx) / 2.;
+    const double c2 = std::sqrt((B + Bz) / 2. / B), s2 = std::sqrt((B - Bz) / 2. / B);
+    U[0] = eiphi(phi) * s2;
+    U[1] = -eiphi(-phi) * c2;
+    U[2] = eiphi(phi) * c2;
+    U[3] = eiphi(-phi) * s2;
+    d(1, 1, 1) = 0.52 * kSpaceAAu;
     return;
   }
   if (t.kind == kGrapheneCostD || t.kind == kGrapheneSymD) {

@@ -66,6 +66,7 @@ struct orc {
   cplx *HR, *xR, *yR, *zR;  /* [n][n][nrpts] as Hvv[i][j][iR] */
   /* tb model constants */
   double tb_a, tb_b, tb_g, tb_t2, tb_phi0, tb_core, tb_rchv, tb_rchc;
+  double tb_c, tb_d, tb_f;  /* GeS hoppings */
   int tb_kind;
   /* dissipation */
   double T[EDUS_MAX_BANDS][EDUS_MAX_BANDS];
@@ -466,8 +467,16 @@ enum {
   TB_COREGRAPHENE,
   TB_GRAPHENE_COSTD,
   TB_GRAPHENE_SYMD,
-  TB_GRAPHENE_ZURRON
+  TB_GRAPHENE_ZURRON,
+  TB_BN1B,
+  TB_VAMPA,
+  TB_GES
 };
+
+/* headers/TightBinding.h:98-122: Vampa2015 cosine-series coefficients [band][axis][j] */
+static const double VAMPA[2][3][6] = {
+    {{-0.0928, 0.0705, 0.0200, -0.0012, 0.0029, 0.0006}, {-0.0307, 0.0307, 0, 0, 0, 0}, {-0.0059, 0.0059, 0, 0, 0, 0}},
+    {{0.0898, -0.0814, -0.0024, -0.0048, -0.0003, -0.0009}, {0.1147, -0.1147, 0, 0, 0, 0}, {0.0435, -0.0435, 0, 0, 0, 0}}};
 
 /* headers/TightBinding.h:43-173 (init / set_hopping) for the models built here */
 static int tb_init(orc* o) {
@@ -496,6 +505,21 @@ static int tb_init(orc* o) {
     o->tb_rchc = o->p.hopping[7];
   } else if (!strcmp(nm, "BoronNitride")) {
     o->tb_kind = TB_BN;
+  } else if (!strcmp(nm, "BN1b")) {
+    o->tb_kind = TB_BN1B;
+  } else if (!strcmp(nm, "Vampa2015")) {
+    o->tb_kind = TB_VAMPA;
+    o->tb_g = 0.1213;
+  } else if (!strcmp(nm, "GeS") || !strcmp(nm, "GeS_HSE06")) {
+    /* TightBinding.h:135-154 */
+    int hse = !strcmp(nm, "GeS_HSE06");
+    o->tb_kind = TB_GES;
+    o->tb_g = (hse ? 0.62 : 0.41) * eV;
+    o->tb_f = (hse ? 2.91 : -2.33) * eV;
+    o->tb_t2 = (hse ? -0.797 : 0.61) * eV;
+    o->tb_b = (hse ? -0.05 : 0.13) * eV;
+    o->tb_c = (hse ? -0.14 : 0.07) * eV;
+    o->tb_d = (hse ? 0.106 : -0.09) * eV;
   } else if (!strcmp(nm, "CoreBN_Nedge") || !strcmp(nm, "CoreBN_Bedge")) {
     o->tb_kind = !strcmp(nm, "CoreBN_Nedge") ? TB_COREBN_N : TB_COREBN_B;
   } else if (!strcmp(nm, "Graphene") || !strcmp(nm, "CoreGraphene") || !strcmp(nm, "Graphene_costD") ||
@@ -528,6 +552,30 @@ static cplx tb_energy(const orc* o, int ic, int jc, const double* k) {
     if (ic == 1) return jc == 1 ? -g / 2. : (jc == 2 ? b * conj(f) : 0);
     if (ic == 2) return jc == 1 ? b * f : (jc == 2 ? g / 2. : 0);
     return 0;
+  }
+  if (o->tb_kind == TB_BN1B) {
+    /* TightBinding.h:307-311 */
+    cplx f = (cexpi(2. * PI * k1) + 1.) + cexpi(2. * PI * k2);
+    return 0.5 * creal(csqrt(g * g + 4. * b * b * f * conj(f)));
+  }
+  if (o->tb_kind == TB_VAMPA) {
+    /* TightBinding.h:312-326 */
+    if (ic != jc) return 0.;
+    cplx e = 0.;
+    for (int x = 0; x < 3; x++)
+      for (int j = 0; j < 6; j++) e += VAMPA[ic][x][j] * cos(j * k[x]);
+    if (ic == 1) e += g;
+    return e;
+  }
+  if (o->tb_kind == TB_GES) {
+    /* TightBinding.h:441-462 */
+    if (ic == jc) {
+      double tor = -2. * o->tb_c * (cos(2. * PI * k1) + cos(2. * PI * k2)) - 2. * o->tb_d * (cos(2. * PI * (k1 - k2)));
+      return ic == 0 ? g + tor : -g + tor;
+    }
+    cplx phix = cexpi(2. * PI * k1) + cexpi(2. * PI * k2);
+    cplx tor = -o->tb_f - t2 * phix - b * conj(phix);
+    return ic == 0 ? conj(tor) : tor;
   }
   if (o->tb_kind == TB_GRAPHENE_COSTD || o->tb_kind == TB_GRAPHENE_SYMD) {
     /* TightBinding.h:225-239 */
@@ -613,7 +661,19 @@ static cplx tb_unitary(const orc* o, int ic, int jc, const double* k) {
     if (ic == 2) return jc == 1 ? (cplx)h : a * conj(f) / cabs(f);
     return 0.;
   }
-  if (o->tb_kind == TB_GRAPHENE_COSTD || o->tb_kind == TB_GRAPHENE_SYMD) return ic == jc ? 1. : 0.; /* :1064-1070 */
+  if (o->tb_kind == TB_GRAPHENE_COSTD || o->tb_kind == TB_GRAPHENE_SYMD || o->tb_kind == TB_BN1B || o->tb_kind == TB_VAMPA)
+    return ic == jc ? 1. : 0.; /* :1064-1070, 1147-1155 */
+  if (o->tb_kind == TB_GES) {
+    /* TightBinding.h:1005-1030 */
+    cplx phix = cexpi(2. * PI * k1) + cexpi(2. * PI * k2);
+    cplx tor = -o->tb_f - t2 * phix - b * conj(phix);
+    double Bx = creal(tor), By = cimag(tor), Bz = g;
+    double B = sqrt(Bx * Bx + By * By + Bz * Bz);
+    double phi = atan2(By, Bx) / 2.;
+    double costh2 = sqrt((B + Bz) / 2. / B), sinth2 = sqrt((B - Bz) / 2. / B);
+    if (ic == 0) return jc == 0 ? cexpi(phi) * sinth2 : -cexpi(-phi) * costh2;
+    return jc == 0 ? cexpi(phi) * costh2 : cexpi(-phi) * sinth2;
+  }
   if (o->tb_kind == TB_GRAPHENE_ZURRON) {
     /* TightBinding.h:1072-1081 */
     if (jc != 1) return 1. / sqrt(2.);
@@ -707,7 +767,13 @@ static cplx tb_dipole(const orc* o, int ic, int jc, int x) {
       return 0.;
     }
     case TB_GRAPHENE_ZURRON:
+    case TB_BN1B:
       return 0.;
+    case TB_VAMPA:
+      if (ic == jc) return 0.;
+      return x == 2 ? 3.94 : 3.46;
+    case TB_GES:
+      return (x == 1 && ic == 1 && jc == 1) ? 0.52 * SPACE_A_AU : 0.;
     case TB_COREGRAPHENE:
       if (x == 0)
         return ((ic == 0 && jc == 2) || (ic == 1 && jc == 3) || (ic == 2 && jc == 0) || (ic == 3 && jc == 1)) ? 0.0780088 : 0.;

@@ -134,7 +134,7 @@ def test_problem_rejects_bad_input(workdir):
     with pytest.raises(E.EdusError):
         E.Problem(p, workdir)
     p = E.parse_input(W.hbn_rk4(workdir, n=12, t_fin_fs=0.1))
-    p.tb_type = b"GeS"
+    p.tb_type = b"DLGraphene"
     with pytest.raises(E.EdusError) as ei:
         E.Problem(p, workdir)
     assert ei.value.code == E.abi.EDUS_EUNSUPPORTED
@@ -199,7 +199,8 @@ def test_listed_grid_in_any_order_propagates_as_the_grid(workdir):
 
 
 @pytest.mark.parametrize("model,nb", [("CoreBN_Nedge", 3), ("CoreBN_Bedge", 3), ("Graphene", 2), ("CoreGraphene", 4),
-                                      ("Graphene_costD", 4), ("Graphene_symmetricD", 4), ("GrapheneZurron", 2)])
+                                      ("Graphene_costD", 4), ("Graphene_symmetricD", 4), ("GrapheneZurron", 2),
+                                      ("BN1b", 1), ("Vampa2015", 2), ("GeS", 2), ("GeS_HSE06", 2)])
 def test_more_tight_binding_models_match_oracle(workdir, model, nb):
     """Tight-binding models with their closed-form H, U and dipoles
     (headers/TightBinding.h:43-1421): the set-up tables against the oracle's,
