@@ -359,7 +359,8 @@ enum TbKind {
   kGrapheneZurron,
   kBN1b,
   kVampa,
-  kGeS
+  kGeS,
+  kDLGraphene
 };
 
 // Vampa2015 model: cosine series of the two bands along each crystal axis,
@@ -411,6 +412,14 @@ int tb_setup(const edus_params& p, Tb& t) {
     t.b = (hse ? -0.05 : 0.13) * eV;
     t.c = (hse ? -0.14 : 0.07) * eV;
     t.d = (hse ? 0.106 : -0.09) * eV;
+  } else if (nm == "DLGraphene") {
+    // headers/TightBinding.h:90-97: bilayer, interlayer distance c and hopping d
+    t.kind = kDLGraphene;
+    t.a = 2.46 * kSpaceAAu;
+    t.b = 2.97 * kEnergyEvAu;
+    t.c = 3.35 * kSpaceAAu;
+    t.d = 0.39 * kEnergyEvAu;
+    t.g = 0;
   } else if (nm == "CoreBN_Nedge" || nm == "CoreBN_Bedge") {
     t.kind = nm == "CoreBN_Nedge" ? kCoreBNN : kCoreBNB;
   } else if (nm == "Graphene" || nm == "CoreGraphene" || nm == "Graphene_costD" || nm == "Graphene_symmetricD" ||
@@ -428,7 +437,7 @@ int tb_setup(const edus_params& p, Tb& t) {
     return fail(EDUS_EUNSUPPORTED,
                 "tight-binding model %s is not built (Haldane_CoreBN_Nedge/Bedge, CoreBN_Nedge/Bedge, gen2d_hexagonal, "
                 "BoronNitride, BN1b, Graphene, CoreGraphene, Graphene_costD, Graphene_symmetricD, GrapheneZurron, "
-                "Vampa2015, GeS, GeS_HSE06 are)",
+                "DLGraphene, Vampa2015, GeS, GeS_HSE06 are)",
                 nm.c_str());
   }
   return 0;
@@ -511,6 +520,42 @@ void tb_eval(const Tb& t, int n, const double* k, const double* kc, cd* H, cd* U
     U[2] = eiphi(phi) * c2;
     U[3] = eiphi(-phi) * s2;
     d(1, 1, 1) = 0.52 * kSpaceAAu;
+    return;
+  }
+  if (t.kind == kDLGraphene) {
+    // headers/TightBinding.h:291-312 (energy), :1083-1145 (unitary: the closed-form
+    // eigenvectors, singular where f = 0), :1300-1308, 1376-1385, 1404-1413 (dipoles)
+    const double b = t.b, dd = t.d;
+    const cd f = (eiphi(tp1) + 1.) + eiphi(tp2);
+    H[1] = H[2 * n + 3] = std::conj(f) * b;
+    H[n] = H[3 * n + 2] = f * b;
+    H[3] = H[3 * n] = dd;
+    const cd s = std::sqrt(dd * dd + 4. * (b * b) * f * std::conj(f)), cs = std::conj(s);
+    const cd bf = b * f, bfc = b * std::conj(f);
+    auto sq = [](double x) { return x * x; };
+    const double n1 = std::sqrt(8. + sq(std::abs((dd - s) / bfc)) + 16. * sq(std::abs(bf / (dd + s))));
+    const double n2 = std::sqrt(8. + 16. * sq(std::abs(bf / (dd - s))) + sq(std::abs((dd + s) / bfc)));
+    U[0] = -2. / n1;
+    U[1] = (-dd + cs) / (bf * n1);
+    U[2] = (-4. * b * f) / (n1 * (dd + cs));
+    U[3] = 2. / n1;
+    U[n] = 2. / n2;
+    U[n + 1] = -((dd + cs) / (bf * n2));
+    U[n + 2] = (4. * b * f) / (n2 * (dd - cs));
+    U[n + 3] = 2. / n2;
+    U[2 * n] = -2. / n2;
+    U[2 * n + 1] = -((dd + cs) / (bf * n2));
+    U[2 * n + 2] = (-4. * b * f) / (n2 * (dd - cs));
+    U[2 * n + 3] = 2. / n2;
+    U[3 * n] = 2. / n1;
+    U[3 * n + 1] = (-dd + cs) / (bf * n1);
+    U[3 * n + 2] = (4. * b * f) / (n1 * (dd + cs));
+    U[3 * n + 3] = 2. / n1;
+    d(2, 2, 0) = d(3, 3, 0) = t.c;
+    d(1, 1, 1) = -t.a / std::sqrt(3.);
+    d(2, 2, 1) = d(3, 3, 1) = t.a / (2. * std::sqrt(3.));
+    d(2, 2, 2) = t.a / 2.;
+    d(3, 3, 2) = -t.a / 2.;
     return;
   }
   if (t.kind == kGrapheneCostD || t.kind == kGrapheneSymD) {

@@ -66,7 +66,7 @@ struct orc {
   cplx *HR, *xR, *yR, *zR;  /* [n][n][nrpts] as Hvv[i][j][iR] */
   /* tb model constants */
   double tb_a, tb_b, tb_g, tb_t2, tb_phi0, tb_core, tb_rchv, tb_rchc;
-  double tb_c, tb_d, tb_f;  /* GeS hoppings */
+  double tb_c, tb_d, tb_f;  /* GeS hoppings; DLGraphene interlayer distance (c) and hopping (d) */
   int tb_kind;
   /* dissipation */
   double T[EDUS_MAX_BANDS][EDUS_MAX_BANDS];
@@ -470,7 +470,8 @@ enum {
   TB_GRAPHENE_ZURRON,
   TB_BN1B,
   TB_VAMPA,
-  TB_GES
+  TB_GES,
+  TB_DLGRAPHENE
 };
 
 /* headers/TightBinding.h:98-122: Vampa2015 cosine-series coefficients [band][axis][j] */
@@ -520,6 +521,14 @@ static int tb_init(orc* o) {
     o->tb_b = (hse ? -0.05 : 0.13) * eV;
     o->tb_c = (hse ? -0.14 : 0.07) * eV;
     o->tb_d = (hse ? 0.106 : -0.09) * eV;
+  } else if (!strcmp(nm, "DLGraphene")) {
+    /* TightBinding.h:90-97 */
+    o->tb_kind = TB_DLGRAPHENE;
+    o->tb_a = 2.46 * SPACE_A_AU;
+    o->tb_b = 2.97 * eV;
+    o->tb_c = 3.35 * SPACE_A_AU;
+    o->tb_d = 0.39 * eV;
+    o->tb_g = 0;
   } else if (!strcmp(nm, "CoreBN_Nedge") || !strcmp(nm, "CoreBN_Bedge")) {
     o->tb_kind = !strcmp(nm, "CoreBN_Nedge") ? TB_COREBN_N : TB_COREBN_B;
   } else if (!strcmp(nm, "Graphene") || !strcmp(nm, "CoreGraphene") || !strcmp(nm, "Graphene_costD") ||
@@ -557,6 +566,15 @@ static cplx tb_energy(const orc* o, int ic, int jc, const double* k) {
     /* TightBinding.h:307-311 */
     cplx f = (cexpi(2. * PI * k1) + 1.) + cexpi(2. * PI * k2);
     return 0.5 * creal(csqrt(g * g + 4. * b * b * f * conj(f)));
+  }
+  if (o->tb_kind == TB_DLGRAPHENE) {
+    /* TightBinding.h:291-312 */
+    if (ic == jc) return 0.;
+    cplx f = (cexpi(2. * PI * k1) + 1.) + cexpi(2. * PI * k2);
+    if ((ic == 0 && jc == 1) || (ic == 2 && jc == 3)) return conj(f) * b;
+    if ((ic == 1 && jc == 0) || (ic == 3 && jc == 2)) return f * b;
+    if ((ic == 3 && jc == 0) || (ic == 0 && jc == 3)) return o->tb_d;
+    return 0.;
   }
   if (o->tb_kind == TB_VAMPA) {
     /* TightBinding.h:312-326 */
@@ -663,6 +681,25 @@ static cplx tb_unitary(const orc* o, int ic, int jc, const double* k) {
   }
   if (o->tb_kind == TB_GRAPHENE_COSTD || o->tb_kind == TB_GRAPHENE_SYMD || o->tb_kind == TB_BN1B || o->tb_kind == TB_VAMPA)
     return ic == jc ? 1. : 0.; /* :1064-1070, 1147-1155 */
+  if (o->tb_kind == TB_DLGRAPHENE) {
+    /* TightBinding.h:1083-1145: rows 0 and 3 normalised by n1, rows 1 and 2 by n2 */
+    double d = o->tb_d;
+    cplx f = (cexpi(2. * PI * k1) + 1.) + cexpi(2. * PI * k2);
+    cplx s = csqrt(pow(d, 2) + 4 * pow(b, 2) * f * conj(f));
+    double n1 = sqrt(8 + pow(cabs((d - s) / (b * conj(f))), 2) + 16 * pow(cabs((b * f) / (d + s)), 2));
+    double n2 = sqrt(8 + 16 * pow(cabs((b * f) / (d - s)), 2) + pow(cabs((d + s) / (b * conj(f))), 2));
+    double nr = (ic == 0 || ic == 3) ? n1 : n2;
+    if (jc == 0) return (ic == 0 || ic == 2) ? -2 / nr : 2 / nr;
+    if (jc == 3) return 2 / nr;
+    if (jc == 1) {
+      if (ic == 0 || ic == 3) return (-d + conj(s)) / (b * f * nr);
+      return -((d + conj(s)) / (b * f * nr));
+    }
+    if (ic == 0) return (-4 * b * f) / (nr * (d + conj(s)));
+    if (ic == 1) return (4 * b * f) / (nr * (d - conj(s)));
+    if (ic == 2) return (-4 * b * f) / (nr * (d - conj(s)));
+    return (4 * b * f) / (nr * (d + conj(s)));
+  }
   if (o->tb_kind == TB_GES) {
     /* TightBinding.h:1005-1030 */
     cplx phix = cexpi(2. * PI * k1) + cexpi(2. * PI * k2);
@@ -769,6 +806,12 @@ static cplx tb_dipole(const orc* o, int ic, int jc, int x) {
     case TB_GRAPHENE_ZURRON:
     case TB_BN1B:
       return 0.;
+    case TB_DLGRAPHENE:
+      /* TightBinding.h:1300-1308, 1376-1385, 1404-1413 */
+      if (ic != jc) return 0.;
+      if (x == 0) return (ic == 2 || ic == 3) ? o->tb_c : 0.;
+      if (x == 1) return ic == 1 ? -a / sqrt(3) : ((ic == 2 || ic == 3) ? a / (2 * sqrt(3)) : 0.);
+      return ic == 2 ? a / 2. : (ic == 3 ? -a / 2. : 0.);
     case TB_VAMPA:
       if (ic == jc) return 0.;
       return x == 2 ? 3.94 : 3.46;

@@ -134,7 +134,7 @@ def test_problem_rejects_bad_input(workdir):
     with pytest.raises(E.EdusError):
         E.Problem(p, workdir)
     p = E.parse_input(W.hbn_rk4(workdir, n=12, t_fin_fs=0.1))
-    p.tb_type = b"DLGraphene"
+    p.tb_type = b"GaSe_kp2"
     with pytest.raises(E.EdusError) as ei:
         E.Problem(p, workdir)
     assert ei.value.code == E.abi.EDUS_EUNSUPPORTED
@@ -200,12 +200,15 @@ def test_listed_grid_in_any_order_propagates_as_the_grid(workdir):
 
 @pytest.mark.parametrize("model,nb", [("CoreBN_Nedge", 3), ("CoreBN_Bedge", 3), ("Graphene", 2), ("CoreGraphene", 4),
                                       ("Graphene_costD", 4), ("Graphene_symmetricD", 4), ("GrapheneZurron", 2),
-                                      ("BN1b", 1), ("Vampa2015", 2), ("GeS", 2), ("GeS_HSE06", 2)])
+                                      ("BN1b", 1), ("Vampa2015", 2), ("GeS", 2), ("GeS_HSE06", 2),
+                                      ("DLGraphene", 4)])
 def test_more_tight_binding_models_match_oracle(workdir, model, nb):
     """Tight-binding models with their closed-form H, U and dipoles
     (headers/TightBinding.h:43-1421): the set-up tables against the oracle's,
     U unitary and U H U^dagger diagonal (the reference's Test_matrices check)."""
-    path = W.hbn_rk4(workdir, n=12, t_fin_fs=0.2, it_res=5)
+    # (DLGraphene's closed-form eigenvectors divide by zero where f = 0, at the K
+    # points a grid of 3m points holds, in the reference as here)
+    path = W.hbn_rk4(workdir, n=10 if model == "DLGraphene" else 12, t_fin_fs=0.2, it_res=5)
     txt = open(path).read()
     txt = txt.replace(txt.splitlines()[3] + "\n", f"tightbinding {model}\n")
     open(path, "w").write(txt)
