@@ -20,6 +20,7 @@ EDUS_ENOTREADY = -11
 
 EDUS_MODE_TB = 1
 EDUS_MODE_WANNIER = 2
+EDUS_MODE_CRYSTAL = 3
 EDUS_SOLVER_RK4 = 0
 EDUS_SOLVER_AB = 1
 EDUS_SOLVER_TAYLOR = 2

@@ -167,6 +167,7 @@ int grid_of(const edus_batch* b, const ClassTab& c) {
 
 int check_problem(const edus_batch* b, const Problem& P) {
   const int n = P.ncv;
+  if (P.p.mode == EDUS_MODE_CRYSTAL) return fail(EDUS_EUNSUPPORTED, "Crystal models keep Hermitian dipoles, which the device kernels (one symmetric dipole plane per band pair) do not run; the set-up tables are available");
   const int prof = profile_of(b, n), kt = tile_len(b, n);
   // the staged forms also run tile lengths the element-parallel form is not built for
   // (their instances must then be on a lattice stencil, checked at admission)

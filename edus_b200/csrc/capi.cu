@@ -1034,6 +1034,7 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   if (!pb || !out) return fail(EDUS_EINVAL, "null argument");
   if (pb->P.model_deferred)
     return fail(EDUS_EUNSUPPORTED, "the problem's model is tabulated on the device only in batches (edus_problem_create)");
+  if (pb->P.p.mode == EDUS_MODE_CRYSTAL) return fail(EDUS_EUNSUPPORTED, "Crystal models keep Hermitian dipoles, which the device kernels (one symmetric dipole plane per band pair) do not run; the set-up tables are available");
   edus_options o;
   edus_options_default(&o);
   if (opt) o = *opt;

@@ -609,7 +609,8 @@ extern "C" int edus_parse_input(const char* path, edus_params* out) {
           if (ieq(k, "Wannier")) {
             P.mode = EDUS_MODE_WANNIER;
           } else if (ieq(k, "Crystal")) {
-            return fail(EDUS_EUNSUPPORTED, "Crystal (interpolated ab-initio) mode is not built");
+            // headers/ReadInput.h:748-751; the lattice comes from kmesh_data.dat at set-up
+            P.mode = EDUS_MODE_CRYSTAL;
           } else if (ieq(k, "tightbinding")) {
             if (t.size() < 2) return fail(EDUS_EPARSE, "Please specify the TightBinding type.");
             rc = set_tb_type(&P, t);
@@ -766,7 +767,7 @@ extern "C" int edus_parse_input(const char* path, edus_params* out) {
     int nstep = (int)(tf / P.dt);
     P.t_fin = nstep * P.dt;
   }
-  if (P.mode == 0) return fail(EDUS_EPARSE, "iMode = none is incorrect (no tightbinding/Wannier in tdse)");
+  if (P.mode == 0) return fail(EDUS_EPARSE, "iMode = none is incorrect (no tightbinding/Wannier/Crystal in tdse)");
   if (P.nk[0] <= 0 || P.nk[1] <= 0 || P.nk[2] <= 0) return fail(EDUS_EPARSE, "nkpt section missing");
   *out = P;
   return EDUS_OK;

@@ -17,9 +17,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
+#include <strings.h>
 
 namespace edus {
 
@@ -698,6 +700,178 @@ int read_wannier(Problem& P, const char* workdir) {
   return 0;
 }
 
+// Whitespace-separated tokens of one line (headers/ReadInput.h:1-30 splits on blanks).
+std::vector<std::string> tokens(const std::string& line) {
+  std::vector<std::string> t;
+  std::string cur;
+  for (char c : line) {
+    if (c == ' ' || c == '\t' || c == '\r' || c == '\n') {
+      if (!cur.empty()) t.push_back(cur);
+      cur.clear();
+    } else {
+      cur += c;
+    }
+  }
+  if (!cur.empty()) t.push_back(cur);
+  return t;
+}
+
+bool last_is(const std::vector<std::string>& t, const char* w) { return !t.empty() && strcasecmp(t.back().c_str(), w) == 0; }
+
+// Crystal model files in the working directory (headers/Crystal_interface.h:19-208):
+// kmesh_data.dat gives the in-plane lattice (a[0] = 15 x, b[0] = x / 15), the
+// orbital count after the line ending in "basis" and the grid size nkf after the
+// line ending in "direction"; hk_orthonormal.dat holds per grid point (k1 major)
+// the lower triangle of Re H, a separator, Im H, two separators;
+// bc_betabetap_{real,imag}.dat hold the x and y Berry connections the same way.
+int read_crystal(Problem& P, const char* workdir) {
+  const std::string wd = workdir ? workdir : ".";
+  const int n = P.ncv;
+  int norb = 0, nkf = 0;
+  {
+    std::string path = wd + "/kmesh_data.dat";
+    std::ifstream f(path);
+    if (!f) return fail(EDUS_EIO, "cannot read %s", path.c_str());
+    std::string line;
+    double v[4][2];
+    for (int r = 0; r < 4; r++) {
+      std::getline(f, line);
+      if (!std::getline(f, line)) return fail(EDUS_EIO, "%s: truncated lattice block", path.c_str());
+      auto t = tokens(line);
+      if (t.size() < 2) return fail(EDUS_EIO, "%s: lattice row %d needs two numbers", path.c_str(), r);
+      v[r][0] = std::atof(t[0].c_str());
+      v[r][1] = std::atof(t[1].c_str());
+    }
+    double(*a)[3] = P.p.a;
+    double(*b)[3] = P.p.b;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) a[i][j] = b[i][j] = 0;
+    a[0][0] = 15.;
+    a[1][1] = v[0][0];
+    a[1][2] = v[0][1];
+    a[2][1] = v[1][0];
+    a[2][2] = v[1][1];
+    b[0][0] = 1. / 15.;
+    b[1][1] = v[2][0];
+    b[1][2] = v[2][1];
+    b[2][1] = v[3][0];
+    b[2][2] = v[3][1];
+    bool found = false;
+    while (std::getline(f, line))
+      if (last_is(tokens(line), "basis")) {
+        found = true;
+        break;
+      }
+    if (!found || !std::getline(f, line) || tokens(line).empty())
+      return fail(EDUS_EIO, "%s: no orbital count after the basis block", path.c_str());
+    norb = std::atoi(tokens(line)[0].c_str());
+    found = false;
+    while (std::getline(f, line))
+      if (last_is(tokens(line), "direction")) {
+        found = true;
+        break;
+      }
+    if (!found || !std::getline(f, line) || tokens(line).empty())
+      return fail(EDUS_EIO, "%s: no k-point count after the direction line", path.c_str());
+    nkf = std::atoi(tokens(line)[0].c_str());
+  }
+  if (norb < n) return fail(EDUS_EINVAL, "kmesh_data.dat has %d orbitals, the input %d bands", norb, n);
+  if (nkf < 2) return fail(EDUS_EINVAL, "kmesh_data.dat grid of %d points per direction (2 or more)", nkf);
+  const size_t g2 = (size_t)nkf * nkf, ne = (size_t)n * (n + 1) / 2;
+  P.cy_nkf = nkf;
+  P.cyH.assign(ne * g2, 0);
+  P.cyDx.assign(ne * g2, 0);
+  P.cyDy.assign(ne * g2, 0);
+  // one block of norb lower-triangle rows; row i keeps its first min(i, n-1)+1 numbers
+  auto block = [&](std::istream& f, const std::string& path, size_t g, std::vector<cd>& dst, bool imag) -> int {
+    std::string line;
+    for (int i = 0; i < norb; i++) {
+      if (!std::getline(f, line)) return fail(EDUS_EIO, "%s: truncated", path.c_str());
+      if (i >= n) continue;
+      auto t = tokens(line);
+      if ((int)t.size() < i + 1) return fail(EDUS_EIO, "%s: row %d needs %d numbers", path.c_str(), i, i + 1);
+      for (int j = 0; j <= i; j++) {
+        const double x = std::atof(t[j].c_str());
+        cd& d = dst[((size_t)i * (i + 1) / 2 + j) * g2 + g];
+        d = imag ? cd(d.real(), d.imag() + x) : cd(d.real() + x, d.imag());
+      }
+    }
+    return 0;
+  };
+  {
+    std::string path = wd + "/hk_orthonormal.dat";
+    std::ifstream f(path);
+    if (!f) return fail(EDUS_EIO, "cannot read %s", path.c_str());
+    std::string line;
+    for (size_t g = 0; g < g2; g++) {
+      int rc = block(f, path, g, P.cyH, false);
+      if (rc) return rc;
+      std::getline(f, line);
+      rc = block(f, path, g, P.cyH, true);
+      if (rc) return rc;
+      std::getline(f, line);
+      std::getline(f, line);
+    }
+  }
+  {
+    std::string pr = wd + "/bc_betabetap_real.dat", pi = wd + "/bc_betabetap_imag.dat";
+    std::ifstream fr(pr), fi(pi);
+    if (!fr) return fail(EDUS_EIO, "cannot read %s", pr.c_str());
+    if (!fi) return fail(EDUS_EIO, "cannot read %s", pi.c_str());
+    std::string line;
+    for (size_t g = 0; g < g2; g++) {
+      std::vector<cd>* dst[2] = {&P.cyDx, &P.cyDy};
+      for (int x = 0; x < 2; x++) {
+        int rc = block(fr, pr, g, *dst[x], false);
+        if (!rc) rc = block(fi, pi, g, *dst[x], true);
+        if (rc) return rc;
+        std::getline(fr, line);
+        std::getline(fi, line);
+      }
+      std::getline(fr, line);
+      std::getline(fi, line);
+    }
+  }
+  return 0;
+}
+
+// The Crystal model's periodic bicubic interpolation of one sampled element
+// (headers/Interpolation.h:120-146, 254-264, the two-dimensional case): the
+// grid spacing is 1/(nkf-1) from -0.5 and the nkf samples repeat with period
+// nkf; inside a cell the value is the Catmull-Rom cubic in k2 of the four rows'
+// Catmull-Rom cubics in k1, written here as the tensor product of the two
+// one-dimensional weight vectors.
+cd crystal_interp(const Problem& P, const std::vector<cd>& tab, int e, const double* k) {
+  const int N = P.cy_nkf;
+  const double h = 1. / (N - 1);
+  int ci[2];
+  double t[2];
+  for (int x = 0; x < 2; x++) {
+    double u = std::fmod((k[x + 1] + 0.5) / h, (double)N);
+    if (u < 0) u += N;
+    const int c = (int)std::floor(u);
+    ci[x] = c;
+    t[x] = u - c;
+  }
+  double w[2][4];
+  for (int x = 0; x < 2; x++) {
+    const double s = t[x], s2 = s * s, s3 = s2 * s;
+    w[x][0] = -0.5 * s + s2 - 0.5 * s3;
+    w[x][1] = 1. - 2.5 * s2 + 1.5 * s3;
+    w[x][2] = 0.5 * s + 2. * s2 - 1.5 * s3;
+    w[x][3] = -0.5 * s2 + 0.5 * s3;
+  }
+  const cd* g = &tab[(size_t)e * N * N];
+  cd acc = 0;
+  for (int r = 0; r < 4; r++) {
+    const int i1 = ((ci[0] - 1 + r) % N + N) % N;
+    cd row = 0;
+    for (int c = 0; c < 4; c++) row += w[1][c] * g[(size_t)i1 * N + ((ci[1] - 1 + c) % N + N) % N];
+    acc += w[0][r] * row;
+  }
+  return acc;
+}
+
 int read_coulomb(Problem& P, const char* workdir) {
   int n = P.ncv, n2 = n * n, c2 = P.ncut * P.ncut;
   std::string wd = workdir ? workdir : ".";
@@ -770,6 +944,34 @@ void eval_k(const Problem& P, const Tb& tb, const double* k, cd* H, cd* U, cd* D
     eig_herm(n, A, ev, Z);
     for (int i = 0; i < n; i++)
       for (int j = 0; j < n; j++) Uk[i * n + j] = std::conj(Z[j * n + i]);
+  } else if (P.p.mode == EDUS_MODE_CRYSTAL) {
+    // headers/Crystal_interface.h:212-304: H and D from the interpolants (the
+    // upper triangle as the conjugate of the lower), D in the order (z, x, y)
+    // with real diagonals, U^dagger the eigenvectors of H
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) {
+        const int lo = i >= j ? i : j, hi = i >= j ? j : i, e = lo * (lo + 1) / 2 + hi;
+        cd h = crystal_interp(P, P.cyH, e, k), dx = crystal_interp(P, P.cyDx, e, k), dy = crystal_interp(P, P.cyDy, e, k);
+        if (i < j) {
+          h = std::conj(h);
+          dx = std::conj(dx);
+          dy = std::conj(dy);
+        }
+        if (i == j) {
+          dx = dx.real();
+          dy = dy.real();
+        }
+        Hk[i * n + j] = h;
+        Dk[(i * n + j) * 3 + 0] = 0.;
+        Dk[(i * n + j) * 3 + 1] = dx;
+        Dk[(i * n + j) * 3 + 2] = dy;
+      }
+    cd A[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Z[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+    double ev[EDUS_MAX_BANDS];
+    std::copy(Hk, Hk + n * n, A);
+    eig_herm(n, A, ev, Z);
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) Uk[i * n + j] = std::conj(Z[j * n + i]);
   } else {
     double kc[3];
     crys_to_cart(P, k, kc);
@@ -794,7 +996,7 @@ void eval_k(const Problem& P, const Tb& tb, const double* k, cd* H, cd* U, cd* D
 
 int model_hud(const Problem& P, const double* kcrys, cd* H, cd* U, cd* D) {
   Tb tb;
-  if (P.p.mode != EDUS_MODE_WANNIER) {
+  if (P.p.mode == EDUS_MODE_TB) {
     int rc = tb_setup(P.p, tb);
     if (rc) return rc;
   }
@@ -815,7 +1017,13 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P, bool de
   if (p.dt <= 0) return fail(EDUS_EINVAL, "dt must be positive");
   if (p.solver != EDUS_SOLVER_RK4 && (p.order < 1 || p.order > 8)) return fail(EDUS_EINVAL, "solver order %d out of range", p.order);
   if (p.solver == EDUS_SOLVER_TAYLOR && p.order < 2) return fail(EDUS_EINVAL, "Taylor order must be >= 2");
-  int rc = setup_geometry(P);
+  int rc = 0;
+  if (p.mode == EDUS_MODE_CRYSTAL) {
+    // the lattice and the model come from the crystal files (Source_Main/input.cpp:57)
+    rc = read_crystal(P, workdir);
+    if (rc) return rc;
+  }
+  rc = setup_geometry(P);
   if (rc) return rc;
   const int nk = P.nk;
   const size_t st = (size_t)nk * n * n;
@@ -829,7 +1037,7 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P, bool de
   Tb tb;
   if (isW) {
     rc = read_wannier(P, workdir);
-  } else {
+  } else if (p.mode == EDUS_MODE_TB) {
     rc = tb_setup(p, tb);
   }
   if (rc) return rc;

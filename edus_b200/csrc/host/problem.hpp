@@ -34,6 +34,11 @@ struct Problem {
   std::vector<double> Rvec;       // [nr][3]
   std::vector<cd> HR;             // [n][n][nr]
   std::vector<cd> rR;             // [3][n][n][nr]
+  // Crystal model (headers/Crystal_interface.h): H and the x, y Berry
+  // connections sampled on an nkf x nkf crystal grid over [-0.5, 0.5], lower
+  // triangle (i >= j) of the first n orbitals, [i*(i+1)/2 + j][k1][k2]
+  int cy_nkf = 0;
+  std::vector<cd> cyH, cyDx, cyDy;
   // Coulomb coefficients (Source_Main/Fourier_Coulomb.cpp:505-622)
   int ncut = 0;
   std::vector<cd> cA, cB, cC, cD; // [ncut^2][n^2]

@@ -191,6 +191,100 @@ def wannier(workdir, nw=8, nside=11, n=96, field=0.4, photon=0.3, duration=40.0,
     return path
 
 
+def crystal_model(nb=2, norb=None, seed=7, nh=2):
+    """Seeded smooth periodic model for the Crystal interface: Hermitian H(k)
+    and x, y Berry connections as short Fourier series in the crystal
+    coordinates (k1, k2), a.u. Returns a function k1, k2 -> (H, Dx, Dy) of
+    norb x norb matrices (norb >= nb; the extra orbitals lie far above)."""
+    norb = nb if norb is None else norb
+    rng = np.random.Generator(np.random.PCG64(seed))
+    terms = []
+    for m1 in range(-nh, nh + 1):
+        for m2 in range(-nh, nh + 1):
+            scale = 0.08 / (1 + m1 * m1 + m2 * m2)
+            c = [(rng.standard_normal((norb, norb)) + 1j * rng.standard_normal((norb, norb))) * scale for _ in range(3)]
+            terms.append((m1, m2, c))
+    onsite = np.diag(np.linspace(-0.2, 0.2, norb) + np.where(np.arange(norb) >= nb, 2.0, 0.0))
+
+    def at(k1, k2):
+        out = [np.zeros((norb, norb), np.complex128) for _ in range(3)]
+        for m1, m2, c in terms:
+            ph = np.exp(2j * np.pi * (m1 * k1 + m2 * k2))
+            for x in range(3):
+                out[x] += c[x] * ph
+        H, Dx, Dy = [(o + o.conj().T) / 2 for o in out]
+        H = H + onsite
+        H[np.diag_indices(norb)] = H.diagonal().real
+        # the files carry an imaginary diagonal in the connections; the model drops it
+        Dx = Dx + 1j * 1e-3 * np.eye(norb)
+        Dy = Dy - 1j * 2e-3 * np.eye(norb)
+        return H, Dx, Dy
+
+    return at
+
+
+def write_crystal_files(workdir, nb=2, norb=None, nkf=13, seed=7, alat=4.72):
+    """The Crystal interface's input files (kmesh_data.dat, hk_orthonormal.dat,
+    bc_betabetap_real.dat, bc_betabetap_imag.dat) for `crystal_model` on an
+    nkf x nkf grid over [-0.5, 0.5] in each crystal direction, k1 major, the
+    lower triangles row by row. Returns (model, grid, a, b) with grid the
+    crystal coordinates of the samples and a, b the in-plane lattice rows."""
+    norb = nb if norb is None else norb
+    model = crystal_model(nb, norb, seed)
+    os.makedirs(workdir, exist_ok=True)
+    a = np.array([[alat * math.cos(math.pi / 6), alat * math.sin(math.pi / 6)],
+                  [alat * math.cos(math.pi / 6), -alat * math.sin(math.pi / 6)]])
+    b = 2 * math.pi * np.linalg.inv(a).T
+    grid = -0.5 + np.arange(nkf) / (nkf - 1)
+    f = lambda v: " ".join(f"{x:.17g}" for x in v)
+    with open(os.path.join(workdir, "kmesh_data.dat"), "w") as fp:
+        fp.write(f"a0 (bohr)\n{f(a[0])}\na1\n{f(a[1])}\nb0 (1/bohr)\n{f(b[0])}\nb1\n{f(b[1])}\n")
+        fp.write("atomic positions\nB 0.0 0.0\nN 0.5 0.5\norbital basis\n")
+        fp.write(f"{norb}\nk points along each direction\n{nkf}\nindex kx ky\n")
+        i = 0
+        for k1 in grid:
+            for k2 in grid:
+                kc = k1 * b[0] + k2 * b[1]
+                i += 1
+                fp.write(f"{i} {f(kc)}\n")
+    lower = lambda M, part: "".join(" ".join(f"{part(M[i, j]):.17g}" for j in range(i + 1)) + "\n" for i in range(norb))
+    with open(os.path.join(workdir, "hk_orthonormal.dat"), "w") as fh, \
+            open(os.path.join(workdir, "bc_betabetap_real.dat"), "w") as fr, \
+            open(os.path.join(workdir, "bc_betabetap_imag.dat"), "w") as fi:
+        for k1 in grid:
+            for k2 in grid:
+                H, Dx, Dy = model(k1, k2)
+                fh.write(lower(H, np.real) + "\n" + lower(H, np.imag) + "\n\n")
+                fr.write(lower(Dx, np.real) + "\n" + lower(Dy, np.real) + "\n\n")
+                fi.write(lower(Dx, np.imag) + "\n" + lower(Dy, np.imag) + "\n\n")
+    return model, grid, a, b
+
+
+def crystal(workdir, nb=(1, 1), norb=None, nkf=13, n=12, field=0.3, photon=0.4, duration=20.0, dt_fs=0.01,
+            t_fin_fs=None, it_res=5, seed=7):
+    """input.txt for the Crystal interface (tdse{ Crystal }) with the files of
+    `write_crystal_files`; nb = (valence, conduction) bands. Returns the path."""
+    write_crystal_files(workdir, nb=sum(nb), norb=norb, nkf=nkf, seed=seed)
+    t_fin = duration if t_fin_fs is None else t_fin_fs
+    txt = (
+        "CRY\n\n"
+        f"bands{{\nvalence {nb[0]}\nconduction {nb[1]}\n}}\n\n"
+        "tdse{\nCrystal\n"
+        f"dt {dt_fs} fs\n"
+        f"t_fin {t_fin} fs\n"
+        "}\n\n"
+        f"nkpt{{\n1 {n} {n}\n}}\n\n"
+        + _pump(photon, field, duration)
+        + "\nobservables{\nCurrent\n"
+        f"it_resolution {it_res}\n"
+        "}\n"
+    )
+    path = os.path.join(workdir, "input.txt")
+    with open(path, "w") as fp:
+        fp.write(txt)
+    return path
+
+
 def sweep(count=256, seed=20261203, nmin=48, nmax=144, emin=0.05, emax=0.8, dmin=10.0, dmax=60.0, it_res=10,
           dt_fs=0.01):
     """Seeded pulse sweep: half hBN (hbn_rk4 model), half the 8-band Wannier

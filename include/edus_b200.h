@@ -48,7 +48,7 @@ enum {
 };
 
 /* ---------------------------------------------------------------- enums */
-enum { EDUS_MODE_TB = 1, EDUS_MODE_WANNIER = 2 };
+enum { EDUS_MODE_TB = 1, EDUS_MODE_WANNIER = 2, EDUS_MODE_CRYSTAL = 3 };
 enum { EDUS_SOLVER_RK4 = 0, EDUS_SOLVER_AB = 1, EDUS_SOLVER_TAYLOR = 2 };
 enum { EDUS_ENV_NONE = 0, EDUS_ENV_SIN2 = 1, EDUS_ENV_GAUSS = 2, EDUS_ENV_PW = 3 };
 enum { EDUS_PREC_FP64 = 0, EDUS_PREC_MIXED = 1 };

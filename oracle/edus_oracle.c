@@ -16,6 +16,7 @@
  * every reduction over k uses a fixed per-thread block order so results do
  * not depend on the thread count.
  */
+#define _POSIX_C_SOURCE 200809L
 #include "edus_oracle.h"
 
 #include <complex.h>
@@ -24,6 +25,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <strings.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -68,6 +70,9 @@ struct orc {
   double tb_a, tb_b, tb_g, tb_t2, tb_phi0, tb_core, tb_rchv, tb_rchc;
   double tb_c, tb_d, tb_f;  /* GeS hoppings; DLGraphene interlayer distance (c) and hopping (d) */
   int tb_kind;
+  /* Crystal model: H, x and y Berry connections on the nkf x nkf file grid, [i][j][k1][k2], i >= j */
+  int cy_nkf;
+  cplx *cyH, *cyDx, *cyDy;
   /* dissipation */
   double T[EDUS_MAX_BANDS][EDUS_MAX_BANDS];
   int n_diss, diss_i[EDUS_MAX_BANDS * EDUS_MAX_BANDS], diss_j[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
@@ -897,6 +902,182 @@ static cplx wannier_sum(const orc* o, const cplx* XR, int i, int j, const double
   return v;
 }
 
+/* ------------------------------------------------------------ Crystal model */
+
+/* next line of f into buf; 0 at end of file */
+static int cy_line(FILE* f, char* buf, int cap) { return fgets(buf, cap, f) != NULL; }
+
+/* splits buf in place on blanks; returns the token count (at most cap) */
+static int cy_split(char* buf, char** tok, int cap) {
+  int n = 0;
+  char* save = NULL;
+  for (char* t = strtok_r(buf, " \t\r\n", &save); t && n < cap; t = strtok_r(NULL, " \t\r\n", &save)) tok[n++] = t;
+  return n;
+}
+
+#define CY_LINE 65536
+#define CY_TOK 512
+
+/* headers/Crystal_interface.h:19-208 (Crystal::init): lattice, orbital count and
+ * grid size from kmesh_data.dat, then H from hk_orthonormal.dat and the x, y Berry
+ * connections from bc_betabetap_real.dat / bc_betabetap_imag.dat */
+static int crystal_read(orc* o, const char* workdir) {
+  char path[2 * EDUS_STRLEN + 32], path2[2 * EDUS_STRLEN + 32];
+  char* buf = malloc(CY_LINE);
+  char* tok[CY_TOK];
+  int rc = EDUS_EIO, norb = 0, nkf = 0, n = o->ncv;
+  const char* wd = workdir ? workdir : ".";
+  FILE *f = NULL, *g = NULL;
+  if (!buf) return EDUS_ENOMEM;
+  snprintf(path, sizeof(path), "%s/kmesh_data.dat", wd);
+  f = fopen(path, "r");
+  if (!f) goto out;
+  double v[4][2];
+  for (int r = 0; r < 4; r++) {
+    if (!cy_line(f, buf, CY_LINE) || !cy_line(f, buf, CY_LINE)) goto out;
+    if (cy_split(buf, tok, CY_TOK) < 2) goto out;
+    v[r][0] = atof(tok[0]);
+    v[r][1] = atof(tok[1]);
+  }
+  memset(o->p.a, 0, sizeof(o->p.a));
+  memset(o->p.b, 0, sizeof(o->p.b));
+  o->p.a[1][1] = v[0][0];
+  o->p.a[1][2] = v[0][1];
+  o->p.a[2][1] = v[1][0];
+  o->p.a[2][2] = v[1][1];
+  o->p.a[0][0] = 15.;
+  o->p.b[1][1] = v[2][0];
+  o->p.b[1][2] = v[2][1];
+  o->p.b[2][1] = v[3][0];
+  o->p.b[2][2] = v[3][1];
+  o->p.b[0][0] = 1. / 15.;
+  for (;;) { /* up to the line whose last word is "basis" */
+    if (!cy_line(f, buf, CY_LINE)) goto out;
+    int nt = cy_split(buf, tok, CY_TOK);
+    if (nt > 0 && !strcasecmp(tok[nt - 1], "basis")) break;
+  }
+  if (!cy_line(f, buf, CY_LINE) || cy_split(buf, tok, CY_TOK) < 1) goto out;
+  norb = atoi(tok[0]);
+  for (;;) { /* up to the line whose last word is "direction" */
+    if (!cy_line(f, buf, CY_LINE)) goto out;
+    int nt = cy_split(buf, tok, CY_TOK);
+    if (nt > 0 && !strcasecmp(tok[nt - 1], "direction")) break;
+  }
+  if (!cy_line(f, buf, CY_LINE) || cy_split(buf, tok, CY_TOK) < 1) goto out;
+  nkf = atoi(tok[0]);
+  fclose(f);
+  f = NULL;
+  if (norb < n || nkf < 2) {
+    rc = EDUS_EINVAL;
+    goto out;
+  }
+  o->cy_nkf = nkf;
+  size_t tab = (size_t)n * n * nkf * nkf;
+  o->cyH = calloc(tab, sizeof(cplx));
+  o->cyDx = calloc(tab, sizeof(cplx));
+  o->cyDy = calloc(tab, sizeof(cplx));
+  if (!o->cyH || !o->cyDx || !o->cyDy) {
+    rc = EDUS_ENOMEM;
+    goto out;
+  }
+#define CY_AT(T, i, j, k1, k2) (T)[(((size_t)(i) * n + (j)) * nkf + (k1)) * nkf + (k2)]
+  snprintf(path, sizeof(path), "%s/hk_orthonormal.dat", wd);
+  f = fopen(path, "r");
+  if (!f) goto out;
+  for (int k1 = 0; k1 < nkf; k1++)
+    for (int k2 = 0; k2 < nkf; k2++) {
+      for (int part = 0; part < 2; part++) { /* real rows, separator, imaginary rows */
+        for (int i = 0; i < norb; i++) {
+          if (!cy_line(f, buf, CY_LINE)) goto out;
+          if (i >= n) continue;
+          if (cy_split(buf, tok, CY_TOK) < i + 1) goto out;
+          for (int j = 0; j <= i; j++) CY_AT(o->cyH, i, j, k1, k2) += part ? I * atof(tok[j]) : atof(tok[j]);
+        }
+        cy_line(f, buf, CY_LINE);
+      }
+      cy_line(f, buf, CY_LINE);
+    }
+  fclose(f);
+  f = NULL;
+  snprintf(path, sizeof(path), "%s/bc_betabetap_real.dat", wd);
+  snprintf(path2, sizeof(path2), "%s/bc_betabetap_imag.dat", wd);
+  f = fopen(path, "r");
+  g = fopen(path2, "r");
+  if (!f || !g) goto out;
+  char* buf2 = malloc(CY_LINE);
+  char* tok2[CY_TOK];
+  if (!buf2) {
+    rc = EDUS_ENOMEM;
+    goto out;
+  }
+  for (int k1 = 0; k1 < nkf; k1++)
+    for (int k2 = 0; k2 < nkf; k2++) {
+      for (int x = 0; x < 2; x++) {
+        cplx* T = x ? o->cyDy : o->cyDx;
+        for (int i = 0; i < norb; i++) {
+          if (!cy_line(f, buf, CY_LINE) || !cy_line(g, buf2, CY_LINE)) goto out2;
+          if (i >= n) continue;
+          if (cy_split(buf, tok, CY_TOK) < i + 1 || cy_split(buf2, tok2, CY_TOK) < i + 1) goto out2;
+          for (int j = 0; j <= i; j++) CY_AT(T, i, j, k1, k2) = atof(tok[j]) + I * atof(tok2[j]);
+        }
+        cy_line(f, buf, CY_LINE);
+        cy_line(g, buf2, CY_LINE);
+      }
+      cy_line(f, buf, CY_LINE);
+      cy_line(g, buf2, CY_LINE);
+    }
+  rc = 0;
+out2:
+  free(buf2);
+out:
+  if (f) fclose(f);
+  if (g) fclose(g);
+  free(buf);
+  return rc;
+}
+
+/* headers/Interpolation.h:86-146 (the two-dimensional fit: periodic padding, the
+ * 16 coefficients a_ab = sum_rs M_ar M_bs p_rs of the 4 x 4 patch around the cell)
+ * and :228-264 (cell location and the polynomial in dy, dz) */
+static cplx crystal_fit(const orc* o, const cplx* T, int i, int j, const double* k) {
+  static const double M[4][4] = {{0, 1, 0, 0}, {-0.5, 0, 0.5, 0}, {1, -2.5, 2, -0.5}, {-0.5, 1.5, -1.5, 0.5}};
+  int n = o->ncv, nkf = o->cy_nkf;
+  double sp = 1. / (nkf - 1);
+  double dy = fmod((k[1] - (-0.5)) / sp, nkf), dz = fmod((k[2] - (-0.5)) / sp, nkf);
+  if (dy < 0) dy += nkf;
+  if (dz < 0) dz += nkf;
+  int yi = (int)floor(dy), zi = (int)floor(dz);
+  dy -= yi;
+  dz -= zi;
+  cplx p[4][4];
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) {
+      int a1 = yi - 1 + r, a2 = zi - 1 + c;
+      a1 = a1 >= 0 ? a1 % nkf : nkf + a1 % nkf;
+      a2 = a2 >= 0 ? a2 % nkf : nkf + a2 % nkf;
+      p[r][c] = CY_AT(T, i, j, a1, a2);
+    }
+  cplx cf[4][4];
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) {
+      cplx acc = 0;
+      for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) acc += M[a][r] * M[b][c] * p[r][c];
+      cf[a][b] = acc;
+    }
+  double y2 = dy * dy, y3 = y2 * dy, z2 = dz * dz, z3 = z2 * dz;
+  return (cf[0][0] + cf[0][1] * dz + cf[0][2] * z2 + cf[0][3] * z3) + (cf[1][0] + cf[1][1] * dz + cf[1][2] * z2 + cf[1][3] * z3) * dy +
+         (cf[2][0] + cf[2][1] * dz + cf[2][2] * z2 + cf[2][3] * z3) * y2 + (cf[3][0] + cf[3][1] * dz + cf[3][2] * z2 + cf[3][3] * z3) * y3;
+}
+
+/* headers/Crystal_interface.h:212-270 (energy and dipoles; the upper triangle is the
+ * conjugate of the fitted lower) */
+static cplx crystal_elem(const orc* o, const cplx* T, int ic, int jc, const double* k) {
+  if (jc < ic + 1) return crystal_fit(o, T, ic, jc, k);
+  return conj(crystal_fit(o, T, jc, ic, k));
+}
+#undef CY_AT
+
 /* ------------------------------------------------------------ model tabulation */
 
 /* Source_Main/save_HUD.cpp:19-53 (+ headers/Wannier.h:477-551 energy_U) and
@@ -922,6 +1103,24 @@ static int tabulate(orc* o) {
           Dk[(ic * n + jc) * 3 + 0] = wannier_sum(o, o->xR, ic, jc, k);
           Dk[(ic * n + jc) * 3 + 1] = wannier_sum(o, o->yR, ic, jc, k);
           Dk[(ic * n + jc) * 3 + 2] = wannier_sum(o, o->zR, ic, jc, k);
+          if (ic == jc)
+            for (int x = 0; x < 3; x++) Dk[(ic * n + jc) * 3 + x] = creal(Dk[(ic * n + jc) * 3 + x]);
+        }
+      cplx A[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Z[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
+      double ev[EDUS_MAX_BANDS];
+      memcpy(A, Hk, sizeof(cplx) * n * n);
+      eig_herm(n, A, ev, Z);
+      for (int ic = 0; ic < n; ic++)
+        for (int jc = 0; jc < n; jc++) Uk[ic * n + jc] = conj(Z[jc * n + ic]);
+    } else if (o->p.mode == EDUS_MODE_CRYSTAL) {
+      /* headers/Crystal_interface.h:272-304: dipoles in the order (z, x, y), real
+       * diagonals; Uk = conj(eigenvectors)^T of the Hermitian H */
+      for (int ic = 0; ic < n; ic++)
+        for (int jc = 0; jc < n; jc++) {
+          Hk[ic * n + jc] = crystal_elem(o, o->cyH, ic, jc, k);
+          Dk[(ic * n + jc) * 3 + 0] = 0.;
+          Dk[(ic * n + jc) * 3 + 1] = crystal_elem(o, o->cyDx, ic, jc, k);
+          Dk[(ic * n + jc) * 3 + 2] = crystal_elem(o, o->cyDy, ic, jc, k);
           if (ic == jc)
             for (int x = 0; x < 3; x++) Dk[(ic * n + jc) * 3 + x] = creal(Dk[(ic * n + jc) * 3 + x]);
         }
@@ -1809,13 +2008,19 @@ int orc_create(const edus_params* p, const char* workdir, orc** out) {
   o->nk = p->nk[0] * p->nk[1] * p->nk[2];
   o->n1 = p->nk[1];
   o->n2 = p->nk[2];
-  int rc = set_crys_to_cart(o);
+  int rc = 0;
+  if (p->mode == EDUS_MODE_CRYSTAL) { /* Source_Main/input.cpp:57: the lattice comes from the crystal files */
+    rc = crystal_read(o, workdir);
+    if (rc) goto fail;
+  }
+  rc = set_crys_to_cart(o);
   if (rc) goto fail;
   /* det_a (Source_Main/input.cpp:63-73) */
+  const double(*la)[3] = o->p.a;
   if (!p->sample_110)
-    o->det_a = fabs(p->a[1][1] * p->a[2][2] - p->a[1][2] * p->a[2][1]);
+    o->det_a = fabs(la[1][1] * la[2][2] - la[1][2] * la[2][1]);
   else
-    o->det_a = fabs(p->a[0][0] * p->a[1][1] - p->a[0][1] * p->a[1][0]);
+    o->det_a = fabs(la[0][0] * la[1][1] - la[0][1] * la[1][0]);
   o->kpt = xcalloc((size_t)o->nk * 3, sizeof(double));
   rc = make_grid(o);
   if (rc) goto fail;
@@ -1832,7 +2037,7 @@ int orc_create(const edus_params* p, const char* workdir, orc** out) {
   o->GE = xcalloc(st * 3, sizeof(cplx));
   if (p->mode == EDUS_MODE_WANNIER) {
     rc = wannier_read(o, workdir);
-  } else {
+  } else if (p->mode == EDUS_MODE_TB) {
     rc = tb_init(o);
   }
   if (rc) goto fail;
@@ -1919,7 +2124,7 @@ void orc_free(orc* o) {
   void* ptrs[] = {o->kpt, o->nbr, o->H, o->U, o->hU, o->D, o->GE, o->Rvec, o->HR, o->xR, o->yR, o->zR,
                   o->P0, o->P1, o->P2, o->Pv, o->Pgrad, o->ring, o->Pprev_diag, o->Psave_diag, o->cA, o->cB,
                   o->cC, o->cD, o->Xcc, o->Xcs, o->Xsc, o->Xss, o->Xcc0, o->Xcs0, o->Xsc0, o->Xss0,
-                  o->cos_m1, o->sin_m1, o->cos_m2, o->sin_m2, o->PW0, o->Hr, o->Pd};
+                  o->cos_m1, o->sin_m1, o->cos_m2, o->sin_m2, o->PW0, o->Hr, o->Pd, o->cyH, o->cyDx, o->cyDy};
   for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
   free(o);
 }

@@ -221,3 +221,53 @@ def test_more_tight_binding_models_match_oracle(workdir, model, nb):
     E2 = np.einsum("kim,kmn,kjn->kij", U, H, U.conj())
     off = E2 - np.einsum("kii->ki", E2)[:, :, None] * np.eye(nb)
     assert np.abs(off).max() < 1e-12 * max(1.0, np.abs(H).max())
+
+
+@pytest.mark.parametrize("norb", [2, 3])
+def test_crystal_setup_matches_oracle(workdir, norb):
+    """Crystal interface (headers/Crystal_interface.h, headers/Interpolation.h):
+    the lattice, H, U, D and rho0 from the interpolated files against the
+    oracle's; a file with more orbitals than bands uses the first ones."""
+    p = E.parse_input(W.crystal(workdir, nb=(1, 1), norb=norb, nkf=13, n=12))
+    assert p.mode == E.abi.EDUS_MODE_CRYSTAL
+    pb, o = compare_setup(p, workdir)
+    H, U = pb.get("H"), pb.get("U")
+    UU = np.einsum("kij,klj->kil", U, U.conj())
+    assert np.abs(UU - np.eye(2)).max() < 1e-12
+    E2 = np.einsum("kim,kmn,kjn->kij", U, H, U.conj())
+    assert np.abs(E2[:, 0, 1]).max() < 1e-12 and np.all(E2[:, 0, 0].real <= E2[:, 1, 1].real)
+    D = pb.get("D")
+    assert np.abs(D[..., 0]).max() == 0.0
+    assert np.abs(D[:, [0, 1], [0, 1], :].imag).max() == 0.0
+    # Hermitian dipoles: the crystal model keeps them as read (no symmetrisation)
+    assert np.abs(D[:, 0, 1, 1:] - D[:, 1, 0, 1:].conj()).max() == 0.0
+    assert np.abs(D[:, 0, 1, 1:].imag).max() > 1e-3
+
+
+def test_crystal_model_reproduces_the_file_samples(workdir):
+    """The bicubic fit passes through the samples: at the file's grid points
+    gHUD returns the file's H and connections (upper triangle conjugated, D in
+    the order z, x, y, real diagonals), and the lattice is the file's."""
+    path = W.crystal(workdir, nb=(1, 2), norb=3, nkf=11, n=10)
+    model, grid, a, b = W.write_crystal_files(workdir, nb=3, norb=3, nkf=11)
+    pb = E.Problem(E.parse_input(path), workdir)
+    for i1 in [0, 3, 7, 10]:
+        for i2 in [0, 5, 9, 10]:
+            k1, k2 = grid[i1], grid[i2]
+            H, U, D = pb.model_hud([0.0, k1, k2])
+            Hf, Dx, Dy = model(k1, k2)
+            np.testing.assert_allclose(H, Hf, rtol=0, atol=1e-13)
+            np.testing.assert_allclose(D[..., 1], Dx - 1j * np.diag(Dx.diagonal().imag), rtol=0, atol=1e-13)
+            np.testing.assert_allclose(D[..., 2], Dy - 1j * np.diag(Dy.diagonal().imag), rtol=0, atol=1e-13)
+            assert np.abs(D[..., 0]).max() == 0.0
+    kc = pb.get("kpt")
+    assert kc.shape == (100, 3)
+
+
+def test_crystal_problem_is_refused_on_the_device(workdir):
+    """Crystal dipoles are Hermitian, which the device's single dipole plane per
+    band pair does not hold: contexts and batches refuse the problem."""
+    pb = E.Problem(E.parse_input(W.crystal(workdir, nb=(1, 1), nkf=9, n=8)), workdir)
+    with pytest.raises(E.EdusError) as ei:
+        E.Context(pb)
+    assert ei.value.code == E.abi.EDUS_EUNSUPPORTED
