@@ -271,3 +271,18 @@ def test_crystal_problem_is_refused_on_the_device(workdir):
     with pytest.raises(E.EdusError) as ei:
         E.Context(pb)
     assert ei.value.code == E.abi.EDUS_EUNSUPPORTED
+
+
+def test_oracle_runs_a_crystal_problem(workdir):
+    """The oracle's RHS reads the full dipole matrix, so it runs Crystal inputs
+    with their Hermitian dipoles: populations stay normalised and the state
+    responds to the pump (the checker a device path will be held to)."""
+    p = E.parse_input(W.crystal(workdir, nb=(1, 1), nkf=9, n=8, field=2.0, duration=4.0, t_fin_fs=0.6, it_res=10))
+    log = Oracle(p, workdir).run(60)
+    pops = np.array([x["pop"] for x in log])
+    # holes in the valence band = electrons in the conduction band
+    assert pops[-1, 1] > 1e-8
+    assert np.abs(pops[:, 0] - pops[:, 1]).max() < 1e-6 * pops[-1, 1]
+    assert max(abs(x["trace_dev"]) for x in log) < 1e-12
+    J1 = np.array([x["J1"] for x in log])
+    assert np.abs(J1[-1]).max() > 0
