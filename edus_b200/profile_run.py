@@ -1,9 +1,9 @@
 """Run a workload for a fixed number of time steps (for ncu / timing).
 
 Single solve (edus_create / edus_step):
-  python -m edus_b200.profile_run --workload cfg1 --steps 60 [--graph] [--n 120]
-    cfg0 (hBN RK4 60x60), cfg1 (hBN + Coulomb AB4 120x120), cfg2 (8-band
-    Wannier RK4 96x96). Eager launches by default so that ncu sees each kernel;
+  python -m edus_b200.profile_run --workload hbn_coulomb --steps 60 [--graph] [--n 120]
+    hbn_rk4 (hBN RK4 60x60), hbn_coulomb (hBN + Coulomb AB4 120x120), wannier8
+    (8-band Wannier RK4 96x96). Eager launches by default so that ncu sees each kernel;
     --graph replays the captured CUDA graph of the whole loop instead.
 
 Batch (edus_batch_*):
@@ -25,11 +25,11 @@ from edus_b200 import workloads as W  # noqa: E402
 
 
 def make(name, workdir, n=None):
-    if name == "cfg0":
+    if name == "hbn_rk4":
         return W.hbn_rk4(workdir, n=n or 60)
-    if name == "cfg1":
+    if name == "hbn_coulomb":
         return W.hbn_coulomb(workdir, n=n or 120)
-    if name == "cfg2":
+    if name == "wannier8":
         return W.wannier(workdir, n=n or 96)
     raise SystemExit(f"unknown workload {name}")
 
@@ -58,7 +58,7 @@ def batch_problems(kind, count, n, root):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="cfg1")
+    ap.add_argument("--workload", default="hbn_coulomb")
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--n", type=int, default=None)
     ap.add_argument("--graph", action="store_true")
