@@ -9,6 +9,9 @@
  * replaced by a cyclic Jacobi eigensolver, Gauss–Jordan inversion and a
  * one-sided Jacobi SVD. The oracle is pinned against the shipped AB5
  * golden run (example/Adams–Bashforth ODE Solver example/AB5_.../Output).
+ * Parity unpinned for the parts no shipped file covers: the tight-binding
+ * models other than Haldane_CoreBN_Nedge and the Crystal interface (the
+ * reference ships no crystal data).
  *
  * Layout: P[k][i][j] complex128 exactly as the reference's vec3x P0
  * (Source_Main/allocate_arr.cpp:39); Dipole[k][i][j][x] as vec4x Dipole.
