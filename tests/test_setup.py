@@ -286,3 +286,17 @@ def test_oracle_runs_a_crystal_problem(workdir):
     assert max(abs(x["trace_dev"]) for x in log) < 1e-12
     J1 = np.array([x["J1"] for x in log])
     assert np.abs(J1[-1]).max() > 0
+
+
+def test_crystal_files_missing_or_short_are_errors(workdir):
+    """A Crystal input without its files, or with fewer orbitals than bands,
+    is an error code (the reference would read past its arrays)."""
+    path = W.crystal(workdir, nb=(1, 1), norb=2, nkf=7, n=6)
+    os.remove(os.path.join(workdir, "bc_betabetap_imag.dat"))
+    with pytest.raises(E.EdusError) as ei:
+        E.Problem(E.parse_input(path), workdir)
+    assert ei.value.code == E.abi.EDUS_EIO
+    path = W.crystal(workdir, nb=(2, 1), norb=2, nkf=7, n=6)  # 2 orbitals in the files, 3 bands in the input
+    with pytest.raises(E.EdusError) as ei:
+        E.Problem(E.parse_input(path), workdir)
+    assert ei.value.code == E.abi.EDUS_EINVAL
