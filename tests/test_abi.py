@@ -84,3 +84,20 @@ def test_edus_run_driver_reports_input_errors(tmp_path):
     bad.write_text("#SYSTEM\nthis is not an input file\n")
     r = subprocess.run([build.EXE, str(bad)], capture_output=True, text=True, cwd=tmp_path)
     assert r.returncode == 1 and "edus_run:" in r.stderr
+
+
+def test_edus_run_sets_up_a_crystal_input_then_refuses_the_device_run(tmp_path):
+    """A Crystal input: the set-up files (kpt.txt, Test_matrices.txt) are
+    written, then the device run is refused with exit status 1 before any GPU
+    work (Hermitian dipoles are not run on the device)."""
+    import subprocess
+
+    from edus_b200 import build
+    from edus_b200 import workloads as W
+
+    if not os.path.exists(build.EXE):
+        build.build()
+    W.crystal(str(tmp_path), nb=(1, 1), nkf=7, n=6)
+    r = subprocess.run([build.EXE, "input.txt", "."], capture_output=True, text=True, cwd=tmp_path, timeout=120)
+    assert r.returncode == 1 and "Hermitian dipoles" in r.stderr
+    assert (tmp_path / "kpt.txt").exists() and (tmp_path / "Test_matrices.txt").exists()
