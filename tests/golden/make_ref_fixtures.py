@@ -1,0 +1,185 @@
+"""Known answers from the reference program itself (anpicon/EDUS), for the parity tests.
+
+Runs oracle/_ref/EDUS.x — the reference's own main_MPI.cpp compiled from its
+sources by `make -C oracle ref` (one MPI rank, the Armadillo subset from
+oracle/ref_shim/) — on the inputs below and stores, per case, the input text
+and the reference's Output/*.txt time series in tests/golden/ref_<case>.npz.
+The inputs are written by edus_b200.workloads (seeded; nothing is read from
+the reference's examples except the packaged Coulomb tables); the Wannier
+model file's SHA-256 is stored so a test can check it regenerates the same
+model. Run here, where the reference sources are:
+
+    python tests/golden/make_ref_fixtures.py [case ...]
+
+Cases: the three single-solve configurations at their own sizes (hBN 60x60
+RK4 30 fs; hBN 120x120 with the Rytova-Keldysh mean field, AB4 from the
+reference's zero derivative history, 30 fs; the 8-band Wannier model 96x96
+RK4 40 fs) and small cases of every other solver / option on the path
+(Coulomb AB4, diagonal-basis Coulomb, Taylor-6 and RK4 with adaptive dt, the
+8- and 16-band Wannier models, per-k snapshot files).
+
+Runs with the Coulomb mean field are repeated at several OpenMP thread
+counts and every distinct outcome is kept (series keys "J1", "J1#1", ...):
+the reference switches its screening correction on when the mean conduction
+population n_cond exceeds 1e-20 (headers/RungeKutta.h:77), and before the
+pulse n_cond is rounding noise of either sign, so the reference itself gives
+one of two results from run to run (their J1 differ by ~3e-8 relative).
+
+    python tests/golden/make_ref_fixtures.py --add [--threads 4,6] CASE   # more runs, merged
+"""
+import hashlib
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from edus_b200 import workloads as W  # noqa: E402
+
+REF_EXE = os.path.join(ROOT, "oracle", "_ref", "EDUS.x")
+SERIES = ("J1", "J2", "Losses", "EF")
+
+
+def _with(path, old, new):
+    txt = open(path).read()
+    assert old in txt, old
+    open(path, "w").write(txt.replace(old, new, 1))
+    return path
+
+
+def _diag_basis(d):
+    return _with(W.hbn_coulomb(d, n=24, t_fin_fs=2.0, it_res=5, rk4_startup=False), "Rytova_Keldysh\n",
+                 "Rytova_Keldysh\nCoulomb_diag_basis\n")
+
+
+def _snapshots(d):
+    return _with(W.hbn_rk4(d, n=12, t_fin_fs=1.5, it_res=10), "Current\n", "Current\nPrintPopulation 0 60 15\n")
+
+
+def _edia(d):
+    return _with(W.hbn_coulomb(d, n=24, t_fin_fs=0.3, it_res=10, rk4_startup=False), "Rytova_Keldysh\n",
+                 "Rytova_Keldysh\nPrint_new_band_dispersion\n")
+
+
+# name -> (input writer, per-k files to keep)
+CASES = {
+    "cfg0_hbn60_rk4": (lambda d: W.hbn_rk4(d, n=60, it_res=10), ()),
+    "cfg1_hbn120_coulomb_ab4": (lambda d: W.hbn_coulomb(d, n=120, it_res=10, rk4_startup=False), ()),
+    "cfg2_wannier8_96_rk4": (lambda d: W.wannier(d, n=96, it_res=10), ()),
+    "hbn24_rk4": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=3.0, it_res=5), ()),
+    "hbn24_coulomb_ab4": (lambda d: W.hbn_coulomb(d, n=24, t_fin_fs=2.0, it_res=5, rk4_startup=False), ()),
+    "hbn24_coulomb_diag_ab4": (_diag_basis, ()),
+    "hbn24_ab2": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=2.0, it_res=5, solver="Adams_Bashforth 2\n"), ()),
+    "hbn24_taylor6_dyn": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=2.0, it_res=3, dt_fs=0.002,
+                                              solver="Taylor\nTaylorOrder 6\ndynamical_dt_evolution\nepsStepAbs 0.02\n"),
+                          ()),
+    "hbn24_rk4_dyn": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=2.0, it_res=3,
+                                          solver="dynamical_dt_evolution\nepsStepAbs 0.001\n"), ()),
+    "wannier8_16_rk4": (lambda d: W.wannier(d, n=16, t_fin_fs=1.0, it_res=5), ()),
+    "wannier16_24_rk4": (lambda d: W.wannier(d, nw=16, nside=13, name="W16", n=24, t_fin_fs=1.0, it_res=5), ()),
+    "hbn12_snapshots": (_snapshots, ("t_Ek", "P_val_cond_in_Eigenstate_12_", "P_val_in_Eigenstate_11_",
+                                     "P_cond_in_Eigenstate_22_", "H_Eigen_", "H_Wannier_cond_", "P_initial_Wannier_",
+                                     "Uk_")),
+    "hbn24_coulomb_edia": (_edia, ("Edia_", "t_Ek")),
+}
+
+
+def _model_hash(d):
+    out = {}
+    for f in sorted(os.listdir(d)):
+        if f.endswith("_tb.dat"):
+            out[f] = hashlib.sha256(open(os.path.join(d, f), "rb").read()).hexdigest()
+    return out
+
+
+def _run_once(name, threads):
+    writer, keep = CASES[name]
+    d = tempfile.mkdtemp(prefix=f"edus_ref_{name}_")
+    path = writer(d)
+    os.makedirs(os.path.join(d, "Output"), exist_ok=True)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    t0 = time.perf_counter()
+    r = subprocess.run([REF_EXE, os.path.basename(path)], cwd=d, env=env, capture_output=True, text=True)
+    wall = time.perf_counter() - t0
+    if r.returncode != 0:
+        raise RuntimeError(f"{name}: reference exited {r.returncode}\n{r.stdout[-2000:]}\n{r.stderr[-2000:]}")
+    out = {"input": np.array(open(path).read()), "threads": np.array(threads), "wall_s": np.array(wall)}
+    for s in SERIES:
+        out[s] = np.loadtxt(os.path.join(d, "Output", f"{s}.txt"), ndmin=2)
+    for f, h in _model_hash(d).items():
+        out[f"sha256:{f}"] = np.array(h)
+    files = sorted(os.listdir(os.path.join(d, "Output")))
+    for prefix in keep:
+        for f in files:
+            if f.startswith(prefix) and f.endswith(".txt"):
+                out[f"file:{f}"] = np.array(open(os.path.join(d, "Output", f)).read())
+    shutil.rmtree(d, ignore_errors=True)
+    return out
+
+
+def _j1(a):
+    return a[:, 1::2] + 1j * a[:, 2::2]
+
+
+def _distinct(variants, J1):
+    for v in variants:
+        if np.linalg.norm(_j1(v) - _j1(J1)) <= 1e-10 * np.linalg.norm(_j1(v)):
+            return False
+    return True
+
+
+def run_case(name, thread_counts, add=False):
+    """Run the reference once per thread count; keep the first run's series
+    under the plain keys and each further distinct outcome under "<key>#<i>"."""
+    path = os.path.join(HERE, f"ref_{name}.npz")
+    out = dict(np.load(path)) if add and os.path.exists(path) else {}
+    walls = []
+    for th in thread_counts:
+        r = _run_once(name, th)
+        walls.append(r["wall_s"])
+        if not out:
+            out = r
+            out["runs"] = np.array([th])
+            continue
+        assert str(r["input"]) == str(out["input"])
+        out["runs"] = np.append(out["runs"], th)
+        nvar = 1 + sum(1 for k in out if k.startswith("J1#"))
+        variants = [out["J1"]] + [out[f"J1#{i}"] for i in range(1, nvar)]
+        if _distinct(variants, r["J1"]):
+            for sname in SERIES:
+                out[f"{sname}#{nvar}"] = r[sname]
+    np.savez_compressed(path, **out)
+    return sum(float(w) for w in walls)
+
+
+def main(argv):
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    add = "--add" in argv
+    given = None
+    if "--threads" in argv:
+        i = argv.index("--threads")
+        given = [int(x) for x in argv[i + 1].split(",")]
+        argv = argv[:i] + argv[i + 2:]
+    names = [a for a in argv if not a.startswith("--")] or list(CASES)
+    # the reference's Coulomb path indexes id_masters[thr_total-4] (headers/Coulomb.h:307-310): >= 4 threads
+    threads = max(4, os.cpu_count() or 4)
+    for name in names:
+        if given:
+            counts = given
+        elif "coulomb" in name:
+            counts = [threads, 4, threads, 4, 6, 5] if not name.startswith("cfg") else [threads, 4]
+        else:
+            counts = [threads]
+        wall = run_case(name, counts, add=add)
+        print(f"{name}: {wall:.1f} s over runs on {counts} threads", flush=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

@@ -72,6 +72,8 @@ class Oracle:
         self.L.orc_info(self.h, C.byref(self.info))
         self.n = self.info.ncv
         self.nk = self.info.nk
+        # adaptive dt shrinks the step: the output count is not known in advance
+        self.dynamic = bool(params.dynamical_dt)
 
     def get(self, name):
         i = self.info
@@ -104,6 +106,8 @@ class Oracle:
     def run(self, max_steps=-1):
         res = max(self.L and 1, 1)
         cap = self.info.nprint + 4 if max_steps < 0 else max_steps + 4
+        if self.dynamic and max_steps < 0:
+            cap = 1 << 16
         cap = max(cap, 16)
         log = (abi.Obs * cap)()
         n = C.c_int()

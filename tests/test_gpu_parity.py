@@ -15,6 +15,7 @@ from edus_b200 import abi
 from edus_b200 import workloads as W
 from conftest import GOLDEN, GOLDEN_INPUT
 from oracle_lib import Oracle
+from ref_fixtures import snapshot_schedule as _snapshot_schedule
 
 pytestmark = pytest.mark.gpu
 
@@ -228,18 +229,6 @@ def test_edus_run_writes_the_reference_outputs(tmp_path):
 
     kg = json.load(open(os.path.join(GOLDEN, "ab5_kgrid.json")))
     assert hashlib.sha256((tmp_path / "Output" / "k_grid.txt").read_bytes()).hexdigest() == kg["sha256"]
-
-
-def _snapshot_schedule(t0, dt, itfi, res, start, end, step):
-    """Output steps that take a snapshot: t > start + icont * step and t < end,
-    icont counted from -1 (Source_Main/if_resolution.cpp:18-33)."""
-    out, icont, t = [], -1, t0
-    for it in range(itfi + 1):
-        if it % res == 0 and t > start + icont * step and t < end:
-            icont += 1
-            out.append((it, t))
-        t += dt
-    return out
 
 
 @pytest.mark.parametrize("graphs", [True, False])
