@@ -216,6 +216,18 @@ class BatchStats(C.Structure):
         ("device_ms", C.c_double),
         ("kpoint_steps", C.c_double),
         ("launches", C.c_int64),
+        ("h2d_bytes", C.c_int64),
+        ("d2h_bytes", C.c_int64),
+    ]
+
+
+class KernelTime(C.Structure):
+    _fields_ = [
+        ("nbands", C.c_int32),
+        ("kind", C.c_int32),
+        ("launches", C.c_int64),
+        ("total_ms", C.c_double),
+        ("kpoints", C.c_int64),
     ]
 
 

@@ -102,6 +102,7 @@ struct edus_batch {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   double device_ms = 0, kpoint_steps = 0;
   long long launches = 0;
+  long long h2d_bytes = 0, d2h_bytes = 0;
 };
 
 namespace {
@@ -208,6 +209,7 @@ void planes(const cd* src, int nk, int n, int comps, std::vector<T>& dst) {
 template <class T>
 int put(edus_batch* b, void* d, const std::vector<T>& h) {
   BCK(cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, b->stream));
+  b->h2d_bytes += (long long)(sizeof(T) * h.size());
   return 0;
 }
 
@@ -598,31 +600,62 @@ std::string graph_key(const edus_batch* b) {
   return k;
 }
 
-int record_chunk(edus_batch* b) {
+// CUDA-event pairs around individual launches (edus_batch_profile): pair i
+// brackets one launch of kernel kind[i] (0 observables, 1-4 stage 0-3) of class nb[i]
+struct LaunchTimer {
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> nb, kind;
+  size_t used = 0;
+  ~LaunchTimer() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+  cudaError_t begin(int n, int k, cudaStream_t s) {
+    while (ev.size() < 2 * (used + 1)) {
+      cudaEvent_t e;
+      cudaError_t r = cudaEventCreate(&e);
+      if (r != cudaSuccess) return r;
+      ev.push_back(e);
+    }
+    if (nb.size() <= used) {
+      nb.resize(used + 1);
+      kind.resize(used + 1);
+    }
+    nb[used] = n;
+    kind[used] = k;
+    return cudaEventRecord(ev[2 * used], s);
+  }
+  cudaError_t end(cudaStream_t s) { return cudaEventRecord(ev[2 * used++ + 1], s); }
+};
+
+int record_chunk(edus_batch* b, LaunchTimer* tm = nullptr) {
   const int S = b->opt.chunk_steps;
   for (int s = 0; s < S; s++) {
     const int parity = s & 1;
     for (auto& kv : b->classes) {
       ClassTab& c = kv.second;
       View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles, c.d_cinst, c.d_ntiles + 1};
+      if (tm) BCK(tm->begin(c.n, 0, b->stream));
       BCK(launch_obs(c.n, c.kt, b->mixed, v, parity, (int)b->slots.size(), c.ogrid, b->stream));
+      if (tm) BCK(tm->end(b->stream));
     }
     for (int st = 0; st < 4; st++)
       for (auto& kv : b->classes) {
         ClassTab& c = kv.second;
         View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles, c.d_cinst, c.d_ntiles + 1};
+        if (tm) BCK(tm->begin(c.n, 1 + st, b->stream));
         if (c.form == 3 || c.form == 4)
           BCK(launch_stage_pipe(c.n, c.kt, c.form == 4, v, st, parity, c.psel, c.pcomp, c.sgrid, b->stream));
         else if (c.form == 2)
           BCK(launch_stage_mm(c.n, c.kt, b->mixed, v, st, parity, c.sgrid, b->stream));
         else
           BCK(launch_stage(c.n, c.kt, c.form, b->mixed, v, st, parity, c.sgrid, b->stream));
+        if (tm) BCK(tm->end(b->stream));
       }
   }
   return 0;
 }
 
-int run_chunk(edus_batch* b) {
+int run_chunk(edus_batch* b, LaunchTimer* tm = nullptr) {
   int rc = sync_tiles(b);
   if (rc) return rc;
   bool any = false;
@@ -630,7 +663,9 @@ int run_chunk(edus_batch* b) {
   if (!any) return 0;
   const std::string key = graph_key(b);
   BCK(cudaEventRecord(b->e0, b->stream));
-  if (b->opt.use_graphs) {
+  if (tm) {
+    if ((rc = record_chunk(b, tm))) return rc;
+  } else if (b->opt.use_graphs) {
     if (!b->gexec || key != b->graph_key) {
       if (b->gexec) cudaGraphExecDestroy(b->gexec);
       if (b->graph) cudaGraphDestroy(b->graph);
@@ -917,6 +952,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   if (cudaMemsetAsync(I.done, 0, sizeof(unsigned int), b->stream) != cudaSuccess ||
       cudaMemcpyAsync(b->d_insts + q, &I, sizeof(Inst), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
     return undo(fail(EDUS_ECUDA, "batch: upload of the instance descriptor"));
+  b->h2d_bytes += (long long)sizeof(Inst);
   if (b->mixed && launch_weq(b->d_insts, q, nt, nk, b->stream) != cudaSuccess)
     return undo(fail(EDUS_ECUDA, "batch: equilibrium terms"));
   const int zero = 0;
@@ -980,6 +1016,7 @@ int edus_batch_obs_get(edus_batch* b, int32_t slot, int32_t first, int32_t count
   BCK(cudaSetDevice(b->device));
   BCK(cudaMemcpyAsync(out, s->inst.log + first, sizeof(edus_obs) * count, cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
+  b->d2h_bytes += (long long)(sizeof(edus_obs) * count);
   return 0;
 }
 
@@ -997,6 +1034,7 @@ int edus_batch_get_state(edus_batch* b, int32_t slot, double* rho) {
     BCK(cudaMemcpyAsync(eq.data(), s->inst.Peq, sizeof(double2) * eq.size(), cudaMemcpyDeviceToHost, b->stream));
   }
   BCK(cudaStreamSynchronize(b->stream));
+  b->d2h_bytes += (long long)(sizeof(double2) * (pl.size() + eq.size()));
   for (size_t q = 0; q < eq.size(); q++) pl[q] = cadd(pl[q], eq[q]);
   cd* o = (cd*)rho;
   for (int k = 0; k < nk; k++)
@@ -1042,12 +1080,45 @@ int edus_batch_stats_get(edus_batch* b, edus_batch_stats* out) {
   out->device_ms = b->device_ms;
   out->kpoint_steps = b->kpoint_steps;
   out->launches = b->launches;
+  out->h2d_bytes = b->h2d_bytes;
+  out->d2h_bytes = b->d2h_bytes;
   return 0;
 }
 
 int edus_batch_tile_k(edus_batch* b, int32_t nbands, int32_t* kt) {
   if (!b || !kt) return fail(EDUS_EINVAL, "null argument");
   *kt = tile_len(b, nbands);
+  return 0;
+}
+
+int edus_batch_profile(edus_batch* b, int32_t nsteps, edus_kernel_time* out, int32_t cap, int32_t* n) {
+  if (!b || nsteps < 0 || !out || cap < 0 || !n) return fail(EDUS_EINVAL, "bad argument");
+  BCK(cudaSetDevice(b->device));
+  std::map<std::pair<int, int>, edus_kernel_time> acc;
+  const int S = b->opt.chunk_steps;
+  for (int done = 0; done < nsteps; done += S) {
+    // k points of each class in this chunk (before instances retire at its end)
+    std::map<int, long long> kp;
+    for (const auto& s : b->slots)
+      if (s.status == EDUS_INST_RUNNING) kp[s.n] += s.nk;
+    LaunchTimer tm;
+    int rc = run_chunk(b, &tm);
+    if (rc) return rc;
+    for (size_t i = 0; i < tm.used; i++) {
+      float ms = 0;
+      BCK(cudaEventElapsedTime(&ms, tm.ev[2 * i], tm.ev[2 * i + 1]));
+      edus_kernel_time& e = acc[{tm.nb[i], tm.kind[i]}];
+      e.nbands = tm.nb[i];
+      e.kind = tm.kind[i];
+      e.launches++;
+      e.total_ms += ms;
+      e.kpoints = kp[tm.nb[i]];
+    }
+  }
+  int m = 0;
+  for (const auto& kv : acc)
+    if (m < cap) out[m++] = kv.second;
+  *n = m;
   return 0;
 }
 

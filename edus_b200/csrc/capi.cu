@@ -105,6 +105,7 @@ struct edus_ctx {
   unsigned int* d_done = nullptr;
   int* d_err = nullptr;  // device error word set by bounded waits
   edus_obs* d_log = nullptr;
+  edus_obs* d_obs_one = nullptr;  // record of edus_observables, allocated on its first call
   int log_cap = 0, nlog = 0;
   double* d_ncond = nullptr;
   double* d_pcmax = nullptr;
@@ -1485,9 +1486,11 @@ int edus_observables(edus_ctx* c, edus_obs* out) {
   memset(&rec, 0, sizeof(rec));
   rec.t = c->time_loop;
   rec.dt = c->dt;
-  edus_obs* tmp = nullptr;
-  int rc = dalloc(c, &tmp, 1);
-  if (rc) return rc;
+  if (!c->d_obs_one) {
+    int rc = dalloc(c, &c->d_obs_one, 1);
+    if (rc) return rc;
+  }
+  edus_obs* tmp = c->d_obs_one;
   double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
   double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
   CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, c->d_part,
@@ -1635,7 +1638,10 @@ std::mutex g_static_mu;
 unsigned char* g_static_base[kStaticMaxDevices] = {};
 
 // Once per device, with that device current: the address of the scratch
-// array in this device's memory.
+// array in this device's memory. The address is kept for the life of the
+// process; it belongs to the device's primary context, so it must not be used
+// after that context is destroyed (cudaDeviceReset): a caller that resets a
+// device must not call edus_observables_static on it again.
 int static_scratch(int device, unsigned char** base) {
   if (device < 0 || device >= kStaticMaxDevices) return fail(EDUS_EINVAL, "device %d out of range", device);
   std::lock_guard<std::mutex> lk(g_static_mu);

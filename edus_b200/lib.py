@@ -84,6 +84,7 @@ def load_library():
         "edus_batch_release": (C.c_int, [vp, i32]),
         "edus_batch_stats_get": (C.c_int, [vp, P(abi.BatchStats)]),
         "edus_batch_tile_k": (C.c_int, [vp, i32, P(i32)]),
+        "edus_batch_profile": (C.c_int, [vp, i32, P(abi.KernelTime), i32, P(i32)]),
         "edus_server_options_default": (C.c_int, [P(abi.ServerOptions)]),
         "edus_server_create": (C.c_int, [P(abi.ServerOptions), P(vp)]),
         "edus_server_submit": (C.c_int, [vp, P(abi.Params), cp, P(C.c_int64)]),
@@ -422,6 +423,15 @@ class Batch:
         s = abi.BatchStats()
         _check(self._L.edus_batch_stats_get(self._h, C.byref(s)), "edus_batch_stats_get")
         return {f: getattr(s, f) for f, _ in abi.BatchStats._fields_ if f != "pad"}
+
+    def profile(self, nsteps):
+        """Advance nsteps with a CUDA-event pair around every launch: list of
+        {nbands, kind (0 observables, 1-4 RK4 stage 0-3), launches, total_ms, kpoints}."""
+        cap = 64
+        buf = (abi.KernelTime * cap)()
+        n = C.c_int32()
+        _check(self._L.edus_batch_profile(self._h, int(nsteps), buf, cap, C.byref(n)), "edus_batch_profile")
+        return [{f: getattr(buf[i], f) for f, _ in abi.KernelTime._fields_} for i in range(n.value)]
 
     def tile_k(self, nbands):
         k = C.c_int32()

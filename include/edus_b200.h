@@ -284,13 +284,13 @@ int edus_observables(edus_ctx* ctx, edus_obs* out);
  * library. For callers that cannot take an allocation at this point: a
  * serving loop whose HBM is fully committed to admitted solves, or a caller
  * that must not run into the device-wide synchronisation a device
- * free brings. No counterpart in the reference (its observables reduce into
- * host arrays over MPI).
+ * free brings. No reference counterpart.
  * Limits: at most 524 288 k points (4096 partials of 128 k points), else
  * EDUS_EINVAL. The first call on a device looks the array up on that device
- * (make it outside any stream capture). The array is shared by every context
- * on a device: calls that overlap in time (two host threads, or two streams)
- * race on it and must be serialised by the caller. */
+ * (make it outside any stream capture); the address is kept until the process
+ * ends, so no call may follow a cudaDeviceReset of that device. The array is
+ * shared by every context on a device: calls that overlap in time (two host
+ * threads, or two streams) race on it and must be serialised by the caller. */
 int edus_observables_static(edus_ctx* ctx, edus_obs* out);
 /* Write Output/{EF,J1,J2,Losses,TransientAbs,k_grid}.txt in the reference's
  * format, the per-k files of the first output step (H_Eigen_*, H_Wannier_cond,
@@ -374,7 +374,19 @@ typedef struct {
   double device_ms;         /* CUDA-event time of all chunk replays */
   double kpoint_steps;      /* k-point steps advanced (sum over instances) */
   int64_t launches;         /* kernel launches replayed */
+  int64_t h2d_bytes;        /* bytes copied host -> device by admissions (tables, state, field, descriptor) */
+  int64_t d2h_bytes;        /* bytes copied device -> host by edus_batch_obs_get / edus_batch_get_state */
 } edus_batch_stats;
+
+/* One kernel of a profiled advance: the band-count class, the kernel (0 =
+ * observables, 1-4 = RK4 stage 0-3), its launches, their summed CUDA-event
+ * time, and the k points of the class per launch. */
+typedef struct {
+  int32_t nbands, kind;
+  int64_t launches;
+  double total_ms;
+  int64_t kpoints;
+} edus_kernel_time;
 
 int edus_batch_options_default(edus_batch_options* o);
 int edus_batch_create(const edus_batch_options* o, edus_batch** out);
@@ -398,6 +410,11 @@ int edus_batch_release(edus_batch* b, int32_t slot);
 int edus_batch_stats_get(edus_batch* b, edus_batch_stats* out);
 /* Tile length in use for a band count (after the autotuner). */
 int edus_batch_tile_k(edus_batch* b, int32_t nbands, int32_t* kt);
+/* Advance like edus_batch_advance, but launch every kernel eagerly (no graph)
+ * between its own pair of CUDA events on the batch's stream; per (class,
+ * kernel) totals go to out[0 .. *n), at most cap entries. For measurement:
+ * the per-launch durations behind a roofline. No counterpart in the reference. */
+int edus_batch_profile(edus_batch* b, int32_t nsteps, edus_kernel_time* out, int32_t cap, int32_t* n);
 
 /* ------------------------------------------------------- serving
  * A request loop over one batch. Submitted solves are set up on host threads
