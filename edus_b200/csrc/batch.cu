@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "ctx_hooks.hpp"
 #include "cuda/batch.cuh"
 #include "cuda/model_build.hpp"
 #include "cuda/tc_contract.hpp"
@@ -52,6 +53,9 @@ struct Slot {
   long long tick_admit = 0;
   std::vector<void*> mem;
   Inst inst{};
+  // an instance with the Coulomb mean field: a single-solve context whose
+  // whole loop runs as one graph on the context's stream (FP64)
+  edus_ctx* sub = nullptr;
 };
 
 struct ClassTab {
@@ -107,6 +111,16 @@ struct edus_batch {
 
 namespace {
 
+// Precision of a class of band count n. A mixed-precision batch runs classes
+// of 4 bands and more in mixed precision and the 2- and 3-band classes in
+// FP64: their stage is dominated by the finite-difference k-gradient, whose
+// terms cancel to ~1/N of their size, so FP32 stage inputs leave a relative
+// error of ~N x 6e-8 in it (J1 error 1.1e-6 measured on a 144 x 144 hBN
+// sweep instance), while FP64 costs these classes little (their kernels are
+// latency-bound).
+constexpr int kMixedMinBands = 4;
+bool cmix(const edus_batch* b, int n) { return b->mixed && n >= kMixedMinBands; }
+
 int tile_len(const edus_batch* b, int n) {
   int kt = (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.tile_k[n] : 0;
   return kt > 0 ? kt : default_tile(n);
@@ -114,12 +128,13 @@ int tile_len(const edus_batch* b, int n) {
 
 Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
   const size_t n = P.ncv, nk = P.nk, nt = n * (n + 1) / 2;
-  const size_t s = b->mixed ? sizeof(float2) : sizeof(double2);
+  const bool mix = cmix(b, (int)n);
+  const size_t s = mix ? sizeof(float2) : sizeof(double2);
   Layout L;
   L.state = align256(nt * nk * sizeof(double2));
-  L.eq = b->mixed ? L.state : 0;
-  L.hdiag = b->mixed ? align256(n * nk * sizeof(double)) : 0;
-  L.w = b->mixed ? align256(3 * nt * nk * sizeof(float2)) : 0;
+  L.eq = mix ? L.state : 0;
+  L.hdiag = mix ? align256(n * nk * sizeof(double)) : 0;
+  L.w = mix ? align256(3 * nt * nk * sizeof(float2)) : 0;
   L.H = align256(nt * nk * s);
   L.D = align256(3 * nt * nk * s);
   L.GE = P.p.current ? align256(3 * nt * nk * s) : 0;
@@ -135,8 +150,8 @@ Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
 // register profile / kernel form of a band count; the matrix-product form is built for FP64 only
 int profile_of(const edus_batch* b, int n) {
   const int p = (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.regs_profile[n] : 0;
-  if (p == 2 && b->mixed) return 0;
-  if (p >= 3 && !b->mixed) return 0;  // asynchronous staging is built for mixed precision
+  if (p == 2 && cmix(b, n)) return 0;
+  if (p >= 3 && !cmix(b, n)) return 0;  // asynchronous staging is built for mixed precision
   return p;
 }
 
@@ -159,16 +174,24 @@ int form_of(const edus_batch* b, const ClassTab& c, int& psel, int& pcomp) {
 
 int grid_of(const edus_batch* b, const ClassTab& c) {
   switch (c.form) {
-    case 2: return stage_grid_mm(c.n, c.kt, b->mixed);
+    case 2: return stage_grid_mm(c.n, c.kt, cmix(b, c.n));
     case 3:
     case 4: return stage_grid_pipe(c.n, c.kt, c.form == 4, c.psel, c.pcomp);
-    default: return stage_grid(c.n, c.kt, c.form ? 1 : 0, b->mixed);
+    default: return stage_grid(c.n, c.kt, c.form ? 1 : 0, cmix(b, c.n));
   }
 }
 
 int check_problem(const edus_batch* b, const Problem& P) {
   const int n = P.ncv;
-  if (P.p.mode == EDUS_MODE_CRYSTAL) return fail(EDUS_EUNSUPPORTED, "Crystal models keep Hermitian dipoles, which the device kernels (one symmetric dipole plane per band pair) do not run; the set-up tables are available");
+  if (P.p.mode == EDUS_MODE_CRYSTAL)
+    return fail(EDUS_EUNSUPPORTED, "batch: Crystal models keep Hermitian dipoles, which the batch kernels (one symmetric dipole "
+                                   "plane per band pair) do not run; single-solve contexts run them");
+  if (P.p.coulomb) {
+    // runs as a single-solve context inside the batch (every solver at constant dt, FP64)
+    if (P.p.dynamical_dt) return fail(EDUS_EUNSUPPORTED, "batch: a Coulomb instance integrates at constant dt");
+    if (P.model_deferred) return fail(EDUS_EUNSUPPORTED, "batch: a Coulomb instance needs host-built model tables");
+    return 0;
+  }
   const int prof = profile_of(b, n), kt = tile_len(b, n);
   // the staged forms also run tile lengths the element-parallel form is not built for
   // (their instances must then be on a lattice stencil, checked at admission)
@@ -176,8 +199,7 @@ int check_problem(const edus_batch* b, const Problem& P) {
   if (!ok)
     return fail(EDUS_EUNSUPPORTED, "batch: %d bands with %d k points per tile (profile %d) is not built", n, tile_len(b, n),
                 profile_of(b, n));
-  if (P.p.coulomb) return fail(EDUS_EUNSUPPORTED, "batch: the Coulomb mean field runs only in single-solve contexts");
-  if (b->mixed && P.nch > 0)
+  if (cmix(b, n) && P.nch > 0)
     return fail(EDUS_EUNSUPPORTED,
                 "batch: mixed precision needs a problem without core bands (edus_problem_drop_decoupled_core, or FP64)");
   if (!P.diss_i.empty()) return fail(EDUS_EUNSUPPORTED, "batch: dissipation runs only in single-solve contexts");
@@ -478,7 +500,8 @@ int build_model_on_device(edus_batch* b, const Problem& P, const Inst& I) {
   // scratch: inputs, and FP64 outputs when the instance stores FP32
   size_t bytes = align256(sizeof(double) * 3 * nk) + align256(sizeof(double) * 3 * nr) + align256(sizeof(double2) * coef.size()) +
                  align256(sizeof(double) * gb.size());
-  if (b->mixed) bytes += align256(sizeof(double2) * plane) * (4 + (I.GE ? 3 : 0)) + align256(sizeof(double2) * n * n * nk);
+  const bool mix = cmix(b, n);
+  if (mix) bytes += align256(sizeof(double2) * plane) * (4 + (I.GE ? 3 : 0)) + align256(sizeof(double2) * n * n * nk);
   char* base = nullptr;
   if (cudaMallocAsync((void**)&base, bytes, b->pool, b->stream) != cudaSuccess) {
     cudaGetLastError();
@@ -515,7 +538,7 @@ int build_model_on_device(edus_batch* b, const Problem& P, const Inst& I) {
   a.gb = dg;
   a.nbr = I.nbr;
   a.P0 = I.P0;
-  if (b->mixed) {
+  if (mix) {
     a.H = (double2*)carve(sizeof(double2) * plane);
     a.D = (double2*)carve(sizeof(double2) * 3 * plane);
     a.U = (double2*)carve(sizeof(double2) * n * n * nk);
@@ -527,7 +550,7 @@ int build_model_on_device(edus_batch* b, const Problem& P, const Inst& I) {
     a.GE = (double2*)I.GE;
   }
   cudaError_t e = build_wannier_model(a, b->stream);
-  if (e == cudaSuccess && b->mixed) {
+  if (e == cudaSuccess && mix) {
     if (e == cudaSuccess) e = planes_diagonal(a.H, (double*)I.Hdiag, n, nk, b->stream);
     if (e == cudaSuccess) e = planes_to_float(a.H, (float2*)I.H, plane, b->stream);
     if (e == cudaSuccess) e = planes_to_float(a.D, (float2*)I.D, 3 * plane, b->stream);
@@ -635,7 +658,7 @@ int record_chunk(edus_batch* b, LaunchTimer* tm = nullptr) {
       ClassTab& c = kv.second;
       View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles, c.d_cinst, c.d_ntiles + 1};
       if (tm) BCK(tm->begin(c.n, 0, b->stream));
-      BCK(launch_obs(c.n, c.kt, b->mixed, v, parity, (int)b->slots.size(), c.ogrid, b->stream));
+      BCK(launch_obs(c.n, c.kt, cmix(b, c.n), v, parity, (int)b->slots.size(), c.ogrid, b->stream));
       if (tm) BCK(tm->end(b->stream));
     }
     for (int st = 0; st < 4; st++)
@@ -646,9 +669,9 @@ int record_chunk(edus_batch* b, LaunchTimer* tm = nullptr) {
         if (c.form == 3 || c.form == 4)
           BCK(launch_stage_pipe(c.n, c.kt, c.form == 4, v, st, parity, c.psel, c.pcomp, c.sgrid, b->stream));
         else if (c.form == 2)
-          BCK(launch_stage_mm(c.n, c.kt, b->mixed, v, st, parity, c.sgrid, b->stream));
+          BCK(launch_stage_mm(c.n, c.kt, cmix(b, c.n), v, st, parity, c.sgrid, b->stream));
         else
-          BCK(launch_stage(c.n, c.kt, c.form, b->mixed, v, st, parity, c.sgrid, b->stream));
+          BCK(launch_stage(c.n, c.kt, c.form, cmix(b, c.n), v, st, parity, c.sgrid, b->stream));
         if (tm) BCK(tm->end(b->stream));
       }
   }
@@ -725,6 +748,81 @@ Slot* slot_of(edus_batch* b, int32_t slot) {
   return &b->slots[slot];
 }
 
+// An instance with the Coulomb mean field: its own FP64 context, the whole loop
+// launched at once on the context's stream (it runs beside the chunk graphs and
+// is retired by polling). Its result equals edus_run's on the same problem.
+int add_coulomb(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* slot_out) {
+  const Problem& P = pb->P;
+  const int64_t est = ctx_footprint_estimate(P);
+  if (b->bytes_used + est > b->budget)
+    return fail(EDUS_ENOMEM, "batch: %lld bytes do not fit the HBM budget (%lld of %lld used)", (long long)est,
+                (long long)b->bytes_used, (long long)b->budget);
+  int q = -1;
+  for (size_t i = 0; i < b->slots.size(); i++)
+    if (b->slots[i].status == EDUS_INST_FREE) {
+      q = (int)i;
+      break;
+    }
+  if (q < 0) return fail(EDUS_ENOMEM, "batch: all %zu slots are in use", b->slots.size());
+  edus_options o;
+  edus_options_default(&o);
+  o.device = b->device;
+  o.use_graphs = 1;
+  edus_ctx* ctx = nullptr;
+  int rc = edus_create(pb, &o, &ctx);
+  if (rc) return rc;
+  const int64_t bytes = (int64_t)ctx_device_bytes(ctx);
+  if (b->bytes_used + bytes > b->budget) {
+    edus_destroy(ctx);
+    return fail(EDUS_ENOMEM, "batch: %lld bytes do not fit the HBM budget", (long long)bytes);
+  }
+  if ((rc = ctx_start_async(ctx))) {
+    edus_destroy(ctx);
+    return rc;
+  }
+  Slot s;
+  s.n = P.ncv;
+  s.nk = P.nk;
+  s.ntri = P.ncv * (P.ncv + 1) / 2;
+  s.itfi = P.itfi;
+  s.res = std::max(1, P.p.it_resolution);
+  s.nlog = s.itfi / s.res + 1;
+  s.tag = tag;
+  s.bytes = bytes;
+  s.sub = ctx;
+  s.status = EDUS_INST_RUNNING;
+  s.tick_admit = b->tick;
+  b->bytes_used += bytes;
+  b->slots[q] = std::move(s);
+  *slot_out = q;
+  return 0;
+}
+
+// Retire the Coulomb instances whose run has ended; with wait, block until the
+// earliest-admitted running one has ended (the batch has no other work).
+int poll_subs(edus_batch* b, bool wait) {
+  Slot* first = nullptr;
+  for (auto& s : b->slots) {
+    if (!s.sub || s.status != EDUS_INST_RUNNING) continue;
+    bool done = false;
+    int rc = ctx_poll(s.sub, &done);
+    if (rc) return rc;
+    if (done) {
+      s.status = EDUS_INST_DONE;
+      b->kpoint_steps += (double)s.nk * (s.itfi + 1);
+    } else if (!first || s.tick_admit < first->tick_admit) {
+      first = &s;
+    }
+  }
+  if (wait && first) {
+    int rc = ctx_wait(first->sub);
+    if (rc) return rc;
+    first->status = EDUS_INST_DONE;
+    b->kpoint_steps += (double)first->nk * (first->itfi + 1);
+  }
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -789,7 +887,11 @@ void edus_batch_destroy(edus_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  for (auto& s : b->slots) free_slot_mem(b, s);
+  for (auto& s : b->slots) {
+    if (s.sub) edus_destroy(s.sub);
+    s.sub = nullptr;
+    free_slot_mem(b, s);
+  }
   for (auto& kv : b->classes) {
     if (kv.second.d_tiles) cudaFreeAsync(kv.second.d_tiles, b->stream);
     if (kv.second.d_ntiles) cudaFree(kv.second.d_ntiles);
@@ -811,7 +913,7 @@ int edus_batch_footprint(edus_batch* b, const edus_problem* pb, int64_t* bytes) 
   if (!b || !pb || !bytes) return fail(EDUS_EINVAL, "null argument");
   int rc = check_problem(b, pb->P);
   if (rc) return rc;
-  *bytes = (int64_t)layout_of(b, pb->P, tile_len(b, pb->P.ncv)).total();
+  *bytes = pb->P.p.coulomb ? ctx_footprint_estimate(pb->P) : (int64_t)layout_of(b, pb->P, tile_len(b, pb->P.ncv)).total();
   return 0;
 }
 
@@ -820,6 +922,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   const Problem& P = pb->P;
   int rc = check_problem(b, P);
   if (rc) return rc;
+  if (P.p.coulomb) return add_coulomb(b, pb, tag, slot_out);
   const int n = P.ncv, nk = P.nk, nt = n * (n + 1) / 2, kt = tile_len(b, n);
   const Layout L = layout_of(b, P, kt);
   const int64_t bytes = (int64_t)L.total();
@@ -912,10 +1015,10 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   }
   if (P.model_deferred) {
     // (the exact segment sums hold up to 1024-deep segments, 512 R vectors)
-    const bool tc = b->mixed && b->opt.tc_contraction && P.p.conduction_shift <= 1e-16 && tc_seg_k(P.nrpts) <= 1024;
+    const bool tc = cmix(b, n) && b->opt.tc_contraction && P.p.conduction_shift <= 1e-16 && tc_seg_k(P.nrpts) <= 1024;
     if ((rc = tc ? build_model_tc(b, P, I) : build_model_on_device(b, P, I))) return undo(rc);
   } else {
-    rc = b->mixed ? upload_model<float2>(b, P, I) : upload_model<double2>(b, P, I);
+    rc = cmix(b, n) ? upload_model<float2>(b, P, I) : upload_model<double2>(b, P, I);
     if (rc) return undo(rc);
     std::vector<double2> st;
     planes<double2>(P.P0.data(), nk, n, 1, st);
@@ -930,7 +1033,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   }
   // mixed precision: Pb starts as the FP32 copy of the deviation P0 = 0 that
   // stage 0 reads (stage 3 refreshes it every step)
-  if (b->mixed && cudaMemsetAsync(I.Pb, 0, L.state, b->stream) != cudaSuccess)
+  if (cmix(b, n) && cudaMemsetAsync(I.Pb, 0, L.state, b->stream) != cudaSuccess)
     return undo(fail(EDUS_ECUDA, "batch: clear stage input"));
   {
     // field table: the single-solve loop's times (t += dt) and fields
@@ -953,7 +1056,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
       cudaMemcpyAsync(b->d_insts + q, &I, sizeof(Inst), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
     return undo(fail(EDUS_ECUDA, "batch: upload of the instance descriptor"));
   b->h2d_bytes += (long long)sizeof(Inst);
-  if (b->mixed && launch_weq(b->d_insts, q, nt, nk, b->stream) != cudaSuccess)
+  if (cmix(b, n) && launch_weq(b->d_insts, q, nt, nk, b->stream) != cudaSuccess)
     return undo(fail(EDUS_ECUDA, "batch: equilibrium terms"));
   const int zero = 0;
   if (cudaMemcpyAsync(b->d_it[b->tick & 1] + q, &zero, sizeof(int), cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
@@ -965,7 +1068,7 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
     c.kt = kt;
     c.occ = profile_of(b, n);
     c.form = -1;  // chosen with the tile table, before the next chunk
-    c.ogrid = obs_grid(n, b->mixed, (int)b->slots.size());
+    c.ogrid = obs_grid(n, cmix(b, n), (int)b->slots.size());
     if (c.ogrid <= 0) return undo(fail(EDUS_ECUDA, "batch: no resident block of the observable kernel for %d bands", n));
     if (cudaMalloc(&c.d_ntiles, 2 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&c.d_cinst, b->slots.size() * sizeof(ClassInst)) != cudaSuccess)
@@ -985,18 +1088,23 @@ int edus_batch_advance(edus_batch* b, int32_t nsteps) {
   if (!b || nsteps < 0) return fail(EDUS_EINVAL, "bad argument");
   BCK(cudaSetDevice(b->device));
   const int S = b->opt.chunk_steps;
+  bool tiles = false;
+  for (auto& kv : b->classes) tiles = tiles || !kv.second.tiles.empty();
   for (int done = 0; done < nsteps; done += S) {
     int rc = run_chunk(b);
     if (rc) return rc;
   }
-  return 0;
+  // with no tile of any class left, only Coulomb instances run: wait for one
+  return poll_subs(b, !tiles && nsteps > 0);
 }
 
 int edus_batch_poll(edus_batch* b, int32_t slot, int32_t* status, int32_t* it, int64_t* tag) {
   Slot* s = slot_of(b, slot);
   if (!s) return fail(EDUS_EINVAL, "bad slot");
   if (status) *status = s->status;
-  if (it) *it = s->status == EDUS_INST_FREE ? 0 : (int32_t)std::min<long long>(b->tick - s->tick_admit, s->itfi + 1);
+  if (it) *it = s->status == EDUS_INST_FREE ? 0
+                : (s->sub && s->status == EDUS_INST_DONE) ? s->itfi + 1
+                                                          : (int32_t)std::min<long long>(b->tick - s->tick_admit, s->itfi + 1);
   if (tag) *tag = s->tag;
   return 0;
 }
@@ -1004,6 +1112,14 @@ int edus_batch_poll(edus_batch* b, int32_t slot, int32_t* status, int32_t* it, i
 int edus_batch_obs_count(edus_batch* b, int32_t slot, int32_t* n) {
   Slot* s = slot_of(b, slot);
   if (!s || !n || s->status == EDUS_INST_FREE) return fail(EDUS_EINVAL, "bad slot");
+  if (s->sub) {
+    // a Coulomb instance's log is complete when its run has ended
+    if (s->status != EDUS_INST_DONE) {
+      *n = 0;
+      return 0;
+    }
+    return edus_obs_count(s->sub, n);
+  }
   const long long it = std::min<long long>(b->tick - s->tick_admit, s->itfi + 1);
   *n = (int32_t)std::min<long long>(s->nlog, (it + s->res - 1) / s->res);
   return 0;
@@ -1012,6 +1128,12 @@ int edus_batch_obs_count(edus_batch* b, int32_t slot, int32_t* n) {
 int edus_batch_obs_get(edus_batch* b, int32_t slot, int32_t first, int32_t count, edus_obs* out) {
   Slot* s = slot_of(b, slot);
   if (!s || !out || s->status == EDUS_INST_FREE) return fail(EDUS_EINVAL, "bad slot");
+  if (s->sub) {
+    if (s->status != EDUS_INST_DONE) return fail(EDUS_EINVAL, "the Coulomb instance is still running");
+    int rc = edus_obs_get(s->sub, first, count, out);
+    if (!rc) b->d2h_bytes += (long long)(sizeof(edus_obs) * count);
+    return rc;
+  }
   if (first < 0 || count < 0 || first + count > s->nlog) return fail(EDUS_EINVAL, "range outside the log");
   BCK(cudaSetDevice(b->device));
   BCK(cudaMemcpyAsync(out, s->inst.log + first, sizeof(edus_obs) * count, cudaMemcpyDeviceToHost, b->stream));
@@ -1023,6 +1145,11 @@ int edus_batch_obs_get(edus_batch* b, int32_t slot, int32_t first, int32_t count
 int edus_batch_get_state(edus_batch* b, int32_t slot, double* rho) {
   Slot* s = slot_of(b, slot);
   if (!s || !rho || s->status == EDUS_INST_FREE) return fail(EDUS_EINVAL, "bad slot");
+  if (s->sub) {
+    int rc = edus_get_state(s->sub, rho);
+    if (!rc) b->d2h_bytes += (long long)(16 * (size_t)s->nk * s->n * s->n);
+    return rc;
+  }
   BCK(cudaSetDevice(b->device));
   const int n = s->n, nk = s->nk;
   std::vector<double2> pl((size_t)s->ntri * nk);
@@ -1052,6 +1179,12 @@ int edus_batch_release(edus_batch* b, int32_t slot) {
   if (!s) return fail(EDUS_EINVAL, "bad slot");
   if (s->status == EDUS_INST_FREE) return 0;
   BCK(cudaSetDevice(b->device));
+  if (s->sub) {
+    edus_destroy(s->sub);  // waits for the context's stream
+    b->bytes_used -= s->bytes;
+    *s = Slot();
+    return 0;
+  }
   if (s->status == EDUS_INST_RUNNING) {
     ClassTab& c = b->classes[s->n];
     c.tiles.erase(std::remove_if(c.tiles.begin(), c.tiles.end(), [&](const Tile& t) { return t.inst == slot; }), c.tiles.end());

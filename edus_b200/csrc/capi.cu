@@ -10,6 +10,7 @@
 // inside a constant-dt run; the observable log stays on the device until read.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -21,6 +22,7 @@
 #include <sys/stat.h>
 #include <vector>
 
+#include "ctx_hooks.hpp"
 #include "cuda/kernels.hpp"
 #include "host/problem.hpp"
 
@@ -106,6 +108,8 @@ struct edus_ctx {
   int* d_err = nullptr;  // device error word set by bounded waits
   edus_obs* d_log = nullptr;
   edus_obs* d_obs_one = nullptr;  // record of edus_observables, allocated on its first call
+  size_t dev_bytes = 0;            // device memory the context holds
+  long long async_l0 = 0;          // launch count at the start of an asynchronous whole run
   int log_cap = 0, nlog = 0;
   double* d_ncond = nullptr;
   double* d_pcmax = nullptr;
@@ -169,6 +173,7 @@ int dalloc(edus_ctx* c, T** p, size_t count) {
   cudaError_t e = cudaMalloc(&v, sizeof(T) * (count ? count : 1));
   if (e != cudaSuccess) return fail(EDUS_ENOMEM, "cudaMalloc(%zu bytes): %s", sizeof(T) * count, cudaGetErrorString(e));
   c->allocs.push_back(v);
+  c->dev_bytes += sizeof(T) * (count ? count : 1);
   *p = (T*)v;
   return 0;
 }
@@ -528,9 +533,13 @@ int run_steps(edus_ctx* c, int nsteps, bool all) {
   return 0;
 }
 
-int timed(edus_ctx* c, int nsteps, bool all) {
+// Enqueue nsteps (or the whole run) between the context's two timing events;
+// *l0 receives the launch count before them. timed_finish waits for the end
+// event and checks the device error word.
+int timed_start(edus_ctx* c, int nsteps, bool all, long long* l0_out) {
   CK(cudaSetDevice(c->device));
   long long l0 = c->launches;
+  *l0_out = l0;
   const bool graph = all && !c->dyn && c->use_graphs && c->it == 0;
   if (graph && !c->gexec) {
     // capture the whole loop once; the captured kernels run at cudaGraphLaunch below
@@ -584,9 +593,11 @@ int timed(edus_ctx* c, int nsteps, bool all) {
     int rc = run_steps(c, nsteps, all);
     if (rc) return rc;
   }
-  {
-  }
   CK(cudaEventRecord(c->ev1, c->stream));
+  return 0;
+}
+
+int timed_finish(edus_ctx* c, long long l0) {
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0;
   CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
@@ -599,7 +610,104 @@ int timed(edus_ctx* c, int nsteps, bool all) {
   return 0;
 }
 
+int timed(edus_ctx* c, int nsteps, bool all) {
+  long long l0 = 0;
+  int rc = timed_start(c, nsteps, all, &l0);
+  if (rc) return rc;
+  return timed_finish(c, l0);
+}
+
 }  // namespace
+
+// ------------------------------------------------------------ bounded-wait self-test
+namespace edus {
+namespace selftest {
+
+// One thread initialises an mbarrier expecting one arrival that nothing makes
+// (no bulk copy is issued) and waits on it with the kernels' bounded wait, cut
+// to `iters` polls: the wait runs out, records the timeout in *err and the
+// kernel returns.
+__global__ void k_wait_selftest(int* err, int iters) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  mbar_wait(&bar, 0, err, iters);
+}
+
+}  // namespace selftest
+}  // namespace edus
+
+extern "C" int edus_selftest_bounded_wait(int32_t device, int32_t iters) {
+  if (iters < 1 || iters > (1 << 20)) return fail(EDUS_EINVAL, "iters must be in [1, 2^20]");
+  CK(cudaSetDevice(device));
+  int* err = nullptr;
+  CK(cudaMalloc(&err, sizeof(int)));
+  int h = 0;
+  cudaError_t e = cudaMemset(err, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    edus::selftest::k_wait_selftest<<<1, 32>>>(err, iters);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(err);
+  if (e != cudaSuccess) return fail(EDUS_ECUDA, "bounded-wait self-test: %s", cudaGetErrorString(e));
+  if (h == kErrTimeout) return fail(EDUS_ETIMEOUT, "a bounded device wait ran out after %d polls (self-test)", iters);
+  return 0;
+}
+
+// ------------------------------------------------------------ batch hooks
+// A batch runs an instance with the Coulomb mean field as a context of its
+// own: the whole loop, captured in one CUDA graph as edus_run replays it, is
+// launched on the context's stream and runs beside the batch's chunk graphs.
+namespace edus {
+
+int ctx_start_async(edus_ctx* c) {
+  if (!c) return fail(EDUS_EINVAL, "null argument");
+  if (c->dyn || !c->use_graphs || c->it != 0)
+    return fail(EDUS_EUNSUPPORTED, "an asynchronous whole run needs a fresh context at constant dt with graphs");
+  return timed_start(c, 0, true, &c->async_l0);
+}
+
+int ctx_poll(edus_ctx* c, bool* done) {
+  if (!c || !done) return fail(EDUS_EINVAL, "null argument");
+  CK(cudaSetDevice(c->device));
+  cudaError_t e = cudaEventQuery(c->ev1);
+  if (e == cudaErrorNotReady) {
+    *done = false;
+    return 0;
+  }
+  if (e != cudaSuccess) return fail(EDUS_ECUDA, "context run: %s", cudaGetErrorString(e));
+  *done = true;
+  return timed_finish(c, c->async_l0);
+}
+
+int ctx_wait(edus_ctx* c) {
+  if (!c) return fail(EDUS_EINVAL, "null argument");
+  CK(cudaSetDevice(c->device));
+  return timed_finish(c, c->async_l0);
+}
+
+size_t ctx_device_bytes(const edus_ctx* c) { return c ? c->dev_bytes : 0; }
+
+double ctx_last_ms(const edus_ctx* c) { return c ? c->last_ms : 0.0; }
+
+// Upper bound of the device memory edus_create takes for a problem: the
+// state, table and ring planes, the observable log, the Coulomb scratch and
+// the snapshot slots, with a margin.
+int64_t ctx_footprint_estimate(const Problem& P) {
+  const double n = P.ncv, nk = P.nk, nt = n * (n + 1) / 2, plane = 16.0 * nt * nk;
+  const int order = P.p.solver == EDUS_SOLVER_RK4 ? 0 : P.p.order;
+  double b = plane * (1 + 3 + 3 + 4 + 1 + order) + 16.0 * n * n * nk + 4.0 * P.nnb * nk;
+  b += (double)(P.nprint + 2) * sizeof(edus_obs) + (double)obs_parts(P.nk) * obs_part_bytes();
+  if (P.p.coulomb) {
+    const double nc = P.ncut, side = std::max(P.n1, P.n2);
+    b += plane * 2 + 16.0 * 4 * nc * nc * n * n * 3 + 16.0 * 4 * nc * side * nt * 2 + 8.0 * 4 * nc * side;
+  }
+  return (int64_t)(1.25 * b) + (1 << 20);
+}
+
+}  // namespace edus
 
 // =================================================================== C ABI
 
@@ -1035,7 +1143,6 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   if (!pb || !out) return fail(EDUS_EINVAL, "null argument");
   if (pb->P.model_deferred)
     return fail(EDUS_EUNSUPPORTED, "the problem's model is tabulated on the device only in batches (edus_problem_create)");
-  if (pb->P.p.mode == EDUS_MODE_CRYSTAL) return fail(EDUS_EUNSUPPORTED, "Crystal models keep Hermitian dipoles, which the device kernels (one symmetric dipole plane per band pair) do not run; the set-up tables are available");
   edus_options o;
   edus_options_default(&o);
   if (opt) o = *opt;
@@ -1070,13 +1177,17 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   c->dyn = P.p.dynamical_dt != 0;
   c->coul = P.p.coulomb != 0;
   c->res = P.p.it_resolution > 0 ? P.p.it_resolution : 1;
-  // symmetric dipoles are stored as upper triangles
+  // dipoles are stored as upper triangles: symmetric ones (Wannier and
+  // tight-binding models) or Hermitian ones (the Crystal interface)
+  const bool herm = P.p.mode == EDUS_MODE_CRYSTAL;
   for (int k = 0; k < nk; k++)
     for (int i = 0; i < n; i++)
-      for (int j = i + 1; j < n; j++)
-        for (int x = 0; x < 3; x++)
-          if (P.D[(((size_t)k * n + i) * n + j) * 3 + x] != P.D[(((size_t)k * n + j) * n + i) * 3 + x])
-            return bail(fail(EDUS_EUNSUPPORTED, "dipole matrix is not symmetric at k=%d (%d,%d)", k, i, j));
+      for (int j = i + (herm ? 0 : 1); j < n; j++)
+        for (int x = 0; x < 3; x++) {
+          const cd u = P.D[(((size_t)k * n + i) * n + j) * 3 + x], l = P.D[(((size_t)k * n + j) * n + i) * 3 + x];
+          if (herm ? (l != std::conj(u)) : (l != u))
+            return bail(fail(EDUS_EUNSUPPORTED, "dipole matrix is not %s at k=%d (%d,%d)", herm ? "Hermitian" : "symmetric", k, i, j));
+        }
   // ---- device tables
   std::vector<double2> pl;
   double2 *dH, *dD, *dU = nullptr, *dGE = nullptr;
@@ -1191,6 +1302,7 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   tb.nbr = dnbr;
   tb.err = c->d_err;
   tb.n_diss = (int)P.diss_i.size();
+  tb.herm_dip = herm ? 1 : 0;
   // ---- Coulomb
   if (c->coul) {
     const int nc = P.ncut, n1 = tb.n1, n2 = tb.n2;

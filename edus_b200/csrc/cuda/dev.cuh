@@ -65,8 +65,8 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t phase, int* err) {
-  for (int it = 0; it < kBulkWaitIters; ++it) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t phase, int* err, int iters = kBulkWaitIters) {
+  for (int it = 0; it < iters; ++it) {
     uint32_t done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -122,6 +122,12 @@ struct DevTables {
   const double2* GE;   // [3][ntri][nk] or null
   const int* nbr;      // [nnb][nk]
   int n_diss;
+  // 1: D is Hermitian (the Crystal interface keeps its Berry connections as
+  // read, headers/Crystal_interface.h:266-268): D_ji = conj(D_ij). 0: D is
+  // symmetric (the reference's 1/2 (D + D^T) of Wannier and tight-binding
+  // models, Source_Main/save_HUD.cpp:47-51): D_ji = D_ij. Only the upper
+  // triangle is stored either way.
+  int herm_dip;
   // Coulomb (null when off)
   int ncut;
   const double2* h;      // [n1][2][ncut][ntri] inverse-transform rows

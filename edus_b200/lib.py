@@ -85,6 +85,7 @@ def load_library():
         "edus_batch_stats_get": (C.c_int, [vp, P(abi.BatchStats)]),
         "edus_batch_tile_k": (C.c_int, [vp, i32, P(i32)]),
         "edus_batch_profile": (C.c_int, [vp, i32, P(abi.KernelTime), i32, P(i32)]),
+        "edus_selftest_bounded_wait": (C.c_int, [i32, i32]),
         "edus_server_options_default": (C.c_int, [P(abi.ServerOptions)]),
         "edus_server_create": (C.c_int, [P(abi.ServerOptions), P(vp)]),
         "edus_server_submit": (C.c_int, [vp, P(abi.Params), cp, P(C.c_int64)]),

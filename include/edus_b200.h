@@ -292,6 +292,12 @@ int edus_observables(edus_ctx* ctx, edus_obs* out);
  * shared by every context on a device: calls that overlap in time (two host
  * threads, or two streams) race on it and must be serialised by the caller. */
 int edus_observables_static(edus_ctx* ctx, edus_obs* out);
+/* Failure-path self-test of the kernels' bounded waits: one kernel waits, with
+ * the same bounded wait the bulk-copy kernels use but cut to `iters` polls, on
+ * an mbarrier nothing arrives on (no copy is issued), records the timeout in
+ * the device error word and returns. Expected result EDUS_ETIMEOUT, with the
+ * device still usable. No reference counterpart. */
+int edus_selftest_bounded_wait(int32_t device, int32_t iters);
 /* Write Output/{EF,J1,J2,Losses,TransientAbs,k_grid}.txt in the reference's
  * format, the per-k files of the first output step (H_Eigen_*, H_Wannier_cond,
  * P_initial_Wannier_, Uk_) and, when the input asks for them, the snapshot

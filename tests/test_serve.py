@@ -26,7 +26,8 @@ def rel(a, b):
 
 def requests(workdir):
     """(params, workdir) of a small mix: hBN (core band dropped -> 2 bands),
-    8-band and 16-band Wannier models, uneven grids and durations."""
+    8-band and 16-band Wannier models, uneven grids and durations, and an hBN
+    request with the Rytova-Keldysh mean field (3 bands, FP64 context)."""
     out = []
     for i, (n, tf, f) in enumerate([(16, 0.5, 0.3), (22, 0.3, 0.6), (12, 0.7, 0.1)]):
         d = f"{workdir}/h{i}"
@@ -35,6 +36,8 @@ def requests(workdir):
     out.append((E.parse_input(W.wannier(d, n=12, t_fin_fs=0.3, it_res=4)), d))
     d = f"{workdir}/w16"
     out.append((E.parse_input(W.wannier(d, nw=16, nside=13, n=10, t_fin_fs=0.2, it_res=5, name="W16")), d))
+    d = f"{workdir}/coul"
+    out.append((E.parse_input(W.hbn_coulomb(d, n=14, t_fin_fs=0.4, it_res=3, field=0.6)), d))
     return out
 
 
@@ -61,6 +64,7 @@ def test_each_result_is_the_same_alone_and_in_the_mix(workdir, precision):
     assert st["p50_latency_s"] > 0 and st["p99_latency_s"] >= st["p50_latency_s"]
     assert infos[0]["nbands"] == 2          # the hBN core band was dropped
     assert infos[4]["nbands"] == 16
+    assert infos[5]["nbands"] == 3          # Coulomb keeps the core band (FP64 context)
     for q, req in enumerate(reqs):
         alone, _, _ = serve([req], precision)
         a, b = alone[0], mix[q]
@@ -99,9 +103,10 @@ def test_admission_waits_for_memory(workdir):
 
 
 def test_unsupported_request_fails_alone(workdir):
+    """A request the batch does not run (adaptive dt) fails alone."""
     reqs = requests(workdir)[:2]
-    d = f"{workdir}/coul"
-    bad = (E.parse_input(W.hbn_coulomb(d, n=12, t_fin_fs=0.2)), d)
+    d = f"{workdir}/dyn"
+    bad = (E.parse_input(W.hbn_rk4(d, n=12, t_fin_fs=0.2, solver="dynamical_dt_evolution\nepsStepAbs 0.001\n")), d)
     s = E.Server(chunk_steps=8)
     ids = [s.submit(*reqs[0]), s.submit(*bad), s.submit(*reqs[1])]
     s.drain(300)
@@ -130,3 +135,17 @@ def test_diverging_request_fails_alone(workdir, precision):
     with pytest.raises(E.EdusError):
         s.obs(ids[1])
     s.close()
+
+
+def test_served_coulomb_request_matches_the_single_solve_path(workdir):
+    """A Coulomb request in the mix runs as its own FP64 context: bit for bit the
+    single-solve result on the same input."""
+    reqs = requests(workdir)
+    out, infos, _ = serve(reqs, abi.EDUS_PREC_MIXED, stagger_s=0.01)
+    p, d = reqs[5]
+    ctx = E.Context(E.Problem(p, d))
+    ctx.run()
+    ref = ctx.obs()
+    assert len(ref) == len(out[5]) > 0
+    for x, y in zip(out[5], ref):
+        assert np.array_equal(x["J1"], y["J1"]) and np.array_equal(x["pop"], y["pop"])
