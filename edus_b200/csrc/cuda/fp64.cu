@@ -323,9 +323,12 @@ __global__ void __launch_bounds__(kObsThreads) k_obs(DevTables tb, const DevCons
             const double2 hil = (i <= l) ? Hs[(size_t)Tri<N>::idx(i, l) * nk + k] : cconj(Hs[(size_t)Tri<N>::idx(l, i) * nk + k]);
             const double2 ph = cmul(pij, hil);
             const int lo = j < l ? j : l, hi = j < l ? l : j;
+            // D_jl: the stored upper entry, conjugated below the diagonal for Hermitian dipoles
+            const bool cj = tb.herm_dip && j > l;
 #pragma unroll
             for (int x = 0; x < 3; x++) {
-              const double2 d = tb.D[(size_t)(x * NT + Tri<N>::idx(lo, hi)) * nk + k];
+              const double2 ds = tb.D[(size_t)(x * NT + Tri<N>::idx(lo, hi)) * nk + k];
+              const double2 d = cj ? cconj(ds) : ds;
               my.J2[x] = cadd(my.J2[x], cmulc(ph, d));
             }
           }

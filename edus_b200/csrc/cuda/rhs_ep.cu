@@ -165,12 +165,14 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
   {
     // H~ = H + E^w . D with w = probe when exactly one of (i, j) is a core band
     // (headers/RungeKutta.h:158-208); the lower entry uses conj(H) and the same D
+    // (symmetric dipoles) or conj(D) (Hermitian dipoles)
     const int w = (i < nch) != (j < nch);
     double2 hu = He, hl = cconj(He);
+    const bool herm = tb.herm_dip != 0;
 #pragma unroll
     for (int x = 0; x < 3; x++) {
       hu = cadd(hu, cscale(De[x], a.EF[w][x]));
-      hl = cadd(hl, cscale(De[x], a.EF[w][x]));
+      hl = cadd(hl, cscale(herm ? cconj(De[x]) : De[x], a.EF[w][x]));
     }
     sP[e][kl] = Pe;
     sHu[e][kl] = hu;

@@ -86,10 +86,10 @@ def test_edus_run_driver_reports_input_errors(tmp_path):
     assert r.returncode == 1 and "edus_run:" in r.stderr
 
 
-def test_edus_run_sets_up_a_crystal_input_then_refuses_the_device_run(tmp_path):
+def test_edus_run_sets_up_a_crystal_input(tmp_path):
     """A Crystal input: the set-up files (kpt.txt, Test_matrices.txt) are
-    written, then the device run is refused with exit status 1 before any GPU
-    work (Hermitian dipoles are not run on the device)."""
+    written before the device run (which needs a GPU: without one the
+    executable exits 1 with the CUDA error)."""
     import subprocess
 
     from edus_b200 import build
@@ -99,5 +99,5 @@ def test_edus_run_sets_up_a_crystal_input_then_refuses_the_device_run(tmp_path):
         build.build()
     W.crystal(str(tmp_path), nb=(1, 1), nkf=7, n=6)
     r = subprocess.run([build.EXE, "input.txt", "."], capture_output=True, text=True, cwd=tmp_path, timeout=120)
-    assert r.returncode == 1 and "Hermitian dipoles" in r.stderr
+    assert r.returncode == 0 or (r.returncode == 1 and "CUDA" in r.stderr), r.stderr
     assert (tmp_path / "kpt.txt").exists() and (tmp_path / "Test_matrices.txt").exists()

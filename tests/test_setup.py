@@ -264,15 +264,6 @@ def test_crystal_model_reproduces_the_file_samples(workdir):
     assert kc.shape == (100, 3)
 
 
-def test_crystal_problem_is_refused_on_the_device(workdir):
-    """Crystal dipoles are Hermitian, which the device's single dipole plane per
-    band pair does not hold: contexts and batches refuse the problem."""
-    pb = E.Problem(E.parse_input(W.crystal(workdir, nb=(1, 1), nkf=9, n=8)), workdir)
-    with pytest.raises(E.EdusError) as ei:
-        E.Context(pb)
-    assert ei.value.code == E.abi.EDUS_EUNSUPPORTED
-
-
 def test_oracle_runs_a_crystal_problem(workdir):
     """The oracle's RHS reads the full dipole matrix, so it runs Crystal inputs
     with their Hermitian dipoles: populations stay normalised and the state
