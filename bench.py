@@ -49,6 +49,9 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# requests with the Coulomb mean field run as contexts on streams of their own:
+# more hardware queues than the default 8 let those streams overlap
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 SWEEP = "pulse_sweep_256_hbn2+wannier8_48-144_10-60fs_rk4_dt0.01fs_mixed"
 COULOMB = "hbn_coulomb_120x120_ab4_rk4start_dt0.005fs_30fs_fp64"

@@ -149,19 +149,27 @@ def sweep_line(count=256, fp64_sample_every=16, err_sample=16):
     }
 
 
-def serve_requests(count, seed=7, nmin=32, nmax=192, dmin=10.0, dmax=100.0):
-    """Request stream of the serving workload: band count 2 (hBN, core band
-    dropped), 8 or 16 (Wannier, 11x11 / 13x13 R); grid N x N, N even in
-    [nmin, nmax]; duration uniform in [dmin, dmax] fs; peak field log-uniform
-    0.05-0.8 V/A; CEP uniform."""
+def serve_requests(count, seed=7, nmin=32, nmax=192, dmin=10.0, dmax=100.0, coulomb_frac=0.5):
+    """Request stream of the serving workload. Each request carries the
+    Rytova-Keldysh mean field with probability coulomb_frac: those use the hBN
+    tight-binding model (the reference's Coulomb path is built for its
+    tight-binding models), 3 bands, r0 uniform over the whole angstroms 5..20,
+    integrated as configuration 1 (Adams-Bashforth 4 with RK4 start-up, dt
+    0.005 fs, output every 0.1 fs); the others draw 2 bands (hBN, core band
+    dropped), 8 or 16 (Wannier, 11x11 / 13x13 R), RK4 at dt 0.01 fs. Grid
+    N x N, N even in [nmin, nmax]; duration uniform in [dmin, dmax] fs; peak
+    field log-uniform 0.05-0.8 V/A; CEP uniform."""
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for _ in range(count):
-        nb = int(rng.choice([2, 8, 16]))
+        coul = bool(rng.random() < coulomb_frac)
+        nb = 3 if coul else int(rng.choice([2, 8, 16]))
         n = 2 * int(rng.integers(nmin // 2, nmax // 2 + 1))
         spec = dict(n=n, field=float(math.exp(rng.uniform(math.log(0.05), math.log(0.8)))),
                     phase=float(rng.uniform(0, 2 * math.pi)), duration=float(rng.uniform(dmin, dmax)), it_res=10, dt_fs=0.01)
-        if nb == 2:
+        if coul:
+            spec.update(kind="hbn_coulomb", r0=int(rng.integers(5, 21)), dt_fs=0.005, it_res=20)
+        elif nb == 2:
             spec["kind"] = "hbn"
         else:
             spec.update(kind="wannier", nw=nb, nside=11 if nb == 8 else 13, name=f"W{nb}")
@@ -169,20 +177,64 @@ def serve_requests(count, seed=7, nmin=32, nmax=192, dmin=10.0, dmax=100.0):
     return out
 
 
-def serve_line(count=2000, rate=None, fp64_sample=9, seed=7, max_s=None, **kw):
-    """Served mixed-precision stream against the plain FP64 single-solve path on
-    the same work: the FP64 path runs, request by request, a sample stratified by
-    band count (the first fp64_sample / 3 requests of each class, in stream
-    order); its per-class rates give the FP64 time of the whole stream (sum over
-    classes of the class's k-point steps / its rate), and the speed-up is that
-    time over the served span."""
+def _class(spec):
+    return "coulomb" if spec["kind"] == "hbn_coulomb" else str(spec.get("nw", 2))
+
+
+def _units(spec):
+    dt = spec["dt_fs"] / 0.02418884326505
+    itfi = int((spec["duration"] + 0.21) / 0.02418884326505 / dt)
+    return spec["n"] ** 2 * (itfi + 1)
+
+
+def serve_line(count=2000, rate=None, per_class=30, seed=7, max_s=None, load=1.25, **kw):
+    """Served mixed-precision stream (configuration 4) against the plain FP64
+    single-solve path on the same requests.
+
+    Arrivals: Poisson at `rate`, by default `load` x the service capacity
+    estimated from measured per-class rates (the autotuner's batch rates of the
+    2-, 8- and 16-band classes, and the FP64 context rate of one Coulomb
+    request): a saturating stream. Coulomb tables are generated on the GPU
+    once per r0 before the stream starts. The FP64 path runs, request by
+    request, the first per_class requests of each class in stream order; its
+    per-class rates give the FP64 time of the whole stream, and the speed-up is
+    that over the served span."""
+    from edus_b200 import autotune
+
     D = _Dirs()
     specs = serve_requests(count, seed=seed, **kw)
-    reqs = [(E.parse_input(p), d) for p, d in (D.instance(s, i) for i, s in enumerate(specs))]
-    arrivals_rng = np.random.Generator(np.random.PCG64(seed + 1))
+    t0 = time.perf_counter()
+    tables = {r0: W.coulomb_tables_for(os.path.join(D.root, "coulomb"), r0)
+              for r0 in sorted({x["r0"] for x in specs if x["kind"] == "hbn_coulomb"})}
+    tables_s = time.perf_counter() - t0
+
+    def write(q):
+        sp = specs[q]
+        if sp["kind"] != "hbn_coulomb":
+            return D.instance(sp, q)
+        d = os.path.join(D.root, f"i{q}")
+        cdir, label = tables[sp["r0"]]
+        return W.hbn_coulomb(d, n=sp["n"], field=sp["field"], duration=sp["duration"], dt_fs=sp["dt_fs"],
+                             it_res=sp["it_res"], phase=sp["phase"], r0_ang=sp["r0"], label=label, tables=cdir), d
+
+    paths = [write(q) for q in range(count)]
+    reqs = [(E.parse_input(p), d) for p, d in paths]
+    units = {}
+    for sp in specs:
+        units[_class(sp)] = units.get(_class(sp), 0.0) + _units(sp)
+    # service capacity from measured per-class rates
+    # mixed batches run the 2-band class in FP64 (its k-gradient needs FP64 stage inputs)
+    tuned = autotune.load().get(autotune.gpu_name(), {})
+    cap_rates = {c: float(tuned.get("fp64" if c == "2" else "mixed", {}).get(c, {}).get("kpoint_steps_per_s", 0))
+                 for c in ("2", "8", "16")}
+    cap_rates = {c: r for c, r in cap_rates.items() if r > 0}
+    qc = next(q for q, sp in enumerate(specs) if sp["kind"] == "hbn_coulomb")
+    u, sec, _ = _single_fp64(*paths[qc])
+    cap_rates["coulomb"] = u / sec
+    capacity = count / sum(units[c] / cap_rates[c] for c in units if c in cap_rates)
     if rate is None:
-        rate = 1e9  # everything arrives at once: the GPU stays saturated from the start
-    gaps = arrivals_rng.exponential(1.0 / rate, size=count)
+        rate = load * capacity
+    gaps = np.random.Generator(np.random.PCG64(seed + 1)).exponential(1.0 / rate, size=count)
     s = E.Server(precision=abi.EDUS_PREC_MIXED)
     t_start = s.clock()
     ids = []
@@ -191,48 +243,40 @@ def serve_line(count=2000, rate=None, fp64_sample=9, seed=7, max_s=None, **kw):
         while s.clock() - t_start < target - 1e-4:
             time.sleep(min(0.01, max(0.0, target - (s.clock() - t_start))))
         ids.append(s.submit(p, d))
+    arrival_span = s.clock() - t_start
     s.drain(max_s or 7200)
     st = s.stats()
-    infos = [s.info(i) for i in ids]
-    nb_of = [int(x["nbands"]) for x in infos]
-    stream_units = {}
-    for x in infos:
-        stream_units[int(x["nbands"])] = stream_units.get(int(x["nbands"]), 0.0) + float(x["nk"]) * float(x["steps"])
-    per_class = max(1, fp64_sample // max(1, len(stream_units)))
     sample = []
-    for nb in sorted(stream_units):
-        sample += [q for q in range(count) if nb_of[q] == nb][:per_class]
+    for c in sorted(units):
+        sample += [q for q in range(count) if _class(specs[q]) == c][:per_class]
     logs = {q: s.obs(ids[q]) for q in sample}
     s.close()
     # plain FP64 single-solve path, request by request (one request on the GPU at a time)
-    cls = {}
-    lat = []
-    errs = []
+    cls, errs = {}, {}
     for q in sample:
-        path, d = D.instance(specs[q], q)
-        u, sec, ref = _single_fp64(path, d)
-        lat.append(sec)
-        c = cls.setdefault(nb_of[q], [0.0, 0.0, 0])
+        u, sec, ref = _single_fp64(*paths[q])
+        c = cls.setdefault(_class(specs[q]), [0.0, 0.0, 0])
         c[0] += u
         c[1] += sec
         c[2] += 1
-        errs.append(_rel(_J1(logs[q]), _J1(ref)))
-    fp64_stream_s = sum(stream_units[nb] / (cls[nb][0] / cls[nb][1]) for nb in stream_units)
-    fp64_sample_rate = sum(c[0] for c in cls.values()) / sum(c[1] for c in cls.values())
+        errs.setdefault(_class(specs[q]), []).append(_rel(_J1(logs[q]), _J1(ref)))
+    fp64_stream_s = sum(units[c] / (cls[c][0] / cls[c][1]) for c in units)
     return {
         "metric": "solves/s", "value": st["solves_per_s"], "unit": "solves/s", "higher_is_better": True,
-        "dtype": "mixed (fp32 commutator, fp64 rho)", "data": "synthetic",
-        "config": {"workload": f"serving_{count}_requests_nb2-8-16_32-192_10-100fs", "arrival_rate_per_s": rate,
-                   "coulomb": "not in the served mix (batch instances run without the mean field)"},
+        "dtype": "mixed (fp32 commutator, fp64 rho); Coulomb requests fp64", "data": "synthetic",
+        "config": {"workload": f"serving_{count}_requests_nb2-8-16_half_coulomb_r0_5-20A_32-192_10-100fs",
+                   "arrival": "Poisson", "arrival_rate_per_s": rate, "capacity_estimate_per_s": capacity,
+                   "capacity_rates": cap_rates, "load": rate / capacity, "arrival_span_s": arrival_span,
+                   "coulomb_tables": {"r0_values": len(tables), "generation_s": tables_s}},
         "kpoint_steps_per_s": st["kpoint_steps_per_s"], "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
         "max_latency_s": st["max_latency_s"], "completed": st["completed"], "failed": st["failed"], "span_s": st["span_s"],
         "device_busy_s": st["device_ms"] * 1e-3,
         "peak_active": st["peak_active"], "peak_bytes": st["peak_bytes"],
-        "stream_kpoint_steps_by_bands": {str(k): v for k, v in sorted(stream_units.items())},
-        "fp64_request_by_request_sample": {
-            "requests": len(lat), "mean_latency_s": float(np.mean(lat)), "kpoint_steps_per_s": fp64_sample_rate,
-            "by_bands": {str(nb): {"requests": c[2], "kpoint_steps_per_s": c[0] / c[1]} for nb, c in sorted(cls.items())},
+        "stream_kpoint_steps_by_class": {k: v for k, v in sorted(units.items())},
+        "fp64_request_by_request": {
+            "requests": sum(c[2] for c in cls.values()),
+            "by_class": {c: {"requests": v[2], "kpoint_steps_per_s": v[0] / v[1]} for c, v in sorted(cls.items())},
             "stream_seconds": fp64_stream_s},
         "speedup_vs_fp64_request_by_request": fp64_stream_s / st["span_s"],
-        "j1_rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "requests": len(errs)},
+        "j1_rel_l2_vs_fp64": {c: {"max": max(v), "median": float(np.median(v)), "requests": len(v)} for c, v in sorted(errs.items())},
     }

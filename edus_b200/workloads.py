@@ -21,6 +21,7 @@ TIME_FS_AU = 1.0 / 0.02418884326505
 EV_AU = 1.0 / 27.211396
 EFIELD_AU_PER_V_A = 1e10 / 5.14221e11
 COULOMB_LABEL = "G_num502657_Ncut20_"
+ANG_AU = 1.0 / 0.52917721092  # bohr per angstrom with the reference's space_au_A (headers/Constants.h:31)
 
 
 def intensity_wcm2(e_v_per_a):
@@ -89,12 +90,22 @@ def hbn_rk4(workdir, n=60, field=0.3, photon=0.4, duration=30.0, dt_fs=0.01, t_f
 
 
 def hbn_coulomb(workdir, n=120, field=0.5, photon=0.4, duration=30.0, dt_fs=0.005, t_fin_fs=None, it_res=10, ab_order=4,
-                rk4_startup=True):
+                rk4_startup=True, rk4=False, phase=0.0, r0_ang=None, label=COULOMB_LABEL, tables=None):
+    """hBN with the Rytova-Keldysh mean field, Adams-Bashforth (or RK4 with
+    rk4=True). Tables: the packaged Ncut=20 files (the reference's shipped ones,
+    r0 = 10 A) unless `tables` names an Output/Coulomb directory made for
+    r0_ang by coulomb_tables_for (label = its file label)."""
     os.makedirs(workdir, exist_ok=True)
-    write_coulomb_files(workdir)
-    solver = f"Adams_Bashforth {ab_order}\n" + ("Adams_Bashforth_RK4_startup\n" if rk4_startup else "")
+    if tables is None:
+        write_coulomb_files(workdir)
+    else:
+        os.makedirs(os.path.join(workdir, "Output"), exist_ok=True)
+        link = os.path.join(workdir, "Output", "Coulomb")
+        if not os.path.exists(link):
+            os.symlink(tables, link)
+    solver = "" if rk4 else f"Adams_Bashforth {ab_order}\n" + ("Adams_Bashforth_RK4_startup\n" if rk4_startup else "")
     path = hbn_rk4(workdir, n=n, field=field, photon=photon, duration=duration, dt_fs=dt_fs, t_fin_fs=t_fin_fs,
-                   it_res=it_res, solver=solver)
+                   it_res=it_res, solver=solver, phase=phase)
     with open(path, "a") as f:
         f.write(
             "\nCoulomb{\n"
@@ -102,11 +113,35 @@ def hbn_coulomb(workdir, n=120, field=0.5, photon=0.4, duration=30.0, dt_fs=0.00
             "Ncut 20\n"
             "epsilon_static 1.0\n"
             "Rytova_Keldysh\n"
-            "Read_Coulomb_from_files\n"
-            f"labelInput {COULOMB_LABEL}\n"
+            + (f"r0 {r0_ang * ANG_AU:.12g}\n" if r0_ang is not None else "")
+            + "Read_Coulomb_from_files\n"
+            f"labelInput {label}\n"
             "}\n"
         )
     return path
+
+
+def coulomb_tables_for(root, r0_ang, device=0):
+    """Generate (once, on the GPU) the Coulomb tables of the hBN model for a
+    screening length r0_ang [A] (Rytova-Keldysh, qTF 0.01, Ncut 20, the
+    reference's default G_distance) under root/r0_<r0>/Output/Coulomb.
+    Returns (directory of the tables, their file label)."""
+    import edus_b200 as E
+
+    d = os.path.join(root, f"r0_{r0_ang:g}")
+    cdir = os.path.join(d, "Output", "Coulomb")
+    stamp = os.path.join(d, "label.txt")
+    if os.path.exists(stamp):
+        return cdir, open(stamp).read().strip()
+    os.makedirs(d, exist_ok=True)
+    path = hbn_rk4(d, n=12, t_fin_fs=0.0)
+    with open(path, "a") as f:
+        f.write(f"\nCoulomb{{\nqTF 0.01\nNcut 20\nepsilon_static 1.0\nRytova_Keldysh\nr0 {r0_ang * ANG_AU:.12g}\n"
+                f"labelInput r0_{r0_ang:g}A_\n}}\n")
+    label, _ = E.coulomb_generate(E.parse_input(path), d, device=device)
+    with open(stamp, "w") as f:
+        f.write(label)
+    return cdir, label
 
 
 def write_wannier_tb(path, nw=8, nside=11, seed=12345, a_ang=2.5, decay_h=1.5, decay_r=1.0, onsite_ev=3.0):

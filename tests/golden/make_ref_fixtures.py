@@ -16,7 +16,8 @@ RK4 30 fs; hBN 120x120 with the Rytova-Keldysh mean field, AB4 from the
 reference's zero derivative history, 30 fs; the 8-band Wannier model 96x96
 RK4 40 fs) and small cases of every other solver / option on the path
 (Coulomb AB4, diagonal-basis Coulomb, Taylor-6 and RK4 with adaptive dt, the
-8- and 16-band Wannier models, per-k snapshot files).
+8- and 16-band Wannier models, per-k snapshot files, the Crystal interface on
+seeded synthetic data files).
 
 Runs with the Coulomb mean field are repeated at several OpenMP thread
 counts and every distinct outcome is kept (series keys "J1", "J1#1", ...):
@@ -88,13 +89,18 @@ CASES = {
                                      "P_cond_in_Eigenstate_22_", "H_Eigen_", "H_Wannier_cond_", "P_initial_Wannier_",
                                      "Uk_")),
     "hbn24_coulomb_edia": (_edia, ("Edia_", "t_Ek")),
+    "crystal12_2band": (lambda d: W.crystal(d, nb=(1, 1), nkf=9, n=12, field=2.0, duration=4.0, t_fin_fs=1.0, it_res=5),
+                        ()),
+    "crystal10_3band": (lambda d: W.crystal(d, nb=(1, 2), norb=3, nkf=11, n=10, field=1.5, duration=4.0, t_fin_fs=1.0,
+                                            it_res=5), ()),
 }
 
 
 def _model_hash(d):
     out = {}
     for f in sorted(os.listdir(d)):
-        if f.endswith("_tb.dat"):
+        if f.endswith("_tb.dat") or f in ("kmesh_data.dat", "hk_orthonormal.dat", "bc_betabetap_real.dat",
+                                           "bc_betabetap_imag.dat"):
             out[f] = hashlib.sha256(open(os.path.join(d, f), "rb").read()).hexdigest()
     return out
 
@@ -140,6 +146,8 @@ def run_case(name, thread_counts, add=False):
     under the plain keys and each further distinct outcome under "<key>#<i>"."""
     path = os.path.join(HERE, f"ref_{name}.npz")
     out = dict(np.load(path)) if add and os.path.exists(path) else {}
+    if out and "runs" not in out:
+        out["runs"] = np.array([int(out["threads"])])
     walls = []
     for th in thread_counts:
         r = _run_once(name, th)

@@ -343,3 +343,15 @@ def test_first_output_step_files_match_oracle(workdir):
         wv = np.stack([np.real(w), np.imag(w)], axis=1)
         assert got.shape == wv.shape, name
         assert np.all(np.abs(got - wv) <= 1e-5 * np.abs(wv) + 1e-12), name
+
+
+def test_bounded_wait_runs_out_with_etimeout(workdir):
+    """A kernel's bounded wait on an mbarrier nothing arrives on runs out: the
+    call returns EDUS_ETIMEOUT (no fault, no hang) and the device still runs a
+    solve afterwards."""
+    L = E.load_library()
+    rc = L.edus_selftest_bounded_wait(0, 1000)
+    assert rc == abi.EDUS_ETIMEOUT, rc
+    assert b"ran out" in L.edus_last_error()
+    ctx, o, g, lo = run_pair(W.hbn_rk4(workdir, n=12, t_fin_fs=0.3, it_res=5), workdir, 30)
+    assert np.abs(ctx.get_state() - o.get("P0")).max() < RHO_TOL
