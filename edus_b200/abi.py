@@ -117,6 +117,7 @@ class Params(C.Structure):
         ("kpt_read", C.c_int32),
         ("kpt_offset", C.c_int64),
         ("input_path", C.c_char * EDUS_STRLEN),
+        ("velocity_gauge", C.c_int32),
     ]
 
 

@@ -748,6 +748,8 @@ Slot* slot_of(edus_batch* b, int32_t slot) {
   return &b->slots[slot];
 }
 
+int occupy_slot(edus_batch* b, int q, edus_ctx* ctx, const Problem& P, int64_t tag, int32_t* slot_out);
+
 // An instance with the Coulomb mean field: its own FP64 context, the whole loop
 // launched at once on the context's stream (it runs beside the chunk graphs and
 // is retired by polling). Its result equals edus_run's on the same problem.
@@ -780,6 +782,12 @@ int add_coulomb(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* slo
     edus_destroy(ctx);
     return rc;
   }
+  return occupy_slot(b, q, ctx, P, tag, slot_out);
+}
+
+// Slot q takes a started Coulomb context.
+int occupy_slot(edus_batch* b, int q, edus_ctx* ctx, const Problem& P, int64_t tag, int32_t* slot_out) {
+  const int64_t bytes = (int64_t)ctx_device_bytes(ctx);
   Slot s;
   s.n = P.ncv;
   s.nk = P.nk;
@@ -797,6 +805,40 @@ int add_coulomb(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* slo
   *slot_out = q;
   return 0;
 }
+
+}  // namespace
+
+namespace edus {
+
+int batch_adopt_context(edus_batch* b, edus_ctx* ctx, const Problem& P, int64_t tag, int32_t* slot_out) {
+  if (!b || !ctx || !slot_out) return fail(EDUS_EINVAL, "null argument");
+  for (size_t i = 0; i < b->slots.size(); i++)
+    if (b->slots[i].status == EDUS_INST_FREE) return occupy_slot(b, (int)i, ctx, P, tag, slot_out);
+  return fail(EDUS_ENOMEM, "batch: all %zu slots are in use", b->slots.size());
+}
+
+}  // namespace edus
+
+namespace {
+int poll_subs(edus_batch* b, bool wait);
+}
+
+namespace edus {
+
+bool batch_has_tiles(const edus_batch* b) {
+  for (const auto& kv : b->classes)
+    if (!kv.second.tiles.empty()) return true;
+  return false;
+}
+
+int batch_poll_contexts(edus_batch* b) {
+  BCK(cudaSetDevice(b->device));
+  return poll_subs(b, false);
+}
+
+}  // namespace edus
+
+namespace {
 
 // Retire the Coulomb instances whose run has ended; with wait, block until the
 // earliest-admitted running one has ended (the batch has no other work).

@@ -133,6 +133,11 @@ struct edus_ctx {
   double P_cond_max = 0, n_cond = 0;
   int solver = 0, order = 0;
   bool dyn = false, coul = false;
+  // velocity gauge: the model tables tb.H, tb.D hold H, D at k + A(t) of the
+  // last stage; A(t) = -int E_pump dt tracked on the host up to time vg_t
+  bool vg = false;
+  VgArgs vga{};
+  double vg_t = 0, vg_A[3] = {0, 0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
   long long launches = 0, last_launches = 0;
@@ -162,6 +167,7 @@ struct edus_ctx {
     double2 *P0, *Pa;
     int icont;
     std::vector<double> snap_t;
+    double vg_t, vg_A[3];
   } after_graph{};
 };
 
@@ -308,10 +314,45 @@ int observe(edus_ctx* c) {
   if (c->nlog < c->log_cap) slot = c->d_log + c->nlog;
   double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
   double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
-  CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, c->d_part,
-                        c->d_done, scaleJ, scaleTA, rec, slot, c->d_ncond, c->d_pcmax, c->stream));
+  // velocity gauge: the populations in the eigenbasis of H(k + A) and J1 from
+  // the stencil gradient of H(k + A), as with a renormalised H
+  const double2* hr = c->vg ? c->vga.H : (c->coul ? c->d_hr : nullptr);
+  CK(launch_observables(c->tb, c->d_cst, c->d_P0, hr, c->P.p.current, c->P.p.tabs, c->d_part, c->d_done, scaleJ, scaleTA,
+                        rec, slot, c->d_ncond, c->d_pcmax, c->stream));
   c->launches += 1;
   c->nlog++;
+  return 0;
+}
+
+// Velocity gauge: A(t) = -int_t0^t E_pump dt by 4-point Gauss-Legendre panels of
+// at most 0.5 a.u. from the tracked time (one panel per RK4 half step).
+void vg_advance_A(edus_ctx* c, double t) {
+  static const double gx[4] = {-0.8611363115940526, -0.3399810435848563, 0.3399810435848563, 0.8611363115940526};
+  static const double gw[4] = {0.3478548451374538, 0.6521451548625461, 0.6521451548625461, 0.3478548451374538};
+  if (t < c->vg_t) {
+    c->vg_t = c->P.t_start;
+    c->vg_A[0] = c->vg_A[1] = c->vg_A[2] = 0.;
+  }
+  const int panels = (int)std::ceil((t - c->vg_t) / 0.5);
+  const double t0 = c->vg_t;
+  for (int q = 0; q < panels; q++) {
+    const double a = t0 + (t - t0) * q / panels, b = t0 + (t - t0) * (q + 1) / panels;
+    const double h = 0.5 * (b - a), m = 0.5 * (a + b);
+    for (int g = 0; g < 4; g++) {
+      double EF[2][3];
+      field_at(c->P.p, m + h * gx[g], EF);
+      for (int x = 0; x < 3; x++) c->vg_A[x] -= h * gw[g] * EF[0][x];
+    }
+  }
+  c->vg_t = t;
+}
+
+// H, D at k + A(t) into the model tables
+int vg_tables(edus_ctx* c, double t) {
+  vg_advance_A(c, t);
+  for (int i = 0; i < 3; i++) c->vga.A[i] = c->P.MI[i][0] * c->vg_A[0] + c->P.MI[i][1] * c->vg_A[1] + c->P.MI[i][2] * c->vg_A[2];
+  CK(launch_vg_tables(c->vga, c->stream));
+  c->launches++;
   return 0;
 }
 
@@ -322,7 +363,8 @@ int step_rk4(edus_ctx* c, bool startup_ring) {
   const double dt = c->dt, dt6 = dt / 6.0, dt3 = dt / 3.0, dt2 = dt / 2.0;
   const double t = c->time_loop;
   StageArgs a = base_args(c);
-  a.e_non0 = c->e_non0;
+  // velocity gauge: no k-gradient term; H, D at k + A of each stage
+  a.e_non0 = c->vg ? false : c->e_non0;
   field_at(c->P.p, t, c->EF);
   set_ef(a, c->EF);
   a.src = c->d_P0;
@@ -336,10 +378,12 @@ int step_rk4(edus_ctx* c, bool startup_ring) {
     a.ring = c->d_ring;
     for (int s = 0; s < c->order; s++) a.ring_idx[s] = c->ring_idx[s];
   }
-  int rc = rhs(c, a);
+  int rc = c->vg ? vg_tables(c, t) : 0;
   if (rc) return rc;
+  if ((rc = rhs(c, a))) return rc;
   a.ring = nullptr;
   field_at(c->P.p, t + dt2, c->EF);
+  if (c->vg && (rc = vg_tables(c, t + dt2))) return rc;
   set_ef(a, c->EF);
   a.src = c->d_Pa;
   a.dst = c->d_Pb;
@@ -352,6 +396,7 @@ int step_rk4(edus_ctx* c, bool startup_ring) {
   a.c2 = dt;
   if ((rc = rhs(c, a))) return rc;
   field_at(c->P.p, t + dt, c->EF);
+  if (c->vg && (rc = vg_tables(c, t + dt))) return rc;
   set_ef(a, c->EF);
   a.src = c->d_Pa;
   a.dst = c->d_P0;
@@ -569,6 +614,8 @@ int timed_start(edus_ctx* c, int nsteps, bool all, long long* l0_out) {
     h.Pa = c->d_Pa;
     h.icont = c->icont;
     h.snap_t = c->snap_t;
+    h.vg_t = c->vg_t;
+    memcpy(h.vg_A, c->vg_A, sizeof(h.vg_A));
     CK(cudaEventRecord(c->ev0, c->stream));
     CK(cudaGraphLaunch(c->gexec, c->stream));
   } else if (graph) {
@@ -588,6 +635,8 @@ int timed_start(edus_ctx* c, int nsteps, bool all, long long* l0_out) {
     c->d_Pa = h.Pa;
     c->icont = h.icont;
     c->snap_t = h.snap_t;
+    c->vg_t = h.vg_t;
+    memcpy(c->vg_A, h.vg_A, sizeof(c->vg_A));
   } else {
     CK(cudaEventRecord(c->ev0, c->stream));
     int rc = run_steps(c, nsteps, all);
@@ -1303,6 +1352,51 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   tb.err = c->d_err;
   tb.n_diss = (int)P.diss_i.size();
   tb.herm_dip = herm ? 1 : 0;
+  // ---- velocity gauge (tdse{ velocity_gauge }): Fourier coefficients of the
+  // model; the tables tb.H, tb.D are rebuilt at k + A for every stage
+  c->vg = P.p.velocity_gauge != 0;
+  if (c->vg) {
+    if (P.p.mode != EDUS_MODE_WANNIER || P.HR.empty())
+      return bail(fail(EDUS_EUNSUPPORTED, "velocity gauge: Wannier models only (H(R), r(R) tables)"));
+    if (c->solver != EDUS_SOLVER_RK4 || c->dyn || P.p.coulomb || P.p.conduction_shift > 1e-16 || !P.diss_i.empty())
+      return bail(fail(EDUS_EUNSUPPORTED,
+                       "velocity gauge: RK4 at constant dt, without the Coulomb mean field, scissor shift or dissipation"));
+    const int nr = P.nrpts;
+    std::vector<double2> coef((size_t)4 * nt * nr);
+    for (int i = 0; i < n; i++)
+      for (int j = i; j < n; j++) {
+        const int e = i * n - (i * (i - 1)) / 2 + (j - i);
+        for (int r = 0; r < nr; r++) {
+          const cd h = P.HR[((size_t)i * n + j) * nr + r];
+          coef[(size_t)e * nr + r] = make_double2(h.real(), h.imag());
+          for (int x = 0; x < 3; x++) {
+            const cd d = 0.5 * (P.rR[(((size_t)x * n + i) * n + j) * nr + r] + P.rR[(((size_t)x * n + j) * n + i) * nr + r]);
+            coef[((size_t)(1 + x) * nt + e) * nr + r] = make_double2(d.real(), d.imag());
+          }
+        }
+      }
+    double2* dcoef = nullptr;
+    double *dk = nullptr, *dR = nullptr;
+    if ((rc = dalloc(c, &dcoef, coef.size())) || (rc = upload(c, dcoef, coef)) || (rc = dalloc(c, &dk, (size_t)3 * nk)) ||
+        (rc = dalloc(c, &dR, (size_t)3 * nr)))
+      return bail(rc);
+    if (cudaMemcpyAsync(dk, P.kpt.data(), sizeof(double) * 3 * nk, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+        cudaMemcpyAsync(dR, P.Rvec.data(), sizeof(double) * 3 * nr, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+      return bail(fail(EDUS_ECUDA, "velocity gauge: upload"));
+    VgArgs& v = c->vga;
+    v.n = n;
+    v.ntri = nt;
+    v.nk = nk;
+    v.nr = nr;
+    v.kpt = dk;
+    v.Rvec = dR;
+    v.coef = dcoef;
+    v.H = dH;
+    v.D = dD;
+    c->vg_t = P.t_start;
+    if ((rc = vg_tables(c, P.t_start))) return bail(rc);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "velocity gauge: initial tables"));
+  }
   // ---- Coulomb
   if (c->coul) {
     const int nc = P.ncut, n1 = tb.n1, n2 = tb.n2;
@@ -1485,6 +1579,14 @@ int edus_reset(edus_ctx* c) {
   c->nlog = 0;
   c->icont = -1;
   c->snap_t.clear();
+  if (c->vg) {
+    // the tables at k + A(t0) = k
+    c->vg_t = c->P.t_start;
+    c->vg_A[0] = c->vg_A[1] = c->vg_A[2] = 0.;
+    int rc = vg_tables(c, c->P.t_start);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));
+  }
   return 0;
 }
 
@@ -1605,7 +1707,7 @@ int edus_observables(edus_ctx* c, edus_obs* out) {
   edus_obs* tmp = c->d_obs_one;
   double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
   double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
-  CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, c->d_part,
+  CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->vg ? c->vga.H : (c->coul ? c->d_hr : nullptr), c->P.p.current, c->P.p.tabs, c->d_part,
                         c->d_done, scaleJ, scaleTA, rec, tmp, nullptr, nullptr, c->stream));
   CK(cudaMemcpyAsync(out, tmp, sizeof(edus_obs), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1790,7 +1892,7 @@ extern "C" int edus_observables_static(edus_ctx* c, edus_obs* out) {
   rec.dt = c->dt;
   double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
   double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
-  CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, base, done,
+  CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->vg ? c->vga.H : (c->coul ? c->d_hr : nullptr), c->P.p.current, c->P.p.tabs, base, done,
                         scaleJ, scaleTA, rec, rec_dev, nullptr, nullptr, c->stream));
   CK(cudaMemcpyAsync(out, rec_dev, sizeof(edus_obs), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));

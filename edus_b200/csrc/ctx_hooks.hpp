@@ -21,5 +21,15 @@ size_t ctx_device_bytes(const edus_ctx* c);
 int64_t ctx_footprint_estimate(const Problem& P);
 // CUDA-event time of the context's last run (ms).
 double ctx_last_ms(const edus_ctx* c);
+// Register a context whose whole run ctx_start_async launched (the server
+// creates and starts Coulomb contexts on a thread of its own) as a running
+// instance of the batch; the batch takes ownership. EDUS_ENOMEM when no slot
+// is free (the context is left to the caller then).
+int batch_adopt_context(edus_batch* b, edus_ctx* ctx, const Problem& P, int64_t tag, int32_t* slot);
+// Whether any class of the batch has tiles to advance, and a non-blocking
+// retirement of the Coulomb contexts whose run has ended (the server's loop
+// must not wait on one while requests arrive).
+bool batch_has_tiles(const edus_batch* b);
+int batch_poll_contexts(edus_batch* b);
 
 }  // namespace edus

@@ -45,6 +45,19 @@ cudaError_t launch_axpy(const double2* a, const double2* v, double dt, double2* 
 // Wannier basis from the inverse-transform rows tb.h.
 cudaError_t launch_pdiag(const DevTables& tb, const double2* rho, double2* pd, cudaStream_t s);
 cudaError_t launch_coulomb_xw(const DevTables& tb, const DevConsts* cst, const double2* pd, double2* xw, cudaStream_t s);
+// Velocity gauge: H(k + A), D(k + A) of a Wannier model at every k point
+// (vgauge.cu). coef: [4][ntri][nr] upper-triangle coefficients of H(R) and of
+// the symmetric dipoles (r_x(R) + r_x(R)^T) / 2; A in crystal coordinates.
+struct VgArgs {
+  int n = 0, ntri = 0, nk = 0, nr = 0;
+  const double* kpt = nullptr;    // [nk][3] crystal coordinates
+  const double* Rvec = nullptr;   // [nr][3]
+  const double2* coef = nullptr;  // [4][ntri][nr]
+  double A[3] = {0, 0, 0};
+  double2* H = nullptr;           // out [ntri][nk]
+  double2* D = nullptr;           // out [3][ntri][nk]
+};
+cudaError_t launch_vg_tables(const VgArgs& a, cudaStream_t s);
 int obs_parts(int nk);
 size_t obs_part_bytes();
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,

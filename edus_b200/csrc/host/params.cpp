@@ -644,6 +644,8 @@ extern "C" int edus_parse_input(const char* path, edus_params* out) {
             if (P.order > 5) P.order = 5;
           } else if (ieq(k, "Adams_Bashforth_RK4_startup")) {
             P.ab_rk4_startup = 1;
+          } else if (ieq(k, "velocity_gauge")) {
+            P.velocity_gauge = 1;
           } else if (ieq(k, "Gap_correction")) {
             P.gap_correction = to_d(t, 1);
           }

@@ -1,9 +1,14 @@
 // serve.cpp — request loop over one batch (C ABI edus_server_*).
 //
 // Threads: submitters (any caller), a pool of setup threads (build the host
-// problem of each request), and one loop thread that owns the batch: it admits
+// problem of each request), one loop thread that owns the batch: it admits
 // ready requests by HBM footprint, advances the batch one chunk at a time and
-// retires finished solves. Only the loop thread calls the batch API.
+// retires finished solves; and one starter thread for requests with the
+// Coulomb mean field, which run as contexts of their own: it creates the
+// context and launches its whole loop as one CUDA graph (capturing a
+// 20 000-step loop takes ~0.4 s of host time), after which the loop thread
+// adopts the running context into a batch slot. Only the loop thread calls
+// the batch API.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -19,6 +24,7 @@
 #include <thread>
 #include <vector>
 
+#include "ctx_hooks.hpp"
 #include "host/problem.hpp"
 
 namespace {
@@ -58,6 +64,20 @@ struct edus_server {
   int loop_error = 0;
   std::vector<std::thread> setup_threads;
   std::thread loop;
+  // Coulomb requests admitted by the loop thread and started by the starter
+  // thread; their footprint and slot stay reserved until adopted
+  struct Started {
+    int64_t id;
+    edus_ctx* ctx;
+    int rc;
+    std::string message;
+  };
+  std::deque<int64_t> start_q;
+  std::vector<Started> started;
+  std::condition_variable cv_start;
+  std::thread starter;
+  int64_t reserved_bytes = 0;
+  int reserved_slots = 0;
 
   double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
@@ -115,6 +135,73 @@ void setup_worker(edus_server* s) {
   }
 }
 
+void starter_main(edus_server* s) {
+  cudaSetDevice(s->opt.batch.device);
+  for (;;) {
+    int64_t id;
+    Request* r;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_start.wait(lk, [&] { return s->stop || !s->start_q.empty(); });
+      if (s->stop) return;
+      id = s->start_q.front();
+      s->start_q.pop_front();
+      r = s->reqs[id].get();
+    }
+    edus_options o;
+    edus_options_default(&o);
+    o.device = s->opt.batch.device;
+    o.use_graphs = 1;
+    edus_ctx* ctx = nullptr;
+    int rc = edus_create(r->pb.get(), &o, &ctx);
+    if (!rc) rc = edus::ctx_start_async(ctx);
+    std::string msg = rc ? edus_last_error() : "";
+    if (rc && ctx) {
+      edus_destroy(ctx);
+      ctx = nullptr;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->started.push_back({id, ctx, rc, msg});
+    s->cv_loop.notify_all();
+  }
+}
+
+// Started Coulomb contexts join the batch (loop thread).
+void adopt(edus_server* s) {
+  std::vector<edus_server::Started> done;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    done.swap(s->started);
+  }
+  for (auto& st : done) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    Request* r = s->reqs[st.id].get();
+    s->reserved_bytes -= r->footprint;
+    s->reserved_slots--;
+    int32_t slot = -1;
+    int rc = st.rc;
+    if (!rc) {
+      rc = edus::batch_adopt_context(s->batch, st.ctx, r->pb->P, st.id, &slot);
+      if (rc) {
+        st.message = edus_last_error();
+        edus_destroy(st.ctx);
+      }
+    }
+    if (rc) {
+      r->error = rc;
+      r->message = st.message;
+      r->pb.reset();
+      s->bytes_in_use -= r->footprint;
+      finish(s, *r, EDUS_REQ_FAILED);
+      continue;
+    }
+    r->slot = slot;
+    r->pb.reset();
+    s->running[slot] = st.id;
+    s->peak_active = std::max(s->peak_active, (int)s->running.size());
+  }
+}
+
 // Admit ready requests in submission order while they fit. A request that
 // does not fit may be passed by younger ones until it has waited max_bypass_s.
 void admit(edus_server* s, edus_batch_stats& st) {
@@ -124,6 +211,12 @@ void admit(edus_server* s, edus_batch_stats& st) {
     order = s->ready;
   }
   const double t = s->now();
+  {
+    // Coulomb requests being started hold their memory and slot already
+    std::lock_guard<std::mutex> lk(s->mu);
+    st.bytes_used += s->reserved_bytes;
+    st.free_slots -= s->reserved_slots;
+  }
   for (int64_t id : order) {
     Request* r;
     {
@@ -142,6 +235,22 @@ void admit(edus_server* s, edus_batch_stats& st) {
     const bool fits = st.free_slots > 0 && st.bytes_used + r->footprint <= st.bytes_budget;
     if (!fits) {
       if (t - r->t_ready > s->opt.max_bypass_s) break;  // hold the line for the oldest
+      continue;
+    }
+    if (r->pb->P.p.coulomb) {
+      // started on the starter thread, adopted by the loop when it runs
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->ready.erase(std::find(s->ready.begin(), s->ready.end(), id));
+      r->status = EDUS_REQ_RUNNING;
+      r->t_admit = s->now();
+      s->reserved_bytes += r->footprint;
+      s->reserved_slots++;
+      s->start_q.push_back(id);
+      st.free_slots--;
+      st.bytes_used += r->footprint;
+      s->bytes_in_use += r->footprint;
+      s->peak_bytes = std::max(s->peak_bytes, s->bytes_in_use);
+      s->cv_start.notify_one();
       continue;
     }
     int32_t slot = -1;
@@ -173,8 +282,8 @@ void admit(edus_server* s, edus_batch_stats& st) {
     s->running[slot] = id;
     st.free_slots--;
     st.bytes_used += r->footprint;
-    s->bytes_in_use = st.bytes_used;
-    s->peak_bytes = std::max(s->peak_bytes, st.bytes_used);
+    s->bytes_in_use += r->footprint;
+    s->peak_bytes = std::max(s->peak_bytes, s->bytes_in_use);
     s->peak_active = std::max(s->peak_active, (int)s->running.size());
   }
 }
@@ -242,11 +351,13 @@ void loop_main(edus_server* s) {
   for (;;) {
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_loop.wait_for(lk, std::chrono::milliseconds(2),
-                          [&] { return s->stop || !s->ready.empty() || !s->running.empty(); });
+      s->cv_loop.wait_for(lk, std::chrono::milliseconds(2), [&] {
+        return s->stop || !s->ready.empty() || !s->running.empty() || !s->started.empty();
+      });
       if (s->stop) return;
-      if (s->ready.empty() && s->running.empty()) continue;
+      if (s->ready.empty() && s->running.empty() && s->started.empty()) continue;
     }
+    adopt(s);
     edus_batch_stats st;
     int rc = edus_batch_stats_get(s->batch, &st);
     if (!rc) admit(s, st);
@@ -255,7 +366,10 @@ void loop_main(edus_server* s) {
       std::lock_guard<std::mutex> lk(s->mu);
       any = !s->running.empty();
     }
-    if (!rc && any) rc = edus_batch_advance(s->batch, s->opt.batch.chunk_steps);
+    // with tiles, one chunk; with Coulomb contexts only, a poll (no wait)
+    if (!rc && any)
+      rc = edus::batch_has_tiles(s->batch) ? edus_batch_advance(s->batch, s->opt.batch.chunk_steps)
+                                           : edus::batch_poll_contexts(s->batch);
     if (!rc && any) rc = retire(s);
     if (rc) {
       // a failed chunk leaves no trustworthy state: fail what is running and stop
@@ -270,6 +384,7 @@ void loop_main(edus_server* s) {
       s->running.clear();
       s->stop = true;
       s->cv_setup.notify_all();
+      s->cv_start.notify_all();
       return;
     }
   }
@@ -302,6 +417,7 @@ int edus_server_create(const edus_server_options* o, edus_server** out) {
     return rc;
   }
   for (int i = 0; i < o->setup_threads; i++) s->setup_threads.emplace_back(setup_worker, s);
+  s->starter = std::thread(starter_main, s);
   s->loop = std::thread(loop_main, s);
   *out = s;
   return 0;
@@ -435,9 +551,13 @@ void edus_server_destroy(edus_server* s) {
   }
   s->cv_setup.notify_all();
   s->cv_loop.notify_all();
+  s->cv_start.notify_all();
   if (s->loop.joinable()) s->loop.join();
+  if (s->starter.joinable()) s->starter.join();
   for (auto& t : s->setup_threads)
     if (t.joinable()) t.join();
+  for (auto& st : s->started)
+    if (st.ctx) edus_destroy(st.ctx);
   edus_batch_destroy(s->batch);
   delete s;
 }

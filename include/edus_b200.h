@@ -131,6 +131,11 @@ typedef struct {
   int32_t kpt_read;
   int64_t kpt_offset;            /* byte offset of the first listed k point in input_path */
   char input_path[EDUS_STRLEN];
+  /* extension (tdse{ velocity_gauge }): Wannier models integrated in the
+   * frame that moves with the vector potential, rho'(k) = rho(k + A(t)), with
+   * H and D evaluated at k + A(t) every stage and no k-gradient term; the
+   * reference integrates the length gauge only */
+  int32_t velocity_gauge;
 } edus_params;
 
 /* Observables at one output instant (headers/Observables_MPI.h). */

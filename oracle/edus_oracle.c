@@ -104,6 +104,10 @@ struct orc {
   double EF[2][3];
   int e_non0;
   double n_cond, P_cond_max, P_cond_max_loc, P_min;
+  /* velocity gauge (an option the reference does not have): vector potential
+   * A(t) = -int_t0^t E_pump, Cartesian, tracked up to time A_t */
+  int vg;
+  double A_t, A_cart[3];
 };
 
 #define IDX3(k, i, j, n) (((size_t)(k) * (n) + (i)) * (n) + (j))
@@ -1161,6 +1165,73 @@ static int tabulate(orc* o) {
   return 0;
 }
 
+/* ------------------------------------------------------------ velocity gauge
+ * An option the reference does not have (its vector potential, Laser::A_crys
+ * in headers/Laser.h:191-213, is only called from dead code). The length-gauge
+ * equation drho(k)/dt = -i[H(k) + E.D(k), rho(k)] + E.grad_k rho(k) becomes,
+ * for rho'(k, t) = rho(k + A(t), t) with A = -int E_pump dt,
+ *   drho'(k)/dt = -i[H(k + A) + E.D(k + A), rho'(k)]
+ * (the gradient term cancels against dA/dt = -E). Wannier models only: H and D
+ * are the reference's Fourier sums (headers/Wannier.h:278-304,336-471,
+ * 489-492, 577-578; Source_Main/save_HUD.cpp:47-51) at k + A. Observables at
+ * k + A: populations in the eigenbasis of H(k + A), J1 from the reference's
+ * stencil gradient of H(k + A) on the grid, J2 with H and D at k + A. */
+
+static void field_at(const orc* o, double t, double EF[2][3]);
+
+/* A(t) by 4-point Gauss-Legendre panels of at most 0.5 a.u. over [A_t, t]
+ * (one panel per RK4 half step; the field period is hundreds of a.u.);
+ * returns A in crystal coordinates */
+static void vg_A(orc* o, double t, double Acrys[3]) {
+  static const double gx[4] = {-0.8611363115940526, -0.3399810435848563, 0.3399810435848563, 0.8611363115940526};
+  static const double gw[4] = {0.3478548451374538, 0.6521451548625461, 0.6521451548625461, 0.3478548451374538};
+  if (t < o->A_t) {
+    o->A_t = -0.21 / TIME_AU_FS;
+    o->A_cart[0] = o->A_cart[1] = o->A_cart[2] = 0.;
+  }
+  const int panels = (int)ceil((t - o->A_t) / 0.5);
+  const double t0 = o->A_t;
+  for (int p = 0; p < panels; p++) {
+    const double a = t0 + (t - t0) * p / panels, b = t0 + (t - t0) * (p + 1) / panels;
+    const double h = 0.5 * (b - a), m = 0.5 * (a + b);
+    for (int q = 0; q < 4; q++) {
+      double EF[2][3];
+      field_at(o, m + h * gx[q], EF);
+      for (int x = 0; x < 3; x++) o->A_cart[x] -= h * gw[q] * EF[0][x];
+    }
+  }
+  o->A_t = t;
+  cart_to_crys(o, o->A_cart, Acrys);
+}
+
+/* H and D of every k point at k + A(t) into o->H, o->D */
+static void vg_tables(orc* o, double t) {
+  int n = o->ncv;
+  double Ac[3];
+  vg_A(o, t, Ac);
+#pragma omp parallel for schedule(static)
+  for (int ik = 0; ik < o->nk; ik++) {
+    double k[3];
+    for (int l = 0; l < 3; l++) k[l] = o->kpt[ik * 3 + l] + Ac[l];
+    cplx Dk[EDUS_MAX_BANDS * EDUS_MAX_BANDS * 3];
+    for (int ic = 0; ic < n; ic++)
+      for (int jc = 0; jc < n; jc++) {
+        cplx h = wannier_sum(o, o->HR, ic, jc, k);
+        if (ic == jc) h = creal(h);
+        o->H[IDX3(ik, ic, jc, n)] = h;
+        Dk[(ic * n + jc) * 3 + 0] = wannier_sum(o, o->xR, ic, jc, k);
+        Dk[(ic * n + jc) * 3 + 1] = wannier_sum(o, o->yR, ic, jc, k);
+        Dk[(ic * n + jc) * 3 + 2] = wannier_sum(o, o->zR, ic, jc, k);
+        if (ic == jc)
+          for (int x = 0; x < 3; x++) Dk[(ic * n + jc) * 3 + x] = creal(Dk[(ic * n + jc) * 3 + x]);
+      }
+    for (int ic = 0; ic < n; ic++)
+      for (int jc = 0; jc < n; jc++)
+        for (int x = 0; x < 3; x++)
+          o->D[IDX4(ik, ic, jc, x, n)] = 0.5 * (Dk[(ic * n + jc) * 3 + x] + Dk[(jc * n + ic) * 3 + x]);
+  }
+}
+
 /* Source_Main/save_HUD.cpp:96-137 (GradientEnergy of H) */
 static void gradient_energy(orc* o, const cplx* Hs) {
   int n = o->ncv;
@@ -1695,6 +1766,7 @@ static void observables(orc* o, const cplx* P, edus_obs* ob) {
   cplx* tap = calloc((size_t)nth * 3, sizeof(cplx));
   for (int t = 0; t < nth; t++) pmin[t] = 1.0;
   if (o->p.coulomb && o->p.current) gradient_energy_renorm(o, o->Hr);
+  if (o->vg && o->p.current) gradient_energy_renorm(o, o->H);
   const cplx* Hs = o->p.coulomb ? o->Hr : o->H;
 #pragma omp parallel for schedule(static)
   for (int t = 0; t < nth; t++) {
@@ -1705,10 +1777,10 @@ static void observables(orc* o, const cplx* P, edus_obs* ob) {
     for (int ik = beg; ik < end; ik++) {
       const cplx* Pk = &P[IDX3(ik, 0, 0, n)];
       cplx Uex[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
-      if (o->p.coulomb) {
+      if (o->p.coulomb || o->vg) {
         cplx A[EDUS_MAX_BANDS * EDUS_MAX_BANDS], Z[EDUS_MAX_BANDS * EDUS_MAX_BANDS];
         double ev[EDUS_MAX_BANDS];
-        memcpy(A, &o->Hr[(size_t)ik * n * n], sizeof(cplx) * n * n);
+        memcpy(A, o->vg ? &o->H[(size_t)ik * n * n] : &o->Hr[(size_t)ik * n * n], sizeof(cplx) * n * n);
         eig_herm(n, A, ev, Z);
         for (int ic = 0; ic < n; ic++)
           for (int jc = 0; jc < n; jc++) Uex[ic * n + jc] = conj(Z[jc * n + ic]);
@@ -1809,20 +1881,25 @@ static void step_rk4_ring(orc* o, int store_ring) {
     for (int ik = 0; ik < o->nk; ik++)
       for (int ic = 0; ic < n; ic++) o->Psave_diag[(size_t)ik * n + ic] = o->P0[IDX3(ik, ic, ic, n)];
   double t = o->time_loop;
+  /* velocity gauge: H, D at k + A(stage time), no k-gradient term */
+  const int grad = o->vg ? 0 : o->e_non0;
   field_at(o, t, o->EF);
-  rhs(o, o->P0, o->Pv, o->EF, wx2, o->e_non0);
+  if (o->vg) vg_tables(o, t);
+  rhs(o, o->P0, o->Pv, o->EF, wx2, grad);
   if (store_ring) memcpy(o->ring + (size_t)o->nk * n * n * o->ring_idx[0], o->Pv, sizeof(cplx) * (size_t)o->nk * n * n);
   rk_ad(o, o->P0, o->P1, o->Pv, dt6);
   rk_ad(o, o->P0, o->P2, o->Pv, dt2);
   field_at(o, t + dt2, o->EF);
-  rhs(o, o->P2, o->Pv, o->EF, wx2, o->e_non0);
+  if (o->vg) vg_tables(o, t + dt2);
+  rhs(o, o->P2, o->Pv, o->EF, wx2, grad);
   rk_ac(o, o->P1, o->Pv, dt3);
   rk_ad(o, o->P0, o->P2, o->Pv, dt2);
-  rhs(o, o->P2, o->Pv, o->EF, wx2, o->e_non0);
+  rhs(o, o->P2, o->Pv, o->EF, wx2, grad);
   rk_ac(o, o->P1, o->Pv, dt3);
   rk_ad(o, o->P0, o->P2, o->Pv, dt);
   field_at(o, t + dt, o->EF);
-  rhs(o, o->P2, o->Pv, o->EF, wx2, o->e_non0);
+  if (o->vg) vg_tables(o, t + dt);
+  rhs(o, o->P2, o->Pv, o->EF, wx2, grad);
   rk_ad(o, o->P1, o->P0, o->Pv, dt6);
   if (o->p.dynamical_dt)
     for (size_t e = 0; e < (size_t)o->nk * n; e++) o->Pprev_diag[e] = o->Psave_diag[e];
@@ -2068,6 +2145,15 @@ int orc_create(const edus_params* p, const char* workdir, orc** out) {
   o->itfi = (int)((p->t_fin - o->time_loop) / p->dt);
   o->e_non0 = 1;
   o->n_cond = p->dynamical_dt ? pow(10, -16) : 0;
+  if (p->velocity_gauge) {
+    if (p->mode != EDUS_MODE_WANNIER || p->solver != EDUS_SOLVER_RK4 || p->dynamical_dt || p->coulomb ||
+        p->conduction_shift > 1e-16 || o->n_diss > 0) {
+      orc_free(o);
+      return EDUS_EUNSUPPORTED;
+    }
+    o->vg = 1;
+    o->A_t = o->time_loop;
+  }
   o->P_cond_max = 0;
   if (p->coulomb) {
     o->ncut = p->ncut;

@@ -130,7 +130,8 @@ def test_mixed_batch_runs_small_band_classes_in_fp64(workdir):
     s = b.add(pb)
     drain(b, [s], 8)
     assert np.abs(b.get_state(s) - rho).max() < 1e-13
-    assert rel(J1(b.obs(s)), J1(log)) < 1e-11
+    # a 0.3 fs run: J1 (~4e-8) is a k sum at its rounding floor, summed in another order
+    assert rel(J1(b.obs(s)), J1(log)) < 5e-11
 
 
 def test_admission_by_hbm_budget(workdir):

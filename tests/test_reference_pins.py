@@ -78,3 +78,39 @@ def test_shim_build_recipe_names_the_reference_sources():
     assert "oracle/_ref/" in ign
     for f in ("mpi.h", "armadillo"):
         assert os.path.exists(os.path.join(ROOT, "oracle", "ref_shim", f))
+
+
+def _vg_case(workdir, n):
+    import os
+
+    from edus_b200 import workloads as W
+
+    os.makedirs(workdir, exist_ok=True)
+    W.write_wannier_tb(os.path.join(workdir, "W2_tb.dat"), nw=2, nside=3)
+    return W.wannier(workdir, nw=2, nside=3, name="W2", n=n, t_fin_fs=4.0, it_res=5, field=0.2, write_model=False)
+
+
+def test_velocity_gauge_keyword_is_parsed(workdir):
+    path = _vg_case(workdir, 8)
+    txt = open(path).read().replace("Wannier\n", "Wannier\nvelocity_gauge\n")
+    open(path, "w").write(txt)
+    assert E.parse_input(path).velocity_gauge == 1
+
+
+def test_oracle_velocity_gauge_converges_to_length_gauge(workdir):
+    """The velocity-gauge restatement (rho'(k) = rho(k + A), H and D at k + A,
+    no k-gradient term) and the reference's length gauge describe the same
+    dynamics: their J1 differ by the length gauge's finite-difference
+    k-gradient error, which falls by more than 8x per grid doubling on a
+    nearest-neighbour model (14.5x and 15.5x measured, 32 -> 64 -> 128)."""
+    diffs = []
+    for n in (32, 64):
+        d = f"{workdir}/n{n}"
+        p = E.parse_input(_vg_case(d, n))
+        lg = Oracle(p, d).run()
+        p.velocity_gauge = 1
+        o = Oracle(p, d)
+        vg = o.run()
+        assert max(abs(x["trace_dev"]) for x in vg) < 1e-12
+        diffs.append(RF.rel_l2([x["J1"] for x in vg], [x["J1"] for x in lg]))
+    assert diffs[0] < 2e-2 and diffs[1] < diffs[0] / 8, diffs
