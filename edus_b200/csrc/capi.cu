@@ -24,6 +24,7 @@
 
 #include "ctx_hooks.hpp"
 #include "cuda/kernels.hpp"
+#include "cuda/tc_contract.hpp"
 #include "host/problem.hpp"
 
 namespace edus {
@@ -137,6 +138,10 @@ struct edus_ctx {
   // last stage; A(t) = -int E_pump dt tracked on the host up to time vg_t
   bool vg = false;
   VgArgs vga{};
+  // velocity gauge with the stage contraction on the tensor cores (precision
+  // EDUS_PREC_MIXED): exact-slice GEMM, FP64 planes
+  bool vg_tc = false;
+  batch::TcVgArgs vgt{};
   double vg_t = 0, vg_A[3] = {0, 0, 0};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0;
@@ -347,12 +352,19 @@ void vg_advance_A(edus_ctx* c, double t) {
   c->vg_t = t;
 }
 
-// H, D at k + A(t) into the model tables
+// H, D at k + A(t) into the model tables (FP64 sums on CUDA cores, or the
+// exact-slice GEMM on the tensor cores)
 int vg_tables(edus_ctx* c, double t) {
   vg_advance_A(c, t);
   for (int i = 0; i < 3; i++) c->vga.A[i] = c->P.MI[i][0] * c->vg_A[0] + c->P.MI[i][1] * c->vg_A[1] + c->P.MI[i][2] * c->vg_A[2];
-  CK(launch_vg_tables(c->vga, c->stream));
-  c->launches++;
+  if (c->vg_tc) {
+    for (int i = 0; i < 3; i++) c->vgt.A[i] = c->vga.A[i];
+    CK(batch::tc_vg_stage(c->vgt, c->stream));
+    c->launches += 3;
+  } else {
+    CK(launch_vg_tables(c->vga, c->stream));
+    c->launches++;
+  }
   return 0;
 }
 
@@ -1393,6 +1405,43 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
     v.coef = dcoef;
     v.H = dH;
     v.D = dD;
+    const int prec = o.precision >= 0 ? o.precision : P.p.precision;
+    c->vg_tc = prec == EDUS_PREC_MIXED && batch::tc_seg_k(nr) <= 1024;
+    if (c->vg_tc) {
+      // power-of-two scale of each GEMM column from max_R |c(R)| (bounds |Re|, |Im| of
+      // e^{2 pi i A.R} c(R) for every A): every sliced value lies in [-1/2, 1/2]
+      const int ncols = 8 * nt, kpad = batch::tc_pad_k(nr);
+      std::vector<double> cs(ncols);
+      for (int ce = 0; ce < 4 * nt; ce++) {
+        double amax = 0.;
+        for (int r = 0; r < nr; r++) amax = std::max(amax, std::hypot(coef[(size_t)ce * nr + r].x, coef[(size_t)ce * nr + r].y));
+        cs[2 * ce] = cs[2 * ce + 1] = amax > 0. ? std::ldexp(1.0, std::ilogb(amax) + 2) : 1.0;
+      }
+      double* dcs = nullptr;
+      uint16_t *dA = nullptr, *dB = nullptr;
+      double* dC = nullptr;
+      if ((rc = dalloc(c, &dcs, (size_t)ncols)) || (rc = dalloc(c, &dA, (size_t)nk * kpad)) ||
+          (rc = dalloc(c, &dB, (size_t)ncols * kpad)) || (rc = dalloc(c, &dC, (size_t)nk * ncols)))
+        return bail(rc);
+      if (cudaMemcpyAsync(dcs, cs.data(), sizeof(double) * ncols, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        return bail(fail(EDUS_ECUDA, "velocity gauge: upload"));
+      batch::TcVgArgs& g = c->vgt;
+      g.n = n;
+      g.ntri = nt;
+      g.nk = nk;
+      g.nr = nr;
+      g.kpt = dk;
+      g.Rvec = dR;
+      g.coef = dcoef;
+      g.colscale = dcs;
+      g.Aw = dA;
+      g.Bw = dB;
+      g.Cw = dC;
+      g.H = dH;
+      g.D = dD;
+      g.err = c->d_err;
+      if (batch::tc_vg_prepare(g, c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "velocity gauge: phase slices"));
+    }
     c->vg_t = P.t_start;
     if ((rc = vg_tables(c, P.t_start))) return bail(rc);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "velocity gauge: initial tables"));

@@ -261,6 +261,46 @@ __global__ void k_diag64(const double* __restrict__ kpt, const double* __restric
   }
 }
 
+// Velocity gauge: coefficient slices of c_A(R) = e^{2 pi i A.R} c(R), one thread per
+// (column, K entry); column 2 ce + part holds [Re c_A ; -Im c_A] (part 0) or
+// [Im c_A ; Re c_A] (part 1), pre-multiplied by 2 scale as the host build's slices
+__global__ void k_vg_bslices(const double2* __restrict__ coef, const double* __restrict__ Rvec, const double* __restrict__ colscale,
+                             double A0, double A1, double A2, int ntri, int nr, int kseg, int kpad, uint16_t* __restrict__ B) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;  // K entry
+  const int col = blockIdx.y;                          // 2 (comp * ntri + e) + part
+  const int K = 2 * nr;
+  if (q >= K) return;
+  const int ce = col / 2, part = col % 2;
+  const int r = q < nr ? q : q - nr;
+  const double* R = Rvec + (size_t)r * 3;
+  double s, c;
+  sincospi(2.0 * (A0 * R[0] + A1 * R[1] + A2 * R[2]), &s, &c);
+  const double2 cf = coef[(size_t)ce * nr + r];
+  const double re = c * cf.x - s * cf.y, im = c * cf.y + s * cf.x;
+  const double v = part == 0 ? (q < nr ? re : -im) : (q < nr ? im : re);
+  const double scale = colscale[col];
+  uint16_t* row = B + (size_t)col * kpad;
+#pragma unroll
+  for (int p = 0; p < kTcPairs; p++) row[(size_t)p * kseg + q] = tc_bf16(2.0 * scale * tc_slice(v / scale, tc_pair_b(p)));
+}
+
+// C[k][col] -> FP64 planes H [ntri][nk], D [3][ntri][nk]; diagonal imaginary parts zero
+__global__ void k_scatter64(const double* __restrict__ C, int nk, int n, int ntri, int ncols, double2* __restrict__ H,
+                            double2* __restrict__ D) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ce = blockIdx.y;
+  if (k >= nk) return;
+  const int comp = ce / ntri, e = ce - comp * ntri;
+  double2 v = make_double2(C[(size_t)k * ncols + 2 * ce], C[(size_t)k * ncols + 2 * ce + 1]);
+  bool diag = false;
+  for (int i = 0; i < n; i++) diag = diag || (e == i * n - (i * (i - 1)) / 2);
+  if (diag) v.y = 0.;
+  if (comp == 0)
+    H[(size_t)e * nk + k] = v;
+  else
+    D[((size_t)(comp - 1) * ntri + e) * nk + k] = v;
+}
+
 }  // namespace
 
 size_t tc_gemm_smem() { return 2 * sizeof(uint16_t) * (TM + TN) * TK + 1024; }
@@ -283,6 +323,30 @@ cudaError_t tc_contract(const TcArgs& a, cudaStream_t s) {
   k_scatter<<<dim3((a.nk + 255) / 256, 4 * a.ntri), 256, 0, s>>>(a.Cw, a.nk, a.n, a.ntri, ncols, a.H32, a.D32);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_diag64<<<dim3((a.nk + 127) / 128, a.n), 128, 0, s>>>(a.kpt, a.Rvec, a.hdiagR, a.H32, a.nk, a.n, a.nr, a.Hdiag, a.Hused);
+  return cudaGetLastError();
+}
+
+cudaError_t tc_vg_prepare(const TcVgArgs& a, cudaStream_t s) {
+  const int kpad = tc_pad_k(a.nr);
+  k_phase_split<<<a.nk, 256, 0, s>>>(a.kpt, a.Rvec, a.nk, a.nr, tc_seg_k(a.nr), kpad, a.Aw);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(a.Bw, 0, sizeof(uint16_t) * (size_t)8 * a.ntri * kpad, s)) != cudaSuccess) return e;
+  const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
+  return cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t tc_vg_stage(const TcVgArgs& a, cudaStream_t s) {
+  const int kpad = tc_pad_k(a.nr), kseg = tc_seg_k(a.nr), ncols = 8 * a.ntri;
+  k_vg_bslices<<<dim3((2 * a.nr + 127) / 128, ncols), 128, 0, s>>>(a.coef, a.Rvec, a.colscale, a.A[0], a.A[1], a.A[2], a.ntri,
+                                                                   a.nr, kseg, kpad, a.Bw);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
+  dim3 grid((a.nk + TM - 1) / TM, (ncols + TN - 1) / TN);
+  k_tc_gemm<<<grid, kThreads, smem, s>>>(a.Aw, a.Bw, a.Cw, a.nk, ncols, kpad, kseg, a.err);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  k_scatter64<<<dim3((a.nk + 255) / 256, 4 * a.ntri), 256, 0, s>>>(a.Cw, a.nk, a.n, a.ntri, ncols, a.H, a.D);
   return cudaGetLastError();
 }
 

@@ -66,5 +66,28 @@ int tc_seg_k(int nr);
 int tc_pad_k(int nr);
 cudaError_t tc_contract(const TcArgs& a, cudaStream_t s);
 
+// Velocity gauge on the tensor cores: H(k + A), D(k + A) of every k point for
+// every RK4 stage as the exact-slice GEMM above. The phase slices of the grid
+// (A' = [cos | sin](2 pi k.R) / 2) are cut once; each stage cuts the
+// coefficient slices of c_A(R) = e^{2 pi i A.R} c(R) on the device (column
+// scales fixed from |c(R)|, which bounds |Re c_A| and |Im c_A| for every A),
+// runs the GEMM and scatters FP64 planes (diagonal imaginary parts zero).
+struct TcVgArgs {
+  int n = 0, ntri = 0, nk = 0, nr = 0;
+  const double* kpt = nullptr;       // [nk][3]
+  const double* Rvec = nullptr;      // [nr][3]
+  const double2* coef = nullptr;     // [4][ntri][nr]: H(R), (r_x(R) + r_x(R)^T) / 2 upper entries
+  const double* colscale = nullptr;  // [8 ntri] power-of-two scale of each GEMM column
+  double A[3] = {0, 0, 0};           // crystal coordinates
+  uint16_t* Aw = nullptr;            // [nk][Kp] phase slices (tc_vg_prepare)
+  uint16_t* Bw = nullptr;            // [8 ntri][Kp] coefficient slices (zero padded once)
+  double* Cw = nullptr;              // [nk][8 ntri]
+  double2* H = nullptr;              // out [ntri][nk]
+  double2* D = nullptr;              // out [3][ntri][nk]
+  int* err = nullptr;                // device error word (bounded waits)
+};
+cudaError_t tc_vg_prepare(const TcVgArgs& a, cudaStream_t s);
+cudaError_t tc_vg_stage(const TcVgArgs& a, cudaStream_t s);
+
 }  // namespace batch
 }  // namespace edus

@@ -324,3 +324,27 @@ def test_velocity_gauge_matches_oracle(workdir, nw, nside, n):
     ctx.reset()
     ctx.run()
     assert np.array_equal(ctx.get_state(), rho)
+
+
+@pytest.mark.parametrize("nw,nside,n", [(8, 11, 16), (16, 13, 10)])
+def test_velocity_gauge_tensor_core_contraction(workdir, nw, nside, n):
+    """Velocity gauge with the stage contraction on the tensor cores (context
+    precision EDUS_PREC_MIXED: exact 8-bit BF16 slices, FP32 sums exact per
+    segment, FP64 across segments; FP64 state and commutator) against the FP64
+    oracle: J1 within the mixed-precision bar 1e-6, rho and populations within
+    1e-8."""
+    name = f"W{nw}"
+    W.write_wannier_tb(f"{workdir}/{name}_tb.dat", nw=nw, nside=nside)
+    path = W.wannier(workdir, nw=nw, nside=nside, name=name, n=n, t_fin_fs=1.5, it_res=5, field=0.5, write_model=False)
+    txt = open(path).read().replace("Wannier\n", "Wannier\nvelocity_gauge\n")
+    open(path, "w").write(txt)
+    p = E.parse_input(path)
+    ctx = E.Context(E.Problem(p, workdir), precision=abi.EDUS_PREC_MIXED)
+    ctx.run()
+    g, rho = ctx.obs(), ctx.get_state()
+    o = Oracle(p, workdir)
+    lo = o.run()
+    drho = float(np.abs(rho - o.get("P0")).max())
+    j1 = RF.rel_l2([x["J1"] for x in g], [x["J1"] for x in lo])
+    dpop = float(np.abs(np.array([x["pop"] for x in g]) - np.array([x["pop"] for x in lo])).max())
+    assert j1 < 1e-6 and drho < 1e-8 and dpop < 1e-8, (j1, drho, dpop)
