@@ -24,6 +24,7 @@
 // alternate between two TMEM accumulators (128 lanes x 32 FP32 columns each);
 // a finished segment is read back with tcgen05.ld.32x32b into FP64 registers
 // while the next one accumulates. All waits are bounded.
+#include <cuda.h>
 #include <stdint.h>
 
 #include "batch.cuh"
@@ -261,6 +262,155 @@ __global__ void k_diag64(const double* __restrict__ kpt, const double* __restric
   }
 }
 
+// ------------------------------------------------------------------ TMA-staged GEMM
+// The same exact-slice GEMM with its operand tiles moved by TMA
+// (cp.async.bulk.tensor.2d, no multicast; both tensor maps cover this GPU's
+// own buffers): one box of 8 BF16 (16 bytes) x rows per 16-byte K chunk, which
+// lands as rows x 16 bytes, the canonical no-swizzle K-major core matrices.
+// N tile 64, four shared-memory stages; thread 0 issues the loads of slice
+// s + 3 and the MMAs of slice s, so three slices are in flight while the
+// tensor core works. Every wait is bounded; on a timeout the block waits
+// (bounded) for its issued loads and MMAs, releases TMEM and ends.
+constexpr int TN2 = 64, kStages2 = 4;
+constexpr uint32_t kTmemCols2 = 64;
+constexpr uint32_t kIdesc2 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN2 >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+               "l"(map), "r"(x), "r"(y), "r"(bar)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 1) k_tc_gemm_tma(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                                                             double* __restrict__ C, int M, int N, int Kp, int kseg, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  constexpr uint32_t kStageA = TM * TK * 2, kStageB = TN2 * TK * 2, kStage = kStageA + kStageB;
+  __shared__ unsigned long long full[kStages2], mmab[kStages2];
+  __shared__ uint32_t tmem_base;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN2;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)), "r"(2 * kTmemCols2));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int b = 0; b < kStages2; b++) {
+      mbar_init(&full[b], 1);
+      mbar_init(&mmab[b], 1);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base;
+  const uint32_t base = (smem_u32(smem) + 1023u) & ~1023u;
+  const int S = Kp / TK, SEG = kseg / TK;
+  double acc[TN2];
+#pragma unroll
+  for (int c = 0; c < TN2; c++) acc[c] = 0.;
+
+  // slice s into stage b: 8 boxes of A (8 x 128) and 8 of B (8 x 64), chunk c at c * rows * 16
+  auto issue_load = [&](int s, int b) {
+    const uint32_t sa = base + (uint32_t)b * kStage, sb = sa + kStageA;
+    mbar_expect_tx(&full[b], kStage);
+    const int k0 = s * TK;
+#pragma unroll
+    for (int c = 0; c < TK / 8; c++) {
+      tma_load_2d(sa + (uint32_t)(c * TM * 16), &mapA, k0 + 8 * c, m0, smem_u32(&full[b]));
+      tma_load_2d(sb + (uint32_t)(c * TN2 * 16), &mapB, k0 + 8 * c, n0, smem_u32(&full[b]));
+    }
+  };
+  auto readout = [&](int p) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+    for (int c0 = 0; c0 < TN2; c0 += 8) {
+      uint32_t v[8];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)((p & 1) * kTmemCols2 + c0);
+      asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                   : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                   : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int u = 0; u < 8; u++) acc[c0 + u] += (double)__uint_as_float(v[u]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+  };
+  // completion number (s / kStages2) of a stage's barrier belongs to slice s
+  auto mma_done = [&](int s) { return mbar_wait(&mmab[s % kStages2], (uint32_t)((s / kStages2) & 1), err); };
+  auto loaded = [&](int s) { return mbar_wait(&full[s % kStages2], (uint32_t)((s / kStages2) & 1), err); };
+
+  bool ok = true;
+  int issued = -1, loads = 0;  // last slice whose MMAs were committed; slices whose loads were issued
+  if (tid == 0)
+    for (; loads < kStages2 - 1 && loads < S; loads++) issue_load(loads, loads);
+  for (int s = 0; s < S; s++) {
+    if (tid == 0) {
+      if (ok) ok = loaded(s);
+      if (ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t sa = base + (uint32_t)(s % kStages2) * kStage, sb = sa + kStageA;
+        const uint32_t dtm = tmem + (uint32_t)(((s / SEG) & 1) * kTmemCols2);
+#pragma unroll
+        for (int j = 0; j < TK / 16; j++) {
+          const uint64_t da = smem_desc(sa + (uint32_t)(2 * j * TM * 16), TM * 16, 128);
+          const uint64_t db = smem_desc(sb + (uint32_t)(2 * j * TN2 * 16), TN2 * 16, 128);
+          const uint32_t accum = (j > 0 || s % SEG != 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtm),
+              "l"(da), "l"(db), "r"(kIdesc2), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&mmab[s % kStages2]))
+                     : "memory");
+        issued = s;
+      }
+      // refill: slice s + 3 goes to the stage slice s - 1 used, once its MMAs are done
+      // (slice s's MMAs are queued behind them meanwhile)
+      if (ok && loads < S) {
+        if (loads >= kStages2) ok = mma_done(loads - kStages2);
+        if (ok) {
+          issue_load(loads, loads % kStages2);
+          loads++;
+        }
+      }
+    }
+    if (__syncthreads_or(!ok)) {
+      ok = false;
+      break;
+    }
+    // the previous segment is complete with slice s - 1: read it while this one accumulates
+    if (s > 0 && s % SEG == 0) {
+      const bool d = mma_done(s - 1);
+      if (__syncthreads_or(!d)) {
+        ok = false;
+        break;
+      }
+      readout((s - 1) / SEG);
+    }
+  }
+  if (__syncthreads_or(!ok)) ok = false;
+  if (ok) {
+    const bool d = mma_done(S - 1);
+    if (__syncthreads_or(!d)) ok = false;
+    else readout((S - 1) / SEG);
+  }
+  if (!__syncthreads_or(!ok)) {
+    const int row = m0 + warp * 32 + lane;
+    if (row < M)
+#pragma unroll
+      for (int c = 0; c < TN2; c++)
+        if (n0 + c < N) C[(size_t)row * N + n0 + c] = acc[c];
+  } else if (tid == 0) {
+    // drain (bounded): issued loads land and committed MMAs finish before the stages and TMEM go away
+    for (int s = issued + 1; s < loads; s++) loaded(s);
+    if (issued >= 0) mma_done(issued);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTmemCols2));
+}
+
 // Velocity gauge: coefficient slices of c_A(R) = e^{2 pi i A.R} c(R), one thread per
 // (column, K entry); column 2 ce + part holds [Re c_A ; -Im c_A] (part 0) or
 // [Im c_A ; Re c_A] (part 1), pre-multiplied by 2 scale as the host build's slices
@@ -326,6 +476,41 @@ cudaError_t tc_contract(const TcArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                   const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// rows x Kp BF16 operand (K contiguous), boxes of 8 x box_rows; out-of-range rows read as zero
+cudaError_t encode_operand(CUtensorMap* map, const uint16_t* ptr, int rows, int Kp, int box_rows) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return cudaErrorNotSupported;
+  const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)Kp * sizeof(uint16_t)};
+  const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1u, 1u};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+size_t tma_gemm_smem() { return (size_t)kStages2 * (TM + TN2) * TK * 2 + 1024; }
+
+}  // namespace
+
 cudaError_t tc_vg_prepare(const TcVgArgs& a, cudaStream_t s) {
   const int kpad = tc_pad_k(a.nr);
   k_phase_split<<<a.nk, 256, 0, s>>>(a.kpt, a.Rvec, a.nk, a.nr, tc_seg_k(a.nr), kpad, a.Aw);
@@ -333,7 +518,16 @@ cudaError_t tc_vg_prepare(const TcVgArgs& a, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(a.Bw, 0, sizeof(uint16_t) * (size_t)8 * a.ntri * kpad, s)) != cudaSuccess) return e;
   const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
-  return cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if ((e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tc_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_gemm_smem());
+}
+
+cudaError_t tc_vg_maps(TcVgArgs& a) {
+  const int kpad = tc_pad_k(a.nr);
+  cudaError_t e = encode_operand(&a.mapA, a.Aw, a.nk, kpad, TM);
+  if (e == cudaSuccess) e = encode_operand(&a.mapB, a.Bw, 8 * a.ntri, kpad, TN2);
+  a.tma = e == cudaSuccess;
+  return e;
 }
 
 cudaError_t tc_vg_stage(const TcVgArgs& a, cudaStream_t s) {
@@ -342,9 +536,14 @@ cudaError_t tc_vg_stage(const TcVgArgs& a, cudaStream_t s) {
                                                                    a.nr, kseg, kpad, a.Bw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
-  dim3 grid((a.nk + TM - 1) / TM, (ncols + TN - 1) / TN);
-  k_tc_gemm<<<grid, kThreads, smem, s>>>(a.Aw, a.Bw, a.Cw, a.nk, ncols, kpad, kseg, a.err);
+  if (a.tma) {
+    dim3 grid((a.nk + TM - 1) / TM, (ncols + TN2 - 1) / TN2);
+    k_tc_gemm_tma<<<grid, kThreads, tma_gemm_smem(), s>>>(a.mapA, a.mapB, a.Cw, a.nk, ncols, kpad, kseg, a.err);
+  } else {
+    const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
+    dim3 grid((a.nk + TM - 1) / TM, (ncols + TN - 1) / TN);
+    k_tc_gemm<<<grid, kThreads, smem, s>>>(a.Aw, a.Bw, a.Cw, a.nk, ncols, kpad, kseg, a.err);
+  }
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_scatter64<<<dim3((a.nk + 255) / 256, 4 * a.ntri), 256, 0, s>>>(a.Cw, a.nk, a.n, a.ntri, ncols, a.H, a.D);
   return cudaGetLastError();

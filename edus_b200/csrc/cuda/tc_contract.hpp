@@ -1,5 +1,6 @@
 // tc_contract.hpp — tensor-core (tcgen05, exact BF16 slices) Wannier contraction.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstring>
 #include <stddef.h>
@@ -85,8 +86,13 @@ struct TcVgArgs {
   double2* H = nullptr;              // out [ntri][nk]
   double2* D = nullptr;              // out [3][ntri][nk]
   int* err = nullptr;                // device error word (bounded waits)
+  // TMA descriptors of Aw and Bw (tc_vg_maps); without them the cp.async form runs
+  bool tma = false;
+  CUtensorMap mapA{}, mapB{};
 };
 cudaError_t tc_vg_prepare(const TcVgArgs& a, cudaStream_t s);
+// Encode the TMA descriptors of a.Aw, a.Bw (sets a.tma on success).
+cudaError_t tc_vg_maps(TcVgArgs& a);
 cudaError_t tc_vg_stage(const TcVgArgs& a, cudaStream_t s);
 
 }  // namespace batch

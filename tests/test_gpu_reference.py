@@ -326,7 +326,7 @@ def test_velocity_gauge_matches_oracle(workdir, nw, nside, n):
     assert np.array_equal(ctx.get_state(), rho)
 
 
-@pytest.mark.parametrize("nw,nside,n", [(8, 11, 16), (16, 13, 10)])
+@pytest.mark.parametrize("nw,nside,n", [(8, 11, 16), (16, 13, 10), (8, 9, 40)])
 def test_velocity_gauge_tensor_core_contraction(workdir, nw, nside, n):
     """Velocity gauge with the stage contraction on the tensor cores (context
     precision EDUS_PREC_MIXED: exact 8-bit BF16 slices, FP32 sums exact per
@@ -348,3 +348,13 @@ def test_velocity_gauge_tensor_core_contraction(workdir, nw, nside, n):
     j1 = RF.rel_l2([x["J1"] for x in g], [x["J1"] for x in lo])
     dpop = float(np.abs(np.array([x["pop"] for x in g]) - np.array([x["pop"] for x in lo])).max())
     assert j1 < 1e-6 and drho < 1e-8 and dpop < 1e-8, (j1, drho, dpop)
+    # the cp.async-staged GEMM gives the same sums bit for bit (every segment's
+    # FP32 sums are exact, so the staging cannot change them)
+    os.environ["EDUS_TC_GEMM"] = "cpasync"
+    try:
+        alt = E.Context(E.Problem(p, workdir), precision=abi.EDUS_PREC_MIXED)
+    finally:
+        del os.environ["EDUS_TC_GEMM"]
+    alt.run()
+    assert np.array_equal(alt.get_state(), rho)
+    assert all(np.array_equal(x["J1"], y["J1"]) for x, y in zip(g, alt.obs()))
