@@ -26,6 +26,7 @@
 #include "ctx_hooks.hpp"
 #include "cuda/kernels.hpp"
 #include "cuda/tc_contract.hpp"
+#include "cuda/dyn.cuh"
 #include "host/problem.hpp"
 
 namespace edus {
@@ -37,46 +38,10 @@ namespace {
     if (e_ != cudaSuccess) return fail(EDUS_ECUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
   } while (0)
 
-// headers/Laser.h:56-76,128-144
-void laser_E(const edus_laser& L, double t, double E[3]) {
-  double env = 0.;
-  if (L.envelope_kind == EDUS_ENV_GAUSS) {
-    double d = t - L.t0;
-    env = (d * d < 40 * L.sigma * L.sigma) ? L.E0 * std::exp(-d * d / (2 * L.sigma * L.sigma)) : 0.;
-  } else if (L.envelope_kind == EDUS_ENV_SIN2) {
-    if (t >= L.t0 && t <= L.tf) {
-      double s = std::sin(kPi * (t - L.t0) / (L.tf - L.t0));
-      env = L.E0 * (s * s);
-    }
-  } else if (L.envelope_kind == EDUS_ENV_PW) {
-    double tr = 0.;
-    if (t >= L.t0 && t < L.w1)
-      tr = (t - L.t0) / (L.w1 - L.t0);
-    else if (t >= L.w1 && t < L.w2)
-      tr = 1.;
-    else if (t >= L.w2 && t <= L.tf)
-      tr = (t - L.tf) / (L.w2 - L.tf);
-    env = L.E0 * tr;
-  }
-  double p1 = L.envelope_only ? 1. : std::sin(L.wl * (t - L.t0) + L.phase);
-  double p2 = L.envelope_only ? 1. : std::cos(L.wl * (t - L.t0) + L.phase);
-  for (int i = 0; i < 3; i++) E[i] = env * (p1 * L.pol1[i] + p2 * L.pol2[i]);
-}
-
 }  // namespace
 
-// Source_Main/RungeKutta.cpp:24-30
-void field_at(const edus_params& p, double t, double EF[2][3]) {
-  for (int i = 0; i < 3; i++) EF[0][i] = 0.;
-  for (int ip = 0; ip < p.n_pumps; ip++) {
-    double e[3];
-    laser_E(p.pump[ip], t, e);
-    for (int i = 0; i < 3; i++) EF[0][i] += e[i];
-  }
-  double e2[3];
-  laser_E(p.probe, t, e2);
-  for (int i = 0; i < 3; i++) EF[1][i] = .5 * e2[i];
-}
+// Source_Main/RungeKutta.cpp:24-30 (laser_field: headers/Laser.h:56-76,128-144)
+void field_at(const edus_params& p, double t, double EF[2][3]) { field_sum(p.pump, p.n_pumps, p.probe, t, EF); }
 
 static bool field_nonzero(const double EF[2][3]) {
   double Emax = 0;
@@ -125,6 +90,20 @@ struct edus_ctx {
   double* d_edia = nullptr;
   std::vector<double> snap_t;
   unsigned long long* d_maxdp = nullptr;
+  // adaptive step on the device (whole runs): the step scalars, a pinned copy
+  // of their active flag, the snapshot times, and the captured chunk of steps
+  // with the host state it was captured from
+  DynStep* d_dyn = nullptr;
+  int* h_active = nullptr;
+  double* d_snapt = nullptr;
+  int snapt_cap = 0;
+  cudaGraph_t dyn_graph = nullptr;
+  cudaGraphExec_t dyn_exec = nullptr;
+  long long dyn_chunk_launches = 0;
+  int dyn_K = 0, dyn_phase = -1;
+  double2* dyn_P0 = nullptr;
+  int dyn_ring[kMaxOrder]{};
+  cudaEvent_t dyn_ev[2]{};
   // loop state (host mirror of the reference's scalars)
   int it = 0, itfi = 0, res = 1;
   double time_loop = 0, dt = 0, dt0 = 0;
@@ -591,6 +570,259 @@ int run_steps(edus_ctx* c, int nsteps, bool all) {
   return 0;
 }
 
+// ------------------------------------------------ adaptive step on the device
+// A whole adaptive run (Source_Main/dyn_dt_evolution.cpp:1-183) as chunks of K
+// captured steps: k_dyn_begin, the output instant where one can fall, the
+// stages reading their scalars from the DynStep, k_dyn_end, and at the end of
+// the chunk a copy of the active flag into pinned memory. K is a multiple of
+// the Taylor ring's period (lcm(2, order): the ring slots rotate and the state
+// buffers swap every step), so every chunk starts from the captured host
+// state; with K also a multiple of it_resolution the instants sit at fixed
+// steps of the chunk, else every step carries a (device-gated) instant.
+
+bool dyn_on_device(const edus_ctx* c) {
+  if (!c->dyn || !c->d_dyn || c->vg || c->profiling) return false;
+  const char* e = std::getenv("EDUS_DYN_HOST");
+  return !(e && std::string(e) == "1");
+}
+
+long long lcm_ll(long long a, long long b) {
+  long long x = a, y = b;
+  while (y) {
+    const long long t = x % y;
+    x = y;
+    y = t;
+  }
+  return a / x * b;
+}
+
+int dyn_period(const edus_ctx* c) { return c->solver == EDUS_SOLVER_TAYLOR ? (int)lcm_ll(2, c->order) : 1; }
+
+// chunk length; *every: an instant launch at every step of the chunk
+int dyn_chunk_len(const edus_ctx* c, bool* every) {
+  const long long P = dyn_period(c);
+  const long long L = lcm_ll(c->res, P);
+  if (L <= 512) {
+    *every = false;
+    return (int)(L * ((16 + L - 1) / L));
+  }
+  *every = true;
+  return (int)(P * ((16 + P - 1) / P));
+}
+
+// One Taylor step's rotation of the ring slots (as step_taylor makes it).
+void taylor_ring_rotate(edus_ctx* c) {
+  const int TO = c->order;
+  const int fill = c->ring_idx[TO - 1];
+  for (int s = TO - 1; s > 0; s--) c->ring_idx[s] = c->ring_idx[s - 1];
+  c->ring_idx[0] = fill;
+}
+
+int dyn_enqueue_chunk(edus_ctx* c, int K, bool every) {
+  DynStep* d = c->d_dyn;
+  const bool taylor = c->solver == EDUS_SOLVER_TAYLOR;
+  double2* hr_out = c->coul ? c->d_hr : nullptr;  // every step: an instant reads the last one
+  for (int j = 0; j < K; j++) {
+    CK(launch_dyn_begin(d, c->stream));
+    c->launches++;
+    if (every || (c->it + j) % c->res == 0) {
+      const double scaleJ = c->P.dk[0] * c->P.dk[1] * c->P.dk[2] / c->P.det_a;
+      const double scaleTA = std::fabs(c->P.jac) * c->P.dk[0] * c->P.dk[1] * c->P.dk[2];
+      edus_obs rec;
+      memset(&rec, 0, sizeof(rec));
+      CK(launch_observables(c->tb, c->d_cst, c->d_P0, c->coul ? c->d_hr : nullptr, c->P.p.current, c->P.p.tabs, c->d_part,
+                            c->d_done, scaleJ, scaleTA, rec, c->d_log, c->d_ncond, c->d_pcmax, c->stream, d));
+      c->launches++;
+      if (c->snap_on && c->d_snap) {
+        CK(launch_snapshot(c->tb, c->d_P0, c->snap_ic, c->snap_jc, c->d_snap, c->stream, d));
+        c->launches++;
+      }
+      if (c->snap_on && c->d_edia) {
+        CK(launch_band_energies(c->tb, c->d_hr, c->d_edia, c->stream, d));
+        c->launches++;
+      }
+    }
+    StageArgs a = base_args(c);
+    a.dyn = d;
+    a.hr_out = nullptr;
+    int rc = 0;
+    if (taylor) {
+      taylor_ring_rotate(c);
+      a.src = c->d_P0;
+      a.dst = c->d_Pa;
+      a.op = OP_TAYLOR;
+      a.ring = c->d_ring;
+      for (int q = 0; q < c->order; q++) a.ring_idx[q] = c->ring_idx[q];
+      a.dyn_stage = 0;
+      a.dyn_field = 0;
+      a.hr_out = hr_out;
+      a.maxdp = &d->maxdp;
+      if ((rc = rhs(c, a))) return rc;
+      std::swap(c->d_P0, c->d_Pa);
+    } else {
+      a.src = c->d_P0;
+      a.base = c->d_P0;
+      a.acc = c->d_P1;
+      a.dst = c->d_Pa;
+      a.op = OP_RK_FIRST;
+      a.dyn_stage = 0;
+      a.dyn_field = 0;
+      if ((rc = rhs(c, a))) return rc;
+      a.src = c->d_Pa;
+      a.dst = c->d_Pb;
+      a.op = OP_RK_MID;
+      a.dyn_stage = 1;
+      a.dyn_field = 1;
+      if ((rc = rhs(c, a))) return rc;
+      a.src = c->d_Pb;
+      a.dst = c->d_Pa;
+      a.dyn_stage = 2;
+      if ((rc = rhs(c, a))) return rc;
+      a.src = c->d_Pa;
+      a.dst = c->d_P0;
+      a.op = OP_RK_LAST;
+      a.dyn_stage = 3;
+      a.dyn_field = 2;
+      a.hr_out = hr_out;
+      a.maxdp = &d->maxdp;
+      if ((rc = rhs(c, a))) return rc;
+    }
+    CK(launch_dyn_end(d, c->stream));
+    c->launches++;
+  }
+  CK(cudaMemcpyAsync(c->h_active, &d->active, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  return 0;
+}
+
+int run_dyn_device(edus_ctx* c) {
+  const edus_params& p = c->P.p;
+  DynStep h;
+  memset(&h, 0, sizeof(h));
+  for (int i = 0; i < EDUS_MAX_PUMPS; i++) h.pump[i] = p.pump[i];
+  h.probe = p.probe;
+  h.n_pumps = p.n_pumps;
+  h.taylor = c->solver == EDUS_SOLVER_TAYLOR;
+  h.order = c->order;
+  h.res = c->res;
+  h.log_cap = c->log_cap;
+  h.snap_on = c->snap_on;
+  h.snap_cap = (c->d_snap || c->d_edia) ? c->snap_cap : 0;
+  h.snap_tcap = c->snapt_cap;
+  h.print_start = p.print_start;
+  h.print_end = p.print_end;
+  h.print_step = p.print_step;
+  h.t_fin = p.t_fin;
+  h.eps = p.eps_step_abs;
+  h.dt0 = c->dt0;
+  h.pcmax = c->d_pcmax;
+  h.ncond = c->d_ncond;
+  h.snap_t = c->d_snapt;
+  h.t = c->time_loop;
+  h.dt = c->dt;
+  h.it = c->it;
+  h.nlog = c->nlog;
+  h.icont = c->icont;
+  h.active = 1;
+  h.e_non0 = c->e_non0;
+  memcpy(h.EF_last, c->EF, sizeof(h.EF_last));
+  memcpy(h.dt_prev, c->dt_prev, sizeof(h.dt_prev));
+  h.snap_slot = -1;
+  CK(cudaMemcpyAsync(c->d_dyn, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *c->h_active = 1;
+
+  bool every = false;
+  const int K = dyn_chunk_len(c, &every);
+  const int phase = every ? 0 : c->it % c->res;
+  const bool graphs = c->use_graphs;
+  if (graphs && c->dyn_exec &&
+      (c->dyn_K != K || c->dyn_phase != phase || c->dyn_P0 != c->d_P0 ||
+       memcmp(c->dyn_ring, c->ring_idx, sizeof(c->dyn_ring)) != 0)) {
+    cudaGraphExecDestroy(c->dyn_exec);
+    cudaGraphDestroy(c->dyn_graph);
+    c->dyn_exec = nullptr;
+    c->dyn_graph = nullptr;
+  }
+  if (graphs && !c->dyn_exec) {
+    c->dyn_K = K;
+    c->dyn_phase = phase;
+    c->dyn_P0 = c->d_P0;
+    memcpy(c->dyn_ring, c->ring_idx, sizeof(c->dyn_ring));
+    const long long l0 = c->launches;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = dyn_enqueue_chunk(c, K, every);
+    cudaGraph_t g = nullptr;
+    cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+    // the capture counted one chunk's kernels; they run at each replay
+    c->dyn_chunk_launches = c->launches - l0;
+    c->launches = l0;
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ec != cudaSuccess) return fail(EDUS_ECUDA, "stream capture: %s", cudaGetErrorString(ec));
+    c->dyn_graph = g;
+    CK(cudaGraphInstantiate(&c->dyn_exec, g, 0));
+  }
+  for (int i = 0; i < 2; i++)
+    if (!c->dyn_ev[i]) CK(cudaEventCreateWithFlags(&c->dyn_ev[i], cudaEventDisableTiming));
+
+  // keep two chunks queued; stop once a finished chunk reports the run over
+  const int it0 = c->it;
+  const long long kMaxChunks = (1ll << 28) / K;
+  long long chunks = 0;
+  auto launch = [&]() -> int {
+    if (graphs) {
+      CK(cudaGraphLaunch(c->dyn_exec, c->stream));
+      c->launches += c->dyn_chunk_launches;
+    } else {
+      int rc = dyn_enqueue_chunk(c, K, every);
+      if (rc) return rc;
+    }
+    CK(cudaEventRecord(c->dyn_ev[chunks & 1], c->stream));
+    chunks++;
+    return 0;
+  };
+  int rc = launch();
+  if (rc) return rc;
+  for (;;) {
+    if ((rc = launch())) return rc;
+    CK(cudaEventSynchronize(c->dyn_ev[(chunks - 2) & 1]));
+    if (!*(volatile int*)c->h_active) break;
+    if (chunks > kMaxChunks) return fail(EDUS_EINVAL, "adaptive run: more than 2^28 steps");
+  }
+  CK(cudaMemcpyAsync(&h, c->d_dyn, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+
+  // the host mirror after the run
+  const int icont0 = c->icont;
+  c->time_loop = h.t;
+  c->dt = h.dt;
+  c->it = h.it;
+  c->nlog = h.nlog;
+  c->icont = h.icont;
+  c->e_non0 = h.e_non0 != 0;
+  memcpy(c->EF, h.EF_last, sizeof(c->EF));
+  memcpy(c->dt_prev, h.dt_prev, sizeof(c->dt_prev));
+  if (c->solver == EDUS_SOLVER_TAYLOR)
+    for (int s = 0; s < (c->it - it0) % dyn_period(c); s++) {
+      taylor_ring_rotate(c);
+      std::swap(c->d_P0, c->d_Pa);
+    }
+  if (h.icont > icont0 && c->d_snapt) {
+    const int first = icont0 + 1, last = std::min(h.icont, c->snapt_cap - 1);
+    if (last >= first) {
+      std::vector<double> ts((size_t)(last - first + 1));
+      CK(cudaMemcpy(ts.data(), c->d_snapt + first, sizeof(double) * ts.size(), cudaMemcpyDeviceToHost));
+      for (double t : ts) c->snap_t.push_back(t);
+    }
+  }
+  if ((rc = sync_scalars(c))) return rc;
+  if (h.fault == kDynFaultSnapshots) return fail(EDUS_EINVAL, "snapshot %d exceeds the %d slots", h.icont, c->snap_cap);
+  if (h.fault == kDynFaultTaylor) return fail(EDUS_EINVAL, "Taylor tau matrix is singular");
+  return 0;
+}
+
 // Enqueue nsteps (or the whole run) between the context's two timing events;
 // *l0 receives the launch count before them. timed_finish waits for the end
 // event and checks the device error word.
@@ -598,6 +830,13 @@ int timed_start(edus_ctx* c, int nsteps, bool all, long long* l0_out) {
   CK(cudaSetDevice(c->device));
   long long l0 = c->launches;
   *l0_out = l0;
+  if (all && dyn_on_device(c)) {
+    CK(cudaEventRecord(c->ev0, c->stream));
+    int rc = run_dyn_device(c);
+    if (rc) return rc;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    return 0;
+  }
   const bool graph = all && !c->dyn && c->use_graphs && c->it == 0;
   if (graph && !c->gexec) {
     // capture the whole loop once; the captured kernels run at cudaGraphLaunch below
@@ -1194,6 +1433,11 @@ void edus_destroy(edus_ctx* c) {
   for (void* p : c->allocs) cudaFree(p);
   if (c->gexec) cudaGraphExecDestroy(c->gexec);
   if (c->graph) cudaGraphDestroy(c->graph);
+  if (c->dyn_exec) cudaGraphExecDestroy(c->dyn_exec);
+  if (c->dyn_graph) cudaGraphDestroy(c->dyn_graph);
+  for (cudaEvent_t e : c->dyn_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->h_active) cudaFreeHost(c->h_active);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1318,6 +1562,16 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
   cudaMemsetAsync(c->d_pcmax, 0, sizeof(double), c->stream);
   c->log_cap = P.p.dynamical_dt ? 1 << 16 : P.nprint + 2;
   if ((rc = dalloc(c, &c->d_log, c->log_cap))) return bail(rc);
+  if (c->dyn) {
+    // adaptive step on the device: its scalars, the pinned flag, snapshot times
+    if ((rc = dalloc(c, &c->d_dyn, 1))) return bail(rc);
+    if (cudaHostAlloc(&c->h_active, sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+      return bail(fail(EDUS_ENOMEM, "pinned flag"));
+    if (P.p.print_population || P.p.print_band_dispersion) {
+      c->snapt_cap = c->log_cap;
+      if ((rc = dalloc(c, &c->d_snapt, (size_t)c->snapt_cap))) return bail(rc);
+    }
+  }
   // ---- per-k snapshots: slots for every snapshot the run can take
   c->snap_on = P.p.print_population || P.p.print_band_dispersion;
   if (c->snap_on && (P.p.print_population || c->coul)) {

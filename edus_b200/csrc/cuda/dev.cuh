@@ -161,6 +161,8 @@ enum StageOp : int {
   OP_TAYLOR = 5,   // ring[slot0] = Pv ; dst = src + Taylor increment
 };
 
+struct DynStep;
+
 // Everything one fused RHS + update launch needs that changes per stage.
 struct StageArgs {
   const double2* src;   // state the RHS is evaluated on
@@ -187,6 +189,12 @@ struct StageArgs {
   // Coulomb in the diagonal basis: the mean-field term already rotated back to
   // the Wannier basis, [ntri][nk] (null: the Wannier-basis term from tb.h)
   const double2* xw;
+  // adaptive step on the device: when set, the stage's field (dyn->EF[dyn_field]),
+  // coefficients (dyn->c[dyn_stage]), dt, Taylor tables, e_non0 and
+  // P_cond_max + n_cond come from *dyn, and the launch does nothing once the
+  // run has ended (dyn->active == 0)
+  const DynStep* dyn;
+  int dyn_stage, dyn_field;
 };
 
 }  // namespace edus

@@ -17,6 +17,7 @@
 #include <algorithm>
 
 #include "eig.cuh"
+#include "dyn.cuh"
 #include "kernels.hpp"
 
 namespace edus {
@@ -225,6 +226,9 @@ struct ObsArgs {
   ObsRecord* log;
   double* ncond_dev;
   double* pcmax_dev;
+  // adaptive step on the device: the instant is taken only when dyn->obs_now,
+  // with the clock, field and step of *dyn, into record dyn->nlog of log
+  const DynStep* dyn;
 };
 
 constexpr int kObsThreads = 128;
@@ -241,6 +245,7 @@ __global__ void __launch_bounds__(kObsThreads) k_obs(DevTables tb, const DevCons
   const double2* rho = a.rho;
   const double2* hr = a.hr;
   pdl_wait();
+  if (a.dyn && !a.dyn->obs_now) return;  // uniform: no instant at this step
   if (k < nk) {
     double2 P[NT];
 #pragma unroll
@@ -370,6 +375,17 @@ __global__ void __launch_bounds__(kObsThreads) k_obs(DevTables tb, const DevCons
   if (threadIdx.x != 0) return;
   const ObsPart& T = sp[0];
   ObsRecord rec = a.rec;
+  ObsRecord* slot = a.log;
+  if (a.dyn) {
+    const DynStep* d = a.dyn;
+    rec.t = d->t;
+    rec.dt = d->dt;
+    for (int x = 0; x < 3; x++) {
+      rec.EF_pump[x] = d->EF_last[0][x];
+      rec.EF_probe[x] = d->EF_last[1][x];
+    }
+    slot = (a.log && d->nlog < d->log_cap) ? a.log + d->nlog : nullptr;
+  }
   const double inv = 1. / nk;
   double trace = -(double)tb.nbands;
   double nc = 0;
@@ -391,7 +407,7 @@ __global__ void __launch_bounds__(kObsThreads) k_obs(DevTables tb, const DevCons
   rec.p_cond_max = T.pmax;
   rec.p_min = T.pmin;
   rec.n_cond = nc;
-  if (a.log) *a.log = rec;
+  if (slot) *slot = rec;
   if (a.ncond_dev) *a.ncond_dev = nc;
   if (a.pcmax_dev) *a.pcmax_dev = T.pmax;
   *a.done = 0u;
@@ -433,9 +449,16 @@ cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2*
 // the model's eigenbasis, P_dia_rc = sum_ii sum_jj conj(U_r,ii) P_ii,jj U_c,jj
 // in the reference's summation order (headers/InitParameters.h:232-255), for
 // the snapshots of Source_Main/if_resolution.cpp:231-270. One thread per k.
-__global__ void k_snapshot(DevTables tb, const double2* __restrict__ rho, int ic, int jc, double2* __restrict__ out) {
+__global__ void k_snapshot(DevTables tb, const double2* __restrict__ rho, int ic, int jc, double2* __restrict__ out,
+                           const DynStep* __restrict__ dyn) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int nk = tb.nk, n = tb.n;
+  if (dyn) {
+    // adaptive step on the device: slot of this instant's snapshot, if one is due
+    const int slot = dyn->snap_slot;
+    if (slot < 0) return;
+    out += (size_t)slot * 3 * nk;
+  }
   if (k >= nk) return;
   auto tri = [n](int i, int j) { return i * n - (i * (i - 1)) / 2 + (j - i); };
   const int rows[3] = {ic, ic, jc}, cols[3] = {jc, ic, jc};
@@ -453,9 +476,10 @@ __global__ void k_snapshot(DevTables tb, const double2* __restrict__ rho, int ic
   }
 }
 
-cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int jc, double2* out, cudaStream_t s) {
+cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int jc, double2* out, cudaStream_t s,
+                            const DynStep* dyn) {
   if (!tb.U || ic < 0 || jc < 0 || ic >= tb.n || jc >= tb.n) return cudaErrorInvalidValue;
-  k_snapshot<<<(tb.nk + 127) / 128, 128, 0, s>>>(tb, rho, ic, jc, out);
+  k_snapshot<<<(tb.nk + 127) / 128, 128, 0, s>>>(tb, rho, ic, jc, out, dyn);
   return cudaGetLastError();
 }
 
@@ -463,8 +487,13 @@ cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int
 // eig_sym returns them; headers/Observables_MPI.h:282-303), for the Edia
 // snapshot files. One thread per k.
 template <int N>
-__global__ void k_band_energies(int nk, const double2* __restrict__ hr, double* __restrict__ out) {
+__global__ void k_band_energies(int nk, const double2* __restrict__ hr, double* __restrict__ out, const DynStep* __restrict__ dyn) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dyn) {
+    const int slot = dyn->snap_slot;
+    if (slot < 0) return;
+    out += (size_t)slot * N * nk;
+  }
   if (k >= nk) return;
   double2 A[N * N], Z[N * N];
 #pragma unroll
@@ -480,16 +509,16 @@ __global__ void k_band_energies(int nk, const double2* __restrict__ hr, double* 
   for (int i = 0; i < N; i++) out[(size_t)i * nk + k] = A[i * N + i].x;
 }
 
-cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double* out, cudaStream_t s) {
+cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double* out, cudaStream_t s, const DynStep* dyn) {
   const dim3 g((tb.nk + 63) / 64), b(64);
   switch (tb.n) {
-    case 1: k_band_energies<1><<<g, b, 0, s>>>(tb.nk, hr, out); break;
-    case 2: k_band_energies<2><<<g, b, 0, s>>>(tb.nk, hr, out); break;
-    case 3: k_band_energies<3><<<g, b, 0, s>>>(tb.nk, hr, out); break;
-    case 4: k_band_energies<4><<<g, b, 0, s>>>(tb.nk, hr, out); break;
-    case 5: k_band_energies<5><<<g, b, 0, s>>>(tb.nk, hr, out); break;
-    case 8: k_band_energies<8><<<g, b, 0, s>>>(tb.nk, hr, out); break;
-    case 16: k_band_energies<16><<<g, b, 0, s>>>(tb.nk, hr, out); break;
+    case 1: k_band_energies<1><<<g, b, 0, s>>>(tb.nk, hr, out, dyn); break;
+    case 2: k_band_energies<2><<<g, b, 0, s>>>(tb.nk, hr, out, dyn); break;
+    case 3: k_band_energies<3><<<g, b, 0, s>>>(tb.nk, hr, out, dyn); break;
+    case 4: k_band_energies<4><<<g, b, 0, s>>>(tb.nk, hr, out, dyn); break;
+    case 5: k_band_energies<5><<<g, b, 0, s>>>(tb.nk, hr, out, dyn); break;
+    case 8: k_band_energies<8><<<g, b, 0, s>>>(tb.nk, hr, out, dyn); break;
+    case 16: k_band_energies<16><<<g, b, 0, s>>>(tb.nk, hr, out, dyn); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -647,8 +676,9 @@ static cudaError_t launch_obs_n(const DevTables& tb, const DevConsts* cst, const
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,
                                int want_current, int want_tabs, void* part, unsigned int* done, double scaleJ,
                                double scaleTA, const ObsRecord& rec, ObsRecord* log, double* ncond_dev,
-                               double* pcmax_dev, cudaStream_t s) {
+                               double* pcmax_dev, cudaStream_t s, const DynStep* dyn) {
   ObsArgs a;
+  a.dyn = dyn;
   a.rho = rho;
   a.hr = hr;
   a.want_current = want_current;

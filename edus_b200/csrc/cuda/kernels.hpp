@@ -35,9 +35,14 @@ cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2*
                            const double2* X0, cudaStream_t s);
 // Elements (ic, jc), (ic, ic), (jc, jc) of rho in the eigenbasis of tb.U for
 // every k: out[3][nk].
-cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int jc, double2* out, cudaStream_t s);
-// Ascending eigenvalues of the Hermitian planes hr at every k: out[n][nk].
-cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double* out, cudaStream_t s);
+// With dyn (adaptive step on the device), out is the base of the snapshot
+// slots and the slot is dyn->snap_slot (nothing when it is negative).
+cudaError_t launch_snapshot(const DevTables& tb, const double2* rho, int ic, int jc, double2* out, cudaStream_t s,
+                            const DynStep* dyn = nullptr);
+// Ascending eigenvalues of the Hermitian planes hr at every k: out[n][nk]
+// (slot dyn->snap_slot of out with dyn, as above).
+cudaError_t launch_band_energies(const DevTables& tb, const double2* hr, double* out, cudaStream_t s,
+                                 const DynStep* dyn = nullptr);
 // d = a + dt * v elementwise (n complex entries; d may alias a).
 cudaError_t launch_axpy(const double2* a, const double2* v, double dt, double2* d, size_t n, cudaStream_t s);
 // Coulomb in the diagonal basis, up to 4 bands: the state in the eigenbasis of
@@ -63,6 +68,6 @@ size_t obs_part_bytes();
 cudaError_t launch_observables(const DevTables& tb, const DevConsts* cst, const double2* rho, const double2* hr,
                                int want_current, int want_tabs, void* part, unsigned int* done, double scaleJ,
                                double scaleTA, const ObsRecord& rec, ObsRecord* log, double* ncond_dev,
-                               double* pcmax_dev, cudaStream_t s);
+                               double* pcmax_dev, cudaStream_t s, const DynStep* dyn = nullptr);
 
 }  // namespace edus

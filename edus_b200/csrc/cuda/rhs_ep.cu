@@ -12,6 +12,7 @@
 // thread per k this gives NT times the parallelism for the small grids of the
 // reference's workloads, where one solve has only 10^3-10^4 k points.
 #include "dev.cuh"
+#include "dyn.cuh"
 #include "kernels.hpp"
 
 namespace edus {
@@ -31,7 +32,9 @@ struct TriEP {
   }
 };
 
-template <int N, int KT>
+// DYN: the stage scalars come from the adaptive step's device copy (a.dyn);
+// a separate instantiation so the constant-step kernel keeps its registers.
+template <int N, int KT, bool DYN>
 __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const DevConsts* __restrict__ cst, StageArgs a) {
   constexpr int NT = TriEP<N>::NT;
   __shared__ double2 sP[NT][KT];
@@ -64,6 +67,7 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
       ts[t] = __ldg((cs == 0 ? tb.t2c : tb.t2s) + m * n2 + i2);
     }
     pdl_wait();
+    if (DYN && !a.dyn->active) return;  // the adaptive run has ended (uniform over the grid)
     if (tid == 0) {
       const int r0 = k0 / n2;
       const int r1 = (min(k0 + KT, nk) - 1) / n2;
@@ -74,7 +78,21 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
     }
   } else {
     pdl_wait();
+    if (DYN && !a.dyn->active) return;
   }
+  // stage scalars: kernel arguments, or the adaptive step's device copy
+  const DynStep* dy = DYN ? a.dyn : nullptr;
+  double ef0[3], ef1[3];  // pump, probe
+#pragma unroll
+  for (int x = 0; x < 3; x++) {
+    ef0[x] = dy ? dy->EF[a.dyn_field][0][x] : a.EF[0][x];
+    ef1[x] = dy ? dy->EF[a.dyn_field][1][x] : a.EF[1][x];
+  }
+  const int e_non0 = dy ? dy->e_non0 : a.e_non0;
+  const double c1 = dy ? dy->c[a.dyn_stage][0] : a.c1;
+  const double c2 = dy ? dy->c[a.dyn_stage][1] : a.c2;
+  const double dtv = dy ? dy->dt : a.dt;
+  const double pcn = dy ? (*dy->pcmax + *dy->ncond) : a.pcond_plus_ncond;
   double2 Pe = cz(), He = cz(), G = cz();
   double2 De[3] = {cz(), cz(), cz()};
   if (valid) {
@@ -147,18 +165,18 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
       }
       if (a.hr_out) a.hr_out[(size_t)e * nk + k] = He;
     }
-    if (a.e_non0) {
+    if (e_non0) {
       // sum_b (w_b E_pump . b) rho_e(k + b)
 #pragma unroll 6
       for (int b = 0; b < tb.nnb; b++) {
         const int kb = tb.nbr[(size_t)b * nk + k];
         const double2 pn = a.src[(size_t)e * nk + kb];
-        const double c0 = cst->wb[b] * a.EF[0][0] * cst->bvec[b][0];
-        const double c1 = cst->wb[b] * a.EF[0][1] * cst->bvec[b][1];
-        const double c2 = cst->wb[b] * a.EF[0][2] * cst->bvec[b][2];
-        G = cadd(G, cscale(pn, c0));
-        G = cadd(G, cscale(pn, c1));
-        G = cadd(G, cscale(pn, c2));
+        const double f0 = cst->wb[b] * ef0[0] * cst->bvec[b][0];
+        const double f1 = cst->wb[b] * ef0[1] * cst->bvec[b][1];
+        const double f2 = cst->wb[b] * ef0[2] * cst->bvec[b][2];
+        G = cadd(G, cscale(pn, f0));
+        G = cadd(G, cscale(pn, f1));
+        G = cadd(G, cscale(pn, f2));
       }
     }
   }
@@ -171,8 +189,9 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
     const bool herm = tb.herm_dip != 0;
 #pragma unroll
     for (int x = 0; x < 3; x++) {
-      hu = cadd(hu, cscale(De[x], a.EF[w][x]));
-      hl = cadd(hl, cscale(herm ? cconj(De[x]) : De[x], a.EF[w][x]));
+      const double f = w ? ef1[x] : ef0[x];
+      hu = cadd(hu, cscale(De[x], f));
+      hl = cadd(hl, cscale(herm ? cconj(De[x]) : De[x], f));
     }
     sP[e][kl] = Pe;
     sHu[e][kl] = hu;
@@ -230,19 +249,19 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
       case OP_RK_FIRST: {
         if (a.ring) a.ring[(size_t)a.ring_idx[0] * NT * nk + o] = v;
         const double2 b0 = a.base[o];
-        a.acc[o] = cadd(b0, cscale(v, a.c1));
-        a.dst[o] = cadd(b0, cscale(v, a.c2));
+        a.acc[o] = cadd(b0, cscale(v, c1));
+        a.dst[o] = cadd(b0, cscale(v, c2));
       } break;
       case OP_RK_MID: {
         const double2 b0 = a.base[o];
-        a.acc[o] = cadd(a.acc[o], cscale(v, a.c1));
-        a.dst[o] = cadd(b0, cscale(v, a.c2));
+        a.acc[o] = cadd(a.acc[o], cscale(v, c1));
+        a.dst[o] = cadd(b0, cscale(v, c2));
       } break;
       case OP_RK_LAST: {
-        const double2 nv = cadd(a.acc[o], cscale(v, a.c1));
+        const double2 nv = cadd(a.acc[o], cscale(v, c1));
         if (a.maxdp && i == j) {
           const double2 old = a.dst[o];
-          dpmax = 2 * hypot(old.x - nv.x, old.y - nv.y) / (a.pcond_plus_ncond + hypot(nv.x, nv.y) + 1.0e-7);
+          dpmax = 2 * hypot(old.x - nv.x, old.y - nv.y) / (pcn + hypot(nv.x, nv.y) + 1.0e-7);
         }
         a.dst[o] = nv;
       } break;
@@ -253,23 +272,23 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
           const double2 f = (s == 0) ? v : a.ring[(size_t)a.ring_idx[s] * NT * nk + o];
           d = cadd(d, cscale(f, a.coef[s]));
         }
-        a.dst[o] = cadd(Pe, cscale(d, a.dt));
+        a.dst[o] = cadd(Pe, cscale(d, dtv));
       } break;
       case OP_TAYLOR: {
         const int TO = a.order, m = TO - 1;
         a.ring[(size_t)a.ring_idx[0] * NT * nk + o] = v;
         double2 dP[kMaxOrder];
         for (int q = 0; q < m; q++) dP[q] = csub(v, a.ring[(size_t)a.ring_idx[q + 1] * NT * nk + o]);
-        double2 d = cscale(v, a.dt);
+        double2 d = cscale(v, dtv);
         for (int r = 1; r < TO; r++) {
           double2 al = cz();
-          for (int q = 0; q < m; q++) al = cadd(al, cscale(dP[q], a.tinv[(r - 1) * m + q]));
-          const double2 inc = cscale(al, a.tpow[r]);
+          for (int q = 0; q < m; q++) al = cadd(al, cscale(dP[q], dy ? dy->tinv[(r - 1) * m + q] : a.tinv[(r - 1) * m + q]));
+          const double2 inc = cscale(al, dy ? dy->tpow[r] : a.tpow[r]);
           d = cadd(d, cmk(inc.x / (double)(r + 1), inc.y / (double)(r + 1)));
         }
         const double2 nv = cadd(Pe, d);
         if (a.maxdp && i == j)
-          dpmax = 2 * hypot(Pe.x - nv.x, Pe.y - nv.y) / (a.pcond_plus_ncond + hypot(nv.x, nv.y) + 1.0e-7);
+          dpmax = 2 * hypot(Pe.x - nv.x, Pe.y - nv.y) / (pcn + hypot(nv.x, nv.y) + 1.0e-7);
         a.dst[o] = nv;
       } break;
     }
@@ -298,7 +317,8 @@ static cudaError_t launch_ep(const DevTables& tb, const DevConsts* cst, const St
       dyn = bytes;
     }
   }
-  return launch_pdl(k_rhs_ep<N, KT>, dim3((tb.nk + KT - 1) / KT), block, dyn, s, tb, cst, b);
+  if (a.dyn) return launch_pdl(k_rhs_ep<N, KT, true>, dim3((tb.nk + KT - 1) / KT), block, dyn, s, tb, cst, b);
+  return launch_pdl(k_rhs_ep<N, KT, false>, dim3((tb.nk + KT - 1) / KT), block, dyn, s, tb, cst, b);
 }
 
 cudaError_t launch_rhs(const DevTables& tb, const DevConsts* cst, const StageArgs& a, cudaStream_t s) {

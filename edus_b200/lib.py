@@ -493,6 +493,13 @@ class Server:
         _check(self._L.edus_server_info(self._h, int(rid), C.byref(o)), "edus_server_info")
         return {f: getattr(o, f) for f, _ in abi.RequestInfo._fields_}
 
+    def failure(self, rid):
+        """(error code, message) of a failed request, else None."""
+        i = self.info(rid)
+        if i["status"] != abi.EDUS_REQ_FAILED:
+            return None
+        return i["error"], self._L.edus_last_error().decode(errors="replace")
+
     def obs(self, rid):
         i = self.info(rid)
         if i["status"] == abi.EDUS_REQ_FAILED:

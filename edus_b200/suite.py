@@ -249,6 +249,14 @@ def serve_line(count=2000, rate=None, per_class=30, seed=7, max_s=None, load=1.2
     sample = []
     for c in sorted(units):
         sample += [q for q in range(count) if _class(specs[q]) == c][:per_class]
+    failures = []
+    for q, rid in enumerate(ids):
+        f = s.failure(rid)
+        if f is not None:
+            sp = specs[q]
+            failures.append({"request": q, "class": _class(sp), "n": sp["n"], "duration_fs": sp["duration"],
+                             "field_V_per_A": sp["field"], "r0_A": sp.get("r0"), "error": f[0], "message": f[1]})
+    sample = [q for q in sample if s.info(ids[q])["status"] == abi.EDUS_REQ_DONE]
     logs = {q: s.obs(ids[q]) for q in sample}
     s.close()
     # plain FP64 single-solve path, request by request (one request on the GPU at a time)
@@ -279,4 +287,5 @@ def serve_line(count=2000, rate=None, per_class=30, seed=7, max_s=None, load=1.2
             "stream_seconds": fp64_stream_s},
         "speedup_vs_fp64_request_by_request": fp64_stream_s / st["span_s"],
         "j1_rel_l2_vs_fp64": {c: {"max": max(v), "median": float(np.median(v)), "requests": len(v)} for c, v in sorted(errs.items())},
+        "failures": failures,
     }

@@ -165,6 +165,79 @@ def test_rk4_dynamic_dt_matches_oracle(workdir):
     assert ctx.clock()[0] == o.clock()[0]
 
 
+def _dyn_input(kind, d):
+    if kind == "rk4":
+        return W.hbn_rk4(d, n=24, t_fin_fs=2.0, it_res=3, solver="dynamical_dt_evolution\nepsStepAbs 0.001\n")
+    if kind == "taylor":
+        return W.hbn_rk4(d, n=24, t_fin_fs=2.0, it_res=3, dt_fs=0.002,
+                         solver="Taylor\nTaylorOrder 6\ndynamical_dt_evolution\nepsStepAbs 0.02\n")
+    if kind == "snapshots":
+        path = W.hbn_rk4(d, n=12, t_fin_fs=1.5, it_res=10, solver="dynamical_dt_evolution\nepsStepAbs 0.001\n")
+        txt = open(path).read().replace("Current\n", "Current\nPrintPopulation 0 60 15\n")
+    else:  # Coulomb mean field with RK4 and band-energy snapshots
+        path = W.hbn_coulomb(d, n=24, t_fin_fs=0.6, it_res=10, rk4=True)
+        txt = open(path).read().replace("tdse{\n", "tdse{\ndynamical_dt_evolution\nepsStepAbs 0.001\n")
+        txt = txt.replace("Rytova_Keldysh\n", "Rytova_Keldysh\nPrint_new_band_dispersion\n")
+    open(path, "w").write(txt)
+    return path
+
+
+@pytest.mark.parametrize("kind", ["rk4", "taylor", "snapshots", "coulomb"])
+def test_adaptive_step_on_device_matches_host_loop(workdir, kind):
+    """A whole adaptive run (dynamical_dt_evolution) with the step picked on the
+    device (k_dyn_begin / k_dyn_end around captured chunks, no host round trip
+    per step) against the host-driven loop (EDUS_DYN_HOST=1: the max copied to
+    the host every step, Source_Main/dyn_dt_evolution.cpp:64-133): the same
+    number of steps and output instants, the same snapshot times, clock and
+    observables within the rounding of the device's sin / cos / exp in the
+    laser field; the device run replays after edus_reset."""
+    d = f"{workdir}/{kind}"
+    path = _dyn_input(kind, d)
+    p = E.parse_input(path)
+    assert p.dynamical_dt
+    pb = E.Problem(p, d)
+    dev = E.Context(pb)
+    dev.run()
+    os.environ["EDUS_DYN_HOST"] = "1"
+    try:
+        host = E.Context(pb)
+        host.run()
+    finally:
+        del os.environ["EDUS_DYN_HOST"]
+    # the device loop launches no host-side step: far fewer host calls, all captured
+    assert dev.last_timing()[1] > 0
+    it_d, t_d, dt_d = dev.clock()
+    it_h, t_h, dt_h = host.clock()
+    assert it_d == it_h
+    assert abs(t_d - t_h) <= 1e-9 * abs(t_h) and abs(dt_d - dt_h) <= 1e-9 * abs(dt_h)
+    gd, gh = dev.obs(), host.obs()
+    assert len(gd) == len(gh) > 0
+    np.testing.assert_allclose([x["t"] for x in gd], [x["t"] for x in gh], rtol=1e-9)
+    np.testing.assert_allclose([x["dt"] for x in gd], [x["dt"] for x in gh], rtol=1e-9)
+    assert rel([x["J1"] for x in gd], [x["J1"] for x in gh]) < 1e-9
+    assert np.abs(np.array([x["pop"] for x in gd]) - np.array([x["pop"] for x in gh])).max() < 1e-12
+    assert np.abs(dev.get_state() - host.get_state()).max() < 1e-10
+    od, oh = f"{d}/out_dev", f"{d}/out_host"
+    dev.write_outputs(od)
+    host.write_outputs(oh)
+    if kind in ("snapshots", "coulomb"):
+        td = [float(x) for x in open(f"{od}/t_Ek.txt").read().split()]
+        th = [float(x) for x in open(f"{oh}/t_Ek.txt").read().split()]
+        assert len(td) == len(th) > 0
+        np.testing.assert_allclose(td, th, rtol=1e-9)
+        names = sorted(f for f in os.listdir(oh) if f.startswith(("P_val", "P_cond", "Edia_")))
+        assert names and names == sorted(f for f in os.listdir(od) if f.startswith(("P_val", "P_cond", "Edia_")))
+        for f in names:
+            a, b = np.loadtxt(f"{od}/{f}"), np.loadtxt(f"{oh}/{f}")
+            assert np.all(np.abs(a - b) <= 1e-6 * np.abs(b) + 1e-12), f
+    # replay of the captured chunk after a reset
+    rho = dev.get_state()
+    dev.reset()
+    dev.run()
+    assert np.array_equal(dev.get_state(), rho)
+    assert dev.clock()[0] == it_d
+
+
 def test_wannier_8band_matches_oracle(workdir):
     ctx, o, g, lo = run_pair(W.wannier(workdir, n=16, t_fin_fs=1.0, it_res=5), workdir, 100)
     assert np.abs(ctx.get_state() - o.get("P0")).max() < RHO_TOL
