@@ -1696,10 +1696,8 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
       g.D = dD;
       g.err = c->d_err;
       if (batch::tc_vg_prepare(g, c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "velocity gauge: phase slices"));
-      // TMA-staged GEMM unless EDUS_TC_GEMM=cpasync selects the cp.async form (the two give
-      // bit-identical sums: every segment's FP32 sums are exact)
-      const char* form = std::getenv("EDUS_TC_GEMM");
-      if (!(form && std::string(form) == "cpasync")) batch::tc_vg_maps(g);
+      // TMA-staged GEMM unless EDUS_TC_GEMM=cpasync selects the cp.async form
+      if (batch::tc_gemm_tma_wanted()) batch::tc_vg_maps(g);
     }
     c->vg_t = P.t_start;
     if ((rc = vg_tables(c, P.t_start))) return bail(rc);

@@ -14,7 +14,10 @@
 // result is the FP64 sum to about 2^-32 of the terms, so the FP32 tables stored
 // from it equal those of the FP64 CUDA-core build up to the last rounding.
 //
-// GEMM kernel: one CTA (4 warps) per 128 x 32 tile of C. The 64-deep K slices
+// Two forms of the GEMM give the same sums bit for bit. k_tc_gemm_tma (the
+// default) moves 128 x 64 and 64 x 64 operand tiles by TMA into 128-byte
+// swizzled stages, four deep (below). k_tc_gemm (EDUS_TC_GEMM=cpasync): one
+// CTA (4 warps) per 128 x 32 tile of C. The 64-deep K slices
 // (128-byte rows of BF16) are staged with cp.async into two shared-memory
 // stages in the K-major canonical layout without swizzle (16-byte chunks of 8
 // BF16, 8-row core matrices 128 bytes apart, the two 16-byte halves of one
@@ -26,6 +29,9 @@
 // while the next one accumulates. All waits are bounded.
 #include <cuda.h>
 #include <stdint.h>
+
+#include <cstdlib>
+#include <cstring>
 
 #include "batch.cuh"
 #include "dev.cuh"
@@ -265,12 +271,15 @@ __global__ void k_diag64(const double* __restrict__ kpt, const double* __restric
 // ------------------------------------------------------------------ TMA-staged GEMM
 // The same exact-slice GEMM with its operand tiles moved by TMA
 // (cp.async.bulk.tensor.2d, no multicast; both tensor maps cover this GPU's
-// own buffers): one box of 8 BF16 (16 bytes) x rows per 16-byte K chunk, which
-// lands as rows x 16 bytes, the canonical no-swizzle K-major core matrices.
-// N tile 64, four shared-memory stages; thread 0 issues the loads of slice
-// s + 3 and the MMAs of slice s, so three slices are in flight while the
-// tensor core works. Every wait is bounded; on a timeout the block waits
-// (bounded) for its issued loads and MMAs, releases TMEM and ends.
+// own buffers) in the 128-byte swizzled K-major layout: one box of 64 BF16
+// (128 bytes) x 128 rows of A' and one of 64 x 64 rows of B' per 64-deep K
+// slice, each landing as 8-row x 128-byte swizzle atoms 1024 bytes apart; the
+// MMA descriptors address K step j of the slice at +32 j bytes inside the
+// atom. N tile 64, four shared-memory stages; thread 0 issues the MMAs of
+// slice s, then the loads of slice s + 3 once slice s - 1's MMAs have freed
+// their stage, so three slices are in flight while the tensor core works.
+// Every wait is bounded; on a timeout the block waits (bounded) for its issued
+// loads and MMAs, releases TMEM and ends.
 constexpr int TN2 = 64, kStages2 = 4;
 constexpr uint32_t kTmemCols2 = 64;
 constexpr uint32_t kIdesc2 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN2 >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
@@ -279,6 +288,19 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
   asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
                "l"(map), "r"(x), "r"(y), "r"(bar)
                : "memory");
+}
+
+// K-major operand in 128-byte swizzle atoms (8 rows x 128 bytes, 1024-byte
+// aligned, atoms 1024 bytes apart along M / N): stride byte offset 1024, the
+// leading offset unused (encoded 1), layout type 2 (128-byte swizzle)
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(1024u >> 4) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;  // 128-byte swizzle
+  return d;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) k_tc_gemm_tma(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
@@ -303,22 +325,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_gemm_tma(const __grid_consta
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = tmem_base;
-  const uint32_t base = (smem_u32(smem) + 1023u) & ~1023u;
+  const uint32_t base = (smem_u32(smem) + 1023u) & ~1023u;  // swizzle atoms need 1024-byte alignment
   const int S = Kp / TK, SEG = kseg / TK;
   double acc[TN2];
 #pragma unroll
   for (int c = 0; c < TN2; c++) acc[c] = 0.;
 
-  // slice s into stage b: 8 boxes of A (8 x 128) and 8 of B (8 x 64), chunk c at c * rows * 16
+  // slice s into stage b: one 64 x 128 box of A', one 64 x 64 box of B' (rows past M, N read as zero)
   auto issue_load = [&](int s, int b) {
     const uint32_t sa = base + (uint32_t)b * kStage, sb = sa + kStageA;
     mbar_expect_tx(&full[b], kStage);
-    const int k0 = s * TK;
-#pragma unroll
-    for (int c = 0; c < TK / 8; c++) {
-      tma_load_2d(sa + (uint32_t)(c * TM * 16), &mapA, k0 + 8 * c, m0, smem_u32(&full[b]));
-      tma_load_2d(sb + (uint32_t)(c * TN2 * 16), &mapB, k0 + 8 * c, n0, smem_u32(&full[b]));
-    }
+    tma_load_2d(sa, &mapA, s * TK, m0, smem_u32(&full[b]));
+    tma_load_2d(sb, &mapB, s * TK, n0, smem_u32(&full[b]));
   };
   auto readout = [&](int p) {
     asm volatile("tcgen05.fence::after_thread_sync;");
@@ -352,8 +370,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_gemm_tma(const __grid_consta
         const uint32_t dtm = tmem + (uint32_t)(((s / SEG) & 1) * kTmemCols2);
 #pragma unroll
         for (int j = 0; j < TK / 16; j++) {
-          const uint64_t da = smem_desc(sa + (uint32_t)(2 * j * TM * 16), TM * 16, 128);
-          const uint64_t db = smem_desc(sb + (uint32_t)(2 * j * TN2 * 16), TN2 * 16, 128);
+          // K step j: 16 BF16 = 32 bytes into every 128-byte swizzled row
+          const uint64_t da = sw128_desc(sa + (uint32_t)(32 * j));
+          const uint64_t db = sw128_desc(sb + (uint32_t)(32 * j));
           const uint32_t accum = (j > 0 || s % SEG != 0) ? 1u : 0u;
           asm volatile(
               "{\n\t.reg .pred p;\n\t"
@@ -458,18 +477,22 @@ size_t tc_gemm_smem() { return 2 * sizeof(uint16_t) * (TM + TN) * TK + 1024; }
 int tc_seg_k(int nr) { return ((2 * nr + TK - 1) / TK) * TK; }
 int tc_pad_k(int nr) { return kTcPairs * tc_seg_k(nr); }
 
+cudaError_t tc_gemm_run(const uint16_t* Aw, const uint16_t* Bw, double* Cw, int M, int ncols, int kpad, int kseg, int* err,
+                        const CUtensorMap* mapA, const CUtensorMap* mapB, cudaStream_t s);
+bool tc_gemm_tma_wanted();
+cudaError_t tc_gemm_maps(const uint16_t* Aw, const uint16_t* Bw, int M, int ncols, int kpad, CUtensorMap* mapA, CUtensorMap* mapB);
+
 cudaError_t tc_contract(const TcArgs& a, cudaStream_t s) {
   const int kpad = tc_pad_k(a.nr);
   const int ncols = 8 * a.ntri;
   k_phase_split<<<a.nk, 256, 0, s>>>(a.kpt, a.Rvec, a.nk, a.nr, tc_seg_k(a.nr), kpad, a.Aw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  // about 55 KB of shared memory per CTA keeps at most four CTAs (256 of the 512 TMEM columns) per SM
-  const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
-  if ((e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
-  dim3 grid((a.nk + TM - 1) / TM, (ncols + TN - 1) / TN);
-  k_tc_gemm<<<grid, kThreads, smem, s>>>(a.Aw, a.Bw, a.Cw, a.nk, ncols, kpad, tc_seg_k(a.nr), a.err);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  CUtensorMap mA, mB;
+  const bool tma = tc_gemm_tma_wanted() && tc_gemm_maps(a.Aw, a.Bw, a.nk, ncols, kpad, &mA, &mB) == cudaSuccess;
+  if ((e = tc_gemm_run(a.Aw, a.Bw, a.Cw, a.nk, ncols, kpad, tc_seg_k(a.nr), a.err, tma ? &mA : nullptr, tma ? &mB : nullptr, s)) !=
+      cudaSuccess)
+    return e;
   k_scatter<<<dim3((a.nk + 255) / 256, 4 * a.ntri), 256, 0, s>>>(a.Cw, a.nk, a.n, a.ntri, ncols, a.H32, a.D32);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   k_diag64<<<dim3((a.nk + 127) / 128, a.n), 128, 0, s>>>(a.kpt, a.Rvec, a.hdiagR, a.H32, a.nk, a.n, a.nr, a.Hdiag, a.Hused);
@@ -494,16 +517,17 @@ EncodeTiledFn encode_fn() {
   return fn;
 }
 
-// rows x Kp BF16 operand (K contiguous), boxes of 8 x box_rows; out-of-range rows read as zero
+// rows x Kp BF16 operand (K contiguous; Kp a multiple of 64), boxes of 64 x
+// box_rows in 128-byte swizzle atoms; out-of-range rows read as zero
 cudaError_t encode_operand(CUtensorMap* map, const uint16_t* ptr, int rows, int Kp, int box_rows) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return cudaErrorNotSupported;
   const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)Kp * sizeof(uint16_t)};
-  const cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  const cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1u, 1u};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
@@ -522,10 +546,40 @@ cudaError_t tc_vg_prepare(const TcVgArgs& a, cudaStream_t s) {
   return cudaFuncSetAttribute(k_tc_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_gemm_smem());
 }
 
+// The TMA form unless EDUS_TC_GEMM=cpasync selects the cp.async form (the two
+// give bit-identical sums: every segment's FP32 sums are exact).
+bool tc_gemm_tma_wanted() {
+  const char* form = std::getenv("EDUS_TC_GEMM");
+  return !(form && std::strcmp(form, "cpasync") == 0);
+}
+
+cudaError_t tc_gemm_maps(const uint16_t* Aw, const uint16_t* Bw, int M, int ncols, int kpad, CUtensorMap* mapA, CUtensorMap* mapB) {
+  cudaError_t e = encode_operand(mapA, Aw, M, kpad, TM);
+  if (e == cudaSuccess) e = encode_operand(mapB, Bw, ncols, kpad, TN2);
+  return e;
+}
+
+// C = A' B'^T over the slice-pair segments: the TMA form with the given tensor maps, else the cp.async form
+cudaError_t tc_gemm_run(const uint16_t* Aw, const uint16_t* Bw, double* Cw, int M, int ncols, int kpad, int kseg, int* err,
+                        const CUtensorMap* mapA, const CUtensorMap* mapB, cudaStream_t s) {
+  cudaError_t e;
+  if (mapA && mapB) {
+    if ((e = cudaFuncSetAttribute(k_tc_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_gemm_smem())) != cudaSuccess)
+      return e;
+    dim3 grid((M + TM - 1) / TM, (ncols + TN2 - 1) / TN2);
+    k_tc_gemm_tma<<<grid, kThreads, tma_gemm_smem(), s>>>(*mapA, *mapB, Cw, M, ncols, kpad, kseg, err);
+  } else {
+    // about 55 KB of shared memory per CTA keeps at most four CTAs (256 of the 512 TMEM columns) per SM
+    const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
+    if ((e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
+    dim3 grid((M + TM - 1) / TM, (ncols + TN - 1) / TN);
+    k_tc_gemm<<<grid, kThreads, smem, s>>>(Aw, Bw, Cw, M, ncols, kpad, kseg, err);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t tc_vg_maps(TcVgArgs& a) {
-  const int kpad = tc_pad_k(a.nr);
-  cudaError_t e = encode_operand(&a.mapA, a.Aw, a.nk, kpad, TM);
-  if (e == cudaSuccess) e = encode_operand(&a.mapB, a.Bw, 8 * a.ntri, kpad, TN2);
+  const cudaError_t e = tc_gemm_maps(a.Aw, a.Bw, a.nk, 8 * a.ntri, tc_pad_k(a.nr), &a.mapA, &a.mapB);
   a.tma = e == cudaSuccess;
   return e;
 }
@@ -536,15 +590,9 @@ cudaError_t tc_vg_stage(const TcVgArgs& a, cudaStream_t s) {
                                                                    a.nr, kseg, kpad, a.Bw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if (a.tma) {
-    dim3 grid((a.nk + TM - 1) / TM, (ncols + TN2 - 1) / TN2);
-    k_tc_gemm_tma<<<grid, kThreads, tma_gemm_smem(), s>>>(a.mapA, a.mapB, a.Cw, a.nk, ncols, kpad, kseg, a.err);
-  } else {
-    const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
-    dim3 grid((a.nk + TM - 1) / TM, (ncols + TN - 1) / TN);
-    k_tc_gemm<<<grid, kThreads, smem, s>>>(a.Aw, a.Bw, a.Cw, a.nk, ncols, kpad, kseg, a.err);
-  }
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = tc_gemm_run(a.Aw, a.Bw, a.Cw, a.nk, ncols, kpad, kseg, a.err, a.tma ? &a.mapA : nullptr, a.tma ? &a.mapB : nullptr, s)) !=
+      cudaSuccess)
+    return e;
   k_scatter64<<<dim3((a.nk + 255) / 256, 4 * a.ntri), 256, 0, s>>>(a.Cw, a.nk, a.n, a.ntri, ncols, a.H, a.D);
   return cudaGetLastError();
 }
