@@ -70,13 +70,6 @@ struct edus_ctx {
   bool diagb = false;
   double2 *d_pdiag = nullptr, *d_xw = nullptr;
   CoulDev cd{};
-  // Coulomb in the Wannier basis: the forward row transform as per-tile
-  // partials, written by the RHS kernel for the state it produces; valid for
-  // the buffer gpart_src (the next RHS's input) until something else writes it
-  double2* d_gpart = nullptr;
-  int gpart_kt = 0, gpart_slots = 0;
-  bool gpart_valid = false;
-  const double2* gpart_src = nullptr;
   void* d_part = nullptr;
   unsigned int* d_done = nullptr;
   int* d_err = nullptr;  // device error word set by bounded waits
@@ -252,11 +245,6 @@ int prof_mark(edus_ctx* c, int kind, bool begin) {
   return 0;
 }
 
-// blocks per column of the mode pass (h rows split between them): 480 blocks
-// for the 20 x 6 columns of a 3-band, Ncut = 20 problem, over three waves of
-// the 148 SMs' first block
-constexpr int kModeSplit = 4;
-
 int run_coulomb(edus_ctx* c, const double2* src) {
   if (!c->coul) return 0;
   int rc = prof_mark(c, 1, true);
@@ -268,14 +256,6 @@ int run_coulomb(edus_ctx* c, const double2* src) {
     CK(launch_coulomb(c->tb, c->cd, c->d_pdiag, c->d_h, nullptr, c->d_X0, c->stream));
     CK(launch_coulomb_xw(c->tb, c->d_cst, c->d_pdiag, c->d_xw, c->stream));
     c->launches += 4;
-  } else if (c->d_gpart) {
-    // the row pass was fused into the RHS launch that wrote src (else it runs here)
-    if (!(c->gpart_valid && c->gpart_src == src)) {
-      CK(launch_coulomb_part(c->tb, src, c->d_gpart, c->gpart_kt, c->gpart_slots, c->stream));
-      c->launches++;
-    }
-    CK(launch_coulomb_modes(c->tb, c->cd, c->d_gpart, c->gpart_kt, c->gpart_slots, c->d_h, c->d_X0, kModeSplit, c->stream));
-    c->launches++;
   } else {
     CK(launch_coulomb(c->tb, c->cd, src, c->d_h, nullptr, c->d_X0, c->stream));
     c->launches += 2;
@@ -292,21 +272,9 @@ int rhs(edus_ctx* c, StageArgs& a) {
   // from src and the older ring slots) to time the kernel back to back
   const bool idem = a.op == OP_PV || a.op == OP_AB || a.op == OP_TAYLOR;
   const int reps = (c->profiling && idem && a.dst != a.src) ? c->prof_reps : 1;
-  // the state this launch writes feeds the next RHS: its row transform rides along
-  const bool parts = c->d_gpart && a.op != OP_PV;
-  if (parts) {
-    a.gpart = c->d_gpart;
-    a.gpart_slots = c->gpart_slots;
-  }
   for (int r = 0; r < reps; r++) {
     CK(launch_rhs(c->tb, c->d_cst, a, c->stream));
     c->launches++;
-  }
-  if (parts) {
-    c->gpart_valid = true;
-    c->gpart_src = a.dst;
-  } else if (a.dst == c->gpart_src || a.acc == c->gpart_src) {
-    c->gpart_valid = false;
   }
   if ((rc = prof_mark(c, 0, false))) return rc;
   if (c->profiling) c->prof_pairs.back().reps = reps;
@@ -760,13 +728,6 @@ int run_dyn_device(edus_ctx* c) {
   memcpy(h.dt_prev, c->dt_prev, sizeof(h.dt_prev));
   h.snap_slot = -1;
   CK(cudaMemcpyAsync(c->d_dyn, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
-  if (c->d_gpart && !(c->gpart_valid && c->gpart_src == c->d_P0)) {
-    // the row-transform partials of the first step's input, outside the captured chunk
-    CK(launch_coulomb_part(c->tb, c->d_P0, c->d_gpart, c->gpart_kt, c->gpart_slots, c->stream));
-    c->launches++;
-    c->gpart_valid = true;
-    c->gpart_src = c->d_P0;
-  }
   CK(cudaStreamSynchronize(c->stream));
   *c->h_active = 1;
 
@@ -1855,13 +1816,6 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
     if (cudaMemcpyAsync(c->d_hr, dH, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
       return bail(fail(EDUS_ECUDA, "copy Hr"));
     if (coulomb_prepare(tb) != cudaSuccess) return bail(fail(EDUS_EUNSUPPORTED, "Coulomb tables exceed shared memory"));
-    if (!P.p.diag_basis) {
-      // per-tile partials of the row transform (tiles of the RHS kernel)
-      c->gpart_kt = rhs_tile_k(n);
-      c->gpart_slots = (c->gpart_kt + n2 - 2) / n2 + 1;
-      const size_t tiles = ((size_t)nk + c->gpart_kt - 1) / c->gpart_kt;
-      if ((rc = dalloc(c, &c->d_gpart, tiles * c->gpart_slots * 2 * nc * nt))) return bail(rc);
-    }
     const double2* eq = c->d_P0;
     if (P.p.diag_basis) {
       // the equilibrium state in the eigenbasis: 1 on the filled bands (main_MPI.cpp:291-304)
@@ -1911,7 +1865,6 @@ int edus_reset(edus_ctx* c) {
     c->d_P0 = c->P0_start;
     c->d_Pa = c->Pa_start;
   }
-  c->gpart_valid = false;
   CK(cudaMemcpyAsync(c->d_P0, c->d_Pinit, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
   if (c->d_ring) CK(cudaMemsetAsync(c->d_ring, 0, sizeof(double2) * c->order * c->plane, c->stream));
   CK(cudaMemsetAsync(c->d_ncond, 0, sizeof(double), c->stream));
@@ -1945,7 +1898,6 @@ int edus_reset(edus_ctx* c) {
 
 int edus_set_state(edus_ctx* c, const double* rho) {
   if (!c || !rho) return fail(EDUS_EINVAL, "null argument");
-  c->gpart_valid = false;
   return state_to_dev(c, rho, c->d_P0);
 }
 int edus_get_state(edus_ctx* c, double* rho) {
@@ -1955,7 +1907,6 @@ int edus_get_state(edus_ctx* c, double* rho) {
 int edus_slot_set(edus_ctx* c, int32_t slot, const double* rho) {
   double2* d = c ? slot_ptr(c, slot) : nullptr;
   if (!d || !rho) return fail(EDUS_EINVAL, "bad slot %d", slot);
-  c->gpart_valid = false;
   return state_to_dev(c, rho, d);
 }
 int edus_slot_get(edus_ctx* c, int32_t slot, double* rho) {
@@ -1966,7 +1917,6 @@ int edus_slot_get(edus_ctx* c, int32_t slot, double* rho) {
 int edus_slot_copy(edus_ctx* c, int32_t src, int32_t dst) {
   double2 *s = c ? slot_ptr(c, src) : nullptr, *d = c ? slot_ptr(c, dst) : nullptr;
   if (!s || !d) return fail(EDUS_EINVAL, "bad slot");
-  c->gpart_valid = false;
   CK(cudaMemcpyAsync(d, s, sizeof(double2) * c->plane, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return 0;
@@ -1998,7 +1948,6 @@ int edus_runge_kutta_ad(edus_ctx* c, int32_t src, int32_t dst, double dt) {
   double2 *s = c ? slot_ptr(c, src) : nullptr, *d = c ? slot_ptr(c, dst) : nullptr;
   if (!s || !d || src == EDUS_SLOT_PV || dst == EDUS_SLOT_PV) return fail(EDUS_EINVAL, "bad slot");
   CK(cudaSetDevice(c->device));
-  c->gpart_valid = false;
   CK(launch_axpy(s, c->d_Pb, dt, d, c->plane, c->stream));
   c->launches++;
   CK(cudaStreamSynchronize(c->stream));

@@ -195,11 +195,6 @@ struct StageArgs {
   // run has ended (dyn->active == 0)
   const DynStep* dyn;
   int dyn_stage, dyn_field;
-  // Coulomb (Wannier basis): when set, the launch also writes the forward row
-  // transform of the state it writes to dst, as per-block partial sums over
-  // its k tile: gpart[block][row part < gpart_slots][cos | sin][ncut][ntri]
-  double2* gpart;
-  int gpart_slots;
 };
 
 }  // namespace edus

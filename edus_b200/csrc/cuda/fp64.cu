@@ -79,33 +79,6 @@ __global__ void __launch_bounds__(kRowThreads) k_coul_rows(const double2* __rest
   }
 }
 
-// Row transform from a state in memory into per-tile partials, in the layout
-// and summation order of the RHS kernel's epilogue (k tiles of gkt points;
-// gpart[tile][row part][cos | sin][ncut][ntri]): the first RHS of a run, or
-// after the state was set from outside the loop.
-__global__ void k_coul_part(const double2* __restrict__ rho, int nk, int n2, int ntri, int ncut, int gkt, int gslots,
-                            const double* __restrict__ t2c, const double* __restrict__ t2s, double2* __restrict__ gpart) {
-  const int blk = blockIdx.x, k0 = blk * gkt, kend = min(k0 + gkt, nk), r0 = k0 / n2;
-  const int nslot = (kend - 1) / n2 - r0 + 1, nq = 2 * ncut;
-  pdl_wait();
-  for (int o = threadIdx.x; o < nslot * nq * ntri; o += blockDim.x) {
-    const int e = o % ntri, q = (o / ntri) % nq, sl = o / (ntri * nq);
-    const int row = r0 + sl;
-    const int qa = max(k0, row * n2) - k0, qb = min(kend, (row + 1) * n2) - k0;
-    const int cs = q / ncut, m = q - cs * ncut;
-    const double* tg = (cs ? t2s : t2c) + m * n2;
-    const int i2off = k0 - row * n2;
-    double ax = 0., ay = 0.;
-    for (int qq = qa; qq < qb; qq++) {
-      const double t = tg[qq + i2off];
-      const double2 v = rho[(size_t)e * nk + k0 + qq];
-      ax += v.x * t;
-      ay += v.y * t;
-    }
-    gpart[((size_t)blk * gslots + sl) * nq * ntri + q * ntri + e] = cmk(ax, ay);
-  }
-}
-
 constexpr int kModeThreads = 128;
 
 // One block per (n, e): f_xy(m,n,e) over m, X_xy = combine(A,B,C,D) - X0,
@@ -118,13 +91,8 @@ __global__ void __launch_bounds__(kModeThreads) k_coul_modes(const double2* __re
                                                              const double2* __restrict__ cD, const double2* __restrict__ X0,
                                                              const unsigned char* __restrict__ is_diag, double2* __restrict__ h,
                                                              double2* __restrict__ Xout, double2* __restrict__ fdiag,
-                                                             const int* __restrict__ diag_of, const double2* __restrict__ gpart,
-                                                             int gkt, int gslots, int n2) {
-  // gpart: the g column is summed from the RHS kernel's per-tile partials (in
-  // tile order) instead of read from g; blockIdx.z: this block's share of the
-  // h rows (every block of a column recomputes f and X, which is cheap)
+                                                             const int* __restrict__ diag_of) {
   const int n = blockIdx.x, e = blockIdx.y;
-  const bool lead = blockIdx.z == 0;
   extern __shared__ double2 sm[];
   double2* gc = sm;           // [2][n1] column of g for this (n, e)
   double2* f = gc + 2 * n1;   // [4][ncut]: cc, cs, sc, ss
@@ -140,29 +108,15 @@ __global__ void __launch_bounds__(kModeThreads) k_coul_modes(const double2* __re
   if (threadIdx.x == 0) {
     // the trig table does not depend on the previous kernel: in flight before the wait
     const uint32_t trig_bytes = ((uint32_t)(2 * ncut * ld * sizeof(double)) + 15u) & ~15u;
-    mbar_expect_tx(&bar, (gpart ? 0u : 2 * col_bytes) + trig_bytes);
+    mbar_expect_tx(&bar, 2 * col_bytes + trig_bytes);
     bulk_g2s(tc, t1P, trig_bytes, &bar);
   }
   pdl_wait();
-  if (gpart) {
-    const int nq = 2 * ncut;
-    for (int o = threadIdx.x; o < 2 * n1; o += kModeThreads) {
-      const int cs = o / n1, i1 = o - cs * n1;
-      const int q = cs * ncut + n;
-      const int b0 = (i1 * n2) / gkt, b1 = (i1 * n2 + n2 - 1) / gkt;
-      double2 acc = cz();
-      for (int b = b0; b <= b1; b++) {
-        const int sl = i1 - (b * gkt) / n2;
-        acc = cadd(acc, gpart[((size_t)b * gslots + sl) * nq * ntri + q * ntri + e]);
-      }
-      gc[o] = acc;
-    }
-  } else if (threadIdx.x == 0) {
+  if (threadIdx.x == 0) {
     bulk_g2s(gc, g + ((size_t)n * ntri + e) * n1, col_bytes, &bar);
     bulk_g2s(gc + n1, g + ((size_t)(ncut + n) * ntri + e) * n1, col_bytes, &bar);
   }
   mbar_wait(&bar, 0, err);
-  if (gpart) __syncthreads();
   for (int o = threadIdx.x; o < 4 * ncut; o += kModeThreads) {
     const int xy = o / ncut, m = o - xy * ncut;
     const double* t = (xy < 2 ? tc : ts) + (size_t)m * ld;
@@ -211,21 +165,18 @@ __global__ void __launch_bounds__(kModeThreads) k_coul_modes(const double2* __re
     X[1 * ncut + m] = xcs;
     X[2 * ncut + m] = xsc;
     X[3 * ncut + m] = xss;
-    if (Xout && lead) {
+    if (Xout) {
       Xout[(0 * ncut * ncut + mm) * ntri + e] = xcc;
       Xout[(1 * ncut * ncut + mm) * ntri + e] = xcs;
       Xout[(2 * ncut * ncut + mm) * ntri + e] = xsc;
       Xout[(3 * ncut * ncut + mm) * ntri + e] = xss;
     }
   }
-  if (n == 0 && dg && threadIdx.x == 0 && fdiag && lead) fdiag[diag_of[e]] = f[0];
+  if (n == 0 && dg && threadIdx.x == 0 && fdiag) fdiag[diag_of[e]] = f[0];
   __syncthreads();
   if (!h) return;
-  // this block's rows [ia, ib) of h
-  const int ia = (int)((long long)blockIdx.z * n1 / gridDim.z), ib = (int)((long long)(blockIdx.z + 1) * n1 / gridDim.z);
-  const int nr = ib - ia;
-  for (int o = threadIdx.x; o < 2 * nr; o += kModeThreads) {
-    const int cs = o / nr, i1 = ia + (o - cs * nr);
+  for (int o = threadIdx.x; o < 2 * n1; o += kModeThreads) {
+    const int cs = o / n1, i1 = o - cs * n1;
     double ax = 0, ay = 0;
     // cs = 0: sum_m X_cc c_m + X_sc s_m ; cs = 1: sum_m X_cs c_m + X_ss s_m
     const double2* Xc = X + (cs == 0 ? 0 : 1) * ncut;
@@ -491,21 +442,7 @@ cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2*
   return launch_pdl(k_coul_modes, grid, dim3(kModeThreads), coulomb_modes_smem(tb), s, (const double2*)c.g, tb.n1, tb.ntri,
                     tb.ncut, 1.0 / tb.nk, (const double*)c.t1P, tb.err, (const double2*)c.A, (const double2*)c.B,
                     (const double2*)c.C, (const double2*)c.D, X0, (const unsigned char*)c.is_diag, h, Xout, c.fdiag,
-                    (const int*)c.diag_of, (const double2*)nullptr, 1, 1, tb.n2);
-}
-
-cudaError_t launch_coulomb_part(const DevTables& tb, const double2* rho, double2* gpart, int gkt, int gslots, cudaStream_t s) {
-  return launch_pdl(k_coul_part, dim3((tb.nk + gkt - 1) / gkt), dim3(128), 0, s, rho, tb.nk, tb.n2, tb.ntri, tb.ncut, gkt, gslots,
-                    tb.t2c, tb.t2s, gpart);
-}
-
-cudaError_t launch_coulomb_modes(const DevTables& tb, const CoulDev& c, const double2* gpart, int gkt, int gslots, double2* h,
-                                 const double2* X0, int split, cudaStream_t s) {
-  dim3 grid(tb.ncut, tb.ntri, split);
-  return launch_pdl(k_coul_modes, grid, dim3(kModeThreads), coulomb_modes_smem(tb), s, (const double2*)c.g, tb.n1, tb.ntri,
-                    tb.ncut, 1.0 / tb.nk, (const double*)c.t1P, tb.err, (const double2*)c.A, (const double2*)c.B,
-                    (const double2*)c.C, (const double2*)c.D, X0, (const unsigned char*)c.is_diag, h, (double2*)nullptr, c.fdiag,
-                    (const int*)c.diag_of, gpart, gkt, gslots, tb.n2);
+                    (const int*)c.diag_of);
 }
 
 // Per-k snapshot: elements (ic, jc), (ic, ic) and (jc, jc) of the state in

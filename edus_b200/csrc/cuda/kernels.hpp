@@ -33,14 +33,6 @@ size_t coulomb_t2T_count(int n2, int ncut);
 size_t coulomb_t1P_count(int n1, int ncut);
 cudaError_t launch_coulomb(const DevTables& tb, const CoulDev& c, const double2* rho, double2* h, double2* Xout,
                            const double2* X0, cudaStream_t s);
-// The forward row transform as per-tile partials (the layout the RHS kernel's
-// epilogue writes, tiles of gkt k points), and the mode pass that sums them
-// (its h rows split over `split` blocks per column).
-cudaError_t launch_coulomb_part(const DevTables& tb, const double2* rho, double2* gpart, int gkt, int gslots, cudaStream_t s);
-cudaError_t launch_coulomb_modes(const DevTables& tb, const CoulDev& c, const double2* gpart, int gkt, int gslots, double2* h,
-                                 const double2* X0, int split, cudaStream_t s);
-// k points per tile (block) of the single-solve RHS kernel for n bands
-int rhs_tile_k(int n);
 // Elements (ic, jc), (ic, ic), (jc, jc) of rho in the eigenbasis of tb.U for
 // every k: out[3][nk].
 // With dyn (adaptive step on the device), out is the base of the snapshot

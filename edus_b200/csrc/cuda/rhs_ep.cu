@@ -200,7 +200,6 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
   __syncthreads();
 
   double dpmax = 0.;
-  double2 wout = cz();  // the value this thread writes to dst
   if (valid) {
     auto Pf = [&](int r, int c) -> double2 {
       return (r <= c) ? sP[TriEP<N>::idx(r, c)][kl] : cconj(sP[TriEP<N>::idx(c, r)][kl]);
@@ -251,14 +250,12 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
         if (a.ring) a.ring[(size_t)a.ring_idx[0] * NT * nk + o] = v;
         const double2 b0 = a.base[o];
         a.acc[o] = cadd(b0, cscale(v, c1));
-        wout = cadd(b0, cscale(v, c2));
-        a.dst[o] = wout;
+        a.dst[o] = cadd(b0, cscale(v, c2));
       } break;
       case OP_RK_MID: {
         const double2 b0 = a.base[o];
         a.acc[o] = cadd(a.acc[o], cscale(v, c1));
-        wout = cadd(b0, cscale(v, c2));
-        a.dst[o] = wout;
+        a.dst[o] = cadd(b0, cscale(v, c2));
       } break;
       case OP_RK_LAST: {
         const double2 nv = cadd(a.acc[o], cscale(v, c1));
@@ -267,7 +264,6 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
           dpmax = 2 * hypot(old.x - nv.x, old.y - nv.y) / (pcn + hypot(nv.x, nv.y) + 1.0e-7);
         }
         a.dst[o] = nv;
-        wout = nv;
       } break;
       case OP_AB: {
         a.ring[(size_t)a.ring_idx[0] * NT * nk + o] = v;
@@ -276,8 +272,7 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
           const double2 f = (s == 0) ? v : a.ring[(size_t)a.ring_idx[s] * NT * nk + o];
           d = cadd(d, cscale(f, a.coef[s]));
         }
-        wout = cadd(Pe, cscale(d, dtv));
-        a.dst[o] = wout;
+        a.dst[o] = cadd(Pe, cscale(d, dtv));
       } break;
       case OP_TAYLOR: {
         const int TO = a.order, m = TO - 1;
@@ -295,37 +290,7 @@ __global__ void __launch_bounds__(KT* TriEP<N>::NT) k_rhs_ep(DevTables tb, const
         if (a.maxdp && i == j)
           dpmax = 2 * hypot(Pe.x - nv.x, Pe.y - nv.y) / (pcn + hypot(nv.x, nv.y) + 1.0e-7);
         a.dst[o] = nv;
-        wout = nv;
       } break;
-    }
-  }
-  if (a.gpart) {
-    // forward row transform of the state written above, for the next RHS's
-    // Coulomb term: per row part of this tile, sum over its k points in k
-    // order of rho_e(k) t_q(i2) (k_coul_part does the same sums from memory)
-    __syncthreads();  // the exchange rows have been read
-    sP[e][kl] = wout;  // zero past nk
-    __syncthreads();
-    const int n2 = tb.n2, nc = tb.ncut, nq = 2 * nc;
-    const int kend = min(k0 + KT, nk), r0 = k0 / n2;
-    const int nslot = (kend - 1) / n2 - r0 + 1;
-    const double* ts = staged ? reinterpret_cast<const double*>(dyn + a.stage_rows * 2 * nc * NT) : nullptr;
-    const int tid = threadIdx.y * KT + threadIdx.x;
-    for (int o = tid; o < nslot * nq * NT; o += KT * NT) {
-      const int e2 = o % NT, q = (o / NT) % nq, sl = o / (NT * nq);
-      const int row = r0 + sl;
-      const int qa = max(k0, row * n2) - k0, qb = min(kend, (row + 1) * n2) - k0;
-      const int cs = q / nc, m = q - cs * nc;
-      const double* tg = (cs ? tb.t2s : tb.t2c) + m * n2;
-      const int i2off = k0 - row * n2;  // i2 of k0 + qq is qq + i2off
-      double ax = 0., ay = 0.;
-      for (int qq = qa; qq < qb; qq++) {
-        const double t = ts ? ts[q * KT + qq] : tg[qq + i2off];
-        const double2 v = sP[e2][qq];
-        ax += v.x * t;
-        ay += v.y * t;
-      }
-      a.gpart[((size_t)blockIdx.x * a.gpart_slots + sl) * nq * NT + q * NT + e2] = cmk(ax, ay);
     }
   }
   if (a.maxdp) {
@@ -355,8 +320,6 @@ static cudaError_t launch_ep(const DevTables& tb, const DevConsts* cst, const St
   if (a.dyn) return launch_pdl(k_rhs_ep<N, KT, true>, dim3((tb.nk + KT - 1) / KT), block, dyn, s, tb, cst, b);
   return launch_pdl(k_rhs_ep<N, KT, false>, dim3((tb.nk + KT - 1) / KT), block, dyn, s, tb, cst, b);
 }
-
-int rhs_tile_k(int n) { return n == 16 ? 4 : n == 8 ? 16 : 32; }
 
 cudaError_t launch_rhs(const DevTables& tb, const DevConsts* cst, const StageArgs& a, cudaStream_t s) {
   switch (tb.n) {

@@ -3,8 +3,10 @@
 Single solve (edus_create / edus_step):
   python -m edus_b200.profile_run --workload hbn_coulomb --steps 60 [--graph] [--n 120]
     hbn_rk4 (hBN RK4 60x60), hbn_coulomb (hBN + Coulomb AB4 120x120), wannier8
-    (8-band Wannier RK4 96x96). Eager launches by default so that ncu sees each kernel;
-    --graph replays the captured CUDA graph of the whole loop instead.
+    (8-band Wannier RK4 96x96), wannier8_vg (the same in the velocity gauge;
+    --precision mixed contracts every stage on the tensor cores). Eager
+    launches by default so that ncu sees each kernel; --graph replays the
+    captured CUDA graph of the whole loop instead.
 
 Batch (edus_batch_*):
   python -m edus_b200.profile_run --batch wannier8 --instances 2 --precision fp64 \\
@@ -31,6 +33,13 @@ def make(name, workdir, n=None):
         return W.hbn_coulomb(workdir, n=n or 120)
     if name == "wannier8":
         return W.wannier(workdir, n=n or 96)
+    if name == "wannier8_vg":
+        path = W.wannier(workdir, n=n or 96)
+        with open(path) as f:
+            txt = f.read().replace("Wannier\n", "Wannier\nvelocity_gauge\n")
+        with open(path, "w") as f:
+            f.write(txt)
+        return path
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -87,7 +96,8 @@ def main():
               f"{(s1['device_ms'] - s0['device_ms']) / a.steps * 1e3:.1f} us per step")
         return
     p = E.parse_input(make(a.workload, d, a.n))
-    ctx = E.Context(E.Problem(p, d), use_graphs=a.graph)
+    prec = abi.EDUS_PREC_MIXED if a.precision == "mixed" else abi.EDUS_PREC_FP64
+    ctx = E.Context(E.Problem(p, d), use_graphs=a.graph, precision=prec)
     if a.graph:
         ctx.run()
         ctx.reset()
