@@ -135,6 +135,7 @@ class Obs(C.Structure):
         ("p_min", C.c_double),
         ("n_cond", C.c_double),
         ("dt", C.c_double),
+        ("pol", C.c_double * 6),
     ]
 
 
@@ -187,6 +188,7 @@ def obs_to_dict(o, ncv):
         "p_min": o.p_min,
         "n_cond": o.n_cond,
         "dt": o.dt,
+        "pol": np.array(o.pol[0::2]) + 1j * np.array(o.pol[1::2]),
     }
 
 

@@ -2089,6 +2089,9 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
     std::ofstream(d + "/Jintra.txt");
   }
   if (c->P.p.tabs) ft.open(d + "/TransientAbs.txt");
+  // extension (no reference counterpart): polarisation per cell (1/Nk) sum_k Tr(D_x rho),
+  // complex x, y, z, in J1.txt's column format
+  std::ofstream fp(d + "/Polarization.txt");
   // k-resolved transient absorption: one file per TAbsK point, opened and left
   // empty as the reference leaves it (Source_Main/open_files.cpp:43-55)
   for (int i = 0; c->P.p.tabs_k && i < c->P.p.n_tabs_k; i++) {
@@ -2097,7 +2100,7 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
     std::ofstream fk(name.str());
     if (!fk) return fail(EDUS_EIO, "cannot write %s", name.str().c_str());
   }
-  if (!fe || !fl) return fail(EDUS_EIO, "cannot write into %s", outdir);
+  if (!fe || !fl || !fp) return fail(EDUS_EIO, "cannot write into %s", outdir);
   const int ncv = c->n;
   for (const edus_obs& o : log) {
     const double tfs = o.t * kTimeAuFs;
@@ -2108,6 +2111,12 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
     for (int i = 0; i < ncv; i++) fl << std::setprecision(16) << o.pop[i] << "   ";
     fl << std::endl;
     fx << std::endl;
+    fp << std::setw(15) << std::setprecision(8) << tfs;
+    for (int x = 0; x < 3; x++) {
+      fp << std::setw(25) << std::setprecision(15) << std::scientific << o.pol[2 * x];
+      fp << std::setw(25) << std::setprecision(15) << std::scientific << o.pol[2 * x + 1];
+    }
+    fp << std::defaultfloat << std::endl;
     if (c->P.p.current) {
       f1 << std::setw(15) << std::setprecision(8) << tfs;
       for (int x = 0; x < 3; x++) {
@@ -2142,9 +2151,9 @@ int edus_write_outputs(edus_ctx* c, const char* outdir) {
 namespace {
 
 // Up to 4096 per-block partials of the observable reduction, i.e. up to
-// 4096 * 128 = 524 288 k points; 320 bytes per partial (the record is 288).
+// 4096 * 128 = 524 288 k points; 384 bytes per partial (the partial is 336).
 constexpr int kStaticObsParts = 4096;
-constexpr size_t kStaticPartBytes = 320;
+constexpr size_t kStaticPartBytes = 384;
 constexpr size_t kStaticDoneOff = (size_t)kStaticObsParts * kStaticPartBytes;  // 256-aligned
 constexpr size_t kStaticRecOff = kStaticDoneOff + 256;
 constexpr size_t kStaticScratchBytes = kStaticRecOff + 512;

@@ -38,10 +38,10 @@ __device__ __forceinline__ To ocvt(From a) {
 
 // Tile partials are stored field-major: part[f][tile], f = 0..kPartF-1:
 // populations 0..kMaxBands-1, then for x = 0..2 (J1 re, J1 im, J2 re, J2 im,
-// TA re, TA im), then max |P - P_eq| and min P.
-constexpr int kPartF = kMaxBands + 20;
+// TA re, TA im, polarisation re, im), then max |P - P_eq| and min P.
+constexpr int kAccF = 26;                 // fields after the populations
+constexpr int kPartF = kMaxBands + kAccF;
 constexpr int kFJ = kMaxBands;            // first current field
-constexpr int kFMax = kMaxBands + 18, kFMin = kMaxBands + 19;
 
 __device__ __forceinline__ double warp_sum(double x) {
   for (int s = 16; s > 0; s >>= 1) x += __shfl_xor_sync(0xffffffffu, x, s);
@@ -59,22 +59,22 @@ __device__ __forceinline__ double warp_min(double x) {
 // What one thread accumulates over the k points of a tile.
 struct Acc {
   double pop;                 // thread (k, c), c < N: band c
-  double2 J1[3], J2[3], TA[3];
+  double2 J1[3], J2[3], TA[3], PL[3];
   double pmax, pmin;
 };
 
-// Value v (0 .. N+19) of a thread's accumulator in the flat field order; pop
+// Value v (0 .. N+25) of a thread's accumulator in the flat field order; pop
 // values sit at their band c = q.
 template <int N>
 __device__ __forceinline__ double acc_val(const Acc& a, int v, int q) {
   if (v < N) return q == v ? a.pop : 0.;
   const int r = v - N;
-  if (r < 18) {
-    const int x = r / 6, m = r % 6;
-    const double2 z = m < 2 ? a.J1[x] : (m < 4 ? a.J2[x] : a.TA[x]);
+  if (r < 24) {
+    const int x = r / 8, m = r % 8;
+    const double2 z = m < 2 ? a.J1[x] : (m < 4 ? a.J2[x] : (m < 6 ? a.TA[x] : a.PL[x]));
     return (m & 1) ? z.y : z.x;
   }
-  return r == 18 ? a.pmax : a.pmin;
+  return r == 24 ? a.pmax : a.pmin;
 }
 template <int N>
 __host__ __device__ constexpr int field_of(int v) { return v < N ? v : kFJ + (v - N); }
@@ -83,21 +83,21 @@ __host__ __device__ constexpr int field_of(int v) { return v < N ? v : kFJ + (v 
 // order (warp butterflies, then warps in index order); field f of the tile
 // goes to part[f * stride + t].
 template <int N, int NW>
-__device__ __forceinline__ void tile_reduce(const Acc& a, int q, double (*sW)[N + 20], double* part, size_t stride, int t) {
+__device__ __forceinline__ void tile_reduce(const Acc& a, int q, double (*sW)[N + kAccF], double* part, size_t stride, int t) {
   const int lane = threadIdx.x % 32, w = threadIdx.x / 32;
 #pragma unroll
-  for (int v = 0; v < N + 20; v++) {
+  for (int v = 0; v < N + kAccF; v++) {
     const double x = acc_val<N>(a, v, q);
-    const double r = v == N + 18 ? warp_max(x) : (v == N + 19 ? warp_min(x) : warp_sum(x));
+    const double r = v == N + 24 ? warp_max(x) : (v == N + 25 ? warp_min(x) : warp_sum(x));
     if (lane == 0) sW[w][v] = r;
   }
   __syncthreads();
   const int v = threadIdx.x;
-  if (v < N + 20) {
-    double r = v == N + 19 ? 1.0 : 0.;
+  if (v < N + kAccF) {
+    double r = v == N + 25 ? 1.0 : 0.;
     for (int ww = 0; ww < NW; ww++) {
       const double y = sW[ww][v];
-      r = v == N + 18 ? fmax(r, y) : (v == N + 19 ? fmin(r, y) : r + y);
+      r = v == N + 24 ? fmax(r, y) : (v == N + 25 ? fmin(r, y) : r + y);
     }
     part[(size_t)field_of<N>(v) * stride + t] = r;
   }
@@ -125,8 +125,8 @@ __global__ void __launch_bounds__(opad32(ObsK<N>::v* N* N), 3) k_bobs(View v, in
   __shared__ double2 sD[3][NN][KO];
   __shared__ double2 sU[NN][KO];
   __shared__ double sTerm[NN][KO];  // population terms
-  __shared__ double sW[NW][N + 20];
-  __shared__ double sT[N + 20];  // the instance's totals (last tile)
+  __shared__ double sW[NW][N + kAccF];
+  __shared__ double sT[N + kAccF];  // the instance's totals (last tile)
   __shared__ int sScan[NTHR];
   __shared__ bool sLast;
   extern __shared__ int sPre[];  // [ninst + 1] first due tile of each instance
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(opad32(ObsK<N>::v* N* N), 3) k_bobs(View v, in
     const bool cur = I->want_current, tabs = I->want_tabs;
     Acc my;
     my.pop = 0.;
-    for (int x = 0; x < 3; x++) my.J1[x] = my.J2[x] = my.TA[x] = cz();
+    for (int x = 0; x < 3; x++) my.J1[x] = my.J2[x] = my.TA[x] = my.PL[x] = cz();
     my.pmax = 0.;
     my.pmin = 1.;
     constexpr int UK = ObsUnit<N>::v;
@@ -236,6 +236,8 @@ __global__ void __launch_bounds__(opad32(ObsK<N>::v* N* N), 3) k_bobs(View v, in
           if (tabs && b < nch && l >= nch)
             for (int x = 0; x < 3; x++) my.TA[x] = csub(my.TA[x], cmul(cscale(sD[x][q][kl], 2.), pe));
         }
+        // polarisation: Tr(D_x rho) = sum_bl D^x_bl P_bl (P_bl = rho_lb), this thread's entry
+        for (int x = 0; x < 3; x++) my.PL[x] = cadd(my.PL[x], cmul(sD[x][q][kl], sP[q][kl]));
         if (cur) {
           // Q_bl = sum_a P_ab H_al; J2_x += Q_bl conj(D^x_bl)
           double2 Q = cz();
@@ -282,14 +284,14 @@ __global__ void __launch_bounds__(opad32(ObsK<N>::v* N* N), 3) k_bobs(View v, in
       // other blocks are read past L1
       __threadfence();
       const int lane = tid % 32, wid = tid / 32;
-      for (int v = wid; v < N + 20; v += NW) {
+      for (int v = wid; v < N + kAccF; v += NW) {
         const double* row = part + (size_t)field_of<N>(v) * stride;
-        double r = v == N + 19 ? 1.0 : 0.;
+        double r = v == N + 25 ? 1.0 : 0.;
         for (int x = lane; x < nunits; x += 32) {
           const double y = __ldcg(row + x);
-          r = v == N + 18 ? fmax(r, y) : (v == N + 19 ? fmin(r, y) : r + y);
+          r = v == N + 24 ? fmax(r, y) : (v == N + 25 ? fmin(r, y) : r + y);
         }
-        r = v == N + 18 ? warp_max(r) : (v == N + 19 ? warp_min(r) : warp_sum(r));
+        r = v == N + 24 ? warp_max(r) : (v == N + 25 ? warp_min(r) : warp_sum(r));
         if (lane == 0) sT[v] = r;
       }
       __syncthreads();
@@ -313,16 +315,18 @@ __global__ void __launch_bounds__(opad32(ObsK<N>::v* N* N), 3) k_bobs(View v, in
           if (val > ncd) ncd = val;
         }
         for (int x = 0; x < 3; x++) {
-          const double* f = sT + N + 6 * x;  // J1 re, im, J2 re, im, TA re, im
+          const double* f = sT + N + 8 * x;  // J1 re, im, J2 re, im, TA re, im, polarisation re, im
           rec.J1[2 * x] = f[0] * I->scaleJ;
           rec.J1[2 * x + 1] = f[1] * I->scaleJ;
           rec.J2[x] = -2. * (f[3] * I->scaleJ);
           rec.tabs[2 * x] = f[4] * I->scaleTA * inv;
           rec.tabs[2 * x + 1] = f[5] * I->scaleTA * inv;
+          rec.pol[2 * x] = f[6] * inv;
+          rec.pol[2 * x + 1] = f[7] * inv;
         }
         rec.trace_dev = trace;
-        rec.p_cond_max = sT[N + 18];
-        rec.p_min = sT[N + 19];
+        rec.p_cond_max = sT[N + 24];
+        rec.p_min = sT[N + 25];
         rec.n_cond = ncd;
         I->log[it / I->res] = rec;
         *I->done = 0u;

@@ -194,13 +194,13 @@ __global__ void __launch_bounds__(kModeThreads) k_coul_modes(const double2* __re
 
 struct ObsPart {
   double pop[kMaxBands];
-  double2 J1[3], J2[3], TA[3];
+  double2 J1[3], J2[3], TA[3], PL[3];
   double pmax, pmin;
 };
 
 __device__ __forceinline__ void obs_zero(ObsPart& p) {
   for (int i = 0; i < kMaxBands; i++) p.pop[i] = 0;
-  for (int x = 0; x < 3; x++) p.J1[x] = p.J2[x] = p.TA[x] = cz();
+  for (int x = 0; x < 3; x++) p.J1[x] = p.J2[x] = p.TA[x] = p.PL[x] = cz();
   p.pmax = 0;
   p.pmin = 1.0;
 }
@@ -210,6 +210,7 @@ __device__ __forceinline__ void obs_add(ObsPart& d, const ObsPart& o, int n) {
     d.J1[x] = cadd(d.J1[x], o.J1[x]);
     d.J2[x] = cadd(d.J2[x], o.J2[x]);
     d.TA[x] = cadd(d.TA[x], o.TA[x]);
+    d.PL[x] = cadd(d.PL[x], o.PL[x]);
   }
   d.pmax = fmax(d.pmax, o.pmax);
   d.pmin = fmin(d.pmin, o.pmin);
@@ -339,6 +340,21 @@ __global__ void __launch_bounds__(kObsThreads) k_obs(DevTables tb, const DevCons
           }
         }
     }
+    // polarisation: Tr(D_x rho) = sum_ij D_x,ij P_ij in the reference's P[k][i][j] = rho_ji
+    // convention (lower D entries: D_ji = D_ij, or conj(D_ij) for Hermitian dipoles)
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        const int lo = i < j ? i : j, hi = i < j ? j : i;
+        const bool cj = tb.herm_dip && i > j;
+        const double2 pij = Pf(i, j);
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+          const double2 ds = tb.D[(size_t)(x * NT + Tri<N>::idx(lo, hi)) * nk + k];
+          my.PL[x] = cadd(my.PL[x], cmul(cj ? cconj(ds) : ds, pij));
+        }
+      }
     if (a.want_tabs)
       for (int i = 0; i < tb.nch; i++)
         for (int j = tb.nch; j < N; j++) {
@@ -402,6 +418,8 @@ __global__ void __launch_bounds__(kObsThreads) k_obs(DevTables tb, const DevCons
     rec.J2[x] = -2. * (T.J2[x].y * a.scaleJ);
     rec.tabs[2 * x] = T.TA[x].x * a.scaleTA * inv;
     rec.tabs[2 * x + 1] = T.TA[x].y * a.scaleTA * inv;
+    rec.pol[2 * x] = T.PL[x].x * inv;
+    rec.pol[2 * x + 1] = T.PL[x].y * inv;
   }
   rec.trace_dev = trace;
   rec.p_cond_max = T.pmax;

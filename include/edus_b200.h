@@ -152,6 +152,8 @@ typedef struct {
   double p_min;                  /* Coulomb_set.P_min */
   double n_cond;
   double dt;                     /* step used after this instant (adaptive dt) */
+  double pol[6];                 /* extension: polarisation per cell, complex (1/Nk) sum_k Tr(D_x rho(k)),
+                                    x,y,z (re, im), a.u.; the reference has no such output */
 } edus_obs;
 
 /* ------------------------------------------------------- input.txt layer */

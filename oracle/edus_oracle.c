@@ -1764,6 +1764,7 @@ static void observables(orc* o, const cplx* P, edus_obs* ob) {
   cplx* j1p = calloc((size_t)nth * 3, sizeof(cplx));
   cplx* j2p = calloc((size_t)nth * 3, sizeof(cplx));
   cplx* tap = calloc((size_t)nth * 3, sizeof(cplx));
+  cplx* plp = calloc((size_t)nth * 3, sizeof(cplx));
   for (int t = 0; t < nth; t++) pmin[t] = 1.0;
   if (o->p.coulomb && o->p.current) gradient_energy_renorm(o, o->Hr);
   if (o->vg && o->p.current) gradient_energy_renorm(o, o->H);
@@ -1800,6 +1801,11 @@ static void observables(orc* o, const cplx* P, edus_obs* ob) {
           if (Pik < pmin[t]) pmin[t] = Pik;
         }
       }
+      /* polarisation (an extension, no reference counterpart): Tr(D_x rho) =
+         sum_ij D_x,ij P_ij with P[k][i][j] = rho_ji */
+      for (int ic = 0; ic < n; ic++)
+        for (int jc = 0; jc < n; jc++)
+          for (int x = 0; x < 3; x++) plp[t * 3 + x] += o->D[IDX4(ik, ic, jc, x, n)] * Pk[ic * n + jc];
       if (o->p.current) {
         for (int ic = 0; ic < n; ic++)
           for (int jc = 0; jc < n; jc++)
@@ -1821,7 +1827,7 @@ static void observables(orc* o, const cplx* P, edus_obs* ob) {
   double nktot_inv = 1. / nk;
   double popg[EDUS_MAX_BANDS];
   double pmx = 0, pmn = 1.0;
-  cplx J1[3] = {0, 0, 0}, J2[3] = {0, 0, 0}, TA[3] = {0, 0, 0};
+  cplx J1[3] = {0, 0, 0}, J2[3] = {0, 0, 0}, TA[3] = {0, 0, 0}, PL[3] = {0, 0, 0};
   for (int ic = 0; ic < n; ic++) popg[ic] = 0;
   for (int t = 0; t < nth; t++) {
     if (pmx < pmax[t]) pmx = pmax[t];
@@ -1830,6 +1836,7 @@ static void observables(orc* o, const cplx* P, edus_obs* ob) {
     for (int x = 0; x < 3; x++) {
       J1[x] += j1p[t * 3 + x];
       J2[x] += j2p[t * 3 + x];
+      PL[x] += plp[t * 3 + x];
     }
   }
   for (int x = 0; x < 3; x++) TA[x] = tap[x];
@@ -1856,7 +1863,10 @@ static void observables(orc* o, const cplx* P, edus_obs* ob) {
     cplx ta = TA[x] * (fabs(o->jac) * o->dk[0] * o->dk[1] * o->dk[2]);
     ob->tabs[2 * x] = creal(ta) / nk;
     ob->tabs[2 * x + 1] = cimag(ta) / nk;
+    ob->pol[2 * x] = creal(PL[x]) / nk;
+    ob->pol[2 * x + 1] = cimag(PL[x]) / nk;
   }
+  free(plp);
   free(popp);
   free(pmax);
   free(pmin);

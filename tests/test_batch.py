@@ -70,6 +70,8 @@ def test_fp64_batch_matches_single_solves(workdir):
         assert rel(J2b, J2s) < 1e-10
         pg, po = np.array([x["pop"] for x in lb]), np.array([x["pop"] for x in log])
         assert np.abs(pg - po).max() < 1e-14
+        Pb, Ps = np.array([x["pol"] for x in lb]), np.array([x["pol"] for x in log])
+        assert np.abs(Pb - Ps).max() < 1e-13 * max(np.abs(Ps).max(), 1.0)
     st = b.stats()
     assert st["done"] == len(slots) and st["kpoint_steps"] > 0 and st["device_ms"] > 0
 

@@ -50,6 +50,9 @@ def check_logs(g, o, pop_abs=2e-15, j2_abs=0.0):
     assert np.abs(J2g - J2o).max() <= 1e-9 * max(np.abs(J2o).max(), 1e-20) + j2_abs
     pg, po = np.array([x["pop"] for x in g]), np.array([x["pop"] for x in o])
     assert np.abs(pg - po).max() <= pop_abs
+    # polarisation per cell, (1/Nk) sum_k Tr(D rho): an O(1) sum, held like the populations
+    Pg, Po = np.array([x["pol"] for x in g]), np.array([x["pol"] for x in o])
+    assert np.abs(Pg - Po).max() <= 1e-13 * max(np.abs(Po).max(), 1.0)
 
 
 def test_rhs_matches_oracle():

@@ -88,3 +88,24 @@ def test_oracle_coulomb_equilibrium_is_stationary(workdir, diag):
     hk = o.coulomb_hk(o.get("P0"))
     assert np.array_equal(hk, np.conj(np.transpose(hk, (0, 2, 1))))
     assert abs(log[-1]["trace_dev"]) < 1e-12
+
+
+def test_oracle_polarisation_is_tr_d_rho(workdir):
+    """The polarisation record (1/Nk) sum_k Tr(D_x rho(k)) (an output the
+    reference does not have) against numpy on the oracle's own state and dipole
+    tables, at the start and after 30 RK4 steps inside the pulse; the dipoles
+    of the reference's models are real symmetric and rho is Hermitian, so the
+    trace is real."""
+    from edus_b200 import workloads as W
+
+    p = E.parse_input(W.hbn_rk4(workdir, n=12, t_fin_fs=1.0, it_res=10, field=0.5))
+    o = Oracle(p, workdir)
+    D = o.get("D")  # [k][i][j][x]
+    for steps in (0, 30):
+        if steps:
+            o.run(steps)
+        P = o.get("P0")
+        rec = o.observables(P)
+        want = np.einsum("kijx,kij->x", D, P) / P.shape[0]
+        np.testing.assert_allclose(rec["pol"], want, rtol=1e-12, atol=1e-15)
+        assert np.abs(np.imag(rec["pol"])).max() < 1e-14
