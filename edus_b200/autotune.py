@@ -20,15 +20,15 @@ from edus_b200 import abi
 from edus_b200 import workloads as W
 
 # built variants per band count: (tile length, register profile); profile 2
-# is the matrix-product form (FP64), profiles 3 and 4 the staged forms
-# (mixed; 4 with the register-blocked commutator)
+# is the matrix-product form (FP64), profiles 3-5 the staged forms (mixed; 4
+# and 5 with the register-blocked commutator, 2 x 2 and 2 x 1 blocks)
 VARIANTS = {
     2: [(16, 0), (16, 1), (32, 0), (32, 1), (32, 3)],
     3: [(16, 0), (16, 1), (32, 0), (32, 1), (32, 3)],
     4: [(16, 0), (16, 1), (16, 3)],
     5: [(16, 0), (16, 1), (16, 3)],
-    8: [(4, 0), (8, 0), (8, 1), (8, 2), (16, 2), (8, 3), (8, 4), (16, 4)],
-    16: [(2, 0), (2, 1), (2, 2), (4, 2), (8, 2), (2, 3), (2, 4), (4, 4)],
+    8: [(4, 0), (8, 0), (8, 1), (8, 2), (16, 2), (8, 3), (8, 4), (16, 4), (8, 5), (16, 5)],
+    16: [(2, 0), (2, 1), (2, 2), (4, 2), (8, 2), (2, 3), (2, 4), (4, 4), (2, 5), (4, 5)],
 }
 PREC = {"fp64": abi.EDUS_PREC_FP64, "mixed": abi.EDUS_PREC_MIXED}
 

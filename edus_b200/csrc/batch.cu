@@ -147,6 +147,10 @@ Layout layout_of(const edus_batch* b, const Problem& P, int kt) {
   return L;
 }
 
+// commutator form of the staged kernel for register profile 3, 4, 5:
+// element-parallel, register blocks of C of 2 x 2, of 2 x 1
+int pipe_cb(int prof) { return prof == 5 ? 2 : (prof == 4 ? 1 : 0); }
+
 // register profile / kernel form of a band count; the matrix-product form is built for FP64 only
 int profile_of(const edus_batch* b, int n) {
   const int p = (n >= 0 && n <= EDUS_MAX_BANDS) ? b->opt.regs_profile[n] : 0;
@@ -160,8 +164,8 @@ int profile_of(const edus_batch* b, int n) {
 // the staging sizes of profiles 3 and 4 (at least one slot each).
 int form_of(const edus_batch* b, const ClassTab& c, int& psel, int& pcomp) {
   psel = pcomp = 1;
-  if (c.occ != 3 && c.occ != 4) return c.occ;
-  if (!pipe_supported(c.n, c.kt, c.occ == 4)) return 0;
+  if (c.occ < 3 || c.occ > 5) return c.occ;
+  if (!pipe_supported(c.n, c.kt, pipe_cb(c.occ))) return 0;
   for (const Slot& s : b->slots) {
     if (s.status != EDUS_INST_RUNNING || s.n != c.n) continue;
     const Inst& I = s.inst;
@@ -176,7 +180,8 @@ int grid_of(const edus_batch* b, const ClassTab& c) {
   switch (c.form) {
     case 2: return stage_grid_mm(c.n, c.kt, cmix(b, c.n));
     case 3:
-    case 4: return stage_grid_pipe(c.n, c.kt, c.form == 4, c.psel, c.pcomp);
+    case 4:
+    case 5: return stage_grid_pipe(c.n, c.kt, pipe_cb(c.form), c.psel, c.pcomp);
     default: return stage_grid(c.n, c.kt, c.form ? 1 : 0, cmix(b, c.n));
   }
 }
@@ -195,7 +200,7 @@ int check_problem(const edus_batch* b, const Problem& P) {
   const int prof = profile_of(b, n), kt = tile_len(b, n);
   // the staged forms also run tile lengths the element-parallel form is not built for
   // (their instances must then be on a lattice stencil, checked at admission)
-  const bool ok = prof == 2 ? mm_supported(n, kt) : (class_supported(n, kt) || (prof >= 3 && pipe_supported(n, kt, prof == 4)));
+  const bool ok = prof == 2 ? mm_supported(n, kt) : (class_supported(n, kt) || (prof >= 3 && pipe_supported(n, kt, pipe_cb(prof))));
   if (!ok)
     return fail(EDUS_EUNSUPPORTED, "batch: %d bands with %d k points per tile (profile %d) is not built", n, tile_len(b, n),
                 profile_of(b, n));
@@ -666,8 +671,8 @@ int record_chunk(edus_batch* b, LaunchTimer* tm = nullptr) {
         ClassTab& c = kv.second;
         View v{b->d_insts, {b->d_it[0], b->d_it[1]}, c.d_tiles, c.d_ntiles, c.d_cinst, c.d_ntiles + 1};
         if (tm) BCK(tm->begin(c.n, 1 + st, b->stream));
-        if (c.form == 3 || c.form == 4)
-          BCK(launch_stage_pipe(c.n, c.kt, c.form == 4, v, st, parity, c.psel, c.pcomp, c.sgrid, b->stream));
+        if (c.form >= 3 && c.form <= 5)
+          BCK(launch_stage_pipe(c.n, c.kt, pipe_cb(c.form), v, st, parity, c.psel, c.pcomp, c.sgrid, b->stream));
         else if (c.form == 2)
           BCK(launch_stage_mm(c.n, c.kt, cmix(b, c.n), v, st, parity, c.sgrid, b->stream));
         else

@@ -254,11 +254,13 @@ __device__ __forceinline__ void pipe_issue(const PipeCarve<N, KT>& S, const Pipe
 }
 
 // Register blocks of the blocked commutator (C = P H~^T, BR x BC entries of C
-// per thread and k point): 2 x 2 (for 16 bands measured 5 % faster than 4 x 2:
-// more threads share the phase).
-template <int N>
+// per thread and k point): CB 1, 2 x 2 (for 16 bands measured 5 % faster than
+// 4 x 2: more threads share the phase); CB 2, 2 x 1 (twice the threads again,
+// about all of the block's). Every entry of C is the same sum over l in l
+// order in every blocking.
+template <int N, int CB>
 struct CBlk {
-  static constexpr int BR = 2, BC = 2;
+  static constexpr int BR = 2, BC = CB == 2 ? 1 : 2;
   static constexpr int NB = (N / BR) * (N / BC);
 };
 
@@ -358,8 +360,9 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
       // conj(C_ji) below. Block (rb, cb) holds rows rb + x N/BR and columns
       // cb + y N/BC, so the blocks of one warp read consecutive rows (the
       // padded row stride puts them on different banks).
-      constexpr int BR = CBlk<N>::BR, BC = CBlk<N>::BC, NBC = N / BC, NBR = N / BR;
-      if (a.x && tid < KT * CBlk<N>::NB) {
+      constexpr int BR = CBlk<N, CB>::BR, BC = CBlk<N, CB>::BC, NBC = N / BC, NBR = N / BR;
+      static_assert(KT * CBlk<N, CB>::NB <= NTHR, "every block of C needs a thread");
+      if (a.x && tid < KT * CBlk<N, CB>::NB) {
         const int kc = tid % KT, blk = tid / KT;
         const int r0 = blk / NBC, c0 = blk % NBC;
         float2 acc[BR][BC];
@@ -486,12 +489,13 @@ int pipe_grid_n(int nsel, int ncomp) {
 }
 
 #define EDUS_PIPE_CLASSES(X) X(2, 32) X(3, 32) X(4, 16) X(5, 16) X(8, 8) X(16, 2)
-// classes with the blocked commutator (register profile 4)
+// classes with the blocked commutator (register profiles 4 and 5)
 #define EDUS_PIPE_CB_CLASSES(X) X(8, 8) X(8, 16) X(16, 2) X(16, 4)
 
 }  // namespace
 
 bool pipe_supported(int N, int kt, int cb) {
+  if (cb < 0 || cb > 2) return false;
 #define X(n, k) \
   if (N == n && kt == k) return true;
   if (cb) {
@@ -509,13 +513,18 @@ cudaError_t launch_stage_pipe(int N, int kt, int cb, const View& v, int stage, i
   if (N == n && kt == k) return pipe_stage<n, k, 0>(v, stage, parity, nsel, ncomp, grid, s);
 #define Y(n, k) \
   if (N == n && kt == k) return pipe_stage<n, k, 1>(v, stage, parity, nsel, ncomp, grid, s);
-  if (cb) {
+#define Z(n, k) \
+  if (N == n && kt == k) return pipe_stage<n, k, 2>(v, stage, parity, nsel, ncomp, grid, s);
+  if (cb == 2) {
+    EDUS_PIPE_CB_CLASSES(Z)
+  } else if (cb) {
     EDUS_PIPE_CB_CLASSES(Y)
   } else {
     EDUS_PIPE_CLASSES(X)
   }
 #undef X
 #undef Y
+#undef Z
   return cudaErrorInvalidValue;
 }
 
@@ -524,13 +533,18 @@ int stage_grid_pipe(int N, int kt, int cb, int nsel, int ncomp) {
   if (N == n && kt == k) return pipe_grid_n<n, k, 0>(nsel, ncomp);
 #define Y(n, k) \
   if (N == n && kt == k) return pipe_grid_n<n, k, 1>(nsel, ncomp);
-  if (cb) {
+#define Z(n, k) \
+  if (N == n && kt == k) return pipe_grid_n<n, k, 2>(nsel, ncomp);
+  if (cb == 2) {
+    EDUS_PIPE_CB_CLASSES(Z)
+  } else if (cb) {
     EDUS_PIPE_CB_CLASSES(Y)
   } else {
     EDUS_PIPE_CLASSES(X)
   }
 #undef X
 #undef Y
+#undef Z
   return 0;
 }
 

@@ -369,7 +369,8 @@ typedef struct {
                                                2 = matrix-product form (FP64; 8 and 16 bands);
                                                3 = staged (cp.async one tile ahead; mixed);
                                                4 = staged with the register-blocked commutator
-                                               (mixed; 8 and 16 bands). 3 and 4 fall back to 0 for
+                                               (mixed; 8 and 16 bands), 2 x 2 blocks of C per thread;
+                                               5 = the same with 2 x 1 blocks. 3-5 fall back to 0 for
                                                an instance without a lattice stencil */
   int32_t tc_contraction;   /* mixed precision: deferred Wannier models contracted on the tensor
                                cores (exact BF16 slices, FP32 sums exact per segment, FP64 across

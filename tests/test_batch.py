@@ -305,6 +305,12 @@ def test_blocked_commutator_form(workdir, nw, nside, name, kt):
         out[prof] = (b.get_state(s), J1(b.obs(s)))
     assert np.abs(out[4][0] - out[3][0]).max() < 1e-6
     assert rel(out[4][1], out[3][1]) < 1e-6
+    # profile 5 (2 x 1 blocks of C) sums every entry of C in the same order as profile 4
+    b = E.Batch(precision=abi.EDUS_PREC_MIXED, chunk_steps=8, regs_profile={nw: 5}, tile_k={nw: kt})
+    s = b.add(E.Problem(p, d))
+    drain(b, [s], 8)
+    assert np.array_equal(b.get_state(s), out[4][0])
+    assert np.array_equal(J1(b.obs(s)), out[4][1])
 
 
 def test_16_band_single_solve_matches_batch(workdir):
