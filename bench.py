@@ -90,13 +90,18 @@ def measured_peaks():
         return 6650.0, "fallback 6.65 TB/s (of fallback)"
 
 
-def ncu_traffic(kernel):
-    """Per-launch DRAM bytes of `kernel` recorded from an ncu capture in profiles/."""
+def ncu_traffic(kernel, kpoints=None):
+    """Per-launch DRAM bytes of `kernel` from an ncu capture recorded in
+    profiles/roofline_traffic.txt: `<kernel> <bytes per launch>`, or
+    `<kernel> per_kpoint <bytes>` for a capture of a smaller launch of the same
+    kernel, scaled here by the k points of this launch."""
     path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
     try:
         for line in open(path):
             s = line.split()
-            if len(s) >= 2 and s[0] == kernel:
+            if len(s) >= 3 and s[0] == kernel and s[1] == "per_kpoint":
+                return float(s[2]) * kpoints if kpoints else None
+            if len(s) >= 2 and s[0] == kernel and s[1] != "per_kpoint":
                 return float(s[1])
     except OSError:
         pass
@@ -473,14 +478,15 @@ def roofline_of_batch(b, n_of_kind, tuned):
     form = regs.get(n, 0) if regs else 0
     if top["kind"] == 0:
         kern = f"k_bobs<{n},1>"
-    elif form in (3, 4):
-        kern = f"k_bpipe<{n},{kt},{top['kind'] - 1},{1 if form == 4 else 0}>"
+    elif form in (3, 4, 5):
+        kern = f"k_bpipe<{n},{kt},{top['kind'] - 1},{form - 3}>"
     else:
         kern = f"k_bstage<{n},{kt}> stage {top['kind'] - 1}"
     achieved = alg / (per_ms * 1e-3) / 1e9
     peak, src = measured_peaks()
     return {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": ncu_traffic(kern), "algorithmic_bytes_per_launch": alg, "launch_ms": per_ms, "share": top["total_ms"] / total,
+            "traffic": ncu_traffic(kern, top["kpoints"]), "algorithmic_bytes_per_launch": alg, "launch_ms": per_ms,
+            "share": top["total_ms"] / total,
             "peak_source": src,
             "launch_timing": "CUDA-event pair around every launch of 64 eagerly launched sweep time steps on the batch stream",
             "kernels": [{"nbands": e["nbands"], "kind": ["observables", "stage0", "stage1", "stage2", "stage3"][e["kind"]],
