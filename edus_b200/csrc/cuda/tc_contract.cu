@@ -430,6 +430,168 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_gemm_tma(const __grid_consta
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTmemCols2));
 }
 
+// ------------------------------------------------------- warp-specialised form
+// The TMA-staged GEMM with its roles on separate warps, so that loads, MMAs and
+// the FP64 read-back of finished segments overlap instead of taking turns on
+// thread 0 between block barriers: warp 4 (one lane) issues the TMA loads of
+// slice s into stage s % 4 once the MMAs of slice s - 4 have released it;
+// warp 5 (one lane) issues the MMAs of slice s once its stage is full, into
+// the TMEM accumulator of its segment's parity, after the read-back of the
+// segment two back has freed that accumulator, and commits them to the
+// stage's "empty" barrier and, at a segment's end, to the accumulator's
+// "full" barrier; warps 0-3 read each finished segment (32 TMEM lanes each)
+// into FP64 registers and arrive on the accumulator's "free" barrier. The
+// sums are those of the other forms, in the same order. Every wait is bounded;
+// a role that times out raises a shared abort flag and stops, the others stop
+// at their next wait, and before TMEM and shared memory are released the
+// producer waits (bounded) for its last loads and the MMA lane for its last
+// commit.
+constexpr int kWsThreads = 192;
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__global__ void __launch_bounds__(kWsThreads, 2) k_tc_gemm_ws(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                                                              double* __restrict__ C, int M, int N, int Kp, int kseg, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  constexpr uint32_t kStageA = TM * TK * 2, kStageB = TN2 * TK * 2, kStage = kStageA + kStageB;
+  __shared__ unsigned long long full[kStages2], empty[kStages2], accf[2], acce[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag, loads_issued, last_commit;
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
+  const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN2;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)), "r"(2 * kTmemCols2));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 32) {
+    for (int b = 0; b < kStages2; b++) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);  // one arrival per read-back warp
+    }
+    abort_flag = 0;
+    loads_issued = 0;
+    last_commit = -1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base;
+  const uint32_t base = (smem_u32(smem) + 1023u) & ~1023u;
+  const int S = Kp / TK, SEG = kseg / TK, P = S / SEG;
+  volatile int* abortp = &abort_flag;
+  double acc[TN2];
+#pragma unroll
+  for (int c = 0; c < TN2; c++) acc[c] = 0.;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      int s = 0;
+      for (; s < S; s++) {
+        const int st = s % kStages2;
+        if (*abortp) break;
+        if (s >= kStages2 && !mbar_wait(&empty[st], (uint32_t)(((s / kStages2) - 1) & 1), err)) {
+          *abortp = 1;
+          break;
+        }
+        const uint32_t sa = base + (uint32_t)st * kStage, sb = sa + kStageA;
+        mbar_expect_tx(&full[st], kStage);
+        tma_load_2d(sa, &mapA, s * TK, m0, smem_u32(&full[st]));
+        tma_load_2d(sb, &mapB, s * TK, n0, smem_u32(&full[st]));
+      }
+      loads_issued = s;
+    }
+  } else if (warp == 5) {
+    if (lane == 0) {
+      int last = -1;
+      for (int s = 0; s < S; s++) {
+        const int st = s % kStages2, p = s / SEG, buf = p & 1;
+        if (*abortp) break;
+        if (!mbar_wait(&full[st], (uint32_t)((s / kStages2) & 1), err)) {
+          *abortp = 1;
+          break;
+        }
+        // a segment's first slice reuses the accumulator of the segment two back: wait for its read-back
+        if (s % SEG == 0 && p >= 2 && !mbar_wait(&acce[buf], (uint32_t)(((p / 2) - 1) & 1), err)) {
+          *abortp = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t sa = base + (uint32_t)st * kStage, sb = sa + kStageA;
+        const uint32_t dtm = tmem + (uint32_t)(buf * kTmemCols2);
+#pragma unroll
+        for (int j = 0; j < TK / 16; j++) {
+          const uint64_t da = sw128_desc(sa + (uint32_t)(32 * j));
+          const uint64_t db = sw128_desc(sb + (uint32_t)(32 * j));
+          const uint32_t accum = (j > 0 || s % SEG != 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtm),
+              "l"(da), "l"(db), "r"(kIdesc2), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&empty[st]))
+                     : "memory");
+        if (s % SEG == SEG - 1)
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(&accf[buf]))
+                       : "memory");
+        last = s;
+      }
+      last_commit = last;
+    }
+  } else {
+    // read-back warps: TMEM lanes 32 warp .. 32 warp + 31 are rows m0 + 32 warp + lane
+    for (int p = 0; p < P; p++) {
+      const int buf = p & 1;
+      const bool ok = !*abortp && mbar_wait(&accf[buf], (uint32_t)((p / 2) & 1), err);
+      if (__any_sync(0xffffffffu, !ok)) {
+        if (lane == 0) *abortp = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+      for (int c0 = 0; c0 < TN2; c0 += 8) {
+        uint32_t v[8];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * kTmemCols2 + c0);
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                     : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc[c0 + u] += (double)__uint_as_float(v[u]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[buf]);
+    }
+  }
+  __syncthreads();
+  if (!*abortp) {
+    if (warp < 4) {
+      const int row = m0 + warp * 32 + lane;
+      if (row < M)
+#pragma unroll
+        for (int c = 0; c < TN2; c++)
+          if (n0 + c < N) C[(size_t)row * N + n0 + c] = acc[c];
+    }
+  } else if (tid == 128) {
+    // the last loads issued (one per stage at most is outstanding) land before the stages go away
+    for (int s = loads_issued - kStages2 < 0 ? 0 : loads_issued - kStages2; s < loads_issued; s++)
+      mbar_wait(&full[s % kStages2], (uint32_t)((s / kStages2) & 1), err);
+  } else if (tid == 160 && last_commit >= 0) {
+    // the last committed MMAs finish before their TMEM is released
+    mbar_wait(&empty[last_commit % kStages2], (uint32_t)((last_commit / kStages2) & 1), err);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kTmemCols2));
+}
+
 // Velocity gauge: coefficient slices of c_A(R) = e^{2 pi i A.R} c(R), one thread per
 // (column, K entry); column 2 ce + part holds [Re c_A ; -Im c_A] (part 0) or
 // [Im c_A ; Re c_A] (part 1), pre-multiplied by 2 scale as the host build's slices
@@ -543,15 +705,20 @@ cudaError_t tc_vg_prepare(const TcVgArgs& a, cudaStream_t s) {
   if ((e = cudaMemsetAsync(a.Bw, 0, sizeof(uint16_t) * (size_t)8 * a.ntri * kpad, s)) != cudaSuccess) return e;
   const size_t smem = std::max(tc_gemm_smem(), (size_t)56 * 1024);
   if ((e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess) return e;
+  if ((e = cudaFuncSetAttribute(k_tc_gemm_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_gemm_smem())) != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_tc_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_gemm_smem());
 }
 
-// The TMA form unless EDUS_TC_GEMM=cpasync selects the cp.async form (the two
-// give bit-identical sums: every segment's FP32 sums are exact).
-bool tc_gemm_tma_wanted() {
+// GEMM form: the single-issuer TMA form by default; EDUS_TC_GEMM=ws selects
+// the warp-specialised TMA form, EDUS_TC_GEMM=cpasync the cp.async form (all
+// three give bit-identical sums: every segment's FP32 sums are exact).
+int tc_gemm_form() {
   const char* form = std::getenv("EDUS_TC_GEMM");
-  return !(form && std::strcmp(form, "cpasync") == 0);
+  if (form && std::strcmp(form, "cpasync") == 0) return 0;
+  if (form && std::strcmp(form, "ws") == 0) return 2;
+  return 1;
 }
+bool tc_gemm_tma_wanted() { return tc_gemm_form() != 0; }
 
 cudaError_t tc_gemm_maps(const uint16_t* Aw, const uint16_t* Bw, int M, int ncols, int kpad, CUtensorMap* mapA, CUtensorMap* mapB) {
   cudaError_t e = encode_operand(mapA, Aw, M, kpad, TM);
@@ -563,7 +730,12 @@ cudaError_t tc_gemm_maps(const uint16_t* Aw, const uint16_t* Bw, int M, int ncol
 cudaError_t tc_gemm_run(const uint16_t* Aw, const uint16_t* Bw, double* Cw, int M, int ncols, int kpad, int kseg, int* err,
                         const CUtensorMap* mapA, const CUtensorMap* mapB, cudaStream_t s) {
   cudaError_t e;
-  if (mapA && mapB) {
+  if (mapA && mapB && tc_gemm_form() == 2) {
+    if ((e = cudaFuncSetAttribute(k_tc_gemm_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_gemm_smem())) != cudaSuccess)
+      return e;
+    dim3 grid((M + TM - 1) / TM, (ncols + TN2 - 1) / TN2);
+    k_tc_gemm_ws<<<grid, kWsThreads, tma_gemm_smem(), s>>>(*mapA, *mapB, Cw, M, ncols, kpad, kseg, err);
+  } else if (mapA && mapB) {
     if ((e = cudaFuncSetAttribute(k_tc_gemm_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_gemm_smem())) != cudaSuccess)
       return e;
     dim3 grid((M + TM - 1) / TM, (ncols + TN2 - 1) / TN2);

@@ -249,16 +249,18 @@ def test_tensor_core_model_build(workdir, nw, nside, name):
     # exact slices: the tensor-core tables equal the FP64 build's to the FP32 rounding
     assert np.abs(runs[True][0] - runs[False][0]).max() < 1e-6
     assert rel(runs[True][1], runs[False][1]) < 1e-6
-    # the cp.async-staged GEMM form gives the TMA form's sums bit for bit
-    os.environ["EDUS_TC_GEMM"] = "cpasync"
-    try:
-        b = E.Batch(precision=abi.EDUS_PREC_MIXED, chunk_steps=8, tc_contraction=True)
-        s = b.add(E.Problem(p, d, defer_model=True))
-    finally:
-        del os.environ["EDUS_TC_GEMM"]
-    drain(b, [s], 8)
-    assert np.array_equal(b.get_state(s), runs[True][0])
-    assert np.array_equal(J1(b.obs(s)), runs[True][1])
+    # the warp-specialised TMA and the cp.async-staged GEMM forms give the
+    # default form's sums bit for bit
+    for form in ("ws", "cpasync"):
+        os.environ["EDUS_TC_GEMM"] = form
+        try:
+            b = E.Batch(precision=abi.EDUS_PREC_MIXED, chunk_steps=8, tc_contraction=True)
+            s = b.add(E.Problem(p, d, defer_model=True))
+        finally:
+            del os.environ["EDUS_TC_GEMM"]
+        drain(b, [s], 8)
+        assert np.array_equal(b.get_state(s), runs[True][0]), form
+        assert np.array_equal(J1(b.obs(s)), runs[True][1]), form
 
 
 def test_staged_form_equals_element_parallel_form(workdir):

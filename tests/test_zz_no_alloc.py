@@ -28,7 +28,7 @@ def static_obs(ctx):
 
 
 def same(a, b):
-    for key in ("J1", "J2", "pop", "tabs"):
+    for key in ("J1", "J2", "pop", "tabs", "pol"):
         x, y = np.asarray(a[key]), np.asarray(b[key])
         assert np.abs(x - y).max() <= 1e-14 * max(np.abs(y).max(), 1e-300), key
     # the trace check and the population extremes of the same reduction
