@@ -249,9 +249,9 @@ def test_tensor_core_model_build(workdir, nw, nside, name):
     # exact slices: the tensor-core tables equal the FP64 build's to the FP32 rounding
     assert np.abs(runs[True][0] - runs[False][0]).max() < 1e-6
     assert rel(runs[True][1], runs[False][1]) < 1e-6
-    # the warp-specialised TMA and the cp.async-staged GEMM forms give the
-    # default form's sums bit for bit
-    for form in ("ws", "cpasync"):
+    # the single-issuer TMA and the cp.async-staged GEMM forms give the
+    # warp-specialised form's sums bit for bit
+    for form in ("tma", "cpasync"):
         os.environ["EDUS_TC_GEMM"] = form
         try:
             b = E.Batch(precision=abi.EDUS_PREC_MIXED, chunk_steps=8, tc_contraction=True)

@@ -348,10 +348,10 @@ def test_velocity_gauge_tensor_core_contraction(workdir, nw, nside, n):
     j1 = RF.rel_l2([x["J1"] for x in g], [x["J1"] for x in lo])
     dpop = float(np.abs(np.array([x["pop"] for x in g]) - np.array([x["pop"] for x in lo])).max())
     assert j1 < 1e-6 and drho < 1e-8 and dpop < 1e-8, (j1, drho, dpop)
-    # the warp-specialised TMA form and the cp.async-staged form give the same
-    # sums bit for bit (every segment's FP32 sums are exact, so staging and
-    # issue order cannot change them)
-    for form in ("ws", "cpasync"):
+    # the single-issuer TMA form and the cp.async-staged form give the
+    # warp-specialised form's sums bit for bit (every segment's FP32 sums are
+    # exact, so staging and issue order cannot change them)
+    for form in ("tma", "cpasync"):
         os.environ["EDUS_TC_GEMM"] = form
         try:
             alt = E.Context(E.Problem(p, workdir), precision=abi.EDUS_PREC_MIXED)
