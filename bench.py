@@ -535,8 +535,11 @@ def config1_line(E, local, steps):
     peak, src = measured_peaks()
     kern = f"k_rhs_ep<{n},32>"
     ctx.close()
+    # AB4 with RK4 start-up: one RHS per step, four in each of the first three steps
+    rhs_per_solve = nsteps + 3 * (4 - 1)
     return {"workload": COULOMB, "value": value, "unit": METRIC, "ms_per_solve": sum(dev) / steps, "solves": steps,
             "time_steps_per_solve": nsteps, "nk": nk, "e2e": e2e, "dtype": "f64",
+            "rhs_evals_per_s": {"value": value * rhs_per_solve / nsteps, "unit": "k-point RHS evaluations/s"},
             "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic(kern), "algorithmic_bytes_per_launch": alg,
                          "launch_ms": per_launch_ms, "peak_source": src,
@@ -634,6 +637,8 @@ def run_ours(args):
                               "how": "plain FP64 single-solve path, request by request, 6 instances per model spread over "
                                      "the grid sizes; per-model rates weighted by the sweep's k-point·steps"},
         "fp64_batch": {"value": fp64_batch, "how": "the same continuous sweep in an FP64 batch, 3 steps"},
+        # RK4: four RHS evaluations per k-point·step
+        "rhs_evals_per_s": {"value": 4 * value, "unit": "k-point RHS evaluations/s"},
         "speedup_vs_fp64_single": value / fp64_single,
         "speedup_batching_fp64": fp64_batch / fp64_single,
         "speedup_precision_batched": value / fp64_batch,
