@@ -54,10 +54,19 @@ def load():
         return {}
 
 
+# band counts below this run in FP64 inside mixed-precision batches (their
+# k-gradient needs FP64 stage inputs), so they take the FP64 kernels' tuning
+MIXED_MIN_BANDS = 4
+
+
 def tuned_options(precision):
     """(tile_k, regs_profile) dicts for Batch / Server from the cache (empty if untuned)."""
-    key = "fp64" if precision == abi.EDUS_PREC_FP64 else "mixed"
-    entry = load().get(gpu_name(), {}).get(key, {})
+    cache = load().get(gpu_name(), {})
+    entry = dict(cache.get("fp64" if precision == abi.EDUS_PREC_FP64 else "mixed", {}))
+    if precision != abi.EDUS_PREC_FP64:
+        for n, v in cache.get("fp64", {}).items():
+            if int(n) < MIXED_MIN_BANDS:
+                entry[n] = v
     tile = {int(n): v["tile_k"] for n, v in entry.items()}
     prof = {int(n): v["regs_profile"] for n, v in entry.items()}
     return tile, prof

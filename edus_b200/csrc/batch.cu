@@ -117,7 +117,8 @@ namespace {
 // terms cancel to ~1/N of their size, so FP32 stage inputs leave a relative
 // error of ~N x 6e-8 in it (J1 error 1.1e-6 measured on a 144 x 144 hBN
 // sweep instance), while FP64 costs these classes little (their kernels are
-// latency-bound).
+// latency-bound). The autotuner's options for mixed batches give these
+// classes their FP64 tuning (edus_b200/autotune.py, MIXED_MIN_BANDS).
 constexpr int kMixedMinBands = 4;
 bool cmix(const edus_batch* b, int n) { return b->mixed && n >= kMixedMinBands; }
 
