@@ -1023,6 +1023,8 @@ int edus_batch_add(edus_batch* b, const edus_problem* pb, int64_t tag, int32_t* 
   I.want_tabs = P.p.tabs && P.nch > 0;
   I.ntiles = s.ntiles;
   I.dt = P.p.dt;
+  I.dt6 = P.p.dt / 6.0;
+  I.dt3 = P.p.dt / 3.0;
   I.wx2 = P.p.probe.wl;
   I.scaleJ = P.dk[0] * P.dk[1] * P.dk[2] / P.det_a;
   I.scaleTA = std::fabs(P.jac) * P.dk[0] * P.dk[1] * P.dk[2];

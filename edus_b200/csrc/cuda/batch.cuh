@@ -42,6 +42,7 @@ struct Inst {
   int nch, nbands, itfi, res;
   int want_current, want_tabs, ntiles, pad0;
   double dt, wx2, scaleJ, scaleTA;
+  double dt6, dt3;         // dt / 6 and dt / 3 of the RK4 stage updates (IEEE divisions, once on the host)
   const int* nbr;          // [nnb][nk]
   const void* H;           // [ntri][nk]   double2 (FP64) or float2 (mixed)
   const void* D;           // [3][ntri][nk]

@@ -330,7 +330,7 @@ __global__ void __launch_bounds__(pad32(KT* TriB<N>::NT), min_blocks(pad32(KT* T
         d = cadd(d, cmi(cscale(Pe, dE)));
       }
       if (i == j) d.y = 0;
-      const double dt = I->dt, dt6 = dt / 6.0, dt3 = dt / 3.0, dt2 = dt / 2.0;
+      const double dt = I->dt, dt6 = I->dt6, dt3 = I->dt3, dt2 = dt / 2.0;
       if constexpr (MIX) {
         // FP64 accumulation of the deviation; FP32 stage inputs
         float2* Pa32 = reinterpret_cast<float2*>(I->Pa);

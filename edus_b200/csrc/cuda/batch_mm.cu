@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(KT* MM<N>::TPK) k_bstage_mm(View v, int stage,
     __syncthreads();
     // ---- (C) element items: beta_ij = C_ij - conj(C_ji), then the stage update
     if (active) {
-      const double dt = I->dt, dt6 = dt / 6.0, dt3 = dt / 3.0, dt2 = dt / 2.0;
+      const double dt = I->dt, dt6 = I->dt6, dt3 = I->dt3, dt2 = dt / 2.0;
       for (int q = tid; q < NT * KT; q += NTHR) {
         const int kl = q % KT, e = q / KT, k = k0 + kl;
         if (k >= nk) continue;

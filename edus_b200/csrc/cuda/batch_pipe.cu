@@ -78,7 +78,7 @@ struct alignas(16) PipeMeta {
   int off[kBatchMaxNb][2];       // lattice steps of the stencil vectors in use
   int delta[kBatchMaxNb];        // d1 n2 + d2: k + b on an interior tile
   float G[kBatchMaxNb];          // their w_b (E_pump . b), in FP32 as the commutator uses it
-  double dt;
+  double dt, dt6, dt3;           // the step, dt / 6, dt / 3 (the instance's host-side divisions)
   int inst, pad;
 };
 
@@ -170,6 +170,8 @@ __device__ __forceinline__ void pipe_meta(PipeMeta& M, const View& v, int inst, 
     M.n2 = I->n2;
     M.nsel = I->nsel;
     M.dt = I->dt;
+    M.dt6 = I->dt6;
+    M.dt3 = I->dt3;
     M.ncomp = (fmask & 1) + ((fmask >> 1) & 1) + ((fmask >> 2) & 1);
   }
   if (lane >= 24 && lane < 27) {
@@ -427,7 +429,7 @@ __global__ void __launch_bounds__(pipe_pad32(KT* TriP<N>::NT), (1152 / pipe_pad3
       const double dE = xEd[j * KT + kl] - xEd[i * KT + kl];
       d = cadd(d, cmi(cscale(Pe, dE)));
       if (i == j) d.y = 0;
-      const double dt = M.dt, dt6 = dt / 6.0, dt3 = dt / 3.0, dt2 = dt / 2.0;
+      const double dt = M.dt, dt6 = M.dt6, dt3 = M.dt3, dt2 = dt / 2.0;
       const int o = e * a.y + cur.k0 + kl;
       const ulonglong2 pw = ldv<ulonglong2>(&M.Hdiag);  // Hdiag, dst
       float2* dst = (float2*)pw.y;
