@@ -1696,7 +1696,7 @@ int edus_create(const edus_problem* pb, const edus_options* opt, edus_ctx** out)
       g.D = dD;
       g.err = c->d_err;
       if (batch::tc_vg_prepare(g, c->stream) != cudaSuccess) return bail(fail(EDUS_ECUDA, "velocity gauge: phase slices"));
-      // TMA-staged GEMM unless EDUS_TC_GEMM=cpasync selects the cp.async form
+      // the TMA tensor maps, unless EDUS_TC_GEMM=cpasync selects the cp.async form
       if (batch::tc_gemm_tma_wanted()) batch::tc_vg_maps(g);
     }
     c->vg_t = P.t_start;

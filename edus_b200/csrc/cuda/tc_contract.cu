@@ -14,9 +14,11 @@
 // result is the FP64 sum to about 2^-32 of the terms, so the FP32 tables stored
 // from it equal those of the FP64 CUDA-core build up to the last rounding.
 //
-// Two forms of the GEMM give the same sums bit for bit. k_tc_gemm_tma (the
-// default) moves 128 x 64 and 64 x 64 operand tiles by TMA into 128-byte
-// swizzled stages, four deep (below). k_tc_gemm (EDUS_TC_GEMM=cpasync): one
+// Three forms of the GEMM give the same sums bit for bit. k_tc_gemm_ws (the
+// default) and k_tc_gemm_tma (EDUS_TC_GEMM=tma) move 128 x 64 and 64 x 64
+// operand tiles by TMA into 128-byte swizzled stages, four deep, with the
+// loads, MMAs and read-back on separate warps or all issued by thread 0
+// (below). k_tc_gemm (EDUS_TC_GEMM=cpasync): one
 // CTA (4 warps) per 128 x 32 tile of C. The 64-deep K slices
 // (128-byte rows of BF16) are staged with cp.async into two shared-memory
 // stages in the K-major canonical layout without swizzle (16-byte chunks of 8

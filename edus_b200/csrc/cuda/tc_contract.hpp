@@ -93,7 +93,8 @@ struct TcVgArgs {
 cudaError_t tc_vg_prepare(const TcVgArgs& a, cudaStream_t s);
 // Encode the TMA descriptors of a.Aw, a.Bw (sets a.tma on success).
 cudaError_t tc_vg_maps(TcVgArgs& a);
-// The TMA-staged GEMM form is used unless EDUS_TC_GEMM=cpasync.
+// A TMA-staged GEMM form (warp-specialised by default, single-issuer with
+// EDUS_TC_GEMM=tma) is used unless EDUS_TC_GEMM=cpasync.
 bool tc_gemm_tma_wanted();
 cudaError_t tc_vg_stage(const TcVgArgs& a, cudaStream_t s);
 
