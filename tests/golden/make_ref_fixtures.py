@@ -17,7 +17,7 @@ reference's zero derivative history, 30 fs; the 8-band Wannier model 96x96
 RK4 40 fs) and small cases of every other solver / option on the path
 (Coulomb AB4, diagonal-basis Coulomb, Taylor-6 and RK4 with adaptive dt, the
 8- and 16-band Wannier models, per-k snapshot files, the Crystal interface on
-seeded synthetic data files).
+seeded synthetic data files, rectangular n1 x n2 grids).
 
 Runs with the Coulomb mean field are repeated at several OpenMP thread
 counts and every distinct outcome is kept (series keys "J1", "J1#1", ...):
@@ -69,6 +69,11 @@ def _edia(d):
                  "Rytova_Keldysh\nPrint_new_band_dispersion\n")
 
 
+def _rect(path, n, n1, n2):
+    """The written input with an n1 x n2 grid in place of the n x n one."""
+    return _with(path, f"nkpt{{\n1 {n} {n}\n}}", f"nkpt{{\n1 {n1} {n2}\n}}")
+
+
 # name -> (input writer, per-k files to keep)
 CASES = {
     "cfg0_hbn60_rk4": (lambda d: W.hbn_rk4(d, n=60, it_res=10), ()),
@@ -93,6 +98,11 @@ CASES = {
                         ()),
     "crystal10_3band": (lambda d: W.crystal(d, nb=(1, 2), norb=3, nkf=11, n=10, field=1.5, duration=4.0, t_fin_fs=1.0,
                                             it_res=5), ()),
+    # rectangular grids (n1 != n2): the stencil shells and the Coulomb row / column passes differ per axis
+    "hbn18x24_rk4": (lambda d: _rect(W.hbn_rk4(d, n=18, t_fin_fs=2.0, it_res=5), 18, 18, 24), ()),
+    "hbn18x24_coulomb_ab4": (lambda d: _rect(W.hbn_coulomb(d, n=18, t_fin_fs=1.5, it_res=5, rk4_startup=False), 18, 18, 24),
+                             ()),
+    "wannier8_12x20_rk4": (lambda d: _rect(W.wannier(d, n=12, t_fin_fs=1.0, it_res=5), 12, 12, 20), ()),
 }
 
 

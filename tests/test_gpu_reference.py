@@ -39,7 +39,8 @@ pytestmark = pytest.mark.gpu
 
 SERIES_CASES = ["cfg0_hbn60_rk4", "cfg1_hbn120_coulomb_ab4", "cfg2_wannier8_96_rk4", "hbn24_rk4", "hbn24_coulomb_ab4",
                 "hbn24_coulomb_diag_ab4", "hbn24_ab2", "hbn24_rk4_dyn", "hbn24_taylor6_dyn", "wannier8_16_rk4",
-                "wannier16_24_rk4", "crystal12_2band", "crystal10_3band"]
+                "wannier16_24_rk4", "crystal12_2band", "crystal10_3band", "hbn18x24_rk4", "hbn18x24_coulomb_ab4",
+                "wannier8_12x20_rk4"]
 # per-case tolerances, measured on the reference itself (tests/test_reference_pins.py): J2 of the
 # diagonal-basis run sits at its k sum's FP64 floor. RK4 with adaptive dt sets each step from a
 # population change of ~1e-9, so rounding moves the time grid: the reference itself spreads by
@@ -119,21 +120,22 @@ def test_config1_rk4_startup_window_matches_oracle(workdir):
 
 def test_fp64_batch_matches_reference_runs(workdir):
     """FP64 batch instances (one batch: hBN 60x60 with its decoupled core band
-    dropped, the 8-band 96x96 model built on the device, the 16-band model)
-    against the reference's output for the same inputs."""
-    names = ["cfg0_hbn60_rk4", "cfg2_wannier8_96_rk4", "wannier16_24_rk4"]
+    dropped, the 8-band 96x96 model built on the device, the 16-band model,
+    and rectangular 18x24 hBN / 12x20 8-band grids) against the reference's
+    output for the same inputs."""
+    names = ["cfg0_hbn60_rk4", "cfg2_wannier8_96_rk4", "wannier16_24_rk4", "hbn18x24_rk4", "wannier8_12x20_rk4"]
     pbs = []
     for nm in names:
         d = f"{workdir}/{nm}"
         pb = E.Problem(E.parse_input(RF.write_input(nm, d)), d, defer_model=nm.startswith(("cfg2", "wannier")))
-        if nm.startswith("cfg0"):
+        if nm.startswith(("cfg0", "hbn")):
             pb.drop_decoupled_core()
         pbs.append(pb)
     b = E.Batch(precision=abi.EDUS_PREC_FP64)
     slots = [b.add(pb) for pb in pbs]
     _drain(b, slots)
     for nm, s in zip(names, slots):
-        bands = (1, 2) if nm.startswith("cfg0") else None
+        bands = (1, 2) if nm.startswith(("cfg0", "hbn")) else None
         RF.compare_log(b.obs(s), RF.load(nm), pop_abs=POP_ABS.get(nm, 1e-13), bands=bands)
 
 
