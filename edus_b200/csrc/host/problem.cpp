@@ -1093,7 +1093,6 @@ int build_problem(const edus_params& p, const char* workdir, Problem& P, bool de
       return fail(EDUS_EUNSUPPORTED,
                   "Coulomb coefficients are read from files (Read_Coulomb_from_files); edus_coulomb_generate computes them");
     if (p.ncut < 1 || p.ncut > 64) return fail(EDUS_EINVAL, "Ncut %d out of range", p.ncut);
-    if (P.n1 != P.n2) return fail(EDUS_EINVAL, "Coulomb needs a square in-plane grid (Coulomb.h:285)");
     if (p.kpt_read) return fail(EDUS_EUNSUPPORTED, "Coulomb with nkpt read (the transforms run on the grid's rows)");
     P.ncut = p.ncut;
     rc = read_coulomb(P, workdir);
