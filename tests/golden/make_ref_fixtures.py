@@ -17,7 +17,8 @@ reference's zero derivative history, 30 fs; the 8-band Wannier model 96x96
 RK4 40 fs) and small cases of every other solver / option on the path
 (Coulomb AB4, diagonal-basis Coulomb, Taylor-6 and RK4 with adaptive dt, the
 8- and 16-band Wannier models, per-k snapshot files, the Crystal interface on
-seeded synthetic data files, rectangular n1 x n2 grids).
+seeded synthetic data files, rectangular n1 x n2 grids, Gaussian and
+pseudo plane-wave pump envelopes and two pumps).
 
 Runs with the Coulomb mean field are repeated at several OpenMP thread
 counts and every distinct outcome is kept (series keys "J1", "J1#1", ...):
@@ -74,6 +75,42 @@ def _rect(path, n, n1, n2):
     return _with(path, f"nkpt{{\n1 {n} {n}\n}}", f"nkpt{{\n1 {n1} {n2}\n}}")
 
 
+def _pump_block(path):
+    txt = open(path).read()
+    i = txt.index("laserpump sin2 {")
+    return txt, i, txt.index("}\n", i) + 2
+
+
+def _gauss(d):
+    """Gaussian pump envelope: sigma 1.5 fs, centred 4 sigma after its t0."""
+    path = W.hbn_rk4(d, n=24, t_fin_fs=8.0, it_res=10, field=0.4)
+    txt, a, b = _pump_block(path)
+    block = ("laserpump gaussian {\nfrequency 0.0146997236011\nintensity 2.12386780644e+12 wcm2\nsigma 1.5 fs\n"
+             "polarization 0 0 1\nphase 0.4\n}\n")
+    open(path, "w").write(txt[:a] + block + txt[b:])
+    return path
+
+
+def _pw(d):
+    """Pseudo plane-wave pump: linear ramp to 2 fs, flat to 5 fs, ramp down to the end of its cycles."""
+    path = W.hbn_rk4(d, n=24, t_fin_fs=8.0, it_res=10, field=0.3)
+    txt, a, b = _pump_block(path)
+    block = ("laserpump pw {\nfrequency 0.0146997236011\nintensity 1.19467564112e+12 wcm2\ncycles 0.67\n"
+             "window 2 5 fs\npolarization 0 0 1\nphase 0\n}\n")
+    open(path, "w").write(txt[:a] + block + txt[b:])
+    return path
+
+
+def _two_pumps(d):
+    """Two sin2 pumps (num_pump_pulses 2): the second polarised across the first and started at 1.5 fs."""
+    path = W.hbn_rk4(d, n=24, t_fin_fs=4.0, it_res=5, field=0.3, duration=4.0, extra_tdse="num_pump_pulses 2\n")
+    txt, a, b = _pump_block(path)
+    second = ("laserpump sin2 {\nfrequency 0.0183746545014\nintensity 5.30966951611e+11 wcm2\ncycles 1.5\n"
+              "polarization 0 1 0\nphase 1.1\nt0_pulse 1.5 fs\n}\n")
+    open(path, "w").write(txt[:b] + second + txt[b:])
+    return path
+
+
 # name -> (input writer, per-k files to keep)
 CASES = {
     "cfg0_hbn60_rk4": (lambda d: W.hbn_rk4(d, n=60, it_res=10), ()),
@@ -103,6 +140,10 @@ CASES = {
     "hbn18x24_coulomb_ab4": (lambda d: _rect(W.hbn_coulomb(d, n=18, t_fin_fs=1.5, it_res=5, rk4_startup=False), 18, 18, 24),
                              ()),
     "wannier8_12x20_rk4": (lambda d: _rect(W.wannier(d, n=12, t_fin_fs=1.0, it_res=5), 12, 12, 20), ()),
+    # the other pump envelopes and a second pump (headers/Laser.h:56-76,128-144, headers/ReadInput.h:236-326)
+    "hbn24_gauss_rk4": (_gauss, ()),
+    "hbn24_pw_rk4": (_pw, ()),
+    "hbn24_two_pumps_rk4": (_two_pumps, ()),
 }
 
 
