@@ -111,6 +111,14 @@ def _two_pumps(d):
     return path
 
 
+def _decoherence(d):
+    """Population (diagonal) and coherence (off-diagonal) relaxation."""
+    path = W.hbn_rk4(d, n=24, t_fin_fs=3.0, it_res=5, field=0.4)
+    with open(path, "a") as f:
+        f.write("\ndecoherence{\ndiagonal 0.002 au\noffdiagonal 0.01 au\n}\n")
+    return path
+
+
 # name -> (input writer, per-k files to keep)
 CASES = {
     "cfg0_hbn60_rk4": (lambda d: W.hbn_rk4(d, n=60, it_res=10), ()),
@@ -144,6 +152,8 @@ CASES = {
     "hbn24_gauss_rk4": (_gauss, ()),
     "hbn24_pw_rk4": (_pw, ()),
     "hbn24_two_pumps_rk4": (_two_pumps, ()),
+    # dissipation with T1 / T2 (headers/InitParameters.h:203-224, headers/RungeKutta.h:219-254)
+    "hbn24_decoherence_rk4": (_decoherence, ()),
 }
 
 
