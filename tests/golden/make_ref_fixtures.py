@@ -18,7 +18,8 @@ RK4 40 fs) and small cases of every other solver / option on the path
 (Coulomb AB4, diagonal-basis Coulomb, Taylor-6 and RK4 with adaptive dt, the
 8- and 16-band Wannier models, per-k snapshot files, the Crystal interface on
 seeded synthetic data files, rectangular n1 x n2 grids, Gaussian and
-pseudo plane-wave pump envelopes and two pumps).
+pseudo plane-wave pump envelopes and two pumps, T1 / T2 decoherence, the
+reference's other tight-binding models).
 
 Runs with the Coulomb mean field are repeated at several OpenMP thread
 counts and every distinct outcome is kept (series keys "J1", "J1#1", ...):
@@ -119,6 +120,30 @@ def _decoherence(d):
     return path
 
 
+def _tb_model(model, n=20):
+    """The hBN RK4 input with another tight-binding model of the reference in its tdse section, the
+    pump polarised along y + z (some models' dipoles have no z component)."""
+    def writer(d):
+        path = W.hbn_rk4(d, n=n, t_fin_fs=1.5, it_res=5, field=0.4)
+        _with(path, "polarization 0 0 1\n", "polarization 0 1 1\n")
+        return _with(path, "tightbinding Haldane_CoreBN_Nedge gap= 5.8 t1= 2.3 t2= 0 phi0= 0\n", f"tightbinding {model}\n")
+    return writer
+
+
+# the reference's other tight-binding models (headers/TightBinding.h); grids of 20 points avoid the
+# K points, where the gapless graphene models' degenerate eigenvectors are arbitrary. BN1b (one band)
+# is left out: the reference program ends with a segmentation fault on it after opening its outputs.
+TB_MODELS = {
+    "tb_corebn_nedge": "CoreBN_Nedge", "tb_corebn_bedge": "CoreBN_Bedge",
+    "tb_haldane_bedge": "Haldane_CoreBN_Bedge gap= 5.8 t1= 2.3 t2= 0.2 phi0= 0.7",
+    "tb_gen2d_hexagonal": "gen2d_hexagonal a= 2.5 gap= 5.0 t1= 2.1 t2= 0.15 phi0= 0.4 core= -12 chv_dipole= 0.2 chc_dipole= 0.1",
+    "tb_boronnitride": "BoronNitride", "tb_graphene": "Graphene", "tb_coregraphene": "CoreGraphene",
+    "tb_graphene_costd": "Graphene_costD", "tb_graphene_symmetricd": "Graphene_symmetricD",
+    "tb_graphenezurron": "GrapheneZurron", "tb_dlgraphene": "DLGraphene", "tb_vampa2015": "Vampa2015", "tb_ges": "GeS",
+    "tb_ges_hse06": "GeS_HSE06",
+}
+
+
 # name -> (input writer, per-k files to keep)
 CASES = {
     "cfg0_hbn60_rk4": (lambda d: W.hbn_rk4(d, n=60, it_res=10), ()),
@@ -155,6 +180,7 @@ CASES = {
     # dissipation with T1 / T2 (headers/InitParameters.h:203-224, headers/RungeKutta.h:219-254)
     "hbn24_decoherence_rk4": (_decoherence, ()),
 }
+CASES.update({name: (_tb_model(model), ()) for name, model in TB_MODELS.items()})
 
 
 def _model_hash(d):

@@ -17,6 +17,7 @@ sys.path.insert(0, GOLDEN)
 import make_ref_fixtures as MRF  # noqa: E402
 
 CASES = MRF.CASES
+TB_MODELS = MRF.TB_MODELS
 
 
 def load(name):
@@ -71,10 +72,17 @@ def rel_l2(a, b):
 J1_TOL = 5e-12
 
 
-def compare_log(log, fx, j1_tol=J1_TOL, pop_abs=1e-13, j2_rel=1e-9, j2_abs=0.0, bands=None, check_t=True):
+# The absolute floor of J1's k sum: runs whose currents stay near 1e-11 (weakly
+# driven models) agree with the reference to this, like the strongly driven
+# ones, while their relative L2 is large
+J1_ABS_FLOOR = 2e-17
+
+
+def compare_log(log, fx, j1_tol=J1_TOL, pop_abs=1e-13, j2_rel=1e-9, j2_abs=0.0, bands=None, check_t=True, j1_abs=0.0):
     """Compare an observable log (list of edus_obs dicts) with the reference's
     printed series; with several reference outcomes (Coulomb runs), with the
-    closest one in J1. J1: relative L2 over t. J2: absolute against its largest
+    closest one in J1. J1: relative L2 over t, or, with j1_abs, max absolute
+    difference at most j1_abs. J2: absolute against its largest
     value (it is a sum over k that cancels to ~1e-8). Populations: absolute
     (Losses.txt prints 16 digits). `bands` selects the reference's band columns
     the log's populations correspond to (a solve without the decoupled core
@@ -94,12 +102,13 @@ def compare_log(log, fx, j1_tol=J1_TOL, pop_abs=1e-13, j2_rel=1e-9, j2_abs=0.0, 
     pop = pop[:, : rp.shape[1]]
     err = {
         "J1_rel_l2": rel_l2(J1, r["J1"]),
+        "J1_abs": float(np.abs(J1 - r["J1"]).max()),
         "J2_abs": float(np.abs(J2 - r["J2"]).max()),
         "J2_max": float(np.abs(r["J2"]).max()),
         "pop_abs": float(np.abs(pop - rp).max()),
         "reference_outcome": best,
     }
-    assert err["J1_rel_l2"] <= j1_tol, err
+    assert err["J1_rel_l2"] <= j1_tol or err["J1_abs"] <= j1_abs, err
     assert err["J2_abs"] <= j2_rel * max(err["J2_max"], 1e-20) + j2_abs, err
     assert err["pop_abs"] <= pop_abs, err
     return err
