@@ -470,4 +470,5 @@ def test_zero_field_keeps_the_initial_state(workdir, kind):
     tr = np.array([x["trace_dev"] for x in log])
     assert np.abs(tr - tr[0]).max() < 1e-13 and abs(tr[0]) < 1e-8
     J1 = np.array([x["J1"] for x in log])
-    assert np.abs(J1 - J1[0]).max() <= 1e-12 * max(np.abs(J1[0]).max(), 1e-15)
+    # relative to the initial current, over the k sum's absolute rounding floor
+    assert np.abs(J1 - J1[0]).max() <= 1e-12 * np.abs(J1[0]).max() + 1e-17
