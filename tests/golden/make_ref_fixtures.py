@@ -19,7 +19,8 @@ RK4 40 fs) and small cases of every other solver / option on the path
 8- and 16-band Wannier models, per-k snapshot files, the Crystal interface on
 seeded synthetic data files, rectangular n1 x n2 grids, Gaussian and
 pseudo plane-wave pump envelopes and two pumps, T1 / T2 decoherence, the
-reference's other tight-binding models).
+reference's other tight-binding models, Adams-Bashforth 1 and 3, Taylor-4 at
+constant dt).
 
 Runs with the Coulomb mean field are repeated at several OpenMP thread
 counts and every distinct outcome is kept (series keys "J1", "J1#1", ...):
@@ -177,6 +178,10 @@ CASES = {
     "hbn24_gauss_rk4": (_gauss, ()),
     "hbn24_pw_rk4": (_pw, ()),
     "hbn24_two_pumps_rk4": (_two_pumps, ()),
+    # the other Adams-Bashforth orders and Taylor at constant dt
+    "hbn24_ab1": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=1.5, it_res=5, solver="Adams_Bashforth 1\n", dt_fs=0.002), ()),
+    "hbn24_ab3": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=2.0, it_res=5, solver="Adams_Bashforth 3\n"), ()),
+    "hbn24_taylor4": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=2.0, it_res=5, dt_fs=0.005, solver="Taylor\nTaylorOrder 4\n"), ()),
     # dissipation with T1 / T2 (headers/InitParameters.h:203-224, headers/RungeKutta.h:219-254)
     "hbn24_decoherence_rk4": (_decoherence, ()),
 }
