@@ -178,6 +178,8 @@ CASES = {
     "hbn24_gauss_rk4": (_gauss, ()),
     "hbn24_pw_rk4": (_pw, ()),
     "hbn24_two_pumps_rk4": (_two_pumps, ()),
+    # the Coulomb mean field with RK4
+    "hbn24_coulomb_rk4": (lambda d: W.hbn_coulomb(d, n=24, t_fin_fs=1.5, it_res=5, rk4=True), ()),
     # the other Adams-Bashforth orders and Taylor at constant dt
     "hbn24_ab1": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=1.5, it_res=5, solver="Adams_Bashforth 1\n", dt_fs=0.002), ()),
     "hbn24_ab3": (lambda d: W.hbn_rk4(d, n=24, t_fin_fs=2.0, it_res=5, solver="Adams_Bashforth 3\n"), ()),

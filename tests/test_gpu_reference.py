@@ -41,7 +41,8 @@ SERIES_CASES = ["cfg0_hbn60_rk4", "cfg1_hbn120_coulomb_ab4", "cfg2_wannier8_96_r
                 "hbn24_coulomb_diag_ab4", "hbn24_ab2", "hbn24_rk4_dyn", "hbn24_taylor6_dyn", "wannier8_16_rk4",
                 "wannier16_24_rk4", "crystal12_2band", "crystal10_3band", "hbn18x24_rk4", "hbn18x24_coulomb_ab4",
                 "wannier8_12x20_rk4", "hbn24_gauss_rk4", "hbn24_pw_rk4", "hbn24_two_pumps_rk4",
-                "hbn24_decoherence_rk4", "hbn24_ab1", "hbn24_ab3", "hbn24_taylor4"] + sorted(RF.TB_MODELS)
+                "hbn24_decoherence_rk4", "hbn24_ab1", "hbn24_ab3", "hbn24_taylor4",
+                "hbn24_coulomb_rk4"] + sorted(RF.TB_MODELS)
 # per-case tolerances, measured on the reference itself (tests/test_reference_pins.py): J2 of the
 # diagonal-basis run sits at its k sum's FP64 floor. RK4 with adaptive dt sets each step from a
 # population change of ~1e-9, so rounding moves the time grid: the reference itself spreads by

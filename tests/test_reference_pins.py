@@ -18,7 +18,7 @@ SMALL = ["hbn24_rk4", "hbn24_coulomb_ab4", "hbn24_coulomb_diag_ab4", "hbn24_ab2"
          "wannier8_16_rk4", "wannier16_24_rk4", "hbn24_coulomb_edia", "hbn12_snapshots", "crystal12_2band",
          "crystal10_3band", "hbn18x24_rk4", "hbn18x24_coulomb_ab4", "wannier8_12x20_rk4", "hbn24_gauss_rk4",
          "hbn24_pw_rk4", "hbn24_two_pumps_rk4", "hbn24_decoherence_rk4", "hbn24_ab1", "hbn24_ab3",
-         "hbn24_taylor4"] + sorted(RF.TB_MODELS)
+         "hbn24_taylor4", "hbn24_coulomb_rk4"] + sorted(RF.TB_MODELS)
 
 # J2 of the diagonal-basis run (~7e-9) sits at the FP64 floor of its k sum after two rotations by U;
 # the 0.3 fs band-dispersion run ends as the pulse starts, so its currents (J2 ~3e-13) are
