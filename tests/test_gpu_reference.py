@@ -147,6 +147,23 @@ def test_fp64_batch_matches_reference_runs(workdir):
         RF.compare_log(b.obs(s), RF.load(nm), pop_abs=POP_ABS.get(nm, 1e-13), bands=bands)
 
 
+def test_fp64_batch_runs_every_tight_binding_model_as_the_reference(workdir):
+    """The reference's other tight-binding models (2, 3 and 4 bands, hexagonal,
+    orthorhombic and rectangular-cell lattices) as instances of one FP64
+    batch, against the reference's output for the same inputs."""
+    names = sorted(RF.TB_MODELS)
+    pbs = []
+    for nm in names:
+        d = f"{workdir}/{nm}"
+        pbs.append(E.Problem(E.parse_input(RF.write_input(nm, d)), d))
+    b = E.Batch(precision=abi.EDUS_PREC_FP64)
+    slots = [b.add(pb) for pb in pbs]
+    _drain(b, slots)
+    for nm, s in zip(names, slots):
+        RF.compare_log(b.obs(s), RF.load(nm), j2_abs=TB_J2_ABS, j1_abs=TB_J1_ABS)
+    b.close()
+
+
 def test_served_fp64_matches_reference_runs(workdir):
     """Requests through the server (FP64) against the reference's output."""
     names = ["cfg0_hbn60_rk4", "cfg2_wannier8_96_rk4", "hbn24_rk4", "wannier16_24_rk4"]
