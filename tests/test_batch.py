@@ -123,6 +123,26 @@ def test_mixed_precision_error_is_small(workdir):
         assert rel(J1(b.obs(s)), J1(log)) < 1e-5
 
 
+def test_mixed_batch_skips_stencil_residue_vectors(workdir):
+    """On a 98 x 98 square grid the in-plane stencil steps carry a z component
+    of 7.4e-17 (rounding of the grid-vector differences): a z-polarised pump
+    makes their gradient coefficients 5e-15 of the largest. The FP32
+    commutator skips them; the instance still follows its FP64 single solve
+    to FP32 rounding, beside a 96 x 96 instance of the same class."""
+    p98 = E.parse_input(W.wannier(f"{workdir}/w98", n=98, t_fin_fs=0.3, it_res=4))
+    p96 = E.parse_input(W.wannier(f"{workdir}/w96", n=96, t_fin_fs=0.3, it_res=4))
+    pb98 = E.Problem(p98, f"{workdir}/w98")
+    bz = pb98.get("bvec")[:, 2]
+    assert np.any((bz != 0) & (np.abs(bz) < 1e-12))  # the residue this test is about
+    rho64, log64 = single(pb98)
+    b = E.Batch(precision=abi.EDUS_PREC_MIXED, chunk_steps=8)
+    s98 = b.add(E.Problem(p98, f"{workdir}/w98"))
+    s96 = b.add(E.Problem(p96, f"{workdir}/w96"))
+    drain(b, [s98, s96], 8)
+    assert np.abs(b.get_state(s98) - rho64).max() < 1e-5
+    assert rel(J1(b.obs(s98)), J1(log64)) < 1e-5
+
+
 def test_mixed_batch_runs_small_band_classes_in_fp64(workdir):
     """A mixed-precision batch runs the 2- and 3-band classes in FP64 (their
     k-gradient needs FP64 stage inputs), core bands included: the 3-band hBN
